@@ -1,0 +1,171 @@
+"""ctypes access to the CPU oracles of the VNLB hot path.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py, always as the checker.  The product
+(vapoursynth-vnlb_b200/) never imports this module.
+
+Two libraries expose the same C interface (oracle/vnlb_oracle.h):
+  * "ref"    oracle/_ref/libvnlb_ref.so, the reference's own src/core,
+             src/linalg and src/aggregate compiled by oracle/Makefile;
+  * "port"   oracle/libvnlb_oracle.so, the plain-C restatement vnlb_oracle.c.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, fields, replace
+from pathlib import Path
+
+import numpy as np
+
+ORACLE_DIR = Path(__file__).resolve().parent
+REF_LIB = ORACLE_DIR / "_ref" / "libvnlb_ref.so"
+REF_GLIBC_LIB = ORACLE_DIR / "_ref" / "libvnlb_ref_glibc.so"
+PORT_LIB = ORACLE_DIR / "libvnlb_oracle.so"
+
+BASIC, FINAL = 0, 1
+EIGHT_BIT = 255.0
+
+
+class _CParams(ctypes.Structure):
+    _fields_ = [
+        ("sigma", ctypes.c_float), ("patch_size", ctypes.c_int),
+        ("patch_time", ctypes.c_int), ("search_window", ctypes.c_int),
+        ("search_bwd", ctypes.c_int), ("search_fwd", ctypes.c_int),
+        ("similar", ctypes.c_int), ("rank", ctypes.c_int),
+        ("similar_cap_factor", ctypes.c_float),
+        ("model_cap_factor", ctypes.c_float), ("beta", ctypes.c_float),
+        ("tau", ctypes.c_float), ("variance_threshold", ctypes.c_float),
+        ("sigma_basic", ctypes.c_float), ("gamma", ctypes.c_float),
+        ("weight_alpha", ctypes.c_float), ("weight_beta", ctypes.c_float),
+        ("weight_gamma", ctypes.c_float), ("weight_epsilon", ctypes.c_float),
+        ("membership_noise_floor", ctypes.c_float),
+        ("proc_step", ctypes.c_int), ("flat_areas", ctypes.c_int),
+        ("couple_channels", ctypes.c_int),
+    ]
+
+
+@dataclass(frozen=True)
+class StageParams:
+    """vnlb::core::StageParameters (src/core/core.hpp:17-41), core units."""
+    sigma: float = 1.0
+    patch_size: int = 8
+    patch_time: int = 1
+    search_window: int = 19
+    search_bwd: int = 1
+    search_fwd: int = 1
+    similar: int = 8
+    rank: int = 8
+    similar_cap_factor: float = 4.0
+    model_cap_factor: float = 1.0
+    beta: float = 1.0
+    tau: float = 0.0
+    variance_threshold: float = 1.1
+    sigma_basic: float = 0.0
+    gamma: float = 0.95
+    weight_alpha: float = 0.75
+    weight_beta: float = 0.35
+    weight_gamma: float = 1.0
+    weight_epsilon: float = 1.0e-6
+    membership_noise_floor: float = 0.25
+    proc_step: int = 8
+    flat_areas: int = 0
+    couple_channels: int = 1
+
+    def to_c(self) -> _CParams:
+        return _CParams(*[getattr(self, f.name) for f in fields(self)])
+
+    @property
+    def slots(self) -> int:
+        return self.search_bwd + self.search_fwd + self.patch_time
+
+
+def cpu_params(stage: int, sigma: float, **kw) -> StageParams:
+    """The vnlb.Basic / vnlb.Final argument rules of parse_stage_parameters
+    (src/vs/plugin.cpp:372-449): 8-bit sigma and tau, radius, bm_range and the
+    Final-stage default overrides."""
+    p = StageParams(sigma=np.float32(sigma) / np.float32(EIGHT_BIT))
+    if stage == FINAL:
+        p = replace(p, tau=float(np.float32(400.0) / np.float32(EIGHT_BIT * EIGHT_BIT)),
+                    variance_threshold=1.7, flat_areas=1, weight_alpha=1.0,
+                    weight_beta=0.5, weight_gamma=1.0)
+    kw = dict(kw)
+    mapping = {"block_size": "patch_size", "group_size": "similar",
+               "cap_factor": "similar_cap_factor", "block_step": "proc_step",
+               "chroma": "couple_channels"}
+    if "radius" in kw:
+        r = kw.pop("radius")
+        p = replace(p, search_bwd=r, search_fwd=r)
+    if "bm_range" in kw:
+        p = replace(p, search_window=2 * kw.pop("bm_range") + 1)
+    if "tau" in kw:
+        p = replace(p, tau=float(np.float32(kw.pop("tau")) / np.float32(EIGHT_BIT * EIGHT_BIT)))
+    if "sigma_basic" in kw:
+        p = replace(p, sigma_basic=float(np.float32(kw.pop("sigma_basic")) / np.float32(EIGHT_BIT)))
+    for key, value in kw.items():
+        p = replace(p, **{mapping.get(key, key): value})
+    return p
+
+
+class Oracle:
+    def __init__(self, kind: str = "port"):
+        path = {"ref": REF_LIB, "ref_glibc": REF_GLIBC_LIB, "port": PORT_LIB}[kind]
+        if not path.exists():
+            raise FileNotFoundError(f"oracle library {path} is not built (make -C oracle)")
+        self.kind = kind
+        self.prefix = "vnlbref_" if kind.startswith("ref") else "vnlboracle_"
+        self.lib = ctypes.CDLL(str(path))
+        self.lib[self.prefix + "last_error"].restype = ctypes.c_char_p
+
+    def _fn(self, name):
+        return self.lib[self.prefix + name]
+
+    def _check(self, status: int):
+        if status != 0:
+            raise ValueError(self._fn("last_error")().decode())
+
+    @staticmethod
+    def _ptr(array):
+        if array is None:
+            return None
+        return array.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+    def stage_stacks(self, stage: int, params: StageParams, clip: np.ndarray,
+                     basic: np.ndarray | None = None, first_anchor: int = 0,
+                     anchor_count: int | None = None, threads: int | None = None):
+        clip = np.ascontiguousarray(clip, dtype=np.float32)
+        frames, channels, height, width = clip.shape
+        if basic is not None:
+            basic = np.ascontiguousarray(basic, dtype=np.float32)
+        if anchor_count is None:
+            anchor_count = frames - first_anchor
+        threads = threads or os.cpu_count() or 1
+        out = np.zeros((anchor_count, channels, params.slots * 2 * height, width), np.float32)
+        cp = params.to_c()
+        self._check(self._fn("stage_stacks")(
+            ctypes.c_int(stage), ctypes.byref(cp), self._ptr(clip), self._ptr(basic),
+            width, height, frames, channels, first_anchor, anchor_count, threads,
+            self._ptr(out)))
+        return out
+
+    def aggregate(self, stacks: np.ndarray, source: np.ndarray, search_bwd: int,
+                  search_fwd: int, patch_time: int) -> np.ndarray:
+        stacks = np.ascontiguousarray(stacks, dtype=np.float32)
+        source = np.ascontiguousarray(source, dtype=np.float32)
+        frames, channels, height, width = source.shape
+        out = np.empty_like(source)
+        self._check(self._fn("aggregate")(
+            self._ptr(stacks), self._ptr(source), width, height, frames, channels,
+            search_bwd, search_fwd, patch_time, self._ptr(out)))
+        return out
+
+    def chain(self, noisy: np.ndarray, basic_params: StageParams,
+              final_params: StageParams, threads: int | None = None):
+        """vnlb.Basic -> vnlb.Aggregate -> vnlb.Final(ref=basic) -> Aggregate."""
+        bs = self.stage_stacks(BASIC, basic_params, noisy, threads=threads)
+        basic = self.aggregate(bs, noisy, basic_params.search_bwd,
+                               basic_params.search_fwd, basic_params.patch_time)
+        fs = self.stage_stacks(FINAL, final_params, noisy, basic, threads=threads)
+        final = self.aggregate(fs, noisy, final_params.search_bwd,
+                               final_params.search_fwd, final_params.patch_time)
+        return basic, final
