@@ -1,0 +1,143 @@
+/*
+ * vnlbgpu: C ABI of the B200-native VNLB denoising hot path.
+ *
+ * This is the boundary a VapourSynth plugin (or any other host) binds to.  It
+ * replaces the CUDA stage pipeline and frame scheduler that the reference's
+ * vnlbcu plugin drives from its getFrame callback, and adds GPU-backed
+ * contribution stacks for the reference's vnlb plugin:
+ *
+ *   reference interface                              entry point here
+ *   ---------------------------------------------    ----------------------------
+ *   create_filter / parse_parameters /               vnlbgpu_create
+ *     validate_parameters / derive_geometry /
+ *     initialize_cuda  (src/vs/cuda_plugin.cpp:
+ *     2066-2131, 370-807, 1866-2020)
+ *   CudaFilterFree (cuda_plugin.cpp:2022-2036)       vnlbgpu_destroy
+ *   upload_source_misses (cuda_plugin.cpp:           vnlbgpu_set_frame,
+ *     1291-1361), noisy/basic FrameCache               vnlbgpu_set_clip_host,
+ *                                                      vnlbgpu_set_clip_device
+ *   render_frame (cuda_plugin.cpp:1635-1864) =       vnlbgpu_render_frame
+ *     vnlbcu.Basic / vnlbcu.Final getFrame
+ *   render_stage_frame (src/vs/plugin.cpp:616-758)   vnlbgpu_render_stack
+ *     = vnlb.Basic / vnlb.Final getFrame
+ *   render_aggregate_frame (plugin.cpp:966-1045)     vnlbgpu_aggregate
+ *     = vnlb.Aggregate getFrame
+ *   setFilterError / mapSetError text                vnlbgpu_last_error
+ *     ("VNLB CUDA: ..." / "VNLB: ...")
+ *
+ * Conventions: every call returns 0 on success and -1 on failure; the failure
+ * text (prefixed like the reference's messages) is then available from
+ * vnlbgpu_last_error() on the calling thread.  No C++ exception crosses this
+ * boundary.  Sizes are in samples (float32); strides are in bytes, as
+ * VapourSynth's getStride reports them.  A session is safe to call from
+ * several threads (calls are serialised inside); results match the reference
+ * CPU core bit for bit for the plain form (see the parity tests).
+ */
+#ifndef VNLBGPU_H
+#define VNLBGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VNLBGPU_STAGE_BASIC 0
+#define VNLBGPU_STAGE_FINAL 1
+
+#define VNLBGPU_SOURCE_CLIP 0 /* the noisy clip ("clip") */
+#define VNLBGPU_SOURCE_REF 1  /* the basic estimate ("ref"), Final only */
+
+/* Parameters in the core's units: sigma and sigma_basic already divided by
+ * 255, tau by 255^2 (the plugin argument rules of parse_parameters,
+ * cuda_plugin.cpp:370-536, and parse_stage_parameters, plugin.cpp:372-449,
+ * are applied by the host-side plugin layer before this call). */
+typedef struct vnlbgpu_params {
+    int stage;
+    float sigma;
+    int patch_size;        /* block_size */
+    int patch_time;
+    int search_window;     /* 2 * bm_range + 1 */
+    int search_bwd;
+    int search_fwd;
+    int similar;           /* group_size */
+    int rank;
+    float similar_cap_factor; /* cap_factor */
+    float model_cap_factor;
+    float beta;
+    float tau;
+    float variance_threshold;
+    float sigma_basic;
+    float gamma;           /* flat-area gamma */
+    float weight_alpha;
+    float weight_beta;
+    float weight_gamma;
+    float weight_epsilon;
+    float membership_noise_floor;
+    int proc_step;         /* block_step; 0 = automatic (patch_size) */
+    int flat_areas;
+    int couple_channels;   /* chroma */
+    int device_id;
+    int num_streams;       /* accepted like vnlbcu (1..32) */
+    int chunk_size;        /* accepted like vnlbcu (> 0) */
+} vnlbgpu_params;
+
+typedef struct vnlbgpu_session vnlbgpu_session;
+
+typedef struct vnlbgpu_stats {
+    long long anchor_frames;   /* anchor frames computed */
+    long long groups;          /* grid anchors matched */
+    long long active_groups;   /* groups filtered (after the paste mask) */
+    long long rows;            /* retained rows filtered and aggregated */
+    long long kernel_launches; /* kernels this session launched */
+} vnlbgpu_stats;
+
+const char* vnlbgpu_last_error(void);
+
+/* Validates the parameters for a clip of `frames` frames of width x height
+ * with 1 (GrayS) or 3 (YUV444PS) planes and reserves device memory. */
+int vnlbgpu_create(const vnlbgpu_params* params, int width, int height, int frames, int channels,
+                   vnlbgpu_session** out);
+void vnlbgpu_destroy(vnlbgpu_session* session);
+
+/* Sources.  set_frame copies one frame from per-plane host pointers with byte
+ * strides; set_clip_host copies a whole clip laid out [frames][planes][H][W];
+ * set_clip_device makes the session read a caller-owned device buffer of that
+ * layout (no copy; it must stay valid while the session uses it). */
+int vnlbgpu_set_frame(vnlbgpu_session* session, int source, int frame, const float* const* planes,
+                      const ptrdiff_t* strides);
+int vnlbgpu_set_clip_host(vnlbgpu_session* session, int source, const float* clip);
+int vnlbgpu_set_clip_device(vnlbgpu_session* session, int source, const float* device_clip);
+
+/* vnlbcu.Basic / vnlbcu.Final: the denoised output frame n (aggregated), into
+ * per-plane host pointers with byte strides. */
+int vnlbgpu_render_frame(vnlbgpu_session* session, int n, float* const* planes, const ptrdiff_t* strides);
+
+/* Whole clip in one call, [frames][planes][H][W], into host or device memory.
+ * The device form enqueues on the session's stream and returns without
+ * waiting; vnlbgpu_synchronize waits and reports device-side errors. */
+int vnlbgpu_render_clip_host(vnlbgpu_session* session, float* out);
+int vnlbgpu_render_clip_device(vnlbgpu_session* session, float* device_out);
+int vnlbgpu_synchronize(vnlbgpu_session* session);
+
+/* vnlb.Basic / vnlb.Final: the contribution stack of anchor frame n in the
+ * plugin's frame layout (per plane, slots*2*H rows: numerators then weights,
+ * weights repeated in every plane). */
+int vnlbgpu_render_stack(vnlbgpu_session* session, int n, float* const* planes, const ptrdiff_t* strides);
+
+/* vnlb.Aggregate over host stacks [frames][planes][slots*2*H][W] and the
+ * source clip [frames][planes][H][W], all frames. */
+int vnlbgpu_aggregate(const float* stacks, const float* source, int width, int height, int frames, int channels,
+                      int search_bwd, int search_fwd, int patch_time, int device_id, float* out);
+
+int vnlbgpu_get_stats(const vnlbgpu_session* session, vnlbgpu_stats* stats);
+
+/* The CUDA stream the session enqueues on (a cudaStream_t), for callers that
+ * time or order device work around it. */
+void* vnlbgpu_stream(vnlbgpu_session* session);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

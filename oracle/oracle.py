@@ -169,3 +169,60 @@ class Oracle:
         final = self.aggregate(fs, noisy, final_params.search_bwd,
                                final_params.search_fwd, final_params.patch_time)
         return basic, final
+
+
+class _Group(ctypes.Structure):
+    _fields_ = [("anchor_x", ctypes.c_int), ("anchor_y", ctypes.c_int), ("similar", ctypes.c_int),
+                ("first_match", ctypes.c_int)]
+
+
+class _Match(ctypes.Structure):
+    _fields_ = [("distance", ctypes.c_float), ("x", ctypes.c_int), ("y", ctypes.c_int),
+                ("frame", ctypes.c_int), ("weight", ctypes.c_float)]
+
+
+ROW_DTYPE = [("distance", "f4"), ("x", "i4"), ("y", "i4"), ("frame", "i4"), ("weight", "f4")]
+
+
+def anchor_groups(stage: int, params: StageParams, clip: np.ndarray, basic: np.ndarray | None,
+                  anchor: int):
+    """Restatement only: the processed groups of one anchor frame in raster
+    order -> (stack, groups [(x, y, S, first)], rows structured array)."""
+    o = Oracle("port")
+    clip = np.ascontiguousarray(clip, dtype=np.float32)
+    frames, channels, height, width = clip.shape
+    if basic is not None:
+        basic = np.ascontiguousarray(basic, dtype=np.float32)
+    stack = np.zeros((channels, params.slots * 2 * height, width), np.float32)
+    cp = params.to_c()
+    total = ctypes.c_int()
+    fn = o.lib["vnlboracle_anchor_groups"]
+    n = fn(ctypes.c_int(stage), ctypes.byref(cp), o._ptr(clip), o._ptr(basic), width, height, frames,
+           channels, anchor, o._ptr(stack), None, 0, None, 0, ctypes.byref(total))
+    if n < 0:
+        o._check(-1)
+    groups = (_Group * max(1, n))()
+    matches = (_Match * max(1, total.value))()
+    fn(ctypes.c_int(stage), ctypes.byref(cp), o._ptr(clip), o._ptr(basic), width, height, frames, channels,
+       anchor, o._ptr(stack), groups, n, matches, total.value, ctypes.byref(total))
+    g = [(x.anchor_x, x.anchor_y, x.similar, x.first_match) for x in groups[:n]]
+    rows = np.array([(m.distance, m.x, m.y, m.frame, m.weight) for m in matches[:total.value]], dtype=ROW_DTYPE)
+    return stack, g, rows
+
+
+def match_anchor(stage: int, params: StageParams, clip: np.ndarray, basic: np.ndarray | None, anchor: int,
+                 x: int, y: int):
+    """Restatement only: the retained rows of one anchor (no paste mask)."""
+    o = Oracle("port")
+    clip = np.ascontiguousarray(clip, dtype=np.float32)
+    frames, channels, height, width = clip.shape
+    if basic is not None:
+        basic = np.ascontiguousarray(basic, dtype=np.float32)
+    cap = 8192
+    out = (_Match * cap)()
+    cp = params.to_c()
+    n = o.lib["vnlboracle_match_anchor"](ctypes.c_int(stage), ctypes.byref(cp), o._ptr(clip), o._ptr(basic),
+                                          width, height, frames, channels, anchor, x, y, out, cap)
+    if n < 0:
+        o._check(-1)
+    return np.array([(m.distance, m.x, m.y, m.frame, m.weight) for m in out[:n]], dtype=ROW_DTYPE)

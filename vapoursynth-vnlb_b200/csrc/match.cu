@@ -1,0 +1,463 @@
+// Exact block matching for one anchor frame (plain form).
+//
+// Reference semantics: find_similar_patches / select_similar_patches and the
+// distance scans of src/core/core.cpp:1033-1362, plus the paste-mask victims
+// of apply_frame_paste_mask (core.cpp:980-1008).
+//
+// Work decomposition.  The host cuts the raster-ordered anchor grid into
+// strips: runs of up to `warps` consecutive anchors of one grid row whose
+// search windows fit in one shared-memory region.  One CTA owns a strip, one
+// warp owns an anchor.  For every scheduled temporal frame (anchor, future
+// ascending, past descending: the CPU's candidate order) the CTA stages the
+// strip's search region of every needed plane in shared memory, each warp
+// computes the SSD of all its candidates in that frame with a register-tiled
+// sweep (lane task = one candidate column x KY candidate rows, reference patch
+// plane in registers), and then replays the CPU's sequential selection over
+// the frame's candidates in raster order.  The replay is exact: it keeps the
+// CPU's K-smallest heap front and its capped match buffer (same replacement
+// slot), and the 32 candidates of a chunk are first tested against the
+// current limit with one ballot -- the limit only shrinks, so a candidate that
+// fails it can never be recorded later.
+//
+// Outputs per anchor g: the retained rows in the CPU's row order (the order
+// std::partial_sort leaves them in), their count, and the later grid anchors
+// whose paste-mask position one of its anchor-frame matches clears.
+#include "vnlb_kernels.h"
+
+namespace vnlbgpu {
+namespace {
+
+constexpr int kKY = 4;           // candidate rows per lane task
+constexpr int kMaxTopPerLane = 4; // K <= 128
+
+struct WarpSelect {
+    int count;       // entries in the match buffer
+    int cap;         // buffer capacity (CPU output_cap)
+    int worst_idx;
+    float worst;
+    int top_count;   // entries in the K-smallest heap
+    float top_front; // its maximum (valid when full)
+};
+
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// First index holding the maximum of buf_d[0, n) (std::max_element).
+__device__ __forceinline__ void refresh_worst(const float* buf_d, int n, int lane, int& worst_idx,
+                                              float& worst) {
+    float best = -kInf;
+    int best_i = 0x7fffffff;
+    for (int i = lane; i < n; i += 32) {
+        const float v = buf_d[i];
+        if (best_i == 0x7fffffff || best < v) {
+            best = v;
+            best_i = i;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, best_i, o);
+        const bool take = (oi != 0x7fffffff) &&
+                          (best_i == 0x7fffffff || best < ov || (!(ov < best) && oi < best_i));
+        if (take) {
+            best = ov;
+            best_i = oi;
+        }
+    }
+    worst = best;
+    worst_idx = best_i;
+}
+
+// std::partial_sort(first, first + middle, first + last) on (distance, id)
+// pairs, reproducing the heap operations of the oracle toolchain's C++
+// library (Floyd sift to a leaf, then sift up).  Single thread.
+__device__ void heap_adjust(float* d, int* id, int hole, int len, float vd, int vid) {
+    const int top = hole;
+    int child = hole;
+    while (child < (len - 1) / 2) {
+        child = 2 * (child + 1);
+        if (d[child] < d[child - 1]) child--;
+        d[hole] = d[child];
+        id[hole] = id[child];
+        hole = child;
+    }
+    if ((len & 1) == 0 && child == (len - 2) / 2) {
+        child = 2 * (child + 1);
+        d[hole] = d[child - 1];
+        id[hole] = id[child - 1];
+        hole = child - 1;
+    }
+    int parent = (hole - 1) / 2;
+    while (hole > top && d[parent] < vd) {
+        d[hole] = d[parent];
+        id[hole] = id[parent];
+        hole = parent;
+        parent = (hole - 1) / 2;
+    }
+    d[hole] = vd;
+    id[hole] = vid;
+}
+
+__device__ void heap_pop_into(float* d, int* id, int len, int result) {
+    const float vd = d[result];
+    const int vid = id[result];
+    d[result] = d[0];
+    id[result] = id[0];
+    heap_adjust(d, id, 0, len, vd, vid);
+}
+
+__device__ void partial_sort_pairs(float* d, int* id, int middle, int last) {
+    if (middle >= 2) {
+        for (int parent = (middle - 2) / 2;; --parent) {
+            heap_adjust(d, id, parent, middle, d[parent], id[parent]);
+            if (parent == 0) break;
+        }
+    }
+    for (int i = middle; i < last; ++i)
+        if (d[i] < d[0]) heap_pop_into(d, id, middle, i);
+    for (int len = middle; len > 1; --len) heap_pop_into(d, id, len - 1, len - 1);
+}
+
+// compute_spatial_range (core.cpp:910-932)
+__device__ __forceinline__ void spatial_range(int center, int axis, int P, int window, int& low, int& high) {
+    const int max_origin = axis - P;
+    const int half = (window - 1) / 2;
+    const int start = center - half;
+    const int end = center + half;
+    const int shift = min(0, start) + max(0, end - max_origin);
+    low = max(0, start - shift);
+    high = min(max_origin, end - shift);
+}
+
+// Distances of one lane task (candidate column cx_rel, rows gy*KY .. +KY-1)
+// against the warp's reference patch, for every plane of scheduled frame k.
+// Planes in shared memory are ordered (channel, t); region row stride `rs`.
+template <int P>
+__device__ __forceinline__ void task_distances(const float* planes, int plane_values, int rs, int col0,
+                                               int row0, const float* ref, int planes_n, int p_dyn,
+                                               float dist[kKY]) {
+    const int PP = P > 0 ? P : p_dyn;
+#pragma unroll
+    for (int j = 0; j < kKY; ++j) dist[j] = 0.0f;
+    for (int q = 0; q < planes_n; ++q) {
+        const float* plane = planes + q * plane_values + row0 * rs + col0;
+        const float* ref_plane = ref + q * PP * PP;
+        if constexpr (P > 0) {
+            float rv[P * P];
+#pragma unroll
+            for (int i = 0; i < P * P; ++i) rv[i] = ref_plane[i];
+#pragma unroll
+            for (int r = 0; r < kKY + P - 1; ++r) {
+                float cv[P];
+#pragma unroll
+                for (int i = 0; i < P; ++i) cv[i] = plane[r * rs + i];
+#pragma unroll
+                for (int j = 0; j < kKY; ++j) {
+                    const int y = r - j;
+                    if (y >= 0 && y < P) {
+                        dist[j] = row_ssd<P>(dist[j], [&](int i) { return rv[y * P + i]; },
+                                             [&](int i) { return cv[i]; });
+                    }
+                }
+            }
+        } else {
+            for (int r = 0; r < kKY + PP - 1; ++r) {
+#pragma unroll
+                for (int j = 0; j < kKY; ++j) {
+                    const int y = r - j;
+                    if (y >= 0 && y < PP)
+                        dist[j] = row_ssd_dyn(dist[j], ref_plane + y * PP, plane + r * rs, PP);
+                }
+            }
+        }
+    }
+}
+
+template <int P>
+__global__ void __launch_bounds__(256) match_kernel(MatchLaunch L) {
+    extern __shared__ __align__(16) float smem[];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    const Strip strip = L.strips[blockIdx.x];
+    const int Pd = L.P;
+    const int Cs = L.search_channels;
+    const int planes_n = Cs * L.Pt;
+    const int plane_values = L.region_rows * L.region_stride;
+
+    float* planes = smem;
+    float* warp_base = planes + planes_n * plane_values + warp * L.warp_floats;
+    float* dist = warp_base;                                  // window_cells
+    float* ref = dist + L.window_cells;                        // planes_n * P * P
+    float* buf_d = ref + planes_n * Pd * Pd;                   // buffer_cap
+    int* buf_i = reinterpret_cast<int*>(buf_d + L.buffer_cap); // buffer_cap
+
+    const bool active_warp = warp < strip.count;
+    const int g = strip.first + warp;
+    int ax = 0, ay = 0;
+    if (active_warp) {
+        const int2 a = L.anchors[g];
+        ax = a.x;
+        ay = a.y;
+    }
+    int xl, xh, yl, yh;
+    spatial_range(ax, L.width, Pd, L.search_window, xl, xh);
+    spatial_range(strip.y, L.height, Pd, L.search_window, yl, yh);
+    const int Wx = xh - xl + 1;
+    const int Wy = yh - yl + 1;
+    const int cells = Wx * Wy;
+    const int tasks = Wx * ((Wy + kKY - 1) / kKY);
+
+    WarpSelect s;
+    s.count = 0;
+    s.cap = min(L.soft_cap, L.search_window * L.search_window * L.schedule_len);
+    s.worst_idx = 0;
+    s.worst = kInf;
+    s.top_count = 0;
+    s.top_front = kInf;
+    float my_top[kMaxTopPerLane];
+#pragma unroll
+    for (int i = 0; i < kMaxTopPerLane; ++i) my_top[i] = -kInf;
+    const int K = L.K;
+
+    for (int k = 0; k < L.schedule_len; ++k) {
+        const int frame = L.schedule[k];
+        __syncthreads();
+        // Stage the strip's region of every plane (channel, t) of frame k.
+        const int rows = strip.region_h;
+        const int cols = strip.region_w;
+        for (int q = 0; q < planes_n; ++q) {
+            const int c = q / L.Pt;
+            const int t = q % L.Pt;
+            const float* src = L.video + ((static_cast<size_t>(frame + t) * L.channels + c) * L.height +
+                                          strip.region_y) * static_cast<size_t>(L.width) + strip.region_x;
+            float* dst = planes + q * plane_values;
+            for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+                const int r = i / cols;
+                const int cx = i - r * cols;
+                dst[r * L.region_stride + cx] = __ldg(src + static_cast<size_t>(r) * L.width + cx);
+            }
+        }
+        __syncthreads();
+        if (!active_warp) continue;
+        if (k == 0) {
+            // Reference patch (anchor frame is scheduled first).
+            for (int i = lane; i < planes_n * Pd * Pd; i += 32) {
+                const int q = i / (Pd * Pd);
+                const int rem = i - q * Pd * Pd;
+                const int py = rem / Pd;
+                const int px = rem - py * Pd;
+                ref[i] = planes[q * plane_values + (ay - strip.region_y + py) * L.region_stride +
+                                (ax - strip.region_x + px)];
+            }
+            __syncwarp();
+        }
+        // Distances of all candidates of frame k.
+        for (int task = lane; task < tasks; task += 32) {
+            const int cx = task % Wx;
+            const int gy = task / Wx;
+            float d[kKY];
+            task_distances<P>(planes, plane_values, L.region_stride, xl - strip.region_x + cx,
+                              yl - strip.region_y + gy * kKY, ref, planes_n, Pd, d);
+#pragma unroll
+            for (int j = 0; j < kKY; ++j) {
+                const int cy = gy * kKY + j;
+                if (cy < Wy) dist[cy * Wx + cx] = d[j];
+            }
+        }
+        __syncwarp();
+        // Replay of the CPU's sequential selection over frame k, raster order.
+        for (int base = 0; base < cells; base += 32) {
+            const int idx = base + lane;
+            const float mine = idx < cells ? dist[idx] : kInf;
+            float limit = s.top_count >= K ? std_max(L.tau, s.top_front) : kInf;
+            if (s.count >= s.cap) limit = std_min(limit, s.worst);
+            unsigned pass = __ballot_sync(0xffffffffu, idx < cells && mine <= limit);
+            while (pass) {
+                const int src_lane = __ffs(pass) - 1;
+                pass &= pass - 1;
+                const float d = __shfl_sync(0xffffffffu, mine, src_lane);
+                limit = s.top_count >= K ? std_max(L.tau, s.top_front) : kInf;
+                if (s.count >= s.cap) limit = std_min(limit, s.worst);
+                if (!(d <= limit)) continue;
+                const int id = (k << 20) | (base + src_lane);
+                // record_candidate_match
+                if (s.count < s.cap) {
+                    if (lane == 0) {
+                        buf_d[s.count] = d;
+                        buf_i[s.count] = id;
+                    }
+                    s.count++;
+                    __syncwarp();
+                    if (s.count == s.cap) refresh_worst(buf_d, s.count, lane, s.worst_idx, s.worst);
+                } else if (d < s.worst) {
+                    if (lane == 0) {
+                        buf_d[s.worst_idx] = d;
+                        buf_i[s.worst_idx] = id;
+                    }
+                    __syncwarp();
+                    refresh_worst(buf_d, s.count, lane, s.worst_idx, s.worst);
+                }
+                // record_candidate_distance
+                if (s.top_count < K) {
+                    const int slot = s.top_count;
+#pragma unroll
+                    for (int i = 0; i < kMaxTopPerLane; ++i)
+                        if (i * 32 + lane == slot) my_top[i] = d;
+                    s.top_count++;
+                    if (s.top_count == K) {
+                        float m = -kInf;
+#pragma unroll
+                        for (int i = 0; i < kMaxTopPerLane; ++i) m = fmaxf(m, my_top[i]);
+                        s.top_front = warp_max(m);
+                    }
+                } else if (d < s.top_front) {
+                    // replace one entry equal to the maximum
+                    int owner = 0x7fffffff;
+#pragma unroll
+                    for (int i = 0; i < kMaxTopPerLane; ++i)
+                        if (owner == 0x7fffffff && my_top[i] == s.top_front) owner = i * 32 + lane;
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) owner = min(owner, __shfl_xor_sync(0xffffffffu, owner, o));
+#pragma unroll
+                    for (int i = 0; i < kMaxTopPerLane; ++i)
+                        if (i * 32 + lane == owner) my_top[i] = d;
+                    float m = -kInf;
+#pragma unroll
+                    for (int i = 0; i < kMaxTopPerLane; ++i) m = fmaxf(m, my_top[i]);
+                    s.top_front = warp_max(m);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (!active_warp) return;
+
+    // select_similar_patches (core.cpp:1200-1243): single lane.
+    int S = 0;
+    if (lane == 0) {
+        const int n = s.count;
+        if (K <= 1) {
+            // similar <= 1: the anchor itself (core.cpp:1253-1257)
+            buf_d[0] = 0.0f;
+            buf_i[0] = -1;
+            S = 1;
+        } else {
+            const int selected = min(K, n);
+            partial_sort_pairs(buf_d, buf_i, selected, n);
+            const float threshold = std_max(L.tau, buf_d[selected - 1]);
+            int out = 0;
+            for (int i = 0; i < n; ++i)
+                if (buf_d[i] <= threshold) {
+                    buf_d[out] = buf_d[i];
+                    buf_i[out] = buf_i[i];
+                    ++out;
+                }
+            const int output_cap = min(L.soft_cap, n);
+            if (out > output_cap) {
+                partial_sort_pairs(buf_d, buf_i, output_cap, out);
+                out = output_cap;
+            }
+            S = out;
+        }
+    }
+    S = __shfl_sync(0xffffffffu, S, 0);
+    __syncwarp();
+    MatchRow* rows_out = L.rows + static_cast<size_t>(g) * L.max_rows;
+    int nvict = 0;
+    for (int i = lane; i < S; i += 32) {
+        const int id = buf_i[i];
+        MatchRow m;
+        m.distance = buf_d[i];
+        if (id < 0) {
+            m.x = ax;
+            m.y = ay;
+            m.frame = L.anchor_frame;
+        } else {
+            const int kk = id >> 20;
+            const int cell = id & 0xfffff;
+            const int cy = cell / Wx;
+            m.x = xl + (cell - cy * Wx);
+            m.y = yl + cy;
+            m.frame = L.schedule[kk];
+        }
+        rows_out[i] = m;
+    }
+    if (lane == 0) L.row_counts[g] = S;
+    // Paste-mask victims (apply_frame_paste_mask, core.cpp:980-1008): later
+    // grid anchors whose position an anchor-frame match clears.
+    int* vict = L.victims + static_cast<size_t>(g) * L.victim_stride;
+    for (int i0 = 0; i0 < S; i0 += 32) {
+        const int i = i0 + lane;
+        int found[5];
+        int nf = 0;
+        if (i < S) {
+            const MatchRow m = rows_out[i];
+            if (m.frame == L.anchor_frame) {
+                const int px[5] = {m.x, m.x, m.x, m.x - 1, m.x + 1};
+                const int py[5] = {m.y, m.y - 1, m.y + 1, m.y, m.y};
+                const bool use[5] = {true, m.y > 2 * Pd, m.y < L.height - 2 * Pd, m.x > 2 * Pd,
+                                     m.x < L.width - 2 * Pd};
+#pragma unroll
+                for (int e = 0; e < 5; ++e) {
+                    if (!use[e] || px[e] < 0 || px[e] >= L.width || py[e] < 0 || py[e] >= L.height) continue;
+                    const int j = L.anchor_map[static_cast<size_t>(py[e]) * L.width + px[e]];
+                    if (j > g) found[nf++] = j;
+                }
+            }
+        }
+        // warp-ordered append
+        int prefix = nf;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, prefix, o);
+            if (lane >= o) prefix += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, prefix, 31);
+        const int start = nvict + prefix - nf;
+        for (int e = 0; e < nf; ++e)
+            if (start + e < L.victim_stride) vict[start + e] = found[e];
+        nvict += total;
+    }
+    if (lane == 0) L.victim_counts[g] = min(nvict, L.victim_stride);
+}
+
+}  // namespace
+
+size_t match_shared_bytes(const MatchLaunch& L, int warps) {
+    const size_t planes = static_cast<size_t>(L.search_channels) * L.Pt * L.region_rows * L.region_stride;
+    return (planes + static_cast<size_t>(warps) * L.warp_floats) * sizeof(float);
+}
+
+int match_warp_floats(int window_cells, int planes_n, int P, int buffer_cap) {
+    int f = window_cells + planes_n * P * P + 2 * buffer_cap;
+    return (f + 3) & ~3;
+}
+
+cudaError_t launch_match(const MatchLaunch& L, int strips, int warps, cudaStream_t stream) {
+    if (strips <= 0) return cudaSuccess;
+    const size_t smem = match_shared_bytes(L, warps);
+    const dim3 block(32 * warps);
+    cudaError_t err = cudaSuccess;
+    auto launch = [&](auto kernel) {
+        err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (err != cudaSuccess) return;
+        kernel<<<strips, block, smem, stream>>>(L);
+        err = cudaGetLastError();
+    };
+    switch (L.P) {
+        case 4: launch(match_kernel<4>); break;
+        case 5: launch(match_kernel<5>); break;
+        case 6: launch(match_kernel<6>); break;
+        case 7: launch(match_kernel<7>); break;
+        case 8: launch(match_kernel<8>); break;
+        default: launch(match_kernel<0>); break;
+    }
+    return err;
+}
+
+}  // namespace vnlbgpu

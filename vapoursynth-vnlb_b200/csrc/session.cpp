@@ -1,0 +1,878 @@
+// Host side of the B200 VNLB path: parameter validation, anchor grids,
+// device buffers, the per-anchor-frame launch sequence and the contribution
+// stack cache behind the C ABI of include/vnlbgpu.h.
+//
+// Reference counterparts: parse/validate/derive (src/vs/cuda_plugin.cpp:
+// 370-807), build_anchor_grid (:628-689) and reference_processing_mask_selected
+// (src/core/core.cpp:934-950), compute_temporal_range / schedule_temporal_range
+// (core.cpp:873-908), render_frame (cuda_plugin.cpp:1635-1864) and
+// render_stage_frame / render_aggregate_frame (src/vs/plugin.cpp:616-1045).
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/vnlbgpu.h"
+#include "../../include/vnlbgpu_diag.h"
+#include "vnlb_kernels.h"
+
+namespace vnlbgpu {
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Failure : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+[[noreturn]] void fail(const std::string& message) { throw Failure(message); }
+
+void check(cudaError_t status, const char* what) {
+    if (status != cudaSuccess) {
+        std::ostringstream m;
+        m << "VNLB CUDA: " << what << " failed: " << cudaGetErrorString(status);
+        throw Failure(m.str());
+    }
+}
+
+template <typename T> struct DeviceArray {
+    T* ptr = nullptr;
+    size_t count = 0;
+    DeviceArray() = default;
+    DeviceArray(const DeviceArray&) = delete;
+    DeviceArray& operator=(const DeviceArray&) = delete;
+    ~DeviceArray() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+    void allocate(size_t n, const char* what) {
+        release();
+        if (n == 0) return;
+        check(cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T)), what);
+        count = n;
+    }
+};
+
+// soft_similar_cap / model_similar_cap (core.cpp:139-172)
+int cap_of(int similar, float factor) {
+    if (factor == 0.0f) return INT_MAX;
+    const float max_factor = static_cast<float>(INT_MAX) / static_cast<float>(similar);
+    if (factor >= max_factor) return INT_MAX;
+    const float cap = std::ceil(static_cast<float>(similar) * factor);
+    return std::max(similar, static_cast<int>(cap));
+}
+
+void temporal_range(int source_frames, int patch_time, int bwd, int fwd, int anchor, int& low, int& high) {
+    const int max_origin = source_frames - patch_time;
+    const int start = anchor - bwd;
+    const int end = anchor + fwd;
+    const int shift = std::min(0, start) + std::max(0, end - max_origin);
+    low = std::max(0, start - shift);
+    high = std::min(max_origin, end - shift);
+}
+
+void spatial_range(int center, int axis, int P, int window, int& low, int& high) {
+    const int max_origin = axis - P;
+    const int half = (window - 1) / 2;
+    const int start = center - half;
+    const int end = center + half;
+    const int shift = std::min(0, start) + std::max(0, end - max_origin);
+    low = std::max(0, start - shift);
+    high = std::min(max_origin, end - shift);
+}
+
+struct Grid {
+    std::vector<int2> anchors;
+    std::vector<Strip> strips;
+    DeviceArray<int2> d_anchors;
+    DeviceArray<Strip> d_strips;
+    DeviceArray<int> d_map;  // [H][W] anchor index or -1
+};
+
+}  // namespace
+
+struct Session {
+    std::mutex lock;
+    vnlbgpu_params params{};
+    StageConfig cfg{};
+    int width = 0, height = 0, frames = 0, channels = 0;
+    int stage = 0;
+    int P = 0, Pt = 0, patch_dim = 0, dim = 0, search_channels = 1;
+    int K = 0, soft_cap = 0, model_cap = 0, step = 0;
+    int slots = 0, valid_anchor_frames = 0, max_rows = 0, buffer_cap = 0;
+    int max_groups = 0, victim_stride = 0, warps = 8;
+    int region_rows = 0, region_stride = 0, region_w_max = 0;
+    bool coupled = true;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    vnlbgpu_stats stats{};
+
+    DeviceArray<float> own_clip, own_ref;
+    const float* clip = nullptr;
+    const float* ref = nullptr;
+    bool clip_ready = false, ref_ready = false;
+
+    DeviceArray<MatchRow> d_rows, d_row_info;
+    DeviceArray<int> d_row_counts, d_victims, d_victim_counts, d_active, d_row_offset, d_row_group;
+    DeviceArray<int2> d_active_xy;
+    DeviceArray<FrameCounters> d_counters;
+    DeviceArray<float> d_filtered, d_weights, d_window, d_out_frame, d_pack;
+    std::map<int, std::unique_ptr<Grid>> grids;
+    int last_grid_key = INT_MIN;
+
+    // contribution stack cache (anchor -> stack), capacity >= slots
+    struct CachedStack {
+        int anchor = -1;
+        long long last_use = 0;
+        DeviceArray<float> data;
+    };
+    std::vector<std::unique_ptr<CachedStack>> cache;
+    long long use_clock = 0;
+    std::vector<float> host_window;
+
+    ~Session() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    size_t plane() const { return static_cast<size_t>(width) * height; }
+    size_t frame_values() const { return plane() * channels; }
+    size_t stack_values() const { return static_cast<size_t>(slots) * (channels + 1) * plane(); }
+
+    void validate(const vnlbgpu_params& p) {
+        // validate_stage_parameters (core.cpp:1948-1995) + vnlbcu checks
+        auto require = [](bool ok, const char* message) {
+            if (!ok) fail(std::string("VNLB CUDA: ") + message);
+        };
+        require(p.stage == 0 || p.stage == 1, "stage must be Basic (0) or Final (1)");
+        require(std::isfinite(p.sigma) && p.sigma > 0.0f, "sigma must be finite and positive");
+        require(p.patch_size > 0 && p.patch_size <= width && p.patch_size <= height,
+                "block_size must fit inside the frame");
+        require(p.patch_time > 0 && p.patch_time <= frames, "patch_time must fit inside the clip");
+        require(p.search_window > 0 && (p.search_window & 1) == 1, "bm_range must describe a positive odd search window");
+        require(p.search_bwd >= 0 && p.search_fwd >= 0, "search_bwd and search_fwd must be non-negative");
+        require(p.similar > 0, "group_size must be positive");
+        require(p.rank >= 0, "rank must be non-negative");
+        require(std::isfinite(p.similar_cap_factor) && (p.similar_cap_factor == 0.0f || p.similar_cap_factor >= 1.0f),
+                "cap_factor must be zero or at least 1.0");
+        require(std::isfinite(p.model_cap_factor) && p.model_cap_factor == 1.0f,
+                "the CUDA backend currently requires model_cap_factor=1");
+        require(std::isfinite(p.beta) && p.beta > 0.0f, "beta must be finite and positive");
+        require(std::isfinite(p.tau) && p.tau >= 0.0f, "tau must be finite and non-negative");
+        require(std::isfinite(p.variance_threshold), "variance_threshold must be finite");
+        require(std::isfinite(p.sigma_basic) && p.sigma_basic >= 0.0f, "sigma_basic must be finite and non-negative");
+        require(std::isfinite(p.gamma) && p.gamma > 0.0f, "gamma must be finite and positive");
+        require(std::isfinite(p.weight_alpha) && p.weight_alpha >= 0.0f, "weight_alpha must be finite and non-negative");
+        require(std::isfinite(p.weight_beta) && p.weight_beta >= 0.0f, "weight_beta must be finite and non-negative");
+        require(std::isfinite(p.weight_gamma) && p.weight_gamma >= 0.0f, "weight_gamma must be finite and non-negative");
+        require(std::isfinite(p.weight_epsilon) && p.weight_epsilon > 0.0f, "weight_epsilon must be finite and positive");
+        require(std::isfinite(p.membership_noise_floor) && p.membership_noise_floor > 0.0f,
+                "membership_noise_floor must be finite and positive");
+        require(p.proc_step >= 0, "block_step must be non-negative; use 0 for auto");
+        require(p.couple_channels != 0 || channels == 1,
+                "the CUDA backend currently requires chroma=1 (coupled channels)");
+        require(p.device_id >= 0, "device_id must be non-negative");
+        require(p.num_streams >= 1 && p.num_streams <= 32, "num_streams must be in the range 1..32");
+        require(p.chunk_size > 0, "chunk_size must be positive");
+    }
+
+    void configure(const vnlbgpu_params& p, int w, int h, int n, int c) {
+        if (!(c == 1 || c == 3) || w <= 0 || h <= 0 || n <= 0)
+            fail("VNLB CUDA: only constant GrayS and YUV444PS clips are supported");
+        width = w;
+        height = h;
+        frames = n;
+        channels = c;
+        validate(p);
+        params = p;
+        stage = p.stage;
+        cfg = StageConfig{p.sigma, p.patch_size, p.patch_time, p.search_window, p.search_bwd, p.search_fwd,
+                          p.similar, p.rank, p.similar_cap_factor, p.model_cap_factor, p.beta, p.tau,
+                          p.variance_threshold, p.sigma_basic, p.gamma, p.weight_alpha, p.weight_beta,
+                          p.weight_gamma, p.weight_epsilon, p.membership_noise_floor, p.proc_step, p.flat_areas,
+                          p.couple_channels};
+        P = p.patch_size;
+        Pt = p.patch_time;
+        patch_dim = P * P * Pt;
+        dim = patch_dim * (p.couple_channels ? channels : 1);
+        coupled = p.couple_channels != 0 && channels > 1;
+        search_channels = stage == 1 ? channels : 1;
+        K = p.similar;
+        soft_cap = cap_of(K, p.similar_cap_factor);
+        model_cap = cap_of(K, p.model_cap_factor);
+        step = p.proc_step > 0 ? p.proc_step : (P <= 1 ? 1 : P);
+        slots = p.search_bwd + p.search_fwd + p.patch_time;
+        valid_anchor_frames = frames - Pt + 1;
+        if (p.rank > dim) fail("VNLB CUDA: rank must not exceed the effective patch dimension");
+        if (K < std::min(dim, p.rank)) fail("VNLB CUDA: group_size must cover the effective VNLB rank");
+        // candidate count (derive_geometry, cuda_plugin.cpp:691-807)
+        const int temporal = std::min(p.search_bwd + p.search_fwd + 1, valid_anchor_frames);
+        const int cw = std::min(p.search_window, width - P + 1);
+        const int ch = std::min(p.search_window, height - P + 1);
+        const long long candidates = static_cast<long long>(cw) * ch * temporal;
+        const int basis = static_cast<int>(std::min<long long>(K, candidates));
+        if (basis > 128) fail("VNLB CUDA: the CUDA dual-PCA filter supports at most 128 model samples");
+        if (p.rank > basis) fail("VNLB CUDA: rank must not exceed min(group_size, candidate_count)");
+        if (!(dim >= 64 && basis < dim))
+            fail("VNLB CUDA: the CUDA backend currently requires the dual-PCA path (min(group_size, "
+                 "candidate_count) must be smaller than the coupled patch dimension, which must be at least 64)");
+        if (slots > kMaxContributors || p.search_bwd + p.search_fwd + 1 > kMaxContributors)
+            fail("VNLB CUDA: search_bwd + search_fwd + patch_time must be at most 32");
+        if (channels > 4) fail("VNLB CUDA: at most four planes are supported");
+        const long long raw = static_cast<long long>(p.search_window) * p.search_window *
+                              (p.search_bwd + p.search_fwd + 1);
+        buffer_cap = static_cast<int>(std::min<long long>(soft_cap, raw));
+        if (buffer_cap > 4096) fail("VNLB CUDA: the B200 matcher keeps at most 4096 retained patches per group");
+        max_rows = buffer_cap;
+        if (K > 128) fail("VNLB CUDA: group_size must be at most 128");
+        if (P > 32) fail("VNLB CUDA: block_size must be at most 32");
+
+        check(cudaSetDevice(p.device_id), "cudaSetDevice");
+        device = p.device_id;
+        check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+
+        // largest grid over the anchor phases
+        for (int key = 0; key < step; ++key) max_groups = std::max(max_groups, static_cast<int>(build_anchor_list(key).size()));
+        victim_stride = max_rows * 5;
+        // match region geometry
+        const int KY = 4;
+        region_rows = std::min(p.search_window, height - P + 1) + P - 1 + KY - 1;
+        const int cw0 = std::min(p.search_window, width - P + 1);
+        const int ch0 = std::min(p.search_window, height - P + 1);
+        for (warps = 8; warps >= 1; warps /= 2) {
+            region_w_max = ((warps - 1) * step + cw0 + P - 1 + 3 + 3) & ~3;
+            region_stride = region_w_max + 1;
+            MatchLaunch probe{};
+            probe.search_channels = search_channels;
+            probe.Pt = Pt;
+            probe.region_rows = region_rows;
+            probe.region_stride = region_stride;
+            probe.warp_floats = match_warp_floats(cw0 * ch0, search_channels * Pt, P, buffer_cap);
+            if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
+        }
+        if (warps < 1) fail("VNLB CUDA: the search region of one anchor does not fit in shared memory");
+
+        const size_t G = static_cast<size_t>(max_groups);
+        d_rows.allocate(G * max_rows, "cudaMalloc(match rows)");
+        d_row_counts.allocate(G, "cudaMalloc(row counts)");
+        d_victims.allocate(G * victim_stride, "cudaMalloc(victims)");
+        d_victim_counts.allocate(G, "cudaMalloc(victim counts)");
+        d_active.allocate(G, "cudaMalloc(active groups)");
+        d_active_xy.allocate(G, "cudaMalloc(active positions)");
+        d_row_offset.allocate(G + 1, "cudaMalloc(row offsets)");
+        d_counters.allocate(1, "cudaMalloc(counters)");
+        const size_t R = G * max_rows;
+        size_t free_bytes = 0, total_bytes = 0;
+        check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
+        const size_t need = R * (static_cast<size_t>(dim) * 4 + 4 + sizeof(MatchRow) + 4);
+        if (need > free_bytes / 2)
+            fail("VNLB CUDA: the group buffers of one anchor frame do not fit in device memory");
+        d_filtered.allocate(R * dim, "cudaMalloc(filtered rows)");
+        d_weights.allocate(R, "cudaMalloc(row weights)");
+        d_row_info.allocate(R, "cudaMalloc(row info)");
+        d_row_group.allocate(R, "cudaMalloc(row groups)");
+        d_out_frame.allocate(frame_values(), "cudaMalloc(output frame)");
+        // aggregation window (prepare_aggregation_window, core.cpp:296-324)
+        host_window.assign(static_cast<size_t>(P) * P, 1.0f);
+        if (!(p.weight_gamma == 0.0f || P <= 1)) {
+            const float center = 0.5f * static_cast<float>(P - 1);
+            const float radius = std_max(center, 0.5f);
+            float max_weight = 0.0f;
+            for (int y = 0; y < P; ++y) {
+                const float dy = (static_cast<float>(y) - center) / radius;
+                for (int x = 0; x < P; ++x) {
+                    const float dx = (static_cast<float>(x) - center) / radius;
+                    const float raw_w = cr_expf(-0.5f * ((dx * dx) + (dy * dy)));
+                    host_window[static_cast<size_t>(y) * P + x] = raw_w;
+                    max_weight = std_max(max_weight, raw_w);
+                }
+            }
+            const float inv_max = max_weight > 0.0f ? 1.0f / max_weight : 1.0f;
+            for (float& v : host_window)
+                v = static_cast<float>(std::pow(static_cast<double>(v * inv_max), static_cast<double>(p.weight_gamma)));
+        }
+        d_window.allocate(host_window.size(), "cudaMalloc(window)");
+        check(cudaMemcpy(d_window.ptr, host_window.data(), host_window.size() * sizeof(float), cudaMemcpyHostToDevice),
+              "cudaMemcpy(window)");
+        const int cache_size = slots + 1;
+        for (int i = 0; i < cache_size; ++i) {
+            auto entry = std::make_unique<CachedStack>();
+            entry->data.allocate(stack_values(), "cudaMalloc(contribution stack)");
+            cache.push_back(std::move(entry));
+        }
+    }
+
+    // staggered anchor grid (reference_processing_mask_selected, core.cpp:934-950)
+    std::vector<int2> build_anchor_list(int phase_key) const {
+        std::vector<int2> out;
+        const int max_x = width - P, max_y = height - P;
+        auto row_selected = [&](int y) { return y == 0 || y == max_y || y % step == phase_key % step; };
+        for (int y = 0; y <= max_y; ++y) {
+            if (!row_selected(y)) {
+                // jump to the next candidate row
+                continue;
+            }
+            const int phase_x = y == max_y ? 0 : phase_key + (y / step);
+            for (int x = 0; x <= max_x; ++x) {
+                if (x == 0 || x == max_x || x % step == phase_x % step) out.push_back(make_int2(x, y));
+            }
+        }
+        return out;
+    }
+
+    int grid_key(int anchor) const {
+        const int max_frame = frames - Pt;
+        const int phase_y = anchor == max_frame ? 0 : anchor;
+        return phase_y % step;
+    }
+
+    Grid& grid_for(int anchor) {
+        const int key = grid_key(anchor);
+        auto it = grids.find(key);
+        if (it != grids.end()) return *it->second;
+        auto grid = std::make_unique<Grid>();
+        grid->anchors = build_anchor_list(key);
+        // strips: runs of consecutive anchors of one row within the region width
+        const auto& a = grid->anchors;
+        size_t i = 0;
+        while (i < a.size()) {
+            Strip s{};
+            s.first = static_cast<int>(i);
+            s.y = a[i].y;
+            int yl, yh;
+            spatial_range(s.y, height, P, params.search_window, yl, yh);
+            s.region_y = yl;
+            s.region_h = yh - yl + 1 + P - 1;
+            int x0 = INT_MAX, x1 = INT_MIN, count = 0;
+            while (i < a.size() && a[i].y == s.y && count < warps) {
+                int xl, xh;
+                spatial_range(a[i].x, width, P, params.search_window, xl, xh);
+                const int nx0 = std::min(x0, xl & ~3);
+                const int nx1 = std::max(x1, xh + P - 1);
+                if (count > 0 && nx1 - nx0 + 1 > region_w_max) break;
+                x0 = nx0;
+                x1 = nx1;
+                ++count;
+                ++i;
+            }
+            s.count = count;
+            s.region_x = x0;
+            s.region_w = x1 - x0 + 1;
+            if (s.region_w > region_w_max) fail("VNLB CUDA: internal error: search region exceeds its reservation");
+            grid->strips.push_back(s);
+        }
+        grid->d_anchors.allocate(a.size(), "cudaMalloc(anchors)");
+        grid->d_strips.allocate(grid->strips.size(), "cudaMalloc(strips)");
+        check(cudaMemcpy(grid->d_anchors.ptr, a.data(), a.size() * sizeof(int2), cudaMemcpyHostToDevice),
+              "cudaMemcpy(anchors)");
+        check(cudaMemcpy(grid->d_strips.ptr, grid->strips.data(), grid->strips.size() * sizeof(Strip),
+                         cudaMemcpyHostToDevice),
+              "cudaMemcpy(strips)");
+        grid->d_map.allocate(plane(), "cudaMalloc(anchor map)");
+        check(cudaMemsetAsync(grid->d_map.ptr, 0xff, plane() * sizeof(int), stream), "cudaMemsetAsync(anchor map)");
+        check(launch_anchor_map(grid->d_anchors.ptr, static_cast<int>(a.size()), width, grid->d_map.ptr, stream),
+              "anchor map kernel launch");
+        stats.kernel_launches += 1;
+        Grid& ref_grid = *grid;
+        grids.emplace(key, std::move(grid));
+        return ref_grid;
+    }
+
+    void require_sources() const {
+        if (!clip_ready) fail("VNLB CUDA: clip frames were not provided");
+        if (stage == 1 && !ref_ready) fail("VNLB CUDA: ref frames were not provided");
+    }
+
+    float* source_buffer(int source) {
+        if (source == VNLBGPU_SOURCE_CLIP) {
+            if (!own_clip.ptr) own_clip.allocate(frame_values() * frames, "cudaMalloc(clip)");
+            clip = own_clip.ptr;
+            return own_clip.ptr;
+        }
+        if (stage != 1) fail("VNLB CUDA: only the Final stage takes a ref clip");
+        if (!own_ref.ptr) own_ref.allocate(frame_values() * frames, "cudaMalloc(ref)");
+        ref = own_ref.ptr;
+        return own_ref.ptr;
+    }
+
+    void invalidate() {
+        for (auto& c : cache) c->anchor = -1;
+    }
+
+    // One anchor frame: grid -> match -> paste mask -> filter -> stack tiles.
+    void compute_anchor(int anchor, float* stack) {
+        Grid& grid = grid_for(anchor);
+        const int G = static_cast<int>(grid.anchors.size());
+        // schedule (compute_temporal_range / schedule_temporal_range)
+        int low, high;
+        temporal_range(frames, Pt, params.search_bwd, params.search_fwd, anchor, low, high);
+        int schedule[kMaxContributors];
+        int schedule_len = 0;
+        schedule[schedule_len++] = anchor;
+        for (int f = anchor + 1; f <= high; ++f) schedule[schedule_len++] = f;
+        for (int f = anchor - 1; f >= low; --f) schedule[schedule_len++] = f;
+        const float* search = stage == 1 ? ref : clip;
+        MatchLaunch m{};
+        m.video = search;
+        m.width = width;
+        m.height = height;
+        m.channels = channels;
+        m.frames = frames;
+        m.search_channels = search_channels;
+        m.P = P;
+        m.Pt = Pt;
+        m.search_window = params.search_window;
+        m.K = K;
+        m.soft_cap = soft_cap;
+        m.max_rows = max_rows;
+        m.tau = params.tau;
+        m.anchor_frame = anchor;
+        for (int i = 0; i < schedule_len; ++i) m.schedule[i] = schedule[i];
+        m.schedule_len = schedule_len;
+        m.anchors = grid.d_anchors.ptr;
+        m.strips = grid.d_strips.ptr;
+        m.anchor_map = grid.d_map.ptr;
+        m.region_rows = region_rows;
+        m.region_stride = region_stride;
+        const int cw = std::min(params.search_window, width - P + 1);
+        const int chh = std::min(params.search_window, height - P + 1);
+        m.window_cells = cw * chh;
+        m.buffer_cap = buffer_cap;
+        m.warp_floats = match_warp_floats(m.window_cells, search_channels * Pt, P, buffer_cap);
+        m.rows = d_rows.ptr;
+        m.row_counts = d_row_counts.ptr;
+        m.victims = d_victims.ptr;
+        m.victim_counts = d_victim_counts.ptr;
+        m.victim_stride = victim_stride;
+        check(launch_match(m, static_cast<int>(grid.strips.size()), warps, stream), "match kernel launch");
+
+        check(cudaMemsetAsync(d_counters.ptr, 0, sizeof(FrameCounters), stream), "cudaMemsetAsync(counters)");
+        PasteLaunch pl{};
+        pl.groups = G;
+        pl.row_counts = d_row_counts.ptr;
+        pl.victims = d_victims.ptr;
+        pl.victim_counts = d_victim_counts.ptr;
+        pl.victim_stride = victim_stride;
+        pl.anchors = grid.d_anchors.ptr;
+        pl.active = d_active.ptr;
+        pl.active_xy = d_active_xy.ptr;
+        pl.row_offset = d_row_offset.ptr;
+        pl.counters = d_counters.ptr;
+        check(launch_paste(pl, stream), "paste kernel launch");
+
+        FilterLaunch fl{};
+        fl.noisy = clip;
+        fl.basic = ref;
+        fl.width = width;
+        fl.height = height;
+        fl.channels = channels;
+        fl.stage = stage;
+        fl.P = P;
+        fl.Pt = Pt;
+        fl.patch_dim = patch_dim;
+        fl.dim = dim;
+        fl.K = K;
+        fl.model_cap = model_cap;
+        fl.rank = params.rank;
+        fl.max_rows = max_rows;
+        fl.coupled = coupled ? 1 : 0;
+        fl.cfg = cfg;
+        fl.rows = d_rows.ptr;
+        fl.row_counts = d_row_counts.ptr;
+        fl.active = d_active.ptr;
+        fl.row_offset = d_row_offset.ptr;
+        fl.counters = d_counters.ptr;
+        fl.filtered = d_filtered.ptr;
+        fl.weights = d_weights.ptr;
+        fl.row_info = d_row_info.ptr;
+        fl.row_group = d_row_group.ptr;
+        check(launch_filter(fl, 148 * 8, stream), "filter kernel launch");
+
+        TileLaunch tl{};
+        tl.width = width;
+        tl.height = height;
+        tl.channels = channels;
+        tl.P = P;
+        tl.Pt = Pt;
+        tl.patch_dim = patch_dim;
+        tl.dim = dim;
+        tl.slots = slots;
+        tl.search_bwd = params.search_bwd;
+        tl.anchor_frame = anchor;
+        tl.search_window = params.search_window;
+        tl.coupled = coupled ? 1 : 0;
+        tl.windowed = params.weight_gamma != 0.0f ? 1 : 0;
+        tl.window = d_window.ptr;
+        tl.active_xy = d_active_xy.ptr;
+        tl.row_offset = d_row_offset.ptr;
+        tl.counters = d_counters.ptr;
+        tl.filtered = d_filtered.ptr;
+        tl.weights = d_weights.ptr;
+        tl.row_info = d_row_info.ptr;
+        tl.stack = stack;
+        tl.tile = 32;
+        tl.tiles_x = (width + 31) / 32;
+        tl.tiles_y = (height + 31) / 32;
+        check(launch_tiles(tl, stream), "tile kernel launch");
+        stats.anchor_frames += 1;
+        stats.groups += G;
+        stats.kernel_launches += 4;
+    }
+
+    float* stack_for(int anchor) {
+        for (auto& c : cache)
+            if (c->anchor == anchor) {
+                c->last_use = ++use_clock;
+                return c->data.ptr;
+            }
+        CachedStack* victim = cache.front().get();
+        for (auto& c : cache)
+            if (c->last_use < victim->last_use) victim = c.get();
+        victim->anchor = anchor;
+        victim->last_use = ++use_clock;
+        compute_anchor(anchor, victim->data.ptr);
+        return victim->data.ptr;
+    }
+
+    // vnlbcu.Basic/Final frame n: normalise over the contributing anchors
+    // (contributing_anchors, cuda_plugin.cpp:809-823; render_aggregate_frame
+    // order: anchors first..last).
+    void render_to_device(int n, float* out) {
+        require_sources();
+        const int first = std::max(0, n - (params.search_fwd + Pt - 1));
+        const int last = std::min(frames - 1, n + params.search_bwd);
+        NormalizeLaunch nl{};
+        nl.width = width;
+        nl.height = height;
+        nl.channels = channels;
+        nl.count = 0;
+        for (int a = first; a <= last; ++a) {
+            if (a > frames - Pt) continue;  // cleared stacks contribute nothing
+            nl.stacks[nl.count] = stack_for(a);
+            nl.slots[nl.count] = n - a + params.search_bwd;
+            ++nl.count;
+        }
+        nl.source = clip + static_cast<size_t>(n) * frame_values();
+        nl.out = out;
+        check(launch_normalize(nl, stream), "normalize kernel launch");
+        stats.kernel_launches += 1;
+    }
+
+    void check_status() {
+        FrameCounters c{};
+        check(cudaMemcpyAsync(&c, d_counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync(status)");
+        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+        if (c.status == kStatusRankNotCovered) fail("VNLB CUDA: group_size must cover the effective VNLB rank");
+        if (c.status != 0) fail("VNLB CUDA: device status " + std::to_string(c.status));
+    }
+};
+
+}  // namespace vnlbgpu
+
+using vnlbgpu::Session;
+
+struct vnlbgpu_session {
+    Session impl;
+};
+
+namespace {
+
+template <typename Fn> int guarded(Fn&& fn) {
+    try {
+        fn();
+        return 0;
+    } catch (const std::exception& error) {
+        vnlbgpu::g_last_error = error.what();
+        return -1;
+    } catch (...) {
+        vnlbgpu::g_last_error = "VNLB CUDA: unknown failure";
+        return -1;
+    }
+}
+
+void copy_planes_in(float* device_frame, const float* const* planes, const ptrdiff_t* strides, int width,
+                    int height, int channels, cudaStream_t stream) {
+    for (int c = 0; c < channels; ++c) {
+        vnlbgpu::check(cudaMemcpy2DAsync(device_frame + static_cast<size_t>(c) * width * height,
+                                         static_cast<size_t>(width) * sizeof(float), planes[c],
+                                         static_cast<size_t>(strides[c]), static_cast<size_t>(width) * sizeof(float),
+                                         height, cudaMemcpyHostToDevice, stream),
+                       "cudaMemcpy2DAsync(frame upload)");
+    }
+}
+
+void copy_planes_out(const float* device_frame, float* const* planes, const ptrdiff_t* strides, int width,
+                     int height, int channels, cudaStream_t stream) {
+    for (int c = 0; c < channels; ++c) {
+        vnlbgpu::check(cudaMemcpy2DAsync(planes[c], static_cast<size_t>(strides[c]),
+                                         device_frame + static_cast<size_t>(c) * width * height,
+                                         static_cast<size_t>(width) * sizeof(float),
+                                         static_cast<size_t>(width) * sizeof(float), height, cudaMemcpyDeviceToHost,
+                                         stream),
+                       "cudaMemcpy2DAsync(frame download)");
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vnlbgpu_last_error(void) { return vnlbgpu::g_last_error.c_str(); }
+
+int vnlbgpu_create(const vnlbgpu_params* params, int width, int height, int frames, int channels,
+                   vnlbgpu_session** out) {
+    return guarded([&]() {
+        if (!params || !out) vnlbgpu::fail("VNLB CUDA: null argument");
+        auto s = std::make_unique<vnlbgpu_session>();
+        s->impl.configure(*params, width, height, frames, channels);
+        *out = s.release();
+    });
+}
+
+void vnlbgpu_destroy(vnlbgpu_session* session) {
+    if (!session) return;
+    cudaSetDevice(session->impl.device);
+    if (session->impl.stream) cudaStreamSynchronize(session->impl.stream);
+    delete session;
+}
+
+int vnlbgpu_set_frame(vnlbgpu_session* session, int source, int frame, const float* const* planes,
+                      const ptrdiff_t* strides) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        if (frame < 0 || frame >= s.frames) vnlbgpu::fail("VNLB CUDA: frame index out of range");
+        for (int c = 0; c < s.channels; ++c)
+            if (strides[c] < static_cast<ptrdiff_t>(s.width * sizeof(float)))
+                vnlbgpu::fail("VNLB CUDA: unsupported frame stride");
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        float* base = s.source_buffer(source);
+        copy_planes_in(base + static_cast<size_t>(frame) * s.frame_values(), planes, strides, s.width, s.height,
+                       s.channels, s.stream);
+        if (source == VNLBGPU_SOURCE_CLIP) s.clip_ready = true; else s.ref_ready = true;
+        s.invalidate();
+    });
+}
+
+int vnlbgpu_set_clip_host(vnlbgpu_session* session, int source, const float* clip) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        float* base = s.source_buffer(source);
+        vnlbgpu::check(cudaMemcpyAsync(base, clip, s.frame_values() * s.frames * sizeof(float), cudaMemcpyHostToDevice,
+                                       s.stream),
+                       "cudaMemcpyAsync(clip upload)");
+        if (source == VNLBGPU_SOURCE_CLIP) s.clip_ready = true; else s.ref_ready = true;
+        s.invalidate();
+    });
+}
+
+int vnlbgpu_set_clip_device(vnlbgpu_session* session, int source, const float* device_clip) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        if (source == VNLBGPU_SOURCE_CLIP) {
+            s.clip = device_clip;
+            s.clip_ready = true;
+        } else {
+            if (s.stage != 1) vnlbgpu::fail("VNLB CUDA: only the Final stage takes a ref clip");
+            s.ref = device_clip;
+            s.ref_ready = true;
+        }
+        s.invalidate();
+    });
+}
+
+int vnlbgpu_render_frame(vnlbgpu_session* session, int n, float* const* planes, const ptrdiff_t* strides) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        if (n < 0 || n >= s.frames) vnlbgpu::fail("VNLB CUDA: frame index out of range");
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.render_to_device(n, s.d_out_frame.ptr);
+        copy_planes_out(s.d_out_frame.ptr, planes, strides, s.width, s.height, s.channels, s.stream);
+        s.check_status();
+    });
+}
+
+int vnlbgpu_render_clip_device(vnlbgpu_session* session, float* device_out) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        for (int n = 0; n < s.frames; ++n) s.render_to_device(n, device_out + static_cast<size_t>(n) * s.frame_values());
+    });
+}
+
+int vnlbgpu_render_clip_host(vnlbgpu_session* session, float* out) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        if (!s.d_pack.ptr || s.d_pack.count < s.frame_values() * s.frames)
+            s.d_pack.allocate(s.frame_values() * s.frames, "cudaMalloc(clip output)");
+        for (int n = 0; n < s.frames; ++n) s.render_to_device(n, s.d_pack.ptr + static_cast<size_t>(n) * s.frame_values());
+        vnlbgpu::check(cudaMemcpyAsync(out, s.d_pack.ptr, s.frame_values() * s.frames * sizeof(float),
+                                       cudaMemcpyDeviceToHost, s.stream),
+                       "cudaMemcpyAsync(clip download)");
+        s.check_status();
+    });
+}
+
+int vnlbgpu_synchronize(vnlbgpu_session* session) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.check_status();
+    });
+}
+
+int vnlbgpu_render_stack(vnlbgpu_session* session, int n, float* const* planes, const ptrdiff_t* strides) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        if (n < 0 || n >= s.frames) vnlbgpu::fail("VNLB CUDA: frame index out of range");
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.require_sources();
+        const size_t packed = static_cast<size_t>(s.channels) * s.slots * 2 * s.plane();
+        if (!s.d_pack.ptr || s.d_pack.count < packed) s.d_pack.allocate(std::max(packed, s.frame_values() * s.frames), "cudaMalloc(stack pack)");
+        if (n > s.frames - s.Pt) {
+            vnlbgpu::check(cudaMemsetAsync(s.d_pack.ptr, 0, packed * sizeof(float), s.stream), "cudaMemsetAsync(stack)");
+        } else {
+            const float* stack = s.stack_for(n);
+            vnlbgpu::check(vnlbgpu::launch_pack_stack(stack, s.width, s.height, s.channels, s.slots, s.d_pack.ptr, s.stream),
+                           "pack kernel launch");
+        }
+        const int rows = s.slots * 2 * s.height;
+        for (int c = 0; c < s.channels; ++c) {
+            vnlbgpu::check(cudaMemcpy2DAsync(planes[c], static_cast<size_t>(strides[c]),
+                                             s.d_pack.ptr + static_cast<size_t>(c) * rows * s.width,
+                                             static_cast<size_t>(s.width) * sizeof(float),
+                                             static_cast<size_t>(s.width) * sizeof(float), rows,
+                                             cudaMemcpyDeviceToHost, s.stream),
+                           "cudaMemcpy2DAsync(stack download)");
+        }
+        s.check_status();
+    });
+}
+
+int vnlbgpu_aggregate(const float* stacks, const float* source, int width, int height, int frames, int channels,
+                      int search_bwd, int search_fwd, int patch_time, int device_id, float* out) {
+    return guarded([&]() {
+        if (!stacks || !source || !out) vnlbgpu::fail("VNLB: null argument");
+        if (width <= 0 || height <= 0 || frames <= 0 || !(channels == 1 || channels == 3))
+            vnlbgpu::fail("VNLB: Aggregate requires matching constant GrayS or YUV444PS clips");
+        if (patch_time <= 0 || search_bwd < 0 || search_fwd < 0)
+            vnlbgpu::fail("VNLB: patch_time must be positive and search_bwd/search_fwd must be non-negative");
+        const int slots = search_bwd + search_fwd + patch_time;
+        if (slots > vnlbgpu::kMaxContributors) vnlbgpu::fail("VNLB: at most 32 contribution slots are supported");
+        vnlbgpu::check(cudaSetDevice(device_id), "cudaSetDevice");
+        const size_t plane = static_cast<size_t>(width) * height;
+        const size_t stack_values = plane * channels * slots * 2;
+        vnlbgpu::DeviceArray<float> d_stacks, d_source, d_out;
+        d_stacks.allocate(stack_values * frames, "cudaMalloc(stacks)");
+        d_source.allocate(plane * channels * frames, "cudaMalloc(source)");
+        d_out.allocate(plane * channels * frames, "cudaMalloc(output)");
+        vnlbgpu::check(cudaMemcpy(d_stacks.ptr, stacks, stack_values * frames * sizeof(float), cudaMemcpyHostToDevice),
+                       "cudaMemcpy(stacks)");
+        vnlbgpu::check(cudaMemcpy(d_source.ptr, source, plane * channels * frames * sizeof(float),
+                                  cudaMemcpyHostToDevice),
+                       "cudaMemcpy(source)");
+        // render_aggregate_frame (src/vs/plugin.cpp:966-1045)
+        for (int n = 0; n < frames; ++n) {
+            vnlbgpu::AggregateLaunch L{};
+            L.width = width;
+            L.height = height;
+            L.channels = channels;
+            L.slots = slots;
+            const int first = std::max(0, n - (search_fwd + patch_time - 1));
+            const int last = std::min(frames - 1, n + search_bwd);
+            for (int a = first; a <= last; ++a) {
+                L.stacks[L.count] = d_stacks.ptr + stack_values * a;
+                L.slots_of[L.count] = n - a + search_bwd;
+                ++L.count;
+            }
+            L.source = d_source.ptr + plane * channels * n;
+            L.out = d_out.ptr + plane * channels * n;
+            vnlbgpu::check(vnlbgpu::launch_aggregate_stacks(L, nullptr), "aggregate kernel launch");
+        }
+        vnlbgpu::check(cudaMemcpy(out, d_out.ptr, plane * channels * frames * sizeof(float), cudaMemcpyDeviceToHost),
+                       "cudaMemcpy(output)");
+    });
+}
+
+int vnlbgpu_get_stats(const vnlbgpu_session* session, vnlbgpu_stats* stats) {
+    return guarded([&]() {
+        if (!session || !stats) vnlbgpu::fail("VNLB CUDA: null argument");
+        *stats = session->impl.stats;
+    });
+}
+
+void* vnlbgpu_stream(vnlbgpu_session* session) { return session ? session->impl.stream : nullptr; }
+
+int vnlbgpu_diag_anchor(vnlbgpu_session* session, int anchor, int* grid_xy, int* grid_counts,
+                        vnlbgpu_diag_row* grid_rows, int grid_capacity, int grid_row_capacity, int* active,
+                        vnlbgpu_diag_row* active_rows, int active_capacity, int active_row_capacity, int* groups,
+                        int* active_groups, int* rows, int* max_rows) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.require_sources();
+        if (anchor < 0 || anchor > s.frames - s.Pt) vnlbgpu::fail("VNLB CUDA: anchor frame out of range");
+        vnlbgpu::DeviceArray<float> stack;
+        stack.allocate(s.stack_values(), "cudaMalloc(diag stack)");
+        s.compute_anchor(anchor, stack.ptr);
+        s.check_status();
+        vnlbgpu::Grid& grid = s.grid_for(anchor);
+        const int G = static_cast<int>(grid.anchors.size());
+        *groups = G;
+        *max_rows = s.max_rows;
+        std::vector<int> counts(G);
+        vnlbgpu::check(cudaMemcpy(counts.data(), s.d_row_counts.ptr, G * sizeof(int), cudaMemcpyDeviceToHost), "copy");
+        std::vector<vnlbgpu::MatchRow> mrows(static_cast<size_t>(G) * s.max_rows);
+        vnlbgpu::check(cudaMemcpy(mrows.data(), s.d_rows.ptr, mrows.size() * sizeof(vnlbgpu::MatchRow),
+                                  cudaMemcpyDeviceToHost),
+                       "copy");
+        for (int g = 0; g < G && g < grid_capacity; ++g) {
+            grid_xy[2 * g] = grid.anchors[g].x;
+            grid_xy[2 * g + 1] = grid.anchors[g].y;
+            grid_counts[g] = counts[g];
+            for (int j = 0; j < counts[g] && static_cast<long long>(g) * s.max_rows + j < grid_row_capacity; ++j) {
+                const auto& m = mrows[static_cast<size_t>(g) * s.max_rows + j];
+                grid_rows[static_cast<size_t>(g) * s.max_rows + j] = vnlbgpu_diag_row{m.distance, m.x, m.y, m.frame, 0.0f};
+            }
+        }
+        vnlbgpu::FrameCounters c{};
+        vnlbgpu::check(cudaMemcpy(&c, s.d_counters.ptr, sizeof(c), cudaMemcpyDeviceToHost), "copy");
+        *active_groups = c.active;
+        *rows = c.rows;
+        std::vector<int> act(c.active);
+        if (c.active > 0)
+            vnlbgpu::check(cudaMemcpy(act.data(), s.d_active.ptr, c.active * sizeof(int), cudaMemcpyDeviceToHost), "copy");
+        for (int i = 0; i < c.active && i < active_capacity; ++i) active[i] = act[i];
+        std::vector<vnlbgpu::MatchRow> info(c.rows);
+        std::vector<float> w(c.rows);
+        if (c.rows > 0) {
+            vnlbgpu::check(cudaMemcpy(info.data(), s.d_row_info.ptr, c.rows * sizeof(vnlbgpu::MatchRow),
+                                      cudaMemcpyDeviceToHost),
+                           "copy");
+            vnlbgpu::check(cudaMemcpy(w.data(), s.d_weights.ptr, c.rows * sizeof(float), cudaMemcpyDeviceToHost), "copy");
+        }
+        for (int r = 0; r < c.rows && r < active_row_capacity; ++r)
+            active_rows[r] = vnlbgpu_diag_row{info[r].distance, info[r].x, info[r].y, info[r].frame, w[r]};
+        s.invalidate();
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,194 @@
+// Shared device-side definitions of the B200 VNLB hot path.
+//
+// Every floating-point helper here reproduces one operation sequence of the
+// reference CPU core exactly (same operands, same order, same roundings), so
+// that the plain GPU form is bit-identical to the reference compiled with an
+// 8-lane vector width (the pinned Highway semantics): a*b+c is written with
+// __fmul_rn/__fadd_rn where the CPU rounds twice and with __fmaf_rn where the
+// CPU uses a fused multiply-add.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vnlbgpu {
+
+constexpr int kLanes = 8;          // CPU vector width the order is pinned to
+constexpr float kInf = __builtin_huge_valf();
+
+struct StageConfig {
+    // vnlb::core::StageParameters (src/core/core.hpp:17-41), core units.
+    float sigma;
+    int patch_size;
+    int patch_time;
+    int search_window;
+    int search_bwd;
+    int search_fwd;
+    int similar;        // K
+    int rank;
+    float similar_cap_factor;
+    float model_cap_factor;
+    float beta;
+    float tau;
+    float variance_threshold;
+    float sigma_basic;
+    float gamma;        // flat-area gamma
+    float weight_alpha;
+    float weight_beta;
+    float weight_gamma;
+    float weight_epsilon;
+    float membership_noise_floor;
+    int proc_step;
+    int flat_areas;
+    int couple_channels;
+};
+
+// Dimensions derived once per session.
+struct Shape {
+    int width, height, frames, channels;
+    int stage;            // 0 Basic, 1 Final
+    int P, Pt, patch_dim; // P*P*Pt
+    int dim;              // estimator dimension (patch_dim * channels, coupled)
+    int search_channels;  // 1 (Basic, luma) or channels (Final)
+    int K;                // requested group size
+    int soft_cap;         // ceil(K*cap_factor) (>= K), or INT_MAX
+    int model_cap;        // ceil(K*model_cap_factor)
+    int max_rows;         // largest retained row count S
+    int slots;            // search_bwd + search_fwd + patch_time
+    int window_w;         // spatial window width (search_window)
+};
+
+struct MatchRow {
+    float distance;
+    int x;
+    int y;
+    int frame;
+};
+
+// ---------------------------------------------------------------------------
+// Pinned lane-structured arithmetic (src/core/distance_highway.hpp:11-58,
+// src/linalg/kernels_highway.hpp).
+__device__ __forceinline__ float reduce8(const float v[kLanes]) {
+    const float a0 = __fadd_rn(v[0], v[4]);
+    const float a1 = __fadd_rn(v[1], v[5]);
+    const float a2 = __fadd_rn(v[2], v[6]);
+    const float a3 = __fadd_rn(v[3], v[7]);
+    return __fadd_rn(__fadd_rn(a0, a2), __fadd_rn(a1, a3));
+}
+
+// add_squared_row_distance_highway: distance + SSD of one patch row of
+// `count` samples, in the pinned order.  `ref` and `cand` may be any
+// addressable memory (registers after unrolling, shared, global).
+template <int Count, typename RefFn, typename CandFn>
+__device__ __forceinline__ float row_ssd(float distance, RefFn ref, CandFn cand) {
+    if constexpr (Count <= 0) {
+        return distance;
+    } else if constexpr (Count == kLanes) {
+        float v[kLanes];
+#pragma unroll
+        for (int i = 0; i < kLanes; ++i) {
+            const float d = __fsub_rn(ref(i), cand(i));
+            v[i] = __fmul_rn(d, d);
+        }
+        return __fadd_rn(distance, reduce8(v));
+    } else if constexpr (Count == 2 * kLanes) {
+        float v[kLanes];
+#pragma unroll
+        for (int i = 0; i < kLanes; ++i) {
+            const float d = __fsub_rn(ref(i), cand(i));
+            v[i] = __fmul_rn(d, d);
+        }
+#pragma unroll
+        for (int i = 0; i < kLanes; ++i) {
+            const float d = __fsub_rn(ref(i + kLanes), cand(i + kLanes));
+            v[i] = __fmaf_rn(d, d, v[i]);
+        }
+        return __fadd_rn(distance, reduce8(v));
+    } else {
+        constexpr int kFull = (Count / kLanes) * kLanes;
+        if constexpr (kFull > 0) {
+            float v[kLanes];
+#pragma unroll
+            for (int i = 0; i < kLanes; ++i) v[i] = 0.0f;
+#pragma unroll
+            for (int base = 0; base < kFull; base += kLanes) {
+#pragma unroll
+                for (int i = 0; i < kLanes; ++i) {
+                    const float d = __fsub_rn(ref(base + i), cand(base + i));
+                    v[i] = __fmaf_rn(d, d, v[i]);
+                }
+            }
+            distance = __fadd_rn(distance, reduce8(v));
+        }
+        // (with no full chunk the CPU adds a zero vector sum: distance + 0,
+        // which leaves a non-negative distance unchanged)
+#pragma unroll
+        for (int i = kFull; i < Count; ++i) {
+            const float d = __fsub_rn(ref(i), cand(i));
+            distance = __fadd_rn(distance, __fmul_rn(d, d));
+        }
+        return distance;
+    }
+}
+
+// Runtime-count version of row_ssd for patch sizes without a specialised
+// kernel.
+__device__ __forceinline__ float row_ssd_dyn(float distance, const float* ref, const float* cand,
+                                             int count) {
+    float v[kLanes];
+    if (count <= 0) return distance;
+    if (count == kLanes) {
+#pragma unroll
+        for (int i = 0; i < kLanes; ++i) {
+            const float d = __fsub_rn(ref[i], cand[i]);
+            v[i] = __fmul_rn(d, d);
+        }
+        return __fadd_rn(distance, reduce8(v));
+    }
+    if (count == 2 * kLanes) {
+#pragma unroll
+        for (int i = 0; i < kLanes; ++i) {
+            const float d = __fsub_rn(ref[i], cand[i]);
+            v[i] = __fmul_rn(d, d);
+        }
+#pragma unroll
+        for (int i = 0; i < kLanes; ++i) {
+            const float d = __fsub_rn(ref[i + kLanes], cand[i + kLanes]);
+            v[i] = __fmaf_rn(d, d, v[i]);
+        }
+        return __fadd_rn(distance, reduce8(v));
+    }
+#pragma unroll
+    for (int i = 0; i < kLanes; ++i) v[i] = 0.0f;
+    int index = 0;
+    for (; index + kLanes <= count; index += kLanes) {
+#pragma unroll
+        for (int i = 0; i < kLanes; ++i) {
+            const float d = __fsub_rn(ref[index + i], cand[index + i]);
+            v[i] = __fmaf_rn(d, d, v[i]);
+        }
+    }
+    distance = __fadd_rn(distance, reduce8(v));
+    for (; index < count; ++index) {
+        const float d = __fsub_rn(ref[index], cand[index]);
+        distance = __fadd_rn(distance, __fmul_rn(d, d));
+    }
+    return distance;
+}
+
+// ---------------------------------------------------------------------------
+// Elementary functions, correctly rounded to float: evaluated in double
+// precision (error below one double ulp) and rounded once.  The reference
+// calls std::exp/std::log/std::log1p/std::pow on floats; the oracle pins those
+// to the same definition.
+__host__ __device__ __forceinline__ float cr_expf(float x) { return static_cast<float>(exp(static_cast<double>(x))); }
+__host__ __device__ __forceinline__ float cr_logf(float x) { return static_cast<float>(log(static_cast<double>(x))); }
+__host__ __device__ __forceinline__ float cr_log1pf(float x) {
+    return static_cast<float>(log1p(static_cast<double>(x)));
+}
+
+// std::max / std::min on floats (first operand wins ties and NaNs).
+__host__ __device__ __forceinline__ float std_max(float a, float b) { return (a < b) ? b : a; }
+__host__ __device__ __forceinline__ float std_min(float a, float b) { return (b < a) ? b : a; }
+
+}  // namespace vnlbgpu

@@ -1,0 +1,163 @@
+// Launch descriptors shared by the host pipeline (session.cpp) and the
+// kernels (match.cu, paste.cu, filter.cu, aggregate.cu).  Plain structs of
+// device pointers and sizes; one descriptor per launch.
+#pragma once
+
+#include <cstddef>
+#include <cuda_runtime.h>
+
+#include "vnlb_common.cuh"
+
+namespace vnlbgpu {
+
+// Most temporal slots (search_bwd + search_fwd + patch_time) and scheduled
+// candidate frames the GPU path handles.
+constexpr int kMaxContributors = 32;
+
+// A run of consecutive grid anchors of one grid row handled by one CTA of the
+// match kernel, with the shared-memory region that covers all their windows.
+struct Strip {
+    int first;     // index of the first anchor in the anchor list
+    int count;     // anchors in the strip (<= warps per CTA)
+    int y;         // their common row
+    int region_x;  // region origin (x multiple of 4), in pixels
+    int region_y;
+    int region_w;  // region extent in pixels
+    int region_h;
+};
+
+struct MatchLaunch {
+    const float* video;   // search source [frames][channels][H][W]
+    int width, height, channels, frames;
+    int search_channels;  // channels compared (1 = first plane only)
+    int P, Pt, search_window;
+    int K, soft_cap, max_rows;
+    float tau;
+    int anchor_frame;
+    int schedule[kMaxContributors];  // scheduled candidate frames (CPU order)
+    int schedule_len;
+    const int2* anchors;  // grid anchors in raster order
+    const Strip* strips;
+    const int* anchor_map;  // [H][W] anchor index or -1
+    int region_rows;      // shared rows per plane (incl. padding)
+    int region_stride;    // shared row stride in floats
+    int window_cells;     // max Wx*Wy
+    int buffer_cap;       // match buffer capacity per warp
+    int warp_floats;      // shared floats per warp
+    // outputs
+    MatchRow* rows;       // [G][max_rows]
+    int* row_counts;      // [G]
+    int* victims;         // [G][victim_stride]
+    int* victim_counts;   // [G]
+    int victim_stride;
+};
+
+size_t match_shared_bytes(const MatchLaunch& L, int warps);
+int match_warp_floats(int window_cells, int planes_n, int P, int buffer_cap);
+cudaError_t launch_match(const MatchLaunch& L, int strips, int warps, cudaStream_t stream);
+
+// Device-side counters of one anchor frame.
+struct FrameCounters {
+    int active;      // active (processed) groups
+    int rows;        // total retained rows of the active groups
+    int status;      // 0 or an error code (see kStatus*)
+    int detail;
+};
+
+constexpr int kStatusRankNotCovered = 1;  // fewer model rows than the rank
+constexpr int kStatusPasteCapacity = 2;   // too many anchors for the paste kernel
+
+struct PasteLaunch {
+    int groups;
+    const int* row_counts;
+    const int* victims;
+    const int* victim_counts;
+    int victim_stride;
+    const int2* anchors;
+    // outputs
+    int* active;          // [G] active anchor indices in raster order
+    int2* active_xy;      // [G] their positions
+    int* row_offset;      // [G + 1] exclusive prefix of retained rows
+    FrameCounters* counters;
+};
+
+cudaError_t launch_paste(const PasteLaunch& L, cudaStream_t stream);
+
+// Fills map[y*width + x] with the index of each grid anchor (the map must be
+// preset to -1).
+cudaError_t launch_anchor_map(const int2* anchors, int count, int width, int* map, cudaStream_t stream);
+
+struct FilterLaunch {
+    const float* noisy;     // [frames][C][H][W]
+    const float* basic;     // Final only
+    int width, height, channels;
+    int stage;
+    int P, Pt, patch_dim, dim;
+    int K, model_cap, rank, max_rows;
+    int coupled;            // sample-major (coupled, C > 1) vs group path
+    StageConfig cfg;
+    const MatchRow* rows;   // [G][max_rows]
+    const int* row_counts;
+    const int* active;
+    const int* row_offset;
+    FrameCounters* counters;
+    // outputs, indexed by global row r = row_offset[a] + i
+    float* filtered;        // [R][dim]
+    float* weights;         // [R]
+    MatchRow* row_info;     // [R]
+    int* row_group;         // [R] active index of the row's group
+};
+
+size_t filter_shared_bytes(const FilterLaunch& L);
+cudaError_t launch_filter(const FilterLaunch& L, int ctas, cudaStream_t stream);
+
+struct TileLaunch {
+    int width, height, channels;
+    int P, Pt, patch_dim, dim;
+    int slots, search_bwd, anchor_frame;
+    int search_window;
+    int coupled;            // sample-major contribution writer (coupled, C > 1)
+    int windowed;           // weight_gamma != 0
+    const float* window;    // [P*P]
+    const int2* active_xy;
+    const int* row_offset;
+    const FrameCounters* counters;
+    const float* filtered;
+    const float* weights;
+    const MatchRow* row_info;
+    float* stack;           // [slots][C+1][H][W]
+    int tile;               // tile edge in pixels
+    int tiles_x, tiles_y;
+};
+
+cudaError_t launch_tiles(const TileLaunch& L, cudaStream_t stream);
+
+struct NormalizeLaunch {
+    int width, height, channels;
+    const float* stacks[kMaxContributors];  // contributing anchor stacks, in anchor order
+    int slots[kMaxContributors];            // slot of the output frame in each stack
+    int count;
+    const float* source;         // fallback plane set of the output frame [C][H][W]
+    float* out;                  // [C][H][W]
+};
+
+cudaError_t launch_normalize(const NormalizeLaunch& L, cudaStream_t stream);
+
+// Packs one anchor stack into the vnlb.Basic/Final frame layout: per channel
+// a plane of slots*2*H rows (numerators, then weights duplicated per channel).
+// vnlb.Aggregate on stacks already in the plugin frame layout.
+struct AggregateLaunch {
+    int width, height, channels, slots;
+    const float* stacks[kMaxContributors];  // [C][slots*2*H][W] per anchor
+    int slots_of[kMaxContributors];
+    int count;
+    const float* source;  // [C][H][W]
+    float* out;           // [C][H][W]
+};
+
+cudaError_t launch_aggregate_stacks(const AggregateLaunch& L, cudaStream_t stream);
+
+cudaError_t launch_pack_stack(const float* stack, int width, int height, int channels, int slots,
+                              float* out, cudaStream_t stream);
+
+}  // namespace vnlbgpu

@@ -1,0 +1,217 @@
+"""ctypes binding of the C ABI in include/vnlbgpu.h (lib/libvnlbgpu.so).
+
+The library is built in-tree by build_native.py.  There is no CPU fallback:
+if the library is missing or no CUDA device is usable, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libvnlbgpu.so"
+
+STAGE_BASIC, STAGE_FINAL = 0, 1
+SOURCE_CLIP, SOURCE_REF = 0, 1
+
+
+class VNLBError(RuntimeError):
+    """Raised with the library's error text (prefixed like the plugin's)."""
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("stage", ctypes.c_int), ("sigma", ctypes.c_float), ("patch_size", ctypes.c_int),
+        ("patch_time", ctypes.c_int), ("search_window", ctypes.c_int), ("search_bwd", ctypes.c_int),
+        ("search_fwd", ctypes.c_int), ("similar", ctypes.c_int), ("rank", ctypes.c_int),
+        ("similar_cap_factor", ctypes.c_float), ("model_cap_factor", ctypes.c_float),
+        ("beta", ctypes.c_float), ("tau", ctypes.c_float), ("variance_threshold", ctypes.c_float),
+        ("sigma_basic", ctypes.c_float), ("gamma", ctypes.c_float), ("weight_alpha", ctypes.c_float),
+        ("weight_beta", ctypes.c_float), ("weight_gamma", ctypes.c_float),
+        ("weight_epsilon", ctypes.c_float), ("membership_noise_floor", ctypes.c_float),
+        ("proc_step", ctypes.c_int), ("flat_areas", ctypes.c_int), ("couple_channels", ctypes.c_int),
+        ("device_id", ctypes.c_int), ("num_streams", ctypes.c_int), ("chunk_size", ctypes.c_int),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_longlong) for name in
+                ("anchor_frames", "groups", "active_groups", "rows", "kernel_launches")]
+
+
+class DiagRow(ctypes.Structure):
+    _fields_ = [("distance", ctypes.c_float), ("x", ctypes.c_int), ("y", ctypes.c_int),
+                ("frame", ctypes.c_int), ("weight", ctypes.c_float)]
+
+
+EXPORTS = [
+    "vnlbgpu_last_error", "vnlbgpu_create", "vnlbgpu_destroy", "vnlbgpu_set_frame",
+    "vnlbgpu_set_clip_host", "vnlbgpu_set_clip_device", "vnlbgpu_render_frame",
+    "vnlbgpu_render_clip_host", "vnlbgpu_render_clip_device", "vnlbgpu_synchronize",
+    "vnlbgpu_render_stack", "vnlbgpu_aggregate", "vnlbgpu_get_stats", "vnlbgpu_stream",
+    "vnlbgpu_diag_anchor",
+]
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def load() -> ctypes.CDLL:
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not LIB_PATH.exists():
+                raise VNLBError(f"VNLB CUDA: native library {LIB_PATH} is not built "
+                                "(run vapoursynth-vnlb_b200/build_native.py)")
+            lib = ctypes.CDLL(str(LIB_PATH))
+            lib.vnlbgpu_last_error.restype = ctypes.c_char_p
+            lib.vnlbgpu_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+            lib.vnlbgpu_destroy.argtypes = [ctypes.c_void_p]
+            lib.vnlbgpu_destroy.restype = None
+            lib.vnlbgpu_set_clip_host.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+            lib.vnlbgpu_set_clip_device.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+            lib.vnlbgpu_set_frame.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ssize_t)]
+            lib.vnlbgpu_render_frame.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                                 ctypes.POINTER(ctypes.c_ssize_t)]
+            lib.vnlbgpu_render_stack.argtypes = lib.vnlbgpu_render_frame.argtypes
+            lib.vnlbgpu_render_clip_host.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.vnlbgpu_render_clip_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.vnlbgpu_synchronize.argtypes = [ctypes.c_void_p]
+            lib.vnlbgpu_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
+            lib.vnlbgpu_stream.argtypes = [ctypes.c_void_p]
+            lib.vnlbgpu_stream.restype = ctypes.c_void_p
+            lib.vnlbgpu_aggregate.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 8 + [ctypes.c_void_p]
+            lib.vnlbgpu_diag_anchor.argtypes = [
+                ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                ctypes.POINTER(ctypes.c_int)]
+            _lib = lib
+    return _lib
+
+
+def _check(status: int):
+    if status != 0:
+        raise VNLBError(load().vnlbgpu_last_error().decode())
+
+
+def _f32(a: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Session:
+    """One configured stage (Basic or Final) over one clip geometry."""
+
+    def __init__(self, params: Params, width: int, height: int, frames: int, channels: int):
+        self.lib = load()
+        self.shape = (frames, channels, height, width)
+        self.params = params
+        handle = ctypes.c_void_p()
+        _check(self.lib.vnlbgpu_create(ctypes.byref(params), width, height, frames, channels,
+                                       ctypes.byref(handle)))
+        self.handle = handle
+        self._keep = {}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.vnlbgpu_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_clip(self, source: int, clip: np.ndarray):
+        clip = _f32(clip)
+        if clip.shape != self.shape:
+            raise VNLBError(f"VNLB CUDA: clip shape {clip.shape} does not match {self.shape}")
+        _check(self.lib.vnlbgpu_set_clip_host(self.handle, source, clip.ctypes.data))
+
+    def set_clip_device(self, source: int, device_ptr: int, keepalive=None):
+        self._keep[source] = keepalive
+        _check(self.lib.vnlbgpu_set_clip_device(self.handle, source, ctypes.c_void_p(device_ptr)))
+
+    def render_clip(self) -> np.ndarray:
+        out = np.empty(self.shape, np.float32)
+        _check(self.lib.vnlbgpu_render_clip_host(self.handle, out.ctypes.data))
+        return out
+
+    def render_clip_into(self, out_ptr: int):
+        _check(self.lib.vnlbgpu_render_clip_host(self.handle, ctypes.c_void_p(out_ptr)))
+
+    def render_clip_device(self, device_ptr: int):
+        _check(self.lib.vnlbgpu_render_clip_device(self.handle, ctypes.c_void_p(device_ptr)))
+
+    def synchronize(self):
+        _check(self.lib.vnlbgpu_synchronize(self.handle))
+
+    def _planes(self, arrays):
+        ptrs = (ctypes.c_void_p * len(arrays))(*[a.ctypes.data for a in arrays])
+        strides = (ctypes.c_ssize_t * len(arrays))(*[a.strides[0] for a in arrays])
+        return ptrs, strides
+
+    def render_frame(self, n: int) -> np.ndarray:
+        frames, channels, height, width = self.shape
+        out = np.empty((channels, height, width), np.float32)
+        ptrs, strides = self._planes([out[c] for c in range(channels)])
+        _check(self.lib.vnlbgpu_render_frame(self.handle, n, ptrs, strides))
+        return out
+
+    def render_stack(self, n: int) -> np.ndarray:
+        frames, channels, height, width = self.shape
+        slots = self.params.search_bwd + self.params.search_fwd + self.params.patch_time
+        out = np.empty((channels, slots * 2 * height, width), np.float32)
+        ptrs, strides = self._planes([out[c] for c in range(channels)])
+        _check(self.lib.vnlbgpu_render_stack(self.handle, n, ptrs, strides))
+        return out
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(self.lib.vnlbgpu_get_stats(self.handle, ctypes.byref(s)))
+        return {name: getattr(s, name) for name, _ in Stats._fields_}
+
+    def stream(self) -> int:
+        return self.lib.vnlbgpu_stream(self.handle) or 0
+
+    def diag_anchor(self, anchor: int):
+        """Runs one anchor frame and returns (grid, active) read-backs."""
+        frames, channels, height, width = self.shape
+        G = ctypes.c_int()
+        A = ctypes.c_int()
+        R = ctypes.c_int()
+        M = ctypes.c_int()
+        # first call with zero capacity to learn the sizes
+        _check(self.lib.vnlbgpu_diag_anchor(self.handle, anchor, None, None, None, 0, 0, None, None, 0, 0,
+                                            ctypes.byref(G), ctypes.byref(A), ctypes.byref(R), ctypes.byref(M)))
+        g, a, r, m = G.value, A.value, R.value, M.value
+        xy = np.zeros((g, 2), np.int32)
+        counts = np.zeros(g, np.int32)
+        grid_rows = (DiagRow * max(1, g * m))()
+        active = np.zeros(max(1, a), np.int32)
+        active_rows = (DiagRow * max(1, r))()
+        _check(self.lib.vnlbgpu_diag_anchor(self.handle, anchor, xy.ctypes.data, counts.ctypes.data, grid_rows,
+                                            g, g * m, active.ctypes.data, active_rows, a, r,
+                                            ctypes.byref(G), ctypes.byref(A), ctypes.byref(R), ctypes.byref(M)))
+        to_np = lambda rows, n: np.array([(x.distance, x.x, x.y, x.frame, x.weight) for x in rows[:n]],
+                                         dtype=[("distance", "f4"), ("x", "i4"), ("y", "i4"), ("frame", "i4"),
+                                                ("weight", "f4")])
+        return {"xy": xy, "counts": counts, "grid_rows": to_np(grid_rows, g * m).reshape(g, m) if g else None,
+                "max_rows": m, "active": active[:a], "active_rows": to_np(active_rows, r)}
+
+
+def aggregate(stacks: np.ndarray, source: np.ndarray, search_bwd: int, search_fwd: int, patch_time: int,
+              device_id: int = 0) -> np.ndarray:
+    lib = load()
+    stacks = _f32(stacks)
+    source = _f32(source)
+    frames, channels, height, width = source.shape
+    out = np.empty_like(source)
+    _check(lib.vnlbgpu_aggregate(stacks.ctypes.data, source.ctypes.data, width, height, frames, channels,
+                                 search_bwd, search_fwd, patch_time, device_id, out.ctypes.data))
+    return out
