@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Throughput of the VNLB hot path: 1080p YUV444PS frames/s, Basic + Final.
+
+Workload (one step): a 16-frame 1920x1080 YUV444PS float32 clip, sigma 20 on
+the 8-bit scale, denoised by vnlbcu.Basic and then vnlbcu.Final with the
+reference CPU core's default parameter set passed explicitly (block 8, step 8,
+group 8, bm_range 9, radius 1, patch_time 1, rank 8, cap_factor 4; Final: tau
+400, variance_threshold 1.7, flat areas, alpha 1, beta 0.5), which makes the
+coupled estimator dimension 192 and the rank 8.  The clip is synthetic
+(vapoursynth-vnlb_b200/synth.py, seed = rank): no public dataset is named for
+this path.  The plain GPU form computes bit-identical output to the reference
+CPU core.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank (one GPU each) denoises its own clip (weak scaling,
+no collective on the data path); rank 0 prints one JSON line.  `value` is
+measured with the clip already resident in HBM; `e2e` goes through the C ABI
+with pinned host buffers, the plugin's copies inside the timed region (clip
+up for Basic, Basic frames down, clip and Basic frames up for Final, Final
+frames down).  `--impl reference` times the reference CPU implementation
+(oracle/_ref, the reference's own sources; the C restatement if that build is
+absent) on a bounded sample of the same workload on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "vapoursynth-vnlb_b200"))
+
+import synth  # noqa: E402
+
+METRIC = "1080p 444 frames/s Basic+Final: chosen vs plain GPU at ≤0.05 dB PSNR loss"
+UNIT = "frames/s"
+WIDTH, HEIGHT, FRAMES, PLANES, SIGMA = 1920, 1080, 16, 3, 20.0
+CPU_DEFAULTS = dict(block_size=8, block_step=8, group_size=8, bm_range=9, radius=1, patch_time=1, rank=8,
+                    cap_factor=4.0)
+# nominal FP32 issue rate of a B200 (148 SMs x 128 lanes at the 1965 MHz max clock)
+FP32_LANE_OPS = 148 * 128 * 1.965e9
+
+
+def workload_config(form: str) -> dict:
+    return {"workload": "vnlbcu.Basic+Final 1920x1080 YUV444PS 16 frames sigma 20, CPU-default parameter set",
+            "form": form, "width": WIDTH, "height": HEIGHT, "frames_per_clip": FRAMES, "planes": PLANES,
+            "sigma": SIGMA, "params": CPU_DEFAULTS, "l2": "inputs larger than L2 (398 MB clip per rank)"}
+
+
+def stage_params(stage: int):
+    import vnlbgpu_lib as lib
+    import vnlbcu
+    clip_shape = np.empty((FRAMES, PLANES, HEIGHT, WIDTH), np.float32)  # shape only for the parser
+    kw = dict(CPU_DEFAULTS)
+    if stage == lib.STAGE_FINAL:
+        kw.update(tau=400.0, variance_threshold=1.7, flat_areas=1, weight_alpha=1.0, weight_beta=0.5,
+                  weight_gamma=1.0)
+    else:
+        kw.update(variance_threshold=1.1, weight_alpha=0.75, weight_beta=0.35, weight_gamma=1.0)
+    return vnlbcu.parse_parameters(stage, clip_shape, SIGMA, kw)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, sm_max, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                sm_max = max(sm_max, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": sm_max or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- CPU reference
+def cpu_reference_sample(threads: int | None = None):
+    """Times the reference CPU implementation on a bounded sample of the
+    workload: a 1920 x 136 horizontal band of the clip (1/7.94 of a frame),
+    Basic + Final anchor-frame processing of `threads` anchor frames in
+    parallel (one thread per anchor frame, as VapourSynth's frame threading
+    does).  Each output frame needs exactly one Basic and one Final anchor
+    frame, so frames/s = threads * band_fraction / step_seconds."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    try:
+        o, kind = O.Oracle("ref"), "reference"
+    except FileNotFoundError:
+        o, kind = O.Oracle("port"), "port"
+    threads = threads or min(os.cpu_count() or 1, 64)
+    band_rows = 136
+    frames = threads + 2
+    _, noisy = synth.make_clip(WIDTH, band_rows, frames, PLANES, SIGMA, seed=0)
+    bp = O.cpu_params(O.BASIC, SIGMA, **CPU_DEFAULTS)
+    fp = O.cpu_params(O.FINAL, SIGMA, **CPU_DEFAULTS)
+    stacks = o.stage_stacks(O.BASIC, bp, noisy, threads=threads)
+    basic = o.aggregate(stacks, noisy, bp.search_bwd, bp.search_fwd, bp.patch_time)
+
+    def step():
+        o.stage_stacks(O.BASIC, bp, noisy, first_anchor=1, anchor_count=threads, threads=threads)
+        o.stage_stacks(O.FINAL, fp, noisy, basic, first_anchor=1, anchor_count=threads, threads=threads)
+
+    fraction = band_rows / HEIGHT
+    sample = (f"Basic+Final anchor frames 1..{threads} of a 1920x{band_rows} band ({frames} frames) of the "
+              f"workload clip, {threads} threads; frames/s = {threads} x {fraction:.4f} / step seconds")
+    return o, kind, threads, fraction, step, sample
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    _, kind, threads, fraction, step, sample = cpu_reference_sample()
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    seconds = (time.perf_counter() - t0) / args.steps
+    value = threads * fraction / seconds
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": workload_config("reference CPU core"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- GPU path
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import vnlbgpu_lib as lib
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    clean, noisy = synth.make_clip(WIDTH, HEIGHT, FRAMES, PLANES, SIGMA, seed=rank)
+    clip_bytes = noisy.nbytes
+    d_noisy = torch.from_numpy(noisy).cuda()
+    d_basic = torch.empty_like(d_noisy)
+    d_final = torch.empty_like(d_noisy)
+    # one dedicated stream for both stages: Final is ordered after the Basic
+    # frames it reads, and the timing events see all of the work
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    bp, fp = stage_params(lib.STAGE_BASIC), stage_params(lib.STAGE_FINAL)
+    bp.device_id = fp.device_id = local
+    sb = lib.Session(bp, WIDTH, HEIGHT, FRAMES, PLANES)
+    sf = lib.Session(fp, WIDTH, HEIGHT, FRAMES, PLANES)
+    for s in (sb, sf):
+        s.set_stream(stream.cuda_stream)
+
+    def step():
+        sb.set_clip_device(lib.SOURCE_CLIP, d_noisy.data_ptr())
+        sf.set_clip_device(lib.SOURCE_CLIP, d_noisy.data_ptr())
+        sf.set_clip_device(lib.SOURCE_REF, d_basic.data_ptr())
+        sb.render_clip_device(d_basic.data_ptr())
+        sf.render_clip_device(d_final.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    sb.synchronize()
+    sf.synchronize()
+    torch.cuda.synchronize()
+    psnr = (synth.psnr(d_basic.cpu().numpy(), clean), synth.psnr(d_final.cpu().numpy(), clean),
+            synth.psnr(noisy, clean))
+    launches0 = sb.stats()["kernel_launches"] + sf.stats()["kernel_launches"]
+    groups0 = sb.stats()["groups"] + sf.stats()["groups"]
+    sb.kernel_timing(True)
+    sf.kernel_timing(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        torch.cuda.synchronize()
+    sb.synchronize()
+    sf.synchronize()
+    elapsed_ms = start.elapsed_time(end)
+    kb, kf = sb.kernel_timing(False), sf.kernel_timing(False)
+    launches = sb.stats()["kernel_launches"] + sf.stats()["kernel_launches"] - launches0
+    groups = sb.stats()["groups"] + sf.stats()["groups"] - groups0
+    t = torch.tensor([elapsed_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * FRAMES * args.steps / (max_ms / 1e3)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    h_noisy = torch.from_numpy(noisy).pin_memory()
+    h_basic = torch.empty_like(h_noisy).pin_memory()
+    h_final = torch.empty_like(h_noisy).pin_memory()
+
+    def e2e_step():
+        sb.set_clip_ptr(lib.SOURCE_CLIP, h_noisy.data_ptr())
+        sb.render_clip_into(h_basic.data_ptr())
+        sf.set_clip_ptr(lib.SOURCE_CLIP, h_noisy.data_ptr())
+        sf.set_clip_ptr(lib.SOURCE_REF, h_basic.data_ptr())
+        sf.render_clip_into(h_final.data_ptr())
+
+    e2e_step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2e_steps = max(1, min(args.steps, 5))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    te = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * FRAMES * e2e_steps / (float(te.item()) / 1e3)
+    same = bool(torch.equal(h_final, d_final.cpu()))
+
+    # ---- roofline of the dominant kernel class
+    kernels = {k: (kb[k][0] + kf[k][0], kb[k][1] + kf[k][1]) for k in kb}
+    dominant = max(kernels, key=lambda k: kernels[k][0])
+    total_kernel_ms = sum(v[0] for v in kernels.values())
+    window = bp.search_window
+    temporal = bp.search_bwd + bp.search_fwd + 1
+    dm_basic = bp.patch_size ** 2 * bp.patch_time
+    dm_final = dm_basic * PLANES
+    groups_per_stage = groups / 2
+    match_ops = 3.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
+    match_ms, match_launches = kernels["match"]
+    roofline = {
+        "kernel": "match (exact FP32 SSD + CPU-order selection)",
+        "bound": "fp32",
+        "achieved": match_ops / (match_ms / 1e3) / 1e12,
+        "peak": FP32_LANE_OPS / 1e12,
+        "unit": "TFLOP/s",
+        "frac": (match_ops / (match_ms / 1e3)) / FP32_LANE_OPS,
+        "peak_source": "nominal FP32 lane-op rate 148 SM x 128 x 1.965 GHz (MEASURED_PEAKS.json has no FP32 figure)",
+        "work": "3 FP32 ops (sub, mul, add; no FMA, the CPU's order) per candidate element, "
+                "G x W^2 x T x d_m per anchor frame",
+        "ms_per_launch": match_ms / max(1, match_launches),
+        "traffic": None,
+    }
+    per_kernel = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1],
+                      "share": v[0] / total_kernel_ms if total_kernel_ms else None} for k, v in kernels.items()}
+
+    cpu_baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        _, kind, threads, fraction, cstep, sample = cpu_reference_sample()
+        cstep()
+        c0 = time.perf_counter()
+        cstep()
+        cs = time.perf_counter() - c0
+        cpu_baseline = {"value": threads * fraction / cs, "unit": UNIT, "cores": threads, "kind": kind,
+                        "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict(workload_config("plain (exact, bit-identical to the CPU core)"),
+                               psnr_db={"noisy": psnr[2], "basic": psnr[0], "final": psnr[1]},
+                               kernels=per_kernel, dominant_kernel=dominant,
+                               e2e_output_matches_device_output=same),
+                "roofline": roofline, "cpu_baseline": cpu_baseline,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * clip_bytes,
+                        "d2h_bytes_per_step": 2 * clip_bytes},
+                "gpu_launches": launches, "clocks": clocks.summary()}
+        print(json.dumps(line), flush=True)
+    sb.close()
+    sf.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def run_profile_case(args):
+    """A small case for ncu: one Basic and one Final anchor frame of a
+    3-frame 1920x1080 YUV444PS clip (the workload's frame size and
+    parameters), each stage launching every kernel class once."""
+    import vnlbgpu_lib as lib
+
+    _, noisy = synth.make_clip(WIDTH, HEIGHT, 3, PLANES, SIGMA, seed=0)
+    shape = np.empty((3, PLANES, HEIGHT, WIDTH), np.float32)
+    out = []
+    for stage in (lib.STAGE_BASIC, lib.STAGE_FINAL):
+        import vnlbcu
+        kw = dict(CPU_DEFAULTS)
+        if stage == lib.STAGE_FINAL:
+            kw.update(tau=400.0, variance_threshold=1.7)
+        else:
+            kw.update(variance_threshold=1.1)
+        s = lib.Session(vnlbcu.parse_parameters(stage, shape, SIGMA, kw), WIDTH, HEIGHT, 3, PLANES)
+        s.set_clip(lib.SOURCE_CLIP, noisy)
+        if stage == lib.STAGE_FINAL:
+            s.set_clip(lib.SOURCE_REF, noisy)
+        out.append(float(s.render_stack(1).sum()))
+        s.close()
+    print(json.dumps({"profile_case": "ok", "checksums": out}))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run only a small case (one anchor frame per stage) for ncu captures")
+    args = ap.parse_args()
+    if args.profile_case:
+        return run_profile_case(args)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -130,11 +130,16 @@ int vnlbgpu_render_stack(vnlbgpu_session* session, int n, float* const* planes, 
 int vnlbgpu_aggregate(const float* stacks, const float* source, int width, int height, int frames, int channels,
                       int search_bwd, int search_fwd, int patch_time, int device_id, float* out);
 
-int vnlbgpu_get_stats(const vnlbgpu_session* session, vnlbgpu_stats* stats);
+int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats);
 
 /* The CUDA stream the session enqueues on (a cudaStream_t), for callers that
  * time or order device work around it. */
 void* vnlbgpu_stream(vnlbgpu_session* session);
+
+/* Makes the session enqueue on a caller-owned stream (NULL: its own stream),
+ * e.g. one stream shared by a Basic and a Final session so that Final is
+ * ordered after the Basic frames it reads. */
+int vnlbgpu_set_stream(vnlbgpu_session* session, void* stream);
 
 #ifdef __cplusplus
 }

@@ -33,6 +33,13 @@ int vnlbgpu_diag_anchor(vnlbgpu_session* session, int anchor, int* grid_xy, int*
                         vnlbgpu_diag_row* active_rows, int active_capacity, int active_row_capacity, int* groups,
                         int* active_groups, int* rows, int* max_rows);
 
+/* Per-kernel device time.  Returns the milliseconds and launch counts
+ * accumulated since the previous call for the kernel classes
+ *   0 match, 1 paste mask, 2 group filter, 3 stack tiles, 4 normalise
+ * (arrays of 5), resets them, and turns event timing on (enable != 0) or off.
+ * Timing brackets each launch with CUDA events on the session's stream. */
+int vnlbgpu_diag_kernel_timing(vnlbgpu_session* session, int enable, double* ms, long long* launches);
+
 #ifdef __cplusplus
 }
 #endif

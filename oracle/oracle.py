@@ -115,10 +115,10 @@ class Oracle:
         self.kind = kind
         self.prefix = "vnlbref_" if kind.startswith("ref") else "vnlboracle_"
         self.lib = ctypes.CDLL(str(path))
-        self.lib[self.prefix + "last_error"].restype = ctypes.c_char_p
+        getattr(self.lib, self.prefix + "last_error").restype = ctypes.c_char_p
 
     def _fn(self, name):
-        return self.lib[self.prefix + name]
+        return getattr(self.lib, self.prefix + name)
 
     def _check(self, status: int):
         if status != 0:
@@ -196,7 +196,7 @@ def anchor_groups(stage: int, params: StageParams, clip: np.ndarray, basic: np.n
     stack = np.zeros((channels, params.slots * 2 * height, width), np.float32)
     cp = params.to_c()
     total = ctypes.c_int()
-    fn = o.lib["vnlboracle_anchor_groups"]
+    fn = o.lib.vnlboracle_anchor_groups
     n = fn(ctypes.c_int(stage), ctypes.byref(cp), o._ptr(clip), o._ptr(basic), width, height, frames,
            channels, anchor, o._ptr(stack), None, 0, None, 0, ctypes.byref(total))
     if n < 0:
@@ -221,7 +221,7 @@ def match_anchor(stage: int, params: StageParams, clip: np.ndarray, basic: np.nd
     cap = 8192
     out = (_Match * cap)()
     cp = params.to_c()
-    n = o.lib["vnlboracle_match_anchor"](ctypes.c_int(stage), ctypes.byref(cp), o._ptr(clip), o._ptr(basic),
+    n = o.lib.vnlboracle_match_anchor(ctypes.c_int(stage), ctypes.byref(cp), o._ptr(clip), o._ptr(basic),
                                           width, height, frames, channels, anchor, x, y, out, cap)
     if n < 0:
         o._check(-1)

@@ -1,0 +1,205 @@
+"""GPU parity: the plain B200 path against the CPU oracle, through the C ABI.
+
+The bar is bit-exactness (the reference's own CUDA matcher test is bit-exact
+too, tests/cpp/test_cuda_block_match.cpp:640-672): the retained rows of every
+grid anchor, the paste-mask active set, the aggregation weights, the
+contribution stacks and the aggregated Basic/Final frames must equal the
+oracle's float for float.  Sizes are small enough for the oracle to finish in
+seconds, except one full-size (1920x1080 YUV444PS) check on three anchor
+frames.
+"""
+import threading
+
+import numpy as np
+import pytest
+
+import oracle as O
+import synth
+import vnlb
+import vnlbcu
+import vnlbgpu_lib as lib
+
+pytestmark = pytest.mark.gpu
+
+
+def session_for(stage, p: O.StageParams, clip, basic=None):
+    d = {f: getattr(p, f) for f in p.__dataclass_fields__}
+    params = lib.Params(stage=stage, device_id=0, num_streams=1, chunk_size=768,
+                        **{k: (float(v) if isinstance(v, (float, np.floating)) else int(v)) for k, v in d.items()})
+    frames, planes, h, w = clip.shape
+    s = lib.Session(params, w, h, frames, planes)
+    s.set_clip(lib.SOURCE_CLIP, clip)
+    if stage == lib.STAGE_FINAL:
+        s.set_clip(lib.SOURCE_REF, basic)
+    return s
+
+
+def vnlb_kwargs(p: O.StageParams, stage):
+    kw = dict(sigma=float(np.float32(p.sigma) * np.float32(255.0)), block_size=p.patch_size,
+              patch_time=p.patch_time, bm_range=(p.search_window - 1) // 2, search_bwd=p.search_bwd,
+              search_fwd=p.search_fwd, group_size=p.similar, rank=p.rank, cap_factor=p.similar_cap_factor,
+              beta=p.beta, tau=float(np.float32(p.tau) * np.float32(65025.0)),
+              variance_threshold=p.variance_threshold, weight_alpha=p.weight_alpha, weight_beta=p.weight_beta,
+              weight_gamma=p.weight_gamma, block_step=p.proc_step)
+    if stage == lib.STAGE_FINAL:
+        kw.update(flat_areas=p.flat_areas, gamma=p.gamma)
+    return kw
+
+
+def gpu_chain(noisy, bp, fp):
+    bs = vnlb.Basic(noisy, **vnlb_kwargs(bp, 0))
+    basic = vnlb.Aggregate(bs, src=noisy, patch_time=bp.patch_time, search_bwd=bp.search_bwd,
+                           search_fwd=bp.search_fwd)
+    fs = vnlb.Final(noisy, ref=basic, **vnlb_kwargs(fp, 1))
+    final = vnlb.Aggregate(fs, src=noisy, patch_time=fp.patch_time, search_bwd=fp.search_bwd,
+                           search_fwd=fp.search_fwd)
+    return bs, basic, fs, final
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.int32)
+
+
+def test_golden_reference_outputs(golden):
+    """Committed outputs of the reference CPU core (tests/golden/ref_outputs.npz)."""
+    data, meta = golden
+    for name, m in meta.items():
+        noisy = data[f"{name}/noisy"]
+        bp = O.cpu_params(O.BASIC, m["sigma"], **m["shared"], **m["basic"])
+        fp = O.cpu_params(O.FINAL, m["sigma"], **m["shared"], **m["final"])
+        _, basic, _, final = gpu_chain(noisy, bp, fp)
+        assert np.array_equal(bits(basic), bits(data[f"{name}/basic"])), name
+        assert np.array_equal(bits(final), bits(data[f"{name}/final"])), name
+
+
+CASES = [
+    ("gray_defaults", 64, 48, 4, 1, 20.0, {}),
+    ("yuv_defaults", 96, 80, 5, 3, 20.0, {}),
+    ("yuv_cuda_like", 96, 72, 4, 3, 20.0, dict(block_size=7, patch_time=2, bm_range=6, group_size=16, rank=15,
+                                               block_step=3)),
+    ("gray_k32_tau", 80, 64, 4, 1, 30.0, dict(group_size=32, rank=20, tau=1500.0, cap_factor=2.0,
+                                              block_step=5)),
+    ("yuv_no_weights", 72, 56, 3, 3, 12.0, dict(weight_alpha=0.0, weight_beta=0.0, weight_gamma=0.0)),
+    ("yuv_alpha_only", 72, 56, 3, 3, 12.0, dict(weight_beta=0.0, cap_factor=0.0)),
+]
+
+
+@pytest.mark.parametrize("name,w,h,f,planes,sigma,kw", CASES, ids=[c[0] for c in CASES])
+def test_stagewise_bit_exact(name, w, h, f, planes, sigma, kw):
+    _, noisy = synth.make_clip(w, h, f, planes, sigma, seed=sum(map(ord, name)))
+    bp = O.cpu_params(O.BASIC, sigma, **kw)
+    fp = O.cpu_params(O.FINAL, sigma, **kw)
+    ob, of = O.Oracle("port").chain(noisy, bp, fp)
+    for stage, p, ref in ((lib.STAGE_BASIC, bp, None), (lib.STAGE_FINAL, fp, ob)):
+        s = session_for(stage, p, noisy, ref)
+        for anchor in range(f - p.patch_time + 1):
+            d = s.diag_anchor(anchor)
+            for gi, (x, y) in enumerate(d["xy"]):
+                want = O.match_anchor(stage, p, noisy, ref, anchor, int(x), int(y))
+                got = d["grid_rows"][gi][:d["counts"][gi]]
+                assert len(got) == len(want), (stage, anchor, gi)
+                for field in ("x", "y", "frame"):
+                    assert np.array_equal(got[field], want[field]), (stage, anchor, gi, field)
+                assert np.array_equal(bits(got["distance"]), bits(want["distance"])), (stage, anchor, gi)
+            stack, groups, rows = O.anchor_groups(stage, p, noisy, ref, anchor)
+            assert [tuple(d["xy"][i]) for i in d["active"]] == [(g[0], g[1]) for g in groups]
+            ar = d["active_rows"]
+            assert len(ar) == len(rows)
+            for field in ("x", "y", "frame"):
+                assert np.array_equal(ar[field], rows[field])
+            assert np.array_equal(bits(ar["weight"]), bits(rows["weight"]))
+            assert np.array_equal(bits(s.render_stack(anchor)), bits(stack))
+        s.close()
+    bs, basic, fs, final = gpu_chain(noisy, bp, fp)
+    assert np.array_equal(bits(basic), bits(ob))
+    assert np.array_equal(bits(final), bits(of))
+
+
+def test_vnlbcu_defaults_match_oracle():
+    """vnlbcu.Basic/Final with every default (block 7, patch_time 2, bm_range
+    13, group 16, rank 15, step 3) against the oracle on the same parameters."""
+    _, noisy = synth.make_clip(80, 64, 5, 3, 20.0, seed=31)
+    basic = vnlbcu.Basic(noisy, sigma=20.0)
+    final = vnlbcu.Final(noisy, ref=basic, sigma=20.0)
+
+    def to_stage(params):
+        return O.StageParams(**{f: getattr(params, f) for f in O.StageParams.__dataclass_fields__})
+
+    pb = vnlbcu.parse_parameters(lib.STAGE_BASIC, noisy, 20.0, {})
+    pf = vnlbcu.parse_parameters(lib.STAGE_FINAL, noisy, 20.0, {})
+    o = O.Oracle("port")
+    ob = o.aggregate(o.stage_stacks(O.BASIC, to_stage(pb), noisy), noisy, pb.search_bwd, pb.search_fwd, pb.patch_time)
+    of = o.aggregate(o.stage_stacks(O.FINAL, to_stage(pf), noisy, ob), noisy, pf.search_bwd, pf.search_fwd,
+                     pf.patch_time)
+    assert np.array_equal(bits(basic), bits(ob))
+    assert np.array_equal(bits(final), bits(of))
+
+
+def test_random_access_and_threads():
+    _, noisy = synth.make_clip(64, 48, 6, 3, 20.0, seed=41)
+    f = vnlbcu.BasicFilter(noisy, sigma=20.0, block_size=8, block_step=8, group_size=8, rank=8, bm_range=5)
+    whole = f.render()
+    order = [5, 0, 3, 1, 4, 2]
+    for n in order:
+        assert np.array_equal(f.get_frame(n), whole[n])
+    results = {}
+
+    def worker(n):
+        results[n] = f.get_frame(n)
+
+    threads = [threading.Thread(target=worker, args=(n,)) for n in range(6)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for n in range(6):
+        assert np.array_equal(results[n], whole[n])
+
+
+def test_aggregate_matches_oracle():
+    _, noisy = synth.make_clip(48, 40, 4, 3, 20.0, seed=51)
+    p = O.cpu_params(O.BASIC, 20.0, radius=2, patch_time=2, group_size=12, rank=10)
+    stacks = O.Oracle("port").stage_stacks(O.BASIC, p, noisy)
+    want = O.Oracle("port").aggregate(stacks, noisy, 2, 2, 2)
+    got = vnlb.Aggregate(stacks, src=noisy, patch_time=2, radius=2)
+    assert np.array_equal(bits(got), bits(want))
+
+
+@pytest.mark.parametrize("planes", [1, 3])
+def test_constant_video(planes):
+    """Equal groups pass through unfiltered (core.cpp:110-131, 516-531); the
+    output reproduces the constant (tests/cpp/test_core.cpp:247-356, 1e-5)
+    and equals the oracle bit for bit."""
+    clip = np.full((4, planes, 40, 48), 0.625, np.float32)
+    kw = dict(block_size=8, block_step=4, group_size=8, rank=8, bm_range=4)
+    out = vnlbcu.Basic(clip, sigma=10.0, **kw)
+    p = O.cpu_params(O.BASIC, 10.0, **kw)
+    want = O.Oracle("port").aggregate(O.Oracle("port").stage_stacks(O.BASIC, p, clip), clip, 1, 1, 1)
+    assert np.array_equal(bits(out), bits(want))
+    assert np.allclose(out, 0.625, atol=1e-5)
+
+
+def test_unsupported_configurations_raise():
+    gray = np.zeros((3, 1, 32, 32), np.float32)
+    with pytest.raises(lib.VNLBError, match="dual-PCA"):
+        vnlb.Basic(gray, sigma=10.0, block_size=4, group_size=8, rank=8)  # covariance model (dim 16)
+    with pytest.raises(lib.VNLBError, match="chroma=1"):
+        vnlb.Basic(np.zeros((3, 3, 32, 32), np.float32), sigma=10.0, chroma=0)
+
+
+def test_full_size_anchor_frames_bit_exact():
+    """1920x1080 YUV444PS, CPU-default parameters: GPU stacks of anchor frames
+    0-2 of both stages equal the oracle's."""
+    _, noisy = synth.make_clip(1920, 1080, 4, 3, 20.0, seed=0)
+    bp = O.cpu_params(O.BASIC, 20.0)
+    fp = O.cpu_params(O.FINAL, 20.0)
+    sb = session_for(lib.STAGE_BASIC, bp, noisy)
+    basic = sb.render_clip()
+    sf = session_for(lib.STAGE_FINAL, fp, noisy, basic)
+    o = O.Oracle("port")
+    for stage, s, p, ref in ((lib.STAGE_BASIC, sb, bp, None), (lib.STAGE_FINAL, sf, fp, basic)):
+        want = o.stage_stacks(stage, p, noisy, ref, first_anchor=0, anchor_count=3, threads=3)
+        for a in range(3):
+            assert np.array_equal(bits(s.render_stack(a)), bits(want[a])), (stage, a)
+    again = session_for(lib.STAGE_BASIC, bp, noisy).render_clip()
+    assert np.array_equal(bits(again), bits(basic))  # deterministic

@@ -182,7 +182,6 @@ __global__ void __launch_bounds__(256) match_kernel(MatchLaunch L) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int nwarps = blockDim.x >> 5;
     const Strip strip = L.strips[blockIdx.x];
     const int Pd = L.P;
     const int Cs = L.search_channels;

@@ -99,6 +99,8 @@ __global__ void __launch_bounds__(32) paste_kernel(PasteLaunch L) {
         L.row_offset[running_active] = running_rows;
         L.counters->active = running_active;
         L.counters->rows = running_rows;
+        atomicAdd(L.totals, static_cast<unsigned long long>(running_active));
+        atomicAdd(L.totals + 1, static_cast<unsigned long long>(running_rows));
     }
 }
 

@@ -113,8 +113,56 @@ struct Session {
     int region_rows = 0, region_stride = 0, region_w_max = 0;
     bool coupled = true;
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // the stream all work is enqueued on
+    cudaStream_t own_stream = nullptr;  // created by the session
     vnlbgpu_stats stats{};
+
+    // optional per-kernel timing: (category, start, stop) event triples
+    bool timing = false;
+    struct Timed {
+        int category;
+        cudaEvent_t start, stop;
+    };
+    std::vector<Timed> timed;
+    std::vector<cudaEvent_t> event_pool;
+    double kernel_ms[kTimedCategories] = {};
+    long long kernel_count[kTimedCategories] = {};
+
+    cudaEvent_t take_event() {
+        if (!event_pool.empty()) {
+            cudaEvent_t e = event_pool.back();
+            event_pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        check(cudaEventCreate(&e), "cudaEventCreate");
+        return e;
+    }
+    cudaEvent_t begin_timed() {
+        if (!timing) return nullptr;
+        cudaEvent_t e = take_event();
+        check(cudaEventRecord(e, stream), "cudaEventRecord");
+        return e;
+    }
+    void end_timed(int category, cudaEvent_t start) {
+        if (!timing) return;
+        cudaEvent_t e = take_event();
+        check(cudaEventRecord(e, stream), "cudaEventRecord");
+        timed.push_back(Timed{category, start, e});
+    }
+    void collect_timing() {
+        if (timed.empty()) return;
+        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize(timing)");
+        for (const Timed& t : timed) {
+            float ms = 0.0f;
+            check(cudaEventElapsedTime(&ms, t.start, t.stop), "cudaEventElapsedTime");
+            kernel_ms[t.category] += ms;
+            kernel_count[t.category] += 1;
+            event_pool.push_back(t.start);
+            event_pool.push_back(t.stop);
+        }
+        timed.clear();
+    }
 
     DeviceArray<float> own_clip, own_ref;
     const float* clip = nullptr;
@@ -125,6 +173,7 @@ struct Session {
     DeviceArray<int> d_row_counts, d_victims, d_victim_counts, d_active, d_row_offset, d_row_group;
     DeviceArray<int2> d_active_xy;
     DeviceArray<FrameCounters> d_counters;
+    DeviceArray<unsigned long long> d_totals;
     DeviceArray<float> d_filtered, d_weights, d_window, d_out_frame, d_pack;
     std::map<int, std::unique_ptr<Grid>> grids;
     int last_grid_key = INT_MIN;
@@ -140,7 +189,13 @@ struct Session {
     std::vector<float> host_window;
 
     ~Session() {
-        if (stream) cudaStreamDestroy(stream);
+        if (stream) cudaStreamSynchronize(stream);
+        for (const Timed& t : timed) {
+            cudaEventDestroy(t.start);
+            cudaEventDestroy(t.stop);
+        }
+        for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+        if (own_stream) cudaStreamDestroy(own_stream);
     }
 
     size_t plane() const { return static_cast<size_t>(width) * height; }
@@ -237,7 +292,8 @@ struct Session {
 
         check(cudaSetDevice(p.device_id), "cudaSetDevice");
         device = p.device_id;
-        check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        check(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        stream = own_stream;
 
         // largest grid over the anchor phases
         for (int key = 0; key < step; ++key) max_groups = std::max(max_groups, static_cast<int>(build_anchor_list(key).size()));
@@ -269,6 +325,8 @@ struct Session {
         d_active_xy.allocate(G, "cudaMalloc(active positions)");
         d_row_offset.allocate(G + 1, "cudaMalloc(row offsets)");
         d_counters.allocate(1, "cudaMalloc(counters)");
+        d_totals.allocate(2, "cudaMalloc(totals)");
+        check(cudaMemset(d_totals.ptr, 0, 2 * sizeof(unsigned long long)), "cudaMemset(totals)");
         const size_t R = G * max_rows;
         size_t free_bytes = 0, total_bytes = 0;
         check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
@@ -452,7 +510,9 @@ struct Session {
         m.victims = d_victims.ptr;
         m.victim_counts = d_victim_counts.ptr;
         m.victim_stride = victim_stride;
+        cudaEvent_t t0 = begin_timed();
         check(launch_match(m, static_cast<int>(grid.strips.size()), warps, stream), "match kernel launch");
+        end_timed(kTimedMatch, t0);
 
         check(cudaMemsetAsync(d_counters.ptr, 0, sizeof(FrameCounters), stream), "cudaMemsetAsync(counters)");
         PasteLaunch pl{};
@@ -466,7 +526,10 @@ struct Session {
         pl.active_xy = d_active_xy.ptr;
         pl.row_offset = d_row_offset.ptr;
         pl.counters = d_counters.ptr;
+        pl.totals = d_totals.ptr;
+        t0 = begin_timed();
         check(launch_paste(pl, stream), "paste kernel launch");
+        end_timed(kTimedPaste, t0);
 
         FilterLaunch fl{};
         fl.noisy = clip;
@@ -494,7 +557,9 @@ struct Session {
         fl.weights = d_weights.ptr;
         fl.row_info = d_row_info.ptr;
         fl.row_group = d_row_group.ptr;
+        t0 = begin_timed();
         check(launch_filter(fl, 148 * 8, stream), "filter kernel launch");
+        end_timed(kTimedFilter, t0);
 
         TileLaunch tl{};
         tl.width = width;
@@ -521,7 +586,9 @@ struct Session {
         tl.tile = 32;
         tl.tiles_x = (width + 31) / 32;
         tl.tiles_y = (height + 31) / 32;
+        t0 = begin_timed();
         check(launch_tiles(tl, stream), "tile kernel launch");
+        end_timed(kTimedTiles, t0);
         stats.anchor_frames += 1;
         stats.groups += G;
         stats.kernel_launches += 4;
@@ -562,7 +629,9 @@ struct Session {
         }
         nl.source = clip + static_cast<size_t>(n) * frame_values();
         nl.out = out;
+        cudaEvent_t t0 = begin_timed();
         check(launch_normalize(nl, stream), "normalize kernel launch");
+        end_timed(kTimedNormalize, t0);
         stats.kernel_launches += 1;
     }
 
@@ -811,14 +880,50 @@ int vnlbgpu_aggregate(const float* stacks, const float* source, int width, int h
     });
 }
 
-int vnlbgpu_get_stats(const vnlbgpu_session* session, vnlbgpu_stats* stats) {
+int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats) {
     return guarded([&]() {
         if (!session || !stats) vnlbgpu::fail("VNLB CUDA: null argument");
-        *stats = session->impl.stats;
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        unsigned long long totals[2] = {0, 0};
+        vnlbgpu::check(cudaMemcpyAsync(totals, s.d_totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s.stream),
+                       "cudaMemcpyAsync(totals)");
+        vnlbgpu::check(cudaStreamSynchronize(s.stream), "cudaStreamSynchronize");
+        s.stats.active_groups = static_cast<long long>(totals[0]);
+        s.stats.rows = static_cast<long long>(totals[1]);
+        *stats = s.stats;
     });
 }
 
 void* vnlbgpu_stream(vnlbgpu_session* session) { return session ? session->impl.stream : nullptr; }
+
+int vnlbgpu_set_stream(vnlbgpu_session* session, void* stream) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.collect_timing();
+        vnlbgpu::check(cudaStreamSynchronize(s.stream), "cudaStreamSynchronize");
+        s.stream = stream ? static_cast<cudaStream_t>(stream) : s.own_stream;
+    });
+}
+
+int vnlbgpu_diag_kernel_timing(vnlbgpu_session* session, int enable, double* ms, long long* launches) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.collect_timing();
+        for (int i = 0; i < vnlbgpu::kTimedCategories; ++i) {
+            if (ms) ms[i] = s.kernel_ms[i];
+            if (launches) launches[i] = s.kernel_count[i];
+            s.kernel_ms[i] = 0.0;
+            s.kernel_count[i] = 0;
+        }
+        s.timing = enable != 0;
+    });
+}
 
 int vnlbgpu_diag_anchor(vnlbgpu_session* session, int anchor, int* grid_xy, int* grid_counts,
                         vnlbgpu_diag_row* grid_rows, int grid_capacity, int grid_row_capacity, int* active,

@@ -10,6 +10,9 @@
 
 namespace vnlbgpu {
 
+// Kernel classes timed by the session (vnlbgpu_diag_kernel_timing).
+enum TimedCategory { kTimedMatch = 0, kTimedPaste, kTimedFilter, kTimedTiles, kTimedNormalize, kTimedCategories };
+
 // Most temporal slots (search_bwd + search_fwd + patch_time) and scheduled
 // candidate frames the GPU path handles.
 constexpr int kMaxContributors = 32;
@@ -79,6 +82,7 @@ struct PasteLaunch {
     int2* active_xy;      // [G] their positions
     int* row_offset;      // [G + 1] exclusive prefix of retained rows
     FrameCounters* counters;
+    unsigned long long* totals;  // session totals: active groups, rows
 };
 
 cudaError_t launch_paste(const PasteLaunch& L, cudaStream_t stream);

@@ -51,8 +51,9 @@ EXPORTS = [
     "vnlbgpu_set_clip_host", "vnlbgpu_set_clip_device", "vnlbgpu_render_frame",
     "vnlbgpu_render_clip_host", "vnlbgpu_render_clip_device", "vnlbgpu_synchronize",
     "vnlbgpu_render_stack", "vnlbgpu_aggregate", "vnlbgpu_get_stats", "vnlbgpu_stream",
-    "vnlbgpu_diag_anchor",
+    "vnlbgpu_set_stream", "vnlbgpu_diag_anchor", "vnlbgpu_diag_kernel_timing",
 ]
+KERNEL_CLASSES = ("match", "paste", "filter", "tiles", "normalize")
 
 _lib = None
 _lib_lock = threading.Lock()
@@ -90,6 +91,9 @@ def load() -> ctypes.CDLL:
                 ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                 ctypes.POINTER(ctypes.c_int)]
+            lib.vnlbgpu_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.vnlbgpu_diag_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                                       ctypes.c_void_p]
             _lib = lib
     return _lib
 
@@ -132,6 +136,10 @@ class Session:
         if clip.shape != self.shape:
             raise VNLBError(f"VNLB CUDA: clip shape {clip.shape} does not match {self.shape}")
         _check(self.lib.vnlbgpu_set_clip_host(self.handle, source, clip.ctypes.data))
+
+    def set_clip_ptr(self, source: int, host_ptr: int):
+        """Uploads a whole clip from a raw host pointer (e.g. pinned memory)."""
+        _check(self.lib.vnlbgpu_set_clip_host(self.handle, source, ctypes.c_void_p(host_ptr)))
 
     def set_clip_device(self, source: int, device_ptr: int, keepalive=None):
         self._keep[source] = keepalive
@@ -178,6 +186,16 @@ class Session:
 
     def stream(self) -> int:
         return self.lib.vnlbgpu_stream(self.handle) or 0
+
+    def set_stream(self, stream_ptr: int):
+        _check(self.lib.vnlbgpu_set_stream(self.handle, ctypes.c_void_p(stream_ptr or None)))
+
+    def kernel_timing(self, enable: bool = True) -> dict:
+        """Per-kernel-class device time (ms) and launches since the last call."""
+        ms = np.zeros(len(KERNEL_CLASSES), np.float64)
+        n = np.zeros(len(KERNEL_CLASSES), np.int64)
+        _check(self.lib.vnlbgpu_diag_kernel_timing(self.handle, 1 if enable else 0, ms.ctypes.data, n.ctypes.data))
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(KERNEL_CLASSES)}
 
     def diag_anchor(self, anchor: int):
         """Runs one anchor frame and returns (grid, active) read-backs."""
