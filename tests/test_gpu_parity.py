@@ -173,8 +173,10 @@ def test_constant_video(planes):
     clip = np.full((4, planes, 40, 48), 0.625, np.float32)
     kw = dict(block_size=8, block_step=4, group_size=8, rank=8, bm_range=4)
     out = vnlbcu.Basic(clip, sigma=10.0, **kw)
-    p = O.cpu_params(O.BASIC, 10.0, **kw)
-    want = O.Oracle("port").aggregate(O.Oracle("port").stage_stacks(O.BASIC, p, clip), clip, 1, 1, 1)
+    pb = vnlbcu.parse_parameters(lib.STAGE_BASIC, clip, 10.0, kw)
+    p = O.StageParams(**{f: getattr(pb, f) for f in O.StageParams.__dataclass_fields__})
+    want = O.Oracle("port").aggregate(O.Oracle("port").stage_stacks(O.BASIC, p, clip), clip, p.search_bwd,
+                                      p.search_fwd, p.patch_time)
     assert np.array_equal(bits(out), bits(want))
     assert np.allclose(out, 0.625, atol=1e-5)
 

@@ -19,26 +19,14 @@
 namespace vnlbgpu {
 namespace {
 
-constexpr int kTileThreads = 256;
+constexpr int kTileThreads = kTile * kTile;
 constexpr int kEntryCap = 1024;
 
 struct Entry {
-    int r;   // global row
-    int t;   // temporal offset inside the patch
-    int x, y;
-    float w;
+    int r;     // global row
+    int xyt;   // x | y << 14 | t << 28
+    float w;   // row weight
 };
-
-__device__ __forceinline__ int lower_bound_xy(const int2* xy, int n, int y, int x) {
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        const int2 v = xy[mid];
-        if (v.y < y || (v.y == y && v.x < x)) lo = mid + 1;
-        else hi = mid;
-    }
-    return lo;
-}
 
 __global__ void __launch_bounds__(kTileThreads) tile_kernel(TileLaunch L) {
     __shared__ Entry entries[kEntryCap];
@@ -46,106 +34,72 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(TileLaunch L) {
     __shared__ int s_done;
     extern __shared__ float window[];
 
-    const int T = L.tile;
-    const int tx0 = blockIdx.x * T;
-    const int ty0 = blockIdx.y * T;
-    const int slot = blockIdx.z;
+    const int tx = blockIdx.x, ty = blockIdx.y, slot = blockIdx.z;
+    const int tx0 = tx * kTile, ty0 = ty * kTile;
     const int P = L.P;
     const int C = L.channels;
-    const int reach = L.search_window - 1;  // |match - anchor| bound per axis
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int lane = tid & 31;
-
     for (int i = tid; i < P * P; i += blockDim.x) window[i] = L.window[i];
-    const int active = L.counters->active;
-    // groups whose anchor row can reach the tile: one contiguous range of the
-    // raster-ordered active list; their anchor x is filtered on the fly
-    const int ay_lo = ty0 - (P - 1) - reach;
-    const int ay_hi = ty0 + T - 1 + reach;
-    const int ax_lo = tx0 - (P - 1) - reach;
-    const int ax_hi = tx0 + T - 1 + reach;
-    int cur_g = 0, g_end = 0, cur_r = -1;  // warp-0 iterator state
-    if (warp == 0) {
-        cur_g = lower_bound_xy(L.active_xy, active, ay_lo, -0x7fffffff);
-        g_end = lower_bound_xy(L.active_xy, active, ay_hi + 1, -0x7fffffff);
-    }
 
-    constexpr int kMaxPix = 4;
-    const int pix_per_thread = (T * T + blockDim.x - 1) / blockDim.x;
-    float num[kMaxPix][4];
-    float wt[kMaxPix];
-#pragma unroll
-    for (int p = 0; p < kMaxPix; ++p) {
-        wt[p] = 0.0f;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) num[p][c] = 0.0f;
-    }
+    // warp-0 iterator over the grid rows that reach this tile; each grid row
+    // contributes one contiguous range of rows [row_offset[a0], row_offset[a1])
+    const int2 grid_rows = L.tile_grid_rows[ty];
+    int cur_row = grid_rows.x;
+    int cur_r = 0, r_end = 0;  // empty range: the first step loads grid row cur_row
+
+    const int px = tx0 + (tid % kTile);
+    const int py = ty0 + (tid / kTile);
+    float num[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float wt = 0.0f;
     __syncthreads();
 
     const int fused_cols = (P == kLanes || P == 2 * kLanes) ? P : (P / kLanes) * kLanes;
     for (;;) {
-        // ---- warp 0 collects the next batch of covering rows, in row order
         if (warp == 0) {
             int count = 0;
             bool full = false;
-            while (cur_g < g_end && !full) {
-                if (cur_r < 0) {
-                    const int gi = cur_g + lane;
-                    bool near = false;
-                    if (gi < g_end) {
-                        const int2 a = L.active_xy[gi];
-                        near = a.x >= ax_lo && a.x <= ax_hi;
-                    }
-                    const unsigned ballot = __ballot_sync(0xffffffffu, near);
-                    if (!ballot) {
-                        cur_g += 32;
-                        continue;
-                    }
-                    cur_g += __ffs(ballot) - 1;
-                    cur_r = L.row_offset[cur_g];
+            while (!full) {
+                if (cur_r >= r_end) {
+                    if (cur_row >= grid_rows.y) break;
+                    const int2 anchors = L.tile_anchors[static_cast<size_t>(cur_row) * L.tiles_x + tx];
+                    ++cur_row;
+                    const int a0 = L.active_prefix[anchors.x];
+                    const int a1 = L.active_prefix[anchors.y];
+                    cur_r = L.row_offset[a0];
+                    r_end = L.row_offset[a1];
+                    continue;
                 }
-                const int rend = L.row_offset[cur_g + 1];
-                while (cur_r < rend) {
-                    const int r = cur_r + lane;
-                    int hits = 0;
-                    int t_hit[4];
-                    MatchRow m = {0.0f, 0, 0, 0};
-                    if (r < rend) {
-                        m = L.row_info[r];
-                        if (m.x <= tx0 + T - 1 && m.x + P - 1 >= tx0 && m.y <= ty0 + T - 1 && m.y + P - 1 >= ty0) {
-                            for (int t = 0; t < L.Pt && hits < 4; ++t)
-                                if (m.frame + t - L.anchor_frame + L.search_bwd == slot) t_hit[hits++] = t;
+                const int r = cur_r + lane;
+                int hits = 0;
+                int t_hit = 0;
+                MatchRow m = {0.0f, 0, 0, 0};
+                if (r < r_end) {
+                    m = L.row_info[r];
+                    if (m.x <= tx0 + kTile - 1 && m.x + P - 1 >= tx0 && m.y <= ty0 + kTile - 1 && m.y + P - 1 >= ty0) {
+                        const int t = slot - L.search_bwd + L.anchor_frame - m.frame;
+                        if (t >= 0 && t < L.Pt) {
+                            hits = 1;
+                            t_hit = t;
                         }
                     }
-                    int prefix = hits;
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int v = __shfl_up_sync(0xffffffffu, prefix, o);
-                        if (lane >= o) prefix += v;
-                    }
-                    const int total = __shfl_sync(0xffffffffu, prefix, 31);
-                    if (count + total > kEntryCap) {
-                        full = true;
-                        break;
-                    }
-                    const int start = count + prefix - hits;
-                    for (int e = 0; e < hits; ++e) {
-                        Entry en;
-                        en.r = r;
-                        en.t = t_hit[e];
-                        en.x = m.x;
-                        en.y = m.y;
-                        en.w = L.weights[r];
-                        entries[start + e] = en;
-                    }
-                    count += total;
-                    cur_r += 32;
                 }
-                if (!full) {
-                    cur_g += 1;
-                    cur_r = -1;
+                const unsigned ballot = __ballot_sync(0xffffffffu, hits != 0);
+                const int total = __popc(ballot);
+                if (count + total > kEntryCap) {
+                    full = true;
+                    break;
                 }
+                if (hits) {
+                    Entry en;
+                    en.r = r;
+                    en.xyt = m.x | (m.y << 14) | (t_hit << 28);
+                    en.w = L.weights[r];
+                    entries[count + __popc(ballot & ((1u << lane) - 1u))] = en;
+                }
+                count += total;
+                cur_r += 32;
             }
             if (lane == 0) {
                 s_count = count;
@@ -153,53 +107,50 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(TileLaunch L) {
             }
         }
         __syncthreads();
-        // ---- apply the batch to this thread's pixels, in order
+        // apply the batch to this thread's pixel, in order
         const int n = s_count;
-        for (int p = 0; p < pix_per_thread && p < kMaxPix; ++p) {
-            const int local = tid + p * blockDim.x;
-            if (local >= T * T) break;
-            const int px = tx0 + local % T;
-            const int py = ty0 + local / T;
-            for (int e = 0; e < n; ++e) {
-                const Entry en = entries[e];
-                const int dx = px - en.x;
-                const int dy = py - en.y;
-                if (dx < 0 || dx >= P || dy < 0 || dy >= P) continue;
-                const int pos = (en.t * P + dy) * P + dx;
-                const float* f = L.filtered + static_cast<size_t>(en.r) * L.dim;
-                if (L.coupled && !L.windowed) {
-                    const bool fused = dx < fused_cols;
-                    for (int c = 0; c < C; ++c) {
-                        const float x = __ldg(f + c * L.patch_dim + pos);
-                        num[p][c] = fused ? __fmaf_rn(en.w, x, num[p][c]) : __fadd_rn(num[p][c], __fmul_rn(en.w, x));
-                    }
-                    wt[p] = __fadd_rn(wt[p], en.w);
-                } else {
-                    const float cw = __fmul_rn(en.w, window[dy * P + dx]);
-                    for (int c = 0; c < C; ++c) {
-                        const float x = __ldg(f + c * L.patch_dim + pos);
-                        num[p][c] = __fadd_rn(num[p][c], __fmul_rn(cw, x));
-                    }
-                    wt[p] = __fadd_rn(wt[p], cw);
+        for (int e = 0; e < n; ++e) {
+            const Entry en = entries[e];
+            const int ex = en.xyt & 0x3fff;
+            const int ey = (en.xyt >> 14) & 0x3fff;
+            const unsigned dx = static_cast<unsigned>(px - ex);
+            const unsigned dy = static_cast<unsigned>(py - ey);
+            if (dx >= static_cast<unsigned>(P) || dy >= static_cast<unsigned>(P)) continue;
+            const int t = en.xyt >> 28;
+            const int pos = (t * P + static_cast<int>(dy)) * P + static_cast<int>(dx);
+            const float* f = L.filtered + static_cast<size_t>(en.r) * L.dim + pos;
+            if (L.coupled && !L.windowed) {
+                const bool fused = static_cast<int>(dx) < fused_cols;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    if (c >= C) break;
+                    const float x = __ldg(f + c * L.patch_dim);
+                    num[c] = fused ? __fmaf_rn(en.w, x, num[c]) : __fadd_rn(num[c], __fmul_rn(en.w, x));
                 }
+                wt = __fadd_rn(wt, en.w);
+            } else {
+                const float cw = __fmul_rn(en.w, window[dy * P + dx]);
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    if (c >= C) break;
+                    const float x = __ldg(f + c * L.patch_dim);
+                    num[c] = __fadd_rn(num[c], __fmul_rn(cw, x));
+                }
+                wt = __fadd_rn(wt, cw);
             }
         }
         const bool done = s_done != 0;
         __syncthreads();
         if (done) break;
     }
-    // ---- write the tile of this slot
-    const size_t plane = static_cast<size_t>(L.width) * L.height;
-    float* base = L.stack + static_cast<size_t>(slot) * (C + 1) * plane;
-    for (int p = 0; p < pix_per_thread && p < kMaxPix; ++p) {
-        const int local = tid + p * blockDim.x;
-        if (local >= T * T) break;
-        const int px = tx0 + local % T;
-        const int py = ty0 + local / T;
-        if (px >= L.width || py >= L.height) continue;
-        const size_t i = static_cast<size_t>(py) * L.width + px;
-        for (int c = 0; c < C; ++c) base[c * plane + i] = num[p][c];
-        base[C * plane + i] = wt[p];
+    // write this slot's tile: every pixel, so the stack needs no clearing
+    if (px < L.width && py < L.height) {
+        const size_t plane = static_cast<size_t>(L.width) * L.height;
+        float* base = L.stack + static_cast<size_t>(slot) * (C + 1) * plane + static_cast<size_t>(py) * L.width + px;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            if (c < C) base[c * plane] = num[c];
+        base[C * plane] = wt;
     }
 }
 
@@ -264,7 +215,7 @@ cudaError_t launch_aggregate_stacks(const AggregateLaunch& L, cudaStream_t strea
 }
 
 cudaError_t launch_tiles(const TileLaunch& L, cudaStream_t stream) {
-    if (L.tile * L.tile > kTileThreads * 4 || L.channels > 4) return cudaErrorInvalidValue;
+    if (L.channels > 4 || L.width >= (1 << 14) || L.height >= (1 << 14) || L.Pt > 7) return cudaErrorInvalidValue;
     const dim3 grid(L.tiles_x, L.tiles_y, L.slots);
     const size_t smem = static_cast<size_t>(L.P) * L.P * sizeof(float);
     tile_kernel<<<grid, kTileThreads, smem, stream>>>(L);

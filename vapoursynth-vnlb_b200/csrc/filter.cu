@@ -9,19 +9,26 @@
 // topk_symmetric_eigen_jacobi and map_dual_eigenvectors_to_basis
 // (src/linalg/linalg.cpp).
 //
-// One CTA (4 warps) per active group, groups taken from the device-side
-// active list in a grid-stride loop.  The B model rows are gathered and
-// centred into shared memory; the B x B Gram is built one pair per thread; the
-// cyclic Jacobi runs on warp 0 with one matrix row per lane; every retained
-// row is then streamed once per warp for its membership score and its
-// shrunken reconstruction.  All dot products use the pinned 8-lane order
-// (per-lane fused accumulators, then the fixed fold), elementwise updates the
-// CPU's fused/unfused split, and the elementary functions are correctly
-// rounded, so results are bit-identical to the CPU core -- with one stated
-// exception: the flat-area variance (double sums) is reduced in a fixed
-// parallel order, which can move its float value by one ulp; that changes
-// the flat decision only when the variance lies within one ulp of
-// gamma*sigma^2.
+// Three kernels, each shaped to its parallelism:
+//   prepare  one warp per group: equality and flat-area tests, the means of
+//            the first B rows, the centred model rows (shared memory) and the
+//            B x B dual Gram, one pair per lane;
+//   jacobi   the cyclic Jacobi of many groups per warp, one lane per matrix
+//            row (a latency-bound chain of dependent rotations, so throughput
+//            comes from the number of groups in flight);
+//   apply    one CTA per group: dual -> primal basis, Wiener coefficients,
+//            precision and volume, then every retained row streamed once per
+//            warp for its membership score and its shrunken reconstruction,
+//            and finally the aggregation weights.
+// Samples are addressed through a per-launch table of column offsets
+// (channel, t, py, px) -> video offset, so a gather is one add and one load.
+// All dot products use the pinned 8-lane order (per-lane fused accumulators,
+// then the fixed fold), elementwise updates the CPU's fused/unfused split, and
+// the elementary functions are correctly rounded, so results are
+// bit-identical to the CPU core -- with one stated exception: the flat-area
+// variance (double sums) is reduced in a fixed parallel order, which can move
+// its float value by one ulp; that changes the flat decision only when the
+// variance lies within one ulp of gamma*sigma^2.
 #include <cfloat>
 
 #include "vnlb_kernels.h"
@@ -29,8 +36,10 @@
 namespace vnlbgpu {
 namespace {
 
-constexpr int kThreads = 128;
-constexpr int kWarps = kThreads / 32;
+constexpr int kApplyThreads = 128;
+constexpr int kApplyWarps = kApplyThreads / 32;
+constexpr int kPrepareWarps = 4;
+constexpr float kEigenFloor = 128.0f * FLT_EPSILON;
 
 // dot_contiguous_highway, one thread.
 __device__ float thread_dot8(const float* l, const float* r, int count) {
@@ -58,6 +67,7 @@ __device__ float thread_dot8(const float* l, const float* r, int count) {
 
 // dot_contiguous_highway computed by an octet of lanes (j = lane & 7): lane j
 // owns accumulator j; the fold follows reduce8.  All 8 lanes return the dot.
+// Every lane of the warp must call it.
 __device__ __forceinline__ float octet_dot8(const float* l, const float* r, int count, int j) {
     float v = 0.0f;
     int index = 0;
@@ -85,11 +95,8 @@ __device__ __forceinline__ float add_scaled_elem(float out, float in, float scal
     return fused_column(col, count) ? __fmaf_rn(scale, in, out) : __fadd_rn(out, __fmul_rn(scale, in));
 }
 
-struct Layout {
-    int D, B, rank, S;
-};
-
-__device__ __forceinline__ float sample_at(const float* video, const FilterLaunch& L, const MatchRow& m, int col) {
+// Offset of column col = (channel, t, py, px) from a patch origin.
+__device__ __forceinline__ int column_offset(const FilterLaunch& L, int col) {
     const int pd = L.patch_dim;
     const int c = col / pd;
     const int pos = col - c * pd;
@@ -98,67 +105,70 @@ __device__ __forceinline__ float sample_at(const float* video, const FilterLaunc
     const int rem = pos - t * pp;
     const int py = rem / L.P;
     const int px = rem - py * L.P;
-    return __ldg(video + ((static_cast<size_t>(m.frame + t) * L.channels + c) * L.height + (m.y + py)) *
-                             static_cast<size_t>(L.width) + (m.x + px));
+    return ((t * L.channels + c) * L.height + py) * L.width + px;
 }
 
-__global__ void __launch_bounds__(kThreads) filter_kernel(FilterLaunch L) {
+__device__ __forceinline__ size_t row_base(const FilterLaunch& L, const MatchRow& m) {
+    return (static_cast<size_t>(m.frame) * L.channels * L.height + m.y) * static_cast<size_t>(L.width) + m.x;
+}
+
+__device__ __forceinline__ int bmax_of(const FilterLaunch& L) { return min(L.model_cap, L.max_rows); }
+
+// ---------------------------------------------------------------------------
+// prepare: one warp per group.
+__global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunch L) {
     extern __shared__ __align__(16) float sm[];
     const int D = L.dim;
-    const int Bmax = min(L.model_cap, L.max_rows);
-    const int R = L.rank;
-    // shared layout
-    float* Xm = sm;                               // Bmax * D   centred model rows
-    float* mean_n = Xm + Bmax * D;                // D
-    float* mean_b = mean_n + D;                   // D
-    float* basis = mean_b + D;                    // R * D
-    float* jm = basis + R * D;                    // Bmax^2
-    float* jv = jm + Bmax * Bmax;                 // Bmax^2
-    float* dual = jv + Bmax * Bmax;               // R * Bmax
-    float* eig = dual + R * Bmax;                 // R
-    float* coef = eig + R;                        // R
-    float* scores = coef + R;                     // max_rows
-    float* logw = scores + L.max_rows;            // max_rows
-    float* scratch = logw + L.max_rows;           // kWarps * 3 * D
-    int* order = reinterpret_cast<int*>(scratch + kWarps * 3 * D);  // Bmax
-    __shared__ float s_misc[8];
-    __shared__ double s_red[2 * kThreads];
-
-    const int tid = threadIdx.x;
-    const int warp = tid >> 5;
-    const int lane = tid & 31;
+    const int Bmax = bmax_of(L);
+    int* coloff = reinterpret_cast<int*>(sm);
+    size_t* bases_all = reinterpret_cast<size_t*>(sm + ((D + 3) & ~3));  // kPrepareWarps * max_rows
+    const int ldx = D + 1;  // padded row stride: lanes on different rows hit different banks
+    float* X = reinterpret_cast<float*>(bases_all + kPrepareWarps * L.max_rows) +
+               (threadIdx.x >> 5) * Bmax * ldx;  // this warp's model rows
+    size_t* bases = bases_all + (threadIdx.x >> 5) * L.max_rows;
+    for (int col = threadIdx.x; col < D; col += blockDim.x) coloff[col] = column_offset(L, col);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
     const StageConfig& P = L.cfg;
     const bool final_stage = L.stage == 1;
     const float* model_video = final_stage ? L.basic : L.noisy;
+    const bool weights_enabled = P.weight_alpha != 0.0f || P.weight_beta != 0.0f || P.weight_gamma != 0.0f;
     const int active_count = L.counters->active;
-
-    for (int a = blockIdx.x; a < active_count; a += gridDim.x) {
+    const int warps_total = gridDim.x * kPrepareWarps;
+    for (int a = blockIdx.x * kPrepareWarps + (threadIdx.x >> 5); a < active_count; a += warps_total) {
         const int g = L.active[a];
         const int S = L.row_counts[g];
         const MatchRow* rows = L.rows + static_cast<size_t>(g) * L.max_rows;
         const int r0 = L.row_offset[a];
         const int B = min(S, L.model_cap);
-        for (int i = tid; i < S; i += kThreads) {
-            L.row_info[r0 + i] = rows[i];
+        for (int i = lane; i < S; i += 32) {
+            const MatchRow m = rows[i];
+            L.row_info[r0 + i] = m;
             L.row_group[r0 + i] = a;
+            bases[i] = row_base(L, m);
         }
-        // ---- equal group (samples_are_equal / group_is_equal)
-        int differs = 0;
+        __syncwarp();
+        // equal group (samples_are_equal / group_is_equal): independent loads
+        bool differs = S <= 1;
         if (S > 1) {
-            for (int e = tid; e < (S - 1) * D; e += kThreads) {
-                const int i = 1 + e / D;
-                const int col = e - (i - 1) * D;
-                if (sample_at(L.noisy, L, rows[i], col) != sample_at(L.noisy, L, rows[0], col)) differs = 1;
+            for (int col = lane; col < D; col += 32) {
+                const float* src = L.noisy + coloff[col];
+                const float v0 = __ldg(src + bases[0]);
+                int i = 1;
+                for (; i + 4 <= S; i += 4) {
+                    const float x0 = __ldg(src + bases[i]), x1 = __ldg(src + bases[i + 1]);
+                    const float x2 = __ldg(src + bases[i + 2]), x3 = __ldg(src + bases[i + 3]);
+                    differs |= (x0 != v0) | (x1 != v0) | (x2 != v0) | (x3 != v0);
+                }
+                for (; i < S; ++i) differs |= __ldg(src + bases[i]) != v0;
             }
         }
-        const bool equal = S > 1 && !__syncthreads_or(differs);
-        const bool weights_enabled = P.weight_alpha != 0.0f || P.weight_beta != 0.0f || P.weight_gamma != 0.0f;
-        if (equal) {
+        if (!__any_sync(0xffffffffu, differs)) {
             // filtered = input, default aggregation model (core.cpp:253-274)
-            for (int e = tid; e < S * D; e += kThreads) {
-                const int i = e / D;
-                const int col = e - i * D;
-                L.filtered[static_cast<size_t>(r0 + i) * D + col] = sample_at(L.noisy, L, rows[i], col);
+            for (int i = 0; i < S; ++i) {
+                const size_t b = bases[i];
+                float* out = L.filtered + static_cast<size_t>(r0 + i) * D;
+                for (int col = lane; col < D; col += 32) out[col] = __ldg(L.noisy + b + coloff[col]);
             }
             const float tau = __fadd_rn(P.weight_epsilon, __fdiv_rn(static_cast<float>(D), static_cast<float>(B)));
             const float lgw = P.weight_alpha == 0.0f ? 0.0f : __fmul_rn(-P.weight_alpha, cr_logf(tau));
@@ -168,11 +178,11 @@ __global__ void __launch_bounds__(kThreads) filter_kernel(FilterLaunch L) {
                 lw = lw < -80.0f ? -80.0f : (80.0f < lw ? 80.0f : lw);
                 w = cr_expf(lw);
             }
-            for (int i = tid; i < S; i += kThreads) L.weights[r0 + i] = w;
-            __syncthreads();
+            for (int i = lane; i < S; i += 32) L.weights[r0 + i] = w;
+            if (lane == 0) L.flags[a] = kGroupDone;
             continue;
         }
-        // ---- flat area (Final): mean channel variance of the noisy rows
+        // flat area (Final): mean channel variance of the noisy rows
         bool flat = false;
         if (final_stage && P.flat_areas) {
             const int pd = L.patch_dim;
@@ -181,232 +191,375 @@ __global__ void __launch_bounds__(kThreads) filter_kernel(FilterLaunch L) {
             float variance = 0.0f;
             for (int c = 0; c < channels; ++c) {
                 double sum = 0.0, sum2 = 0.0;
-                for (int e = tid; e < per_channel; e += kThreads) {
-                    const int i = e / pd;
-                    const int q = e - i * pd;
-                    const float v = sample_at(L.noisy, L, rows[i], c * pd + q);
-                    sum += static_cast<double>(v);
-                    sum2 += static_cast<double>(v) * static_cast<double>(v);
-                }
-                s_red[tid] = sum;
-                s_red[kThreads + tid] = sum2;
-                __syncthreads();
-                for (int half = kThreads / 2; half > 0; half >>= 1) {
-                    if (tid < half) {
-                        s_red[tid] += s_red[tid + half];
-                        s_red[kThreads + tid] += s_red[kThreads + tid + half];
+                for (int i = 0; i < S; ++i) {
+                    const float* src = L.noisy + bases[i];
+                    for (int q = lane; q < pd; q += 32) {
+                        const float v = __ldg(src + coloff[c * pd + q]);
+                        sum += static_cast<double>(v);
+                        sum2 += static_cast<double>(v) * static_cast<double>(v);
                     }
-                    __syncthreads();
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+                    sum2 += __shfl_xor_sync(0xffffffffu, sum2, o);
                 }
                 if (per_channel > 1) {
                     const double count = static_cast<double>(per_channel);
-                    const double s1 = s_red[0], s2 = s_red[kThreads];
-                    variance = __fadd_rn(variance, static_cast<float>((s2 - (s1 * s1 / count)) / (count - 1.0)));
+                    variance = __fadd_rn(variance, static_cast<float>((sum2 - (sum * sum / count)) / (count - 1.0)));
                 }
-                __syncthreads();
             }
             if (per_channel > 1) variance = __fdiv_rn(variance, static_cast<float>(channels));
             flat = variance < __fmul_rn(__fmul_rn(P.sigma, P.sigma), P.gamma);
         }
-        if (B < min(D, R)) {
-            if (tid == 0) {
+        if (B < min(D, L.rank)) {
+            if (lane == 0) {
                 atomicCAS(&L.counters->status, 0, kStatusRankNotCovered);
                 L.counters->detail = g;
+                L.flags[a] = kGroupSkip;
             }
-            __syncthreads();
             continue;
         }
-        // ---- means over the first B rows (compute_mean) and centred model rows
-        const float inv_b = __fdiv_rn(1.0f, static_cast<float>(B));
-        for (int col = tid; col < D; col += kThreads) {
-            float mb = 0.0f, mn = 0.0f;
-            if (final_stage) {
-                for (int r = 0; r < B; ++r) mb = __fadd_rn(mb, sample_at(L.basic, L, rows[r], col));
-                mb = __fmul_rn(mb, inv_b);
-            }
-            if (!final_stage || !flat) {
-                for (int r = 0; r < B; ++r) mn = __fadd_rn(mn, sample_at(L.noisy, L, rows[r], col));
-                mn = __fmul_rn(mn, inv_b);
-            }
-            mean_b[col] = mb;
-            mean_n[col] = mn;
-            const float mm = final_stage ? mb : mn;
-            for (int r = 0; r < B; ++r) Xm[r * D + col] = __fsub_rn(sample_at(model_video, L, rows[r], col), mm);
+        // model rows, means over the first B rows (compute_mean), centring
+        for (int s = 0; s < B; ++s) {
+            const size_t b = bases[s];
+            for (int col = lane; col < D; col += 32) X[s * ldx + col] = __ldg(model_video + b + coloff[col]);
         }
-        __syncthreads();
-        const float* center_vec = (final_stage && flat) ? mean_b : mean_n;
-        const float* member_mean = final_stage ? mean_b : mean_n;
-
-        // ---- model noise constants (core.cpp:190-241, 616-636)
-        const float sigma2 = __fmul_rn(__fmul_rn(P.beta, P.sigma), P.sigma);
-        const float model_noise2 = final_stage ? __fmul_rn(__fmul_rn(P.beta, P.sigma_basic), P.sigma_basic) : sigma2;
-        const float match_sigma = final_stage ? P.sigma_basic : P.sigma;
-        const float mem2 = std_max(__fmul_rn(match_sigma, match_sigma),
-                                   __fmul_rn(__fmul_rn(P.membership_noise_floor, P.sigma), P.sigma));
-
-        if (R > 0) {
-            // ---- dual Gram (compute_gram_centered)
-            const float scale = __fdiv_rn(1.0f, static_cast<float>(B));
-            const int pairs = B * (B + 1) / 2;
-            for (int e = tid; e < pairs; e += kThreads) {
-                int r = static_cast<int>((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
-                while ((r + 1) * (r + 2) / 2 <= e) ++r;
-                while (r * (r + 1) / 2 > e) --r;
-                const int c = e - r * (r + 1) / 2;
-                const float v = __fmul_rn(scale, thread_dot8(Xm + r * D, Xm + c * D, D));
-                jm[r * B + c] = v;
-                jm[c * B + r] = v;
+        const float inv_b = __fdiv_rn(1.0f, static_cast<float>(B));
+        float* means = L.means + static_cast<size_t>(a) * 2 * D;
+        for (int col = lane; col < D; col += 32) {
+            float mm = 0.0f;
+            for (int s = 0; s < B; ++s) mm = __fadd_rn(mm, X[s * ldx + col]);
+            mm = __fmul_rn(mm, inv_b);
+            float center = mm;  // Basic: noisy mean; Final flat: basic mean
+            if (final_stage && !flat) {
+                float mn = 0.0f;
+                for (int s = 0; s < B; ++s) mn = __fadd_rn(mn, __ldg(L.noisy + bases[s] + coloff[col]));
+                center = __fmul_rn(mn, inv_b);
             }
-            for (int e = tid; e < B * B; e += kThreads) jv[e] = (e / B == e % B) ? 1.0f : 0.0f;
-            __syncthreads();
-            // ---- cyclic Jacobi (topk_symmetric_eigen_jacobi), warp 0
-            if (warp == 0) {
-                float mx = 0.0f;
-                for (int e = lane; e < B * B; e += 32) mx = std_max(mx, fabsf(jm[e]));
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-                const float threshold = std_max(0.0f, __fmul_rn(64.0f * FLT_EPSILON, std_max(1.0f, mx)));
-                if (B > 1) {
-                    for (int sweep = 0; sweep < 64; ++sweep) {
-                        float off = 0.0f;
-                        for (int e = lane; e < B * B; e += 32) {
-                            const int r = e / B, c = e - (e / B) * B;
-                            if (c > r) off = std_max(off, fabsf(jm[e]));
-                        }
-#pragma unroll
-                        for (int o = 16; o > 0; o >>= 1) off = fmaxf(off, __shfl_xor_sync(0xffffffffu, off, o));
-                        if (off <= threshold) break;
-                        for (int p = 0; p + 1 < B; ++p) {
-                            for (int q = p + 1; q < B; ++q) {
-                                const float apq = jm[p * B + q];
-                                if (!(fabsf(apq) > threshold)) continue;
-                                const float app = jm[p * B + p];
-                                const float aqq = jm[q * B + q];
-                                __syncwarp();
-                                if (apq == 0.0f) continue;
-                                const float tau = __fdiv_rn(__fsub_rn(aqq, app), __fmul_rn(2.0f, apq));
-                                const float tau_abs = fabsf(tau);
-                                const float t_abs = __fdiv_rn(
-                                    1.0f, __fadd_rn(tau_abs, __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(tau, tau)))));
-                                const float t = tau < 0.0f ? -t_abs : t_abs;
-                                const float c = __fdiv_rn(1.0f, __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(t, t))));
-                                const float s = __fmul_rn(t, c);
-                                const float cc = __fmul_rn(c, c), ss = __fmul_rn(s, s), cs = __fmul_rn(c, s);
-                                for (int r = lane; r < B; r += 32) {
-                                    if (r == p || r == q) continue;
-                                    const float arp = jm[r * B + p];
-                                    const float arq = jm[r * B + q];
-                                    const float nrp = __fsub_rn(__fmul_rn(c, arp), __fmul_rn(s, arq));
-                                    const float nrq = __fadd_rn(__fmul_rn(s, arp), __fmul_rn(c, arq));
-                                    jm[r * B + p] = nrp;
-                                    jm[p * B + r] = nrp;
-                                    jm[r * B + q] = nrq;
-                                    jm[q * B + r] = nrq;
-                                }
-                                for (int r = lane; r < B; r += 32) {
-                                    const float vrp = jv[r * B + p];
-                                    const float vrq = jv[r * B + q];
-                                    jv[r * B + p] = __fsub_rn(__fmul_rn(c, vrp), __fmul_rn(s, vrq));
-                                    jv[r * B + q] = __fadd_rn(__fmul_rn(s, vrp), __fmul_rn(c, vrq));
-                                }
-                                if (lane == 0) {
-                                    const float cs2 = __fmul_rn(2.0f, cs);
-                                    jm[p * B + p] = __fadd_rn(__fsub_rn(__fmul_rn(cc, app), __fmul_rn(cs2, apq)),
-                                                              __fmul_rn(ss, aqq));
-                                    jm[q * B + q] = __fadd_rn(__fadd_rn(__fmul_rn(ss, app), __fmul_rn(cs2, apq)),
-                                                              __fmul_rn(cc, aqq));
-                                    jm[p * B + q] = 0.0f;
-                                    jm[q * B + p] = 0.0f;
-                                }
-                                __syncwarp();
+            means[col] = mm;
+            means[D + col] = center;
+            for (int s = 0; s < B; ++s) X[s * ldx + col] = __fsub_rn(X[s * ldx + col], mm);
+        }
+        __syncwarp();
+        if (L.rank > 0) {
+            // dual Gram (compute_gram_centered), one pair per lane
+            const float scale = __fdiv_rn(1.0f, static_cast<float>(B));
+            float* gram = L.gram + static_cast<size_t>(a) * Bmax * Bmax;
+            const int pairs = B * (B + 1) / 2;
+            for (int e = lane; e < pairs; e += 32) {
+                int r = 0;
+                while ((r + 1) * (r + 2) / 2 <= e) ++r;
+                const int c = e - r * (r + 1) / 2;
+                const float v = __fmul_rn(scale, thread_dot8(X + r * ldx, X + c * ldx, D));
+                gram[r * B + c] = v;
+                gram[c * B + r] = v;
+            }
+        }
+        if (lane == 0) L.flags[a] = 0;
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// jacobi: topk_symmetric_eigen_jacobi (linalg.cpp:447-519) for many groups per
+// warp.  A group owns a segment of `seg` lanes (a power of two >= its rows,
+// at most 32); lane r of the segment owns matrix rows r, r + seg, ...
+__global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg) {
+    extern __shared__ __align__(16) float sm[];
+    const int Bmax = bmax_of(L);
+    const int R = L.rank;
+    const int lane = threadIdx.x & 31;
+    const int groups_per_warp = 32 / seg;
+    const int slot = (threadIdx.x >> 5) * groups_per_warp + lane / seg;  // group slot in the CTA
+    const int r0 = lane % seg;
+    const unsigned seg_mask = seg == 32 ? 0xffffffffu : (((1u << seg) - 1u) << ((lane / seg) * seg));
+    float* m = sm + static_cast<size_t>(slot) * (2 * Bmax * Bmax + Bmax);
+    float* v = m + Bmax * Bmax;
+    int* order = reinterpret_cast<int*>(v + Bmax * Bmax);
+    const int active_count = L.counters->active;
+    const int slots_per_cta = (blockDim.x >> 5) * groups_per_warp;
+    for (int base = blockIdx.x * slots_per_cta; base < active_count; base += gridDim.x * slots_per_cta) {
+        const int a = base + slot;
+        bool valid = a < active_count && R > 0;
+        int B = 0;
+        if (valid) {
+            valid = L.flags[a] == 0;
+            B = min(L.row_counts[L.active[a]], L.model_cap);
+        }
+        if (!valid) B = 0;
+        const float* gram = L.gram + static_cast<size_t>(max(a, 0)) * Bmax * Bmax;
+        float mx = 0.0f;
+        for (int r = r0; r < B; r += seg) {
+            for (int c = 0; c < B; ++c) {
+                const float x = gram[r * B + c];
+                m[r * Bmax + c] = x;
+                v[r * Bmax + c] = r == c ? 1.0f : 0.0f;
+                mx = std_max(mx, fabsf(x));
+            }
+        }
+        for (int o = seg / 2; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        const float threshold = std_max(0.0f, __fmul_rn(64.0f * FLT_EPSILON, std_max(1.0f, mx)));
+        __syncwarp();
+        if (__any_sync(0xffffffffu, B > 1)) {
+            for (int sweep = 0; sweep < 64; ++sweep) {
+                float off = 0.0f;
+                for (int r = r0; r < B; r += seg)
+                    for (int c = r + 1; c < B; ++c) off = std_max(off, fabsf(m[r * Bmax + c]));
+                for (int o = seg / 2; o > 0; o >>= 1) off = fmaxf(off, __shfl_xor_sync(0xffffffffu, off, o));
+                const bool busy = B > 1 && !(off <= threshold);
+                if (!__any_sync(0xffffffffu, busy)) break;
+                for (int p = 0; p + 1 < Bmax; ++p) {
+                    for (int q = p + 1; q < Bmax; ++q) {
+                        bool rot = false;
+                        float app = 0.0f, aqq = 0.0f, apq = 0.0f;
+                        if (busy && q < B) {
+                            apq = m[p * Bmax + q];
+                            rot = fabsf(apq) > threshold && apq != 0.0f;
+                            if (rot) {
+                                app = m[p * Bmax + p];
+                                aqq = m[q * Bmax + q];
                             }
                         }
-                    }
-                }
-                // stable sort of the diagonal, descending
-                for (int i = lane; i < B; i += 32) {
-                    const float di = jm[i * B + i];
-                    int pos = 0;
-                    for (int j = 0; j < B; ++j) {
-                        const float dj = jm[j * B + j];
-                        if (dj > di || (j < i && !(di > dj))) ++pos;
-                    }
-                    order[pos] = i;
-                }
-                __syncwarp();
-                // canonicalised top-rank dual vectors (canonicalize_vector_row)
-                for (int out = lane; out < R; out += 32) {
-                    const int src = order[out];
-                    eig[out] = jm[src * B + src];
-                    float* row = dual + out * Bmax;
-                    float norm2 = 0.0f, best = 0.0f;
-                    int pivot = 0;
-                    for (int r = 0; r < B; ++r) {
-                        const float v = jv[r * B + src];
-                        row[r] = v;
-                        norm2 = __fadd_rn(norm2, __fmul_rn(v, v));
-                        const float av = fabsf(v);
-                        if (av > best) {
-                            best = av;
-                            pivot = r;
+                        __syncwarp();
+                        if (rot) {
+                            // jacobi_rotate (linalg.cpp:152-196)
+                            const float tau = __fdiv_rn(__fsub_rn(aqq, app), __fmul_rn(2.0f, apq));
+                            const float tau_abs = fabsf(tau);
+                            const float t_abs =
+                                __fdiv_rn(1.0f, __fadd_rn(tau_abs, __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(tau, tau)))));
+                            const float t = tau < 0.0f ? -t_abs : t_abs;
+                            const float c = __fdiv_rn(1.0f, __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(t, t))));
+                            const float s = __fmul_rn(t, c);
+                            for (int r = r0; r < B; r += seg) {
+                                if (r != p && r != q) {
+                                    const float arp = m[r * Bmax + p];
+                                    const float arq = m[r * Bmax + q];
+                                    const float nrp = __fsub_rn(__fmul_rn(c, arp), __fmul_rn(s, arq));
+                                    const float nrq = __fadd_rn(__fmul_rn(s, arp), __fmul_rn(c, arq));
+                                    m[r * Bmax + p] = nrp;
+                                    m[p * Bmax + r] = nrp;
+                                    m[r * Bmax + q] = nrq;
+                                    m[q * Bmax + r] = nrq;
+                                }
+                                const float vrp = v[r * Bmax + p];
+                                const float vrq = v[r * Bmax + q];
+                                v[r * Bmax + p] = __fsub_rn(__fmul_rn(c, vrp), __fmul_rn(s, vrq));
+                                v[r * Bmax + q] = __fadd_rn(__fmul_rn(s, vrp), __fmul_rn(c, vrq));
+                                const float cc = __fmul_rn(c, c), ss = __fmul_rn(s, s);
+                                const float cs2 = __fmul_rn(2.0f, __fmul_rn(c, s));
+                                if (r == p) {
+                                    m[p * Bmax + p] = __fadd_rn(__fsub_rn(__fmul_rn(cc, app), __fmul_rn(cs2, apq)),
+                                                                __fmul_rn(ss, aqq));
+                                    m[p * Bmax + q] = 0.0f;
+                                } else if (r == q) {
+                                    m[q * Bmax + q] = __fadd_rn(__fadd_rn(__fmul_rn(ss, app), __fmul_rn(cs2, apq)),
+                                                                __fmul_rn(cc, aqq));
+                                    m[q * Bmax + p] = 0.0f;
+                                }
+                            }
                         }
-                    }
-                    if (!(norm2 <= FLT_MIN)) {
-                        float sc = __fdiv_rn(1.0f, __fsqrt_rn(norm2));
-                        if (row[pivot] < 0.0f) sc = -sc;
-                        for (int r = 0; r < B; ++r) row[r] = __fmul_rn(row[r], sc);
+                        __syncwarp();
                     }
                 }
             }
+        }
+        // stable sort of the diagonal (descending), canonicalised top-rank
+        // eigenvectors (canonicalize_vector_row, linalg.cpp:198-227)
+        for (int r = r0; r < B; r += seg) {
+            const float dr = m[r * Bmax + r];
+            int pos = 0;
+            for (int j = 0; j < B; ++j) {
+                const float dj = m[j * Bmax + j];
+                if (dj > dr || (j < r && !(dr > dj))) ++pos;
+            }
+            order[pos] = r;
+        }
+        __syncwarp();
+        if (valid) {
+            float* eig = L.eig + static_cast<size_t>(a) * R;
+            float* dual = L.dual + static_cast<size_t>(a) * R * Bmax;
+            for (int out = r0; out < R; out += seg) {
+                const int src = order[out];
+                eig[out] = m[src * Bmax + src];
+                float norm2 = 0.0f, best = 0.0f;
+                int pivot = 0;
+                for (int r = 0; r < B; ++r) {
+                    const float x = v[r * Bmax + src];
+                    norm2 = __fadd_rn(norm2, __fmul_rn(x, x));
+                    const float ax = fabsf(x);
+                    if (ax > best) {
+                        best = ax;
+                        pivot = r;
+                    }
+                }
+                float sc = 1.0f;
+                const bool scale = !(norm2 <= FLT_MIN);
+                if (scale) {
+                    sc = __fdiv_rn(1.0f, __fsqrt_rn(norm2));
+                    if (v[pivot * Bmax + src] < 0.0f) sc = -sc;
+                }
+                for (int r = 0; r < B; ++r) {
+                    const float x = v[r * Bmax + src];
+                    dual[out * Bmax + r] = scale ? __fmul_rn(x, sc) : x;
+                }
+            }
+        }
+        __syncwarp();
+        (void)seg_mask;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// apply: one CTA per group.  Shared layout (floats unless noted):
+//   coloff[D] (int), means[2D], X[B][ldx] centred model rows, basis[R][ldb],
+//   dual[R*Bmax], per-component scalars (5R), scores[max_rows],
+//   per-warp scratch (3 rows of ldb), row bases[max_rows] (size_t).
+// Row strides are padded (ldx = D + 1, ldb = D + 8) so that lanes reading
+// different rows at the same column hit different banks.
+struct ApplyLayout {
+    int D, Bmax, R, ldx, ldb, colpad;
+    size_t means, X, basis, dual, scal, scores, scratch, bases, bytes;
+};
+
+__host__ __device__ inline ApplyLayout apply_layout(int D, int Bmax, int R, int max_rows, int warps) {
+    ApplyLayout a{};
+    a.D = D;
+    a.Bmax = Bmax;
+    a.R = R;
+    a.ldx = D + 1;
+    a.ldb = D + 8;
+    a.colpad = (D + 3) & ~3;
+    size_t off = static_cast<size_t>(a.colpad);
+    a.means = off;   off += 2 * static_cast<size_t>(D);
+    a.X = off;       off += static_cast<size_t>(Bmax) * a.ldx;
+    a.basis = off;   off += static_cast<size_t>(R) * a.ldb;
+    a.dual = off;    off += static_cast<size_t>(R) * Bmax;
+    a.scal = off;    off += 5 * static_cast<size_t>(R);
+    a.scores = off;  off += static_cast<size_t>(max_rows);
+    a.scratch = off; off += static_cast<size_t>(warps) * 3 * a.ldb;
+    off = (off + 1) & ~static_cast<size_t>(1);
+    a.bases = off;   off += 2 * static_cast<size_t>(max_rows);
+    a.bytes = off * sizeof(float);
+    return a;
+}
+
+__global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
+    extern __shared__ __align__(16) float sm[];
+    const int D = L.dim;
+    const int Bmax = bmax_of(L);
+    const int R = L.rank;
+    const ApplyLayout lay = apply_layout(D, Bmax, R, L.max_rows, kApplyWarps);
+    const int ldx = lay.ldx, ldb = lay.ldb;
+    int* coloff = reinterpret_cast<int*>(sm);
+    float* means = sm + lay.means;  // membership mean, reconstruction centre
+    float* X = sm + lay.X;
+    float* basis = sm + lay.basis;
+    float* dual = sm + lay.dual;
+    float* eig = sm + lay.scal;     // eigenvalues
+    float* coef = eig + R;          // Wiener coefficients
+    float* denom = coef + R;        // signal eigenvalue + membership noise
+    float* inv_sqrt = denom + R;    // 1 / sqrt(eigenvalue)
+    float* terms = inv_sqrt + R;    // log1p(signal / membership noise)
+    float* scores = sm + lay.scores;
+    float* scratch = sm + lay.scratch;
+    size_t* bases = reinterpret_cast<size_t*>(sm + lay.bases);
+    __shared__ float s_misc[4];
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    for (int col = tid; col < D; col += kApplyThreads) coloff[col] = column_offset(L, col);
+    const StageConfig& P = L.cfg;
+    const bool final_stage = L.stage == 1;
+    const float* model_video = final_stage ? L.basic : L.noisy;
+    const bool weights_enabled = P.weight_alpha != 0.0f || P.weight_beta != 0.0f || P.weight_gamma != 0.0f;
+    const float sigma2 = __fmul_rn(__fmul_rn(P.beta, P.sigma), P.sigma);
+    const float model_noise2 = final_stage ? __fmul_rn(__fmul_rn(P.beta, P.sigma_basic), P.sigma_basic) : sigma2;
+    const float match_sigma = final_stage ? P.sigma_basic : P.sigma;
+    const float mem2 = std_max(__fmul_rn(match_sigma, match_sigma),
+                               __fmul_rn(__fmul_rn(P.membership_noise_floor, P.sigma), P.sigma));
+    const bool membership_on = P.weight_beta != 0.0f;
+    const int active_count = L.counters->active;
+    __syncthreads();
+    for (int a = blockIdx.x; a < active_count; a += gridDim.x) {
+        if (L.flags[a] != 0) continue;  // uniform: equal groups are done, skipped ones reported
+        const int g = L.active[a];
+        const int S = L.row_counts[g];
+        const MatchRow* rows = L.rows + static_cast<size_t>(g) * L.max_rows;
+        const int r0 = L.row_offset[a];
+        const int B = min(S, L.model_cap);
+        const float* gm = L.means + static_cast<size_t>(a) * 2 * D;
+        for (int i = tid; i < 2 * D; i += kApplyThreads) means[i] = gm[i];
+        for (int i = tid; i < R * Bmax; i += kApplyThreads) dual[i] = L.dual[static_cast<size_t>(a) * R * Bmax + i];
+        for (int i = tid; i < S; i += kApplyThreads) bases[i] = row_base(L, rows[i]);
+        // per-component scalars, computed once per group (same operations as
+        // the CPU, which recomputes them where it uses them)
+        for (int c = tid; c < R; c += kApplyThreads) {
+            const float lambda = L.eig[static_cast<size_t>(a) * R + c];
+            eig[c] = lambda;
+            const float diff = __fsub_rn(lambda, model_noise2);
+            const float signal = diff > 0.0f ? diff : 0.0f;
+            denom[c] = __fadd_rn(signal, mem2);
+            inv_sqrt[c] = lambda > kEigenFloor ? __fdiv_rn(1.0f, __fsqrt_rn(lambda)) : 0.0f;
+            terms[c] = (membership_on && signal > 0.0f) ? cr_log1pf(__fdiv_rn(signal, mem2)) : 0.0f;
+            const float sigma_basic2 = final_stage ? model_noise2 : sigma2;
+            const float threshold = __fmul_rn(P.variance_threshold, sigma2);
+            float variance = lambda;
+            if (sigma_basic2 > 0.0f) variance = __fsub_rn(variance, std_min(variance, sigma_basic2));
+            coef[c] = variance > threshold ? __fdiv_rn(1.0f, __fadd_rn(1.0f, __fdiv_rn(sigma2, variance))) : 0.0f;
+        }
+        __syncthreads();
+        const float* member_mean = means;
+        const float* center_vec = means + D;
+        if (R > 0) {
+            // centred model rows (compute_mean + center_rows of the first B rows)
+            for (int e = tid; e < B * D; e += kApplyThreads) {
+                const int s = e / D;
+                const int col = e - s * D;
+                X[s * ldx + col] = __fsub_rn(__ldg(model_video + bases[s] + coloff[col]), member_mean[col]);
+            }
             __syncthreads();
-            // ---- dual -> primal basis (map_dual_eigenvectors_to_basis)
-            const float floor_value = 128.0f * FLT_EPSILON;
-            for (int e = tid; e < R * D; e += kThreads) {
+            // dual -> primal basis (map_dual_eigenvectors_to_basis): one output
+            // per thread, the samples accumulated in order
+            for (int e = tid; e < R * D; e += kApplyThreads) {
                 const int b = e / D;
                 const int col = e - b * D;
                 float acc = 0.0f;
-                const float lambda = eig[b];
-                if (lambda > floor_value) {
-                    for (int s = 0; s < B; ++s) acc = add_scaled_elem(acc, Xm[s * D + col], dual[b * Bmax + s], col, D);
-                    acc = __fmul_rn(acc, __fdiv_rn(1.0f, __fsqrt_rn(lambda)));
+                if (eig[b] > kEigenFloor) {
+                    const bool fused = fused_column(col, D);
+                    for (int s = 0; s < B; ++s) {
+                        const float x = X[s * ldx + col];
+                        const float w = dual[b * Bmax + s];
+                        acc = fused ? __fmaf_rn(w, x, acc) : __fadd_rn(acc, __fmul_rn(w, x));
+                    }
+                    acc = __fmul_rn(acc, inv_sqrt[b]);
                 }
-                basis[e] = acc;
+                basis[b * ldb + col] = acc;
             }
             __syncthreads();
-            for (int b = warp; b < R; b += kWarps) {
-                if (!(eig[b] > floor_value)) continue;
-                float* row = basis + b * D;
+            for (int b = warp; b < R; b += kApplyWarps) {
+                if (!(eig[b] > kEigenFloor)) continue;
+                float* row = basis + b * ldb;
                 const float norm2 = octet_dot8(row, row, D, lane & 7);
                 __syncwarp();
-                if (norm2 <= floor_value) {
+                if (norm2 <= kEigenFloor) {
                     for (int col = lane; col < D; col += 32) row[col] = 0.0f;
                 } else {
                     const float sc = __fdiv_rn(1.0f, __fsqrt_rn(norm2));
                     for (int col = lane; col < D; col += 32) row[col] = __fmul_rn(row[col], sc);
                 }
             }
-            // ---- Wiener coefficients (compute_filter_coefficients)
-            if (tid < R) {
-                const float sigma_basic2 = final_stage ? model_noise2 : sigma2;
-                const float threshold = __fmul_rn(P.variance_threshold, sigma2);
-                float variance = eig[tid];
-                if (sigma_basic2 > 0.0f) variance = __fsub_rn(variance, std_min(variance, sigma_basic2));
-                coef[tid] = variance > threshold
-                                ? __fdiv_rn(1.0f, __fadd_rn(1.0f, __fdiv_rn(sigma2, variance)))
-                                : 0.0f;
-            }
-            __syncthreads();
         }
-        // ---- group precision and volume (group_precision_tau, core.cpp:222-241, 346-358)
+        // group precision and volume (group_precision_tau, core.cpp:222-241,
+        // 346-358): the terms are ready, the sums run in component order
         if (tid == 0) {
-            const float estimate_noise2 = sigma2;
             float trace = 0.0f, volume = 0.0f;
             for (int c = 0; c < R; ++c) {
                 const float diff = __fsub_rn(eig[c], model_noise2);
                 const float lambda = diff > 0.0f ? diff : 0.0f;
                 if (lambda > 0.0f) {
-                    trace = __fadd_rn(trace, __fdiv_rn(lambda, __fadd_rn(lambda, estimate_noise2)));
-                    volume = __fadd_rn(volume, cr_log1pf(__fdiv_rn(lambda, mem2)));
+                    trace = __fadd_rn(trace, __fdiv_rn(lambda, __fadd_rn(lambda, sigma2)));
+                    volume = __fadd_rn(volume, terms[c]);
                 }
             }
             const float tau = __fadd_rn(
@@ -417,71 +570,69 @@ __global__ void __launch_bounds__(kThreads) filter_kernel(FilterLaunch L) {
         __syncthreads();
         const float lgw = s_misc[0];
         const float volume = s_misc[1];
-        const bool membership_on = P.weight_beta != 0.0f && !(P.weight_alpha == 0.0f && P.weight_beta == 0.0f);
-        // ---- per row: membership score and reconstruction
-        float* u = scratch + warp * 3 * D;  // centred membership row
-        float* v = u + D;                   // centred noisy row
-        float* o = v + D;                   // reconstruction accumulator
+        // per row: membership score and reconstruction.  In the Basic stage the
+        // membership row and the reconstruction row are the same centred noisy
+        // row, so its projections serve both.
+        float* u = scratch + warp * 3 * ldb;  // centred membership row
+        float* v = u + ldb;                   // centred noisy row (Final)
+        float* o = v + ldb;                   // reconstruction accumulator
         const int j8 = lane & 7;
         const int oct = lane >> 3;
-        for (int i = warp; i < S; i += kWarps) {
-            const MatchRow m = rows[i];
+        const float score_scale = __fsqrt_rn(__fmul_rn(2.0f, static_cast<float>(D)));
+        for (int i = warp; i < S; i += kApplyWarps) {
+            const size_t b = bases[i];
             for (int col = lane; col < D; col += 32) {
-                const float xn = sample_at(L.noisy, L, m, col);
-                const float xu = final_stage ? sample_at(L.basic, L, m, col) : xn;
-                u[col] = __fsub_rn(xu, member_mean[col]);
-                v[col] = __fsub_rn(xn, center_vec[col]);
+                const float xn = __ldg(L.noisy + b + coloff[col]);
+                if (final_stage) {
+                    u[col] = __fsub_rn(__ldg(L.basic + b + coloff[col]), member_mean[col]);
+                    v[col] = __fsub_rn(xn, center_vec[col]);
+                } else {
+                    u[col] = __fsub_rn(xn, member_mean[col]);
+                }
                 o[col] = 0.0f;
             }
             __syncwarp();
-            if (membership_on) {
-                // norm2 and the rank projections of the membership row, four
-                // dots per pass (one per octet), consumed in component order
-                float distance = 0.0f, projected = 0.0f, norm2 = 0.0f;
-                for (int c0 = -1; c0 < R; c0 += 4) {
-                    const int c = min(c0 + oct, R - 1);
-                    const float d = octet_dot8(u, c < 0 ? u : basis + c * D, D, j8);
-                    for (int k = 0; k < 4; ++k) {
-                        const int ck = c0 + k;
-                        const float dk = __shfl_sync(0xffffffffu, d, k * 8);
-                        if (ck >= R) break;
-                        if (ck < 0) {
-                            norm2 = dk;
-                        } else {
-                            const float proj2 = __fmul_rn(dk, dk);
-                            const float diff = __fsub_rn(eig[ck], model_noise2);
-                            const float lambda = diff > 0.0f ? diff : 0.0f;
-                            distance = __fadd_rn(distance, __fdiv_rn(proj2, __fadd_rn(lambda, mem2)));
-                            projected = __fadd_rn(projected, proj2);
-                        }
-                    }
-                }
-                const float res = __fsub_rn(norm2, projected);
-                distance = __fadd_rn(distance, __fdiv_rn(res > 0.0f ? res : 0.0f, mem2));
-                const float score = __fdiv_rn(__fsub_rn(distance, static_cast<float>(D)),
-                                              __fsqrt_rn(__fmul_rn(2.0f, static_cast<float>(D))));
-                if (lane == 0) scores[i] = score;
-            }
-            // reconstruction (project_bayes_estimate): components in order
-            for (int c0 = 0; c0 < R; c0 += 4) {
+            float distance = 0.0f, projected = 0.0f, norm2 = 0.0f;
+            // pass over c0 = -1 (norm), 0, 4, ...: octet k computes component c0 + k
+            for (int c0 = membership_on ? -1 : 0; c0 < R; c0 += 4) {
                 const int c = min(c0 + oct, R - 1);
-                const float d = octet_dot8(v, basis + c * D, D, j8);
+                const float dm = (membership_on || !final_stage) ? octet_dot8(u, c < 0 ? u : basis + c * ldb, D, j8)
+                                                                 : 0.0f;
+                const float dr = final_stage ? octet_dot8(v, basis + max(c, 0) * ldb, D, j8) : dm;
                 for (int k = 0; k < 4; ++k) {
                     const int ck = c0 + k;
-                    const float dk = __shfl_sync(0xffffffffu, d, k * 8);
+                    const float mk = __shfl_sync(0xffffffffu, dm, k * 8);
+                    const float rk = __shfl_sync(0xffffffffu, dr, k * 8);
                     if (ck >= R) break;
-                    if (coef[ck] == 0.0f) continue;
-                    const float scaled = __fmul_rn(coef[ck], dk);
-                    const float* bc = basis + ck * D;
-                    for (int col = lane; col < D; col += 32) o[col] = add_scaled_elem(o[col], bc[col], scaled, col, D);
+                    if (ck < 0) {
+                        norm2 = mk;
+                        continue;
+                    }
+                    if (membership_on) {
+                        const float proj2 = __fmul_rn(mk, mk);
+                        distance = __fadd_rn(distance, __fdiv_rn(proj2, denom[ck]));
+                        projected = __fadd_rn(projected, proj2);
+                    }
+                    if (coef[ck] != 0.0f) {
+                        const float scaled = __fmul_rn(coef[ck], rk);
+                        const float* bc = basis + ck * ldb;
+                        for (int col = lane; col < D; col += 32)
+                            o[col] = add_scaled_elem(o[col], bc[col], scaled, col, D);
+                    }
                 }
+            }
+            if (membership_on) {
+                const float res = __fsub_rn(norm2, projected);
+                distance = __fadd_rn(distance, __fdiv_rn(res > 0.0f ? res : 0.0f, mem2));
+                const float score = __fdiv_rn(__fsub_rn(distance, static_cast<float>(D)), score_scale);
+                if (lane == 0) scores[i] = score;
             }
             float* out = L.filtered + static_cast<size_t>(r0 + i) * D;
             for (int col = lane; col < D; col += 32) out[col] = __fadd_rn(o[col], center_vec[col]);
             __syncwarp();
         }
         __syncthreads();
-        // ---- aggregation weights (accumulate_aggregation_model + finalize)
+        // aggregation weights (accumulate_aggregation_model + finalize)
         if (tid == 0) {
             float mn = kInf;
             if (membership_on)
@@ -490,7 +641,7 @@ __global__ void __launch_bounds__(kThreads) filter_kernel(FilterLaunch L) {
         }
         __syncthreads();
         const float min_score = s_misc[2];
-        for (int i = tid; i < S; i += kThreads) {
+        for (int i = tid; i < S; i += kApplyThreads) {
             float w = 1.0f;
             if (weights_enabled) {
                 float lw;
@@ -514,22 +665,52 @@ __global__ void __launch_bounds__(kThreads) filter_kernel(FilterLaunch L) {
 
 }  // namespace
 
-size_t filter_shared_bytes(const FilterLaunch& L) {
-    const size_t D = L.dim;
-    const size_t Bmax = std::min(L.model_cap, L.max_rows);
-    const size_t R = L.rank;
-    const size_t floats = Bmax * D + 2 * D + R * D + 2 * Bmax * Bmax + R * Bmax + 2 * R + 2 * L.max_rows +
-                          kWarps * 3 * D + Bmax;
-    return floats * sizeof(float);
-}
-
-cudaError_t launch_filter(const FilterLaunch& L, int ctas, cudaStream_t stream) {
-    const size_t smem = filter_shared_bytes(L);
-    cudaError_t err = cudaFuncSetAttribute(filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast<int>(smem));
-    if (err != cudaSuccess) return err;
-    filter_kernel<<<ctas, kThreads, smem, stream>>>(L);
-    return cudaGetLastError();
+cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t stream) {
+    if (max_groups <= 0) return cudaSuccess;
+    const int D = L.dim;
+    const int Bmax = std::min(L.model_cap, L.max_rows);
+    const int R = L.rank;
+    const size_t colpad = static_cast<size_t>((D + 3) & ~3);
+    // prepare
+    {
+        const size_t smem = (colpad + static_cast<size_t>(kPrepareWarps) * Bmax * (D + 1)) * sizeof(float) +
+                            static_cast<size_t>(kPrepareWarps) * L.max_rows * sizeof(size_t);
+        cudaError_t err = cudaFuncSetAttribute(prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(smem));
+        if (err != cudaSuccess) return err;
+        const int ctas = std::min((max_groups + kPrepareWarps - 1) / kPrepareWarps, 148 * 16);
+        prepare_kernel<<<ctas, 32 * kPrepareWarps, smem, stream>>>(L);
+        if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    }
+    // jacobi
+    if (R > 0) {
+        int seg = 1;
+        while (seg < Bmax && seg < 32) seg <<= 1;
+        seg = std::max(seg, 1);
+        const size_t per_group = static_cast<size_t>(2 * Bmax * Bmax + Bmax) * sizeof(float);
+        int warps = 8;
+        while (warps > 1 && static_cast<size_t>(warps) * (32 / seg) * per_group > 160 * 1024) warps /= 2;
+        const size_t smem = static_cast<size_t>(warps) * (32 / seg) * per_group;
+        cudaError_t err = cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(smem));
+        if (err != cudaSuccess) return err;
+        const int per_cta = warps * (32 / seg);
+        const int ctas = std::max(1, std::min((max_groups + per_cta - 1) / per_cta, 148 * 32));
+        jacobi_kernel<<<ctas, 32 * warps, smem, stream>>>(L, seg);
+        if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    }
+    // apply
+    {
+        const ApplyLayout lay = apply_layout(D, Bmax, R, L.max_rows, kApplyWarps);
+        const size_t smem = lay.bytes;
+        cudaError_t err = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(smem));
+        if (err != cudaSuccess) return err;
+        const int ctas = std::min(max_groups, 148 * 12);
+        apply_kernel<<<ctas, kApplyThreads, smem, stream>>>(L);
+        if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace vnlbgpu

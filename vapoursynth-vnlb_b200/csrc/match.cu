@@ -222,6 +222,10 @@ __global__ void __launch_bounds__(256) match_kernel(MatchLaunch L) {
 #pragma unroll
     for (int i = 0; i < kMaxTopPerLane; ++i) my_top[i] = -kInf;
     const int K = L.K;
+    // register-resident buffer and heap when both fit in a warp
+    const bool fast = s.cap <= 32 && K <= 32;
+    unsigned reg_d = 0u, reg_top = 0u;  // bits of non-negative distances (0 = empty)
+    int reg_id = 0;
 
     for (int k = 0; k < L.schedule_len; ++k) {
         const int frame = L.schedule[k];
@@ -269,6 +273,61 @@ __global__ void __launch_bounds__(256) match_kernel(MatchLaunch L) {
             }
         }
         __syncwarp();
+        // Replay of the CPU's sequential selection over frame k, raster order.
+        if (fast) {
+            // buffer slot i and heap entry i live in lane i; non-negative float
+            // distances order like their bit patterns, so the first maximum
+            // (std::max_element) is a max-reduction and a ballot
+            for (int base = 0; base < cells; base += 32) {
+                const int idx = base + lane;
+                const float mine = idx < cells ? dist[idx] : kInf;
+                float limit = s.top_count >= K ? std_max(L.tau, s.top_front) : kInf;
+                if (s.count >= s.cap) limit = std_min(limit, s.worst);
+                unsigned pass = __ballot_sync(0xffffffffu, idx < cells && mine <= limit);
+                while (pass) {
+                    const int src_lane = __ffs(pass) - 1;
+                    pass &= pass - 1;
+                    const float d = __shfl_sync(0xffffffffu, mine, src_lane);
+                    limit = s.top_count >= K ? std_max(L.tau, s.top_front) : kInf;
+                    if (s.count >= s.cap) limit = std_min(limit, s.worst);
+                    if (!(d <= limit)) continue;
+                    const int id = (k << 20) | (base + src_lane);
+                    // record_candidate_match
+                    if (s.count < s.cap) {
+                        if (lane == s.count) {
+                            reg_d = __float_as_uint(d);
+                            reg_id = id;
+                        }
+                        s.count++;
+                        if (s.count == s.cap) {
+                            const unsigned w = __reduce_max_sync(0xffffffffu, reg_d);
+                            s.worst_idx = __ffs(__ballot_sync(0xffffffffu, reg_d == w)) - 1;
+                            s.worst = __uint_as_float(w);
+                        }
+                    } else if (d < s.worst) {
+                        if (lane == s.worst_idx) {
+                            reg_d = __float_as_uint(d);
+                            reg_id = id;
+                        }
+                        const unsigned w = __reduce_max_sync(0xffffffffu, reg_d);
+                        s.worst_idx = __ffs(__ballot_sync(0xffffffffu, reg_d == w)) - 1;
+                        s.worst = __uint_as_float(w);
+                    }
+                    // record_candidate_distance: the K smallest so far
+                    if (s.top_count < K) {
+                        if (lane == s.top_count) reg_top = __float_as_uint(d);
+                        s.top_count++;
+                        if (s.top_count == K) s.top_front = __uint_as_float(__reduce_max_sync(0xffffffffu, reg_top));
+                    } else if (d < s.top_front) {
+                        const unsigned f = __float_as_uint(s.top_front);
+                        const int owner = __ffs(__ballot_sync(0xffffffffu, lane < K && reg_top == f)) - 1;
+                        if (lane == owner) reg_top = __float_as_uint(d);
+                        s.top_front = __uint_as_float(__reduce_max_sync(0xffffffffu, reg_top));
+                    }
+                }
+            }
+            continue;
+        }
         // Replay of the CPU's sequential selection over frame k, raster order.
         for (int base = 0; base < cells; base += 32) {
             const int idx = base + lane;
@@ -335,6 +394,13 @@ __global__ void __launch_bounds__(256) match_kernel(MatchLaunch L) {
         __syncwarp();
     }
     if (!active_warp) return;
+    if (fast) {
+        if (lane < s.count) {
+            buf_d[lane] = __uint_as_float(reg_d);
+            buf_i[lane] = reg_id;
+        }
+        __syncwarp();
+    }
 
     // select_similar_patches (core.cpp:1200-1243): single lane.
     int S = 0;

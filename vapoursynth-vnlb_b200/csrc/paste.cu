@@ -21,25 +21,35 @@ namespace {
 
 constexpr int kPrefetch = 8;
 
-struct VictimCache {
-    int n;
-    int v[kPrefetch];
+// Everything the walk needs about one grid anchor, loaded a batch ahead.
+struct AnchorInfo {
+    int n;             // victims
+    int v[kPrefetch];  // the first victims
+    int rows;          // retained rows
+    int2 xy;
 };
 
-__device__ __forceinline__ VictimCache fetch(const PasteLaunch& L, int j) {
-    VictimCache c;
+__device__ __forceinline__ AnchorInfo fetch(const PasteLaunch& L, int j) {
+    AnchorInfo c;
     c.n = 0;
+    c.rows = 0;
+    c.xy = make_int2(0, 0);
     if (j < L.groups) {
-        c.n = L.victim_counts[j];
+        c.n = __ldg(L.victim_counts + j);
+        c.rows = __ldg(L.row_counts + j);
+        c.xy = __ldg(L.anchors + j);
+        // the first entries are loaded unconditionally (in bounds: every anchor
+        // owns victim_stride >= kPrefetch slots), so no load waits on the count
         const int* v = L.victims + static_cast<size_t>(j) * L.victim_stride;
 #pragma unroll
-        for (int e = 0; e < kPrefetch; ++e) c.v[e] = e < c.n ? __ldg(v + e) : -1;
+        for (int e = 0; e < kPrefetch; ++e) c.v[e] = __ldg(v + e);
     }
     return c;
 }
 
 __global__ void __launch_bounds__(32) paste_kernel(PasteLaunch L) {
     extern __shared__ unsigned alive[];
+    __shared__ unsigned masks[32];
     const int lane = threadIdx.x;
     const int words = (L.groups + 31) / 32;
     for (int w = lane; w < words; w += 32) {
@@ -49,27 +59,38 @@ __global__ void __launch_bounds__(32) paste_kernel(PasteLaunch L) {
     __syncwarp();
     int running_active = 0;
     int running_rows = 0;
-    VictimCache next = fetch(L, lane);
+    // two batches in flight ahead of the one being resolved
+    AnchorInfo next = fetch(L, lane);
+    AnchorInfo after = fetch(L, lane + 32);
     for (int b = 0; b < words; ++b) {
-        const VictimCache cur = next;
+        const AnchorInfo cur = next;
+        next = after;
         const int j = b * 32 + lane;
         const int batch_end = (b + 1) * 32;
-        next = fetch(L, j + 32);
+        after = fetch(L, j + 64);
+        const int* vlist = L.victims + static_cast<size_t>(j) * L.victim_stride;
         // in-batch victims of this lane's anchor
         unsigned mine = 0;
-        const int* vlist = L.victims + static_cast<size_t>(j) * L.victim_stride;
+        bool later = false;
         for (int e = 0; e < cur.n; ++e) {
             const int v = e < kPrefetch ? cur.v[e] : __ldg(vlist + e);
             if (v < batch_end) mine |= 1u << (v - b * 32);
+            else later = true;
         }
         unsigned bits = alive[b];
+        if (__any_sync(0xffffffffu, mine != 0)) {
+            masks[lane] = mine;
+            __syncwarp();
+            unsigned mk[32];
 #pragma unroll
-        for (int k = 0; k < 32; ++k) {
-            const unsigned mk = __shfl_sync(0xffffffffu, mine, k);
-            if ((bits >> k) & 1u) bits &= ~mk;
+            for (int k = 0; k < 32; ++k) mk[k] = masks[k];
+#pragma unroll
+            for (int k = 0; k < 32; ++k)
+                if ((bits >> k) & 1u) bits &= ~mk[k];
+            __syncwarp();
         }
         const bool me = j < L.groups && ((bits >> lane) & 1u);
-        if (me) {
+        if (me && later) {
             for (int e = 0; e < cur.n; ++e) {
                 const int v = e < kPrefetch ? cur.v[e] : __ldg(vlist + e);
                 if (v >= batch_end) atomicAnd(&alive[v >> 5], ~(1u << (v & 31)));
@@ -78,17 +99,18 @@ __global__ void __launch_bounds__(32) paste_kernel(PasteLaunch L) {
         // ordered compaction
         const unsigned ballot = __ballot_sync(0xffffffffu, me);
         const int rank = __popc(ballot & ((1u << lane) - 1u));
-        const int s = me ? L.row_counts[j] : 0;
+        const int s = me ? cur.rows : 0;
         int prefix = s;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int v = __shfl_up_sync(0xffffffffu, prefix, o);
             if (lane >= o) prefix += v;
         }
+        if (j < L.groups) L.active_prefix[j] = running_active + rank;
         if (me) {
             const int a = running_active + rank;
             L.active[a] = j;
-            L.active_xy[a] = L.anchors[j];
+            L.active_xy[a] = cur.xy;
             L.row_offset[a] = running_rows + prefix - s;
         }
         running_active += __popc(ballot);
@@ -97,6 +119,7 @@ __global__ void __launch_bounds__(32) paste_kernel(PasteLaunch L) {
     }
     if (lane == 0) {
         L.row_offset[running_active] = running_rows;
+        L.active_prefix[L.groups] = running_active;
         L.counters->active = running_active;
         L.counters->rows = running_rows;
         atomicAdd(L.totals, static_cast<unsigned long long>(running_active));

@@ -96,6 +96,9 @@ struct Grid {
     DeviceArray<int2> d_anchors;
     DeviceArray<Strip> d_strips;
     DeviceArray<int> d_map;  // [H][W] anchor index or -1
+    // stack-tile reach tables (TileLaunch)
+    DeviceArray<int2> d_tile_grid_rows;  // [tiles_y]
+    DeviceArray<int2> d_tile_anchors;    // [grid rows][tiles_x]
 };
 
 }  // namespace
@@ -170,11 +173,13 @@ struct Session {
     bool clip_ready = false, ref_ready = false;
 
     DeviceArray<MatchRow> d_rows, d_row_info;
-    DeviceArray<int> d_row_counts, d_victims, d_victim_counts, d_active, d_row_offset, d_row_group;
+    DeviceArray<int> d_row_counts, d_victims, d_victim_counts, d_active, d_row_offset, d_row_group, d_active_prefix;
     DeviceArray<int2> d_active_xy;
     DeviceArray<FrameCounters> d_counters;
     DeviceArray<unsigned long long> d_totals;
     DeviceArray<float> d_filtered, d_weights, d_window, d_out_frame, d_pack;
+    DeviceArray<float> d_gmeans, d_gram, d_eig, d_dual;
+    DeviceArray<int> d_gflags;
     std::map<int, std::unique_ptr<Grid>> grids;
     int last_grid_key = INT_MIN;
 
@@ -297,7 +302,7 @@ struct Session {
 
         // largest grid over the anchor phases
         for (int key = 0; key < step; ++key) max_groups = std::max(max_groups, static_cast<int>(build_anchor_list(key).size()));
-        victim_stride = max_rows * 5;
+        victim_stride = std::max(8, max_rows * 5);
         // match region geometry
         const int KY = 4;
         region_rows = std::min(p.search_window, height - P + 1) + P - 1 + KY - 1;
@@ -305,7 +310,10 @@ struct Session {
         const int ch0 = std::min(p.search_window, height - P + 1);
         for (warps = 8; warps >= 1; warps /= 2) {
             region_w_max = ((warps - 1) * step + cw0 + P - 1 + 3 + 3) & ~3;
-            region_stride = region_w_max + 1;
+            // stride = 4 (mod 8): the 4 candidate rows of one lane task start 16
+            // banks apart, which keeps neighbouring lane tasks off each other's banks
+            region_stride = region_w_max;
+            while (region_stride % 8 != 4) ++region_stride;
             MatchLaunch probe{};
             probe.search_channels = search_channels;
             probe.Pt = Pt;
@@ -324,6 +332,7 @@ struct Session {
         d_active.allocate(G, "cudaMalloc(active groups)");
         d_active_xy.allocate(G, "cudaMalloc(active positions)");
         d_row_offset.allocate(G + 1, "cudaMalloc(row offsets)");
+        d_active_prefix.allocate(G + 1, "cudaMalloc(active prefix)");
         d_counters.allocate(1, "cudaMalloc(counters)");
         d_totals.allocate(2, "cudaMalloc(totals)");
         check(cudaMemset(d_totals.ptr, 0, 2 * sizeof(unsigned long long)), "cudaMemset(totals)");
@@ -334,6 +343,12 @@ struct Session {
         if (need > free_bytes / 2)
             fail("VNLB CUDA: the group buffers of one anchor frame do not fit in device memory");
         d_filtered.allocate(R * dim, "cudaMalloc(filtered rows)");
+        const size_t Bmax = static_cast<size_t>(std::min(model_cap, max_rows));
+        d_gmeans.allocate(G * 2 * dim, "cudaMalloc(group means)");
+        d_gram.allocate(G * Bmax * Bmax, "cudaMalloc(group Gram)");
+        d_eig.allocate(G * std::max(1, p.rank), "cudaMalloc(group eigenvalues)");
+        d_dual.allocate(G * std::max(1, p.rank) * Bmax, "cudaMalloc(group dual vectors)");
+        d_gflags.allocate(G, "cudaMalloc(group flags)");
         d_weights.allocate(R, "cudaMalloc(row weights)");
         d_row_info.allocate(R, "cudaMalloc(row info)");
         d_row_group.allocate(R, "cudaMalloc(row groups)");
@@ -434,6 +449,44 @@ struct Session {
         check(cudaMemcpy(grid->d_strips.ptr, grid->strips.data(), grid->strips.size() * sizeof(Strip),
                          cudaMemcpyHostToDevice),
               "cudaMemcpy(strips)");
+        // reach tables: a match lies within search_window - 1 of its anchor on
+        // each axis, so a stack tile gathers from the anchors in that reach
+        {
+            std::vector<int> row_y, row_first;
+            for (size_t j = 0; j < a.size(); ++j)
+                if (j == 0 || a[j].y != a[j - 1].y) {
+                    row_y.push_back(a[j].y);
+                    row_first.push_back(static_cast<int>(j));
+                }
+            row_first.push_back(static_cast<int>(a.size()));
+            const int rows_n = static_cast<int>(row_y.size());
+            const int reach = params.search_window - 1;
+            const int tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
+            std::vector<int2> tgr(tiles_y), tan(static_cast<size_t>(rows_n) * tiles_x);
+            for (int ty = 0; ty < tiles_y; ++ty) {
+                const int lo = ty * kTile - (P - 1) - reach, hi = ty * kTile + kTile - 1 + reach;
+                int k0 = 0;
+                while (k0 < rows_n && row_y[k0] < lo) ++k0;
+                int k1 = k0;
+                while (k1 < rows_n && row_y[k1] <= hi) ++k1;
+                tgr[ty] = make_int2(k0, k1);
+            }
+            for (int k = 0; k < rows_n; ++k)
+                for (int tx = 0; tx < tiles_x; ++tx) {
+                    const int lo = tx * kTile - (P - 1) - reach, hi = tx * kTile + kTile - 1 + reach;
+                    int j0 = row_first[k];
+                    while (j0 < row_first[k + 1] && a[j0].x < lo) ++j0;
+                    int j1 = j0;
+                    while (j1 < row_first[k + 1] && a[j1].x <= hi) ++j1;
+                    tan[static_cast<size_t>(k) * tiles_x + tx] = make_int2(j0, j1);
+                }
+            grid->d_tile_grid_rows.allocate(tgr.size(), "cudaMalloc(tile rows)");
+            grid->d_tile_anchors.allocate(tan.size(), "cudaMalloc(tile anchors)");
+            check(cudaMemcpy(grid->d_tile_grid_rows.ptr, tgr.data(), tgr.size() * sizeof(int2), cudaMemcpyHostToDevice),
+                  "cudaMemcpy(tile rows)");
+            check(cudaMemcpy(grid->d_tile_anchors.ptr, tan.data(), tan.size() * sizeof(int2), cudaMemcpyHostToDevice),
+                  "cudaMemcpy(tile anchors)");
+        }
         grid->d_map.allocate(plane(), "cudaMalloc(anchor map)");
         check(cudaMemsetAsync(grid->d_map.ptr, 0xff, plane() * sizeof(int), stream), "cudaMemsetAsync(anchor map)");
         check(launch_anchor_map(grid->d_anchors.ptr, static_cast<int>(a.size()), width, grid->d_map.ptr, stream),
@@ -525,6 +578,7 @@ struct Session {
         pl.active = d_active.ptr;
         pl.active_xy = d_active_xy.ptr;
         pl.row_offset = d_row_offset.ptr;
+        pl.active_prefix = d_active_prefix.ptr;
         pl.counters = d_counters.ptr;
         pl.totals = d_totals.ptr;
         t0 = begin_timed();
@@ -557,8 +611,13 @@ struct Session {
         fl.weights = d_weights.ptr;
         fl.row_info = d_row_info.ptr;
         fl.row_group = d_row_group.ptr;
+        fl.means = d_gmeans.ptr;
+        fl.gram = d_gram.ptr;
+        fl.eig = d_eig.ptr;
+        fl.dual = d_dual.ptr;
+        fl.flags = d_gflags.ptr;
         t0 = begin_timed();
-        check(launch_filter(fl, 148 * 8, stream), "filter kernel launch");
+        check(launch_filter(fl, G, stream), "filter kernel launch");
         end_timed(kTimedFilter, t0);
 
         TileLaunch tl{};
@@ -572,26 +631,25 @@ struct Session {
         tl.slots = slots;
         tl.search_bwd = params.search_bwd;
         tl.anchor_frame = anchor;
-        tl.search_window = params.search_window;
         tl.coupled = coupled ? 1 : 0;
         tl.windowed = params.weight_gamma != 0.0f ? 1 : 0;
         tl.window = d_window.ptr;
-        tl.active_xy = d_active_xy.ptr;
         tl.row_offset = d_row_offset.ptr;
-        tl.counters = d_counters.ptr;
+        tl.active_prefix = d_active_prefix.ptr;
         tl.filtered = d_filtered.ptr;
         tl.weights = d_weights.ptr;
         tl.row_info = d_row_info.ptr;
         tl.stack = stack;
-        tl.tile = 32;
-        tl.tiles_x = (width + 31) / 32;
-        tl.tiles_y = (height + 31) / 32;
+        tl.tiles_x = (width + kTile - 1) / kTile;
+        tl.tiles_y = (height + kTile - 1) / kTile;
+        tl.tile_grid_rows = grid.d_tile_grid_rows.ptr;
+        tl.tile_anchors = grid.d_tile_anchors.ptr;
         t0 = begin_timed();
         check(launch_tiles(tl, stream), "tile kernel launch");
         end_timed(kTimedTiles, t0);
         stats.anchor_frames += 1;
         stats.groups += G;
-        stats.kernel_launches += 4;
+        stats.kernel_launches += params.rank > 0 ? 6 : 5;
     }
 
     float* stack_for(int anchor) {

@@ -81,6 +81,7 @@ struct PasteLaunch {
     int* active;          // [G] active anchor indices in raster order
     int2* active_xy;      // [G] their positions
     int* row_offset;      // [G + 1] exclusive prefix of retained rows
+    int* active_prefix;   // [G + 1] active groups before grid anchor j
     FrameCounters* counters;
     unsigned long long* totals;  // session totals: active groups, rows
 };
@@ -105,6 +106,12 @@ struct FilterLaunch {
     const int* active;
     const int* row_offset;
     FrameCounters* counters;
+    // per active group a (intermediates between the three filter kernels)
+    float* means;           // [G][2][dim]: model (membership) mean, reconstruction centre
+    float* gram;            // [G][Bmax*Bmax]
+    float* eig;             // [G][rank]
+    float* dual;            // [G][rank*Bmax]
+    int* flags;             // [G]: kGroupDone / kGroupSkip
     // outputs, indexed by global row r = row_offset[a] + i
     float* filtered;        // [R][dim]
     float* weights;         // [R]
@@ -112,27 +119,33 @@ struct FilterLaunch {
     int* row_group;         // [R] active index of the row's group
 };
 
-size_t filter_shared_bytes(const FilterLaunch& L);
-cudaError_t launch_filter(const FilterLaunch& L, int ctas, cudaStream_t stream);
+constexpr int kGroupDone = 1;  // equal group: passed through, weights written
+constexpr int kGroupSkip = 2;  // rank not covered: reported through the status word
+
+// Three launches: prepare (equality, flat flag, means, Gram), batched Jacobi,
+// and apply (basis, coefficients, weights, reconstruction).
+cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t stream);
 
 struct TileLaunch {
     int width, height, channels;
     int P, Pt, patch_dim, dim;
     int slots, search_bwd, anchor_frame;
-    int search_window;
     int coupled;            // sample-major contribution writer (coupled, C > 1)
     int windowed;           // weight_gamma != 0
     const float* window;    // [P*P]
-    const int2* active_xy;
-    const int* row_offset;
-    const FrameCounters* counters;
+    const int* row_offset;  // [active + 1]
+    const int* active_prefix;  // [G + 1]
     const float* filtered;
     const float* weights;
     const MatchRow* row_info;
     float* stack;           // [slots][C+1][H][W]
-    int tile;               // tile edge in pixels
     int tiles_x, tiles_y;
+    // reach tables of the anchor grid (host-built per grid)
+    const int2* tile_grid_rows;  // [tiles_y]: grid rows whose anchors can reach tile row
+    const int2* tile_anchors;    // [grid rows][tiles_x]: anchor index range reaching tile column
 };
+
+constexpr int kTile = 16;  // stack tile edge, one pixel per thread
 
 cudaError_t launch_tiles(const TileLaunch& L, cudaStream_t stream);
 
