@@ -214,8 +214,7 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
         }
         if (B < min(D, L.rank)) {
             if (lane == 0) {
-                atomicCAS(&L.counters->status, 0, kStatusRankNotCovered);
-                L.counters->detail = g;
+                atomicCAS(L.status, 0, kStatusRankNotCovered);
                 L.flags[a] = kGroupSkip;
             }
             continue;

@@ -141,21 +141,22 @@ struct Session {
         check(cudaEventCreate(&e), "cudaEventCreate");
         return e;
     }
-    cudaEvent_t begin_timed() {
+    cudaEvent_t begin_timed(cudaStream_t on) {
         if (!timing) return nullptr;
         cudaEvent_t e = take_event();
-        check(cudaEventRecord(e, stream), "cudaEventRecord");
+        check(cudaEventRecord(e, on), "cudaEventRecord");
         return e;
     }
-    void end_timed(int category, cudaEvent_t start) {
+    void end_timed(int category, cudaEvent_t start, cudaStream_t on) {
         if (!timing) return;
         cudaEvent_t e = take_event();
-        check(cudaEventRecord(e, stream), "cudaEventRecord");
+        check(cudaEventRecord(e, on), "cudaEventRecord");
         timed.push_back(Timed{category, start, e});
     }
     void collect_timing() {
         if (timed.empty()) return;
         check(cudaStreamSynchronize(stream), "cudaStreamSynchronize(timing)");
+        for (Lane& l : lanes) check(cudaStreamSynchronize(l.stream), "cudaStreamSynchronize(timing)");
         for (const Timed& t : timed) {
             float ms = 0.0f;
             check(cudaEventElapsedTime(&ms, t.start, t.stop), "cudaEventElapsedTime");
@@ -172,22 +173,38 @@ struct Session {
     const float* ref = nullptr;
     bool clip_ready = false, ref_ready = false;
 
-    DeviceArray<MatchRow> d_rows, d_row_info;
-    DeviceArray<int> d_row_counts, d_victims, d_victim_counts, d_active, d_row_offset, d_row_group, d_active_prefix;
-    DeviceArray<int2> d_active_xy;
-    DeviceArray<FrameCounters> d_counters;
-    DeviceArray<unsigned long long> d_totals;
-    DeviceArray<float> d_filtered, d_weights, d_window, d_out_frame, d_pack;
-    DeviceArray<float> d_gmeans, d_gram, d_eig, d_dual;
-    DeviceArray<int> d_gflags;
-    std::map<int, std::unique_ptr<Grid>> grids;
-    int last_grid_key = INT_MIN;
+    // Two pipeline lanes: consecutive anchor frames alternate between them,
+    // each lane with its own stream and scratch, so that one anchor frame's
+    // serial paste-mask walk and kernel tails overlap the other's kernels.
+    struct Lane {
+        cudaStream_t stream = nullptr;
+        DeviceArray<MatchRow> rows, row_info;
+        DeviceArray<int> row_counts, victims, victim_counts, active, row_offset, row_group, active_prefix, gflags;
+        DeviceArray<int2> active_xy;
+        DeviceArray<FrameCounters> counters;
+        DeviceArray<float> filtered, weights, gmeans, gram, eig, dual;
+    };
+    static constexpr int kLaneCount = 2;
+    Lane lanes[kLaneCount];
+    int next_lane = 0;
+    cudaEvent_t ev_fork = nullptr;     // main-stream point the lanes start after
+    cudaEvent_t ev_lane[kLaneCount] = {nullptr, nullptr};
 
-    // contribution stack cache (anchor -> stack), capacity >= slots
+    DeviceArray<unsigned long long> d_totals;
+    DeviceArray<int> d_status;
+    DeviceArray<float> d_window, d_out_frame, d_pack;
+    std::map<int, std::unique_ptr<Grid>> grids;
+
+    // contribution stack cache (anchor -> stack), capacity >= slots.  `ready`
+    // is recorded on the producing lane, `released` on the main stream after
+    // the last normalisation that read the stack.
     struct CachedStack {
         int anchor = -1;
         long long last_use = 0;
         DeviceArray<float> data;
+        cudaEvent_t ready = nullptr;
+        cudaEvent_t released = nullptr;
+        bool pending_release = false;
     };
     std::vector<std::unique_ptr<CachedStack>> cache;
     long long use_clock = 0;
@@ -195,12 +212,36 @@ struct Session {
 
     ~Session() {
         if (stream) cudaStreamSynchronize(stream);
+        for (Lane& l : lanes)
+            if (l.stream) cudaStreamSynchronize(l.stream);
         for (const Timed& t : timed) {
             cudaEventDestroy(t.start);
             cudaEventDestroy(t.stop);
         }
         for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
+        for (auto& c : cache) {
+            if (c->ready) cudaEventDestroy(c->ready);
+            if (c->released) cudaEventDestroy(c->released);
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        for (cudaEvent_t e : ev_lane)
+            if (e) cudaEventDestroy(e);
+        for (Lane& l : lanes)
+            if (l.stream) cudaStreamDestroy(l.stream);
         if (own_stream) cudaStreamDestroy(own_stream);
+    }
+
+    // Lanes start after everything enqueued so far on the main stream ...
+    void fork() {
+        check(cudaEventRecord(ev_fork, stream), "cudaEventRecord(fork)");
+        for (Lane& l : lanes) check(cudaStreamWaitEvent(l.stream, ev_fork, 0), "cudaStreamWaitEvent(fork)");
+    }
+    // ... and the main stream continues after everything the lanes did.
+    void join() {
+        for (int i = 0; i < kLaneCount; ++i) {
+            check(cudaEventRecord(ev_lane[i], lanes[i].stream), "cudaEventRecord(join)");
+            check(cudaStreamWaitEvent(stream, ev_lane[i], 0), "cudaStreamWaitEvent(join)");
+        }
     }
 
     size_t plane() const { return static_cast<size_t>(width) * height; }
@@ -325,33 +366,40 @@ struct Session {
         if (warps < 1) fail("VNLB CUDA: the search region of one anchor does not fit in shared memory");
 
         const size_t G = static_cast<size_t>(max_groups);
-        d_rows.allocate(G * max_rows, "cudaMalloc(match rows)");
-        d_row_counts.allocate(G, "cudaMalloc(row counts)");
-        d_victims.allocate(G * victim_stride, "cudaMalloc(victims)");
-        d_victim_counts.allocate(G, "cudaMalloc(victim counts)");
-        d_active.allocate(G, "cudaMalloc(active groups)");
-        d_active_xy.allocate(G, "cudaMalloc(active positions)");
-        d_row_offset.allocate(G + 1, "cudaMalloc(row offsets)");
-        d_active_prefix.allocate(G + 1, "cudaMalloc(active prefix)");
-        d_counters.allocate(1, "cudaMalloc(counters)");
-        d_totals.allocate(2, "cudaMalloc(totals)");
-        check(cudaMemset(d_totals.ptr, 0, 2 * sizeof(unsigned long long)), "cudaMemset(totals)");
         const size_t R = G * max_rows;
+        const size_t Bmax = static_cast<size_t>(std::min(model_cap, max_rows));
         size_t free_bytes = 0, total_bytes = 0;
         check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
-        const size_t need = R * (static_cast<size_t>(dim) * 4 + 4 + sizeof(MatchRow) + 4);
+        const size_t need = kLaneCount * R * (static_cast<size_t>(dim) * 4 + 4 + sizeof(MatchRow) + 4);
         if (need > free_bytes / 2)
             fail("VNLB CUDA: the group buffers of one anchor frame do not fit in device memory");
-        d_filtered.allocate(R * dim, "cudaMalloc(filtered rows)");
-        const size_t Bmax = static_cast<size_t>(std::min(model_cap, max_rows));
-        d_gmeans.allocate(G * 2 * dim, "cudaMalloc(group means)");
-        d_gram.allocate(G * Bmax * Bmax, "cudaMalloc(group Gram)");
-        d_eig.allocate(G * std::max(1, p.rank), "cudaMalloc(group eigenvalues)");
-        d_dual.allocate(G * std::max(1, p.rank) * Bmax, "cudaMalloc(group dual vectors)");
-        d_gflags.allocate(G, "cudaMalloc(group flags)");
-        d_weights.allocate(R, "cudaMalloc(row weights)");
-        d_row_info.allocate(R, "cudaMalloc(row info)");
-        d_row_group.allocate(R, "cudaMalloc(row groups)");
+        for (Lane& l : lanes) {
+            check(cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking), "cudaStreamCreate(lane)");
+            l.rows.allocate(G * max_rows, "cudaMalloc(match rows)");
+            l.row_counts.allocate(G, "cudaMalloc(row counts)");
+            l.victims.allocate(G * victim_stride, "cudaMalloc(victims)");
+            l.victim_counts.allocate(G, "cudaMalloc(victim counts)");
+            l.active.allocate(G, "cudaMalloc(active groups)");
+            l.active_xy.allocate(G, "cudaMalloc(active positions)");
+            l.row_offset.allocate(G + 1, "cudaMalloc(row offsets)");
+            l.active_prefix.allocate(G + 1, "cudaMalloc(active prefix)");
+            l.counters.allocate(1, "cudaMalloc(counters)");
+            l.filtered.allocate(R * dim, "cudaMalloc(filtered rows)");
+            l.gmeans.allocate(G * 2 * dim, "cudaMalloc(group means)");
+            l.gram.allocate(G * Bmax * Bmax, "cudaMalloc(group Gram)");
+            l.eig.allocate(G * std::max(1, p.rank), "cudaMalloc(group eigenvalues)");
+            l.dual.allocate(G * std::max(1, p.rank) * Bmax, "cudaMalloc(group dual vectors)");
+            l.gflags.allocate(G, "cudaMalloc(group flags)");
+            l.weights.allocate(R, "cudaMalloc(row weights)");
+            l.row_info.allocate(R, "cudaMalloc(row info)");
+            l.row_group.allocate(R, "cudaMalloc(row groups)");
+        }
+        d_totals.allocate(2, "cudaMalloc(totals)");
+        check(cudaMemset(d_totals.ptr, 0, 2 * sizeof(unsigned long long)), "cudaMemset(totals)");
+        d_status.allocate(1, "cudaMalloc(status)");
+        check(cudaMemset(d_status.ptr, 0, sizeof(int)), "cudaMemset(status)");
+        check(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "cudaEventCreate");
+        for (cudaEvent_t& e : ev_lane) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
         d_out_frame.allocate(frame_values(), "cudaMalloc(output frame)");
         // aggregation window (prepare_aggregation_window, core.cpp:296-324)
         host_window.assign(static_cast<size_t>(P) * P, 1.0f);
@@ -375,10 +423,12 @@ struct Session {
         d_window.allocate(host_window.size(), "cudaMalloc(window)");
         check(cudaMemcpy(d_window.ptr, host_window.data(), host_window.size() * sizeof(float), cudaMemcpyHostToDevice),
               "cudaMemcpy(window)");
-        const int cache_size = slots + 1;
+        const int cache_size = slots + 2;  // every contributor of a frame, plus the lanes' work in flight
         for (int i = 0; i < cache_size; ++i) {
             auto entry = std::make_unique<CachedStack>();
             entry->data.allocate(stack_values(), "cudaMalloc(contribution stack)");
+            check(cudaEventCreateWithFlags(&entry->ready, cudaEventDisableTiming), "cudaEventCreate");
+            check(cudaEventCreateWithFlags(&entry->released, cudaEventDisableTiming), "cudaEventCreate");
             cache.push_back(std::move(entry));
         }
     }
@@ -491,6 +541,7 @@ struct Session {
         check(cudaMemsetAsync(grid->d_map.ptr, 0xff, plane() * sizeof(int), stream), "cudaMemsetAsync(anchor map)");
         check(launch_anchor_map(grid->d_anchors.ptr, static_cast<int>(a.size()), width, grid->d_map.ptr, stream),
               "anchor map kernel launch");
+        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize(anchor grid)");  // once per grid phase
         stats.kernel_launches += 1;
         Grid& ref_grid = *grid;
         grids.emplace(key, std::move(grid));
@@ -518,10 +569,12 @@ struct Session {
         for (auto& c : cache) c->anchor = -1;
     }
 
-    // One anchor frame: grid -> match -> paste mask -> filter -> stack tiles.
-    void compute_anchor(int anchor, float* stack) {
+    // One anchor frame on one lane: match -> paste mask -> filter -> stack
+    // tiles.  Everything is enqueued on the lane's stream.
+    void compute_anchor(int anchor, float* stack, Lane& lane) {
         Grid& grid = grid_for(anchor);
         const int G = static_cast<int>(grid.anchors.size());
+        cudaStream_t ls = lane.stream;
         // schedule (compute_temporal_range / schedule_temporal_range)
         int low, high;
         temporal_range(frames, Pt, params.search_bwd, params.search_fwd, anchor, low, high);
@@ -558,32 +611,32 @@ struct Session {
         m.window_cells = cw * chh;
         m.buffer_cap = buffer_cap;
         m.warp_floats = match_warp_floats(m.window_cells, search_channels * Pt, P, buffer_cap);
-        m.rows = d_rows.ptr;
-        m.row_counts = d_row_counts.ptr;
-        m.victims = d_victims.ptr;
-        m.victim_counts = d_victim_counts.ptr;
+        m.rows = lane.rows.ptr;
+        m.row_counts = lane.row_counts.ptr;
+        m.victims = lane.victims.ptr;
+        m.victim_counts = lane.victim_counts.ptr;
         m.victim_stride = victim_stride;
-        cudaEvent_t t0 = begin_timed();
-        check(launch_match(m, static_cast<int>(grid.strips.size()), warps, stream), "match kernel launch");
-        end_timed(kTimedMatch, t0);
+        cudaEvent_t t0 = begin_timed(ls);
+        check(launch_match(m, static_cast<int>(grid.strips.size()), warps, ls), "match kernel launch");
+        end_timed(kTimedMatch, t0, ls);
 
-        check(cudaMemsetAsync(d_counters.ptr, 0, sizeof(FrameCounters), stream), "cudaMemsetAsync(counters)");
+        check(cudaMemsetAsync(lane.counters.ptr, 0, sizeof(FrameCounters), ls), "cudaMemsetAsync(counters)");
         PasteLaunch pl{};
         pl.groups = G;
-        pl.row_counts = d_row_counts.ptr;
-        pl.victims = d_victims.ptr;
-        pl.victim_counts = d_victim_counts.ptr;
+        pl.row_counts = lane.row_counts.ptr;
+        pl.victims = lane.victims.ptr;
+        pl.victim_counts = lane.victim_counts.ptr;
         pl.victim_stride = victim_stride;
         pl.anchors = grid.d_anchors.ptr;
-        pl.active = d_active.ptr;
-        pl.active_xy = d_active_xy.ptr;
-        pl.row_offset = d_row_offset.ptr;
-        pl.active_prefix = d_active_prefix.ptr;
-        pl.counters = d_counters.ptr;
+        pl.active = lane.active.ptr;
+        pl.active_xy = lane.active_xy.ptr;
+        pl.row_offset = lane.row_offset.ptr;
+        pl.active_prefix = lane.active_prefix.ptr;
+        pl.counters = lane.counters.ptr;
         pl.totals = d_totals.ptr;
-        t0 = begin_timed();
-        check(launch_paste(pl, stream), "paste kernel launch");
-        end_timed(kTimedPaste, t0);
+        t0 = begin_timed(ls);
+        check(launch_paste(pl, ls), "paste kernel launch");
+        end_timed(kTimedPaste, t0, ls);
 
         FilterLaunch fl{};
         fl.noisy = clip;
@@ -602,23 +655,24 @@ struct Session {
         fl.max_rows = max_rows;
         fl.coupled = coupled ? 1 : 0;
         fl.cfg = cfg;
-        fl.rows = d_rows.ptr;
-        fl.row_counts = d_row_counts.ptr;
-        fl.active = d_active.ptr;
-        fl.row_offset = d_row_offset.ptr;
-        fl.counters = d_counters.ptr;
-        fl.filtered = d_filtered.ptr;
-        fl.weights = d_weights.ptr;
-        fl.row_info = d_row_info.ptr;
-        fl.row_group = d_row_group.ptr;
-        fl.means = d_gmeans.ptr;
-        fl.gram = d_gram.ptr;
-        fl.eig = d_eig.ptr;
-        fl.dual = d_dual.ptr;
-        fl.flags = d_gflags.ptr;
-        t0 = begin_timed();
-        check(launch_filter(fl, G, stream), "filter kernel launch");
-        end_timed(kTimedFilter, t0);
+        fl.rows = lane.rows.ptr;
+        fl.row_counts = lane.row_counts.ptr;
+        fl.active = lane.active.ptr;
+        fl.row_offset = lane.row_offset.ptr;
+        fl.counters = lane.counters.ptr;
+        fl.status = d_status.ptr;
+        fl.filtered = lane.filtered.ptr;
+        fl.weights = lane.weights.ptr;
+        fl.row_info = lane.row_info.ptr;
+        fl.row_group = lane.row_group.ptr;
+        fl.means = lane.gmeans.ptr;
+        fl.gram = lane.gram.ptr;
+        fl.eig = lane.eig.ptr;
+        fl.dual = lane.dual.ptr;
+        fl.flags = lane.gflags.ptr;
+        t0 = begin_timed(ls);
+        check(launch_filter(fl, G, ls), "filter kernel launch");
+        end_timed(kTimedFilter, t0, ls);
 
         TileLaunch tl{};
         tl.width = width;
@@ -634,44 +688,53 @@ struct Session {
         tl.coupled = coupled ? 1 : 0;
         tl.windowed = params.weight_gamma != 0.0f ? 1 : 0;
         tl.window = d_window.ptr;
-        tl.row_offset = d_row_offset.ptr;
-        tl.active_prefix = d_active_prefix.ptr;
-        tl.filtered = d_filtered.ptr;
-        tl.weights = d_weights.ptr;
-        tl.row_info = d_row_info.ptr;
+        tl.row_offset = lane.row_offset.ptr;
+        tl.active_prefix = lane.active_prefix.ptr;
+        tl.filtered = lane.filtered.ptr;
+        tl.weights = lane.weights.ptr;
+        tl.row_info = lane.row_info.ptr;
         tl.stack = stack;
         tl.tiles_x = (width + kTile - 1) / kTile;
         tl.tiles_y = (height + kTile - 1) / kTile;
         tl.tile_grid_rows = grid.d_tile_grid_rows.ptr;
         tl.tile_anchors = grid.d_tile_anchors.ptr;
-        t0 = begin_timed();
-        check(launch_tiles(tl, stream), "tile kernel launch");
-        end_timed(kTimedTiles, t0);
+        t0 = begin_timed(ls);
+        check(launch_tiles(tl, ls), "tile kernel launch");
+        end_timed(kTimedTiles, t0, ls);
         stats.anchor_frames += 1;
         stats.groups += G;
         stats.kernel_launches += params.rank > 0 ? 6 : 5;
     }
 
-    float* stack_for(int anchor) {
+    // The stack of `anchor`, computed on the next lane when not cached.  The
+    // returned slot's `ready` event marks the end of its production.
+    CachedStack* stack_for(int anchor, int* lane_used = nullptr) {
         for (auto& c : cache)
             if (c->anchor == anchor) {
                 c->last_use = ++use_clock;
-                return c->data.ptr;
+                return c.get();
             }
         CachedStack* victim = cache.front().get();
         for (auto& c : cache)
             if (c->last_use < victim->last_use) victim = c.get();
         victim->anchor = anchor;
         victim->last_use = ++use_clock;
-        compute_anchor(anchor, victim->data.ptr);
-        return victim->data.ptr;
+        const int li = next_lane;
+        next_lane = (next_lane + 1) % kLaneCount;
+        Lane& lane = lanes[li];
+        if (victim->pending_release)  // its previous contents are still being read
+            check(cudaStreamWaitEvent(lane.stream, victim->released, 0), "cudaStreamWaitEvent(stack release)");
+        victim->pending_release = false;
+        compute_anchor(anchor, victim->data.ptr, lane);
+        check(cudaEventRecord(victim->ready, lane.stream), "cudaEventRecord(stack ready)");
+        if (lane_used) *lane_used = li;
+        return victim;
     }
 
     // vnlbcu.Basic/Final frame n: normalise over the contributing anchors
     // (contributing_anchors, cuda_plugin.cpp:809-823; render_aggregate_frame
-    // order: anchors first..last).
+    // order: anchors first..last).  Call between fork() and join().
     void render_to_device(int n, float* out) {
-        require_sources();
         const int first = std::max(0, n - (params.search_fwd + Pt - 1));
         const int last = std::min(frames - 1, n + params.search_bwd);
         NormalizeLaunch nl{};
@@ -679,26 +742,39 @@ struct Session {
         nl.height = height;
         nl.channels = channels;
         nl.count = 0;
+        CachedStack* used[kMaxContributors];
         for (int a = first; a <= last; ++a) {
             if (a > frames - Pt) continue;  // cleared stacks contribute nothing
-            nl.stacks[nl.count] = stack_for(a);
+            CachedStack* c = stack_for(a);
+            used[nl.count] = c;
+            nl.stacks[nl.count] = c->data.ptr;
             nl.slots[nl.count] = n - a + params.search_bwd;
             ++nl.count;
         }
+        for (int i = 0; i < nl.count; ++i)
+            check(cudaStreamWaitEvent(stream, used[i]->ready, 0), "cudaStreamWaitEvent(stack ready)");
         nl.source = clip + static_cast<size_t>(n) * frame_values();
         nl.out = out;
-        cudaEvent_t t0 = begin_timed();
+        cudaEvent_t t0 = begin_timed(stream);
         check(launch_normalize(nl, stream), "normalize kernel launch");
-        end_timed(kTimedNormalize, t0);
+        end_timed(kTimedNormalize, t0, stream);
+        for (int i = 0; i < nl.count; ++i) {
+            check(cudaEventRecord(used[i]->released, stream), "cudaEventRecord(stack release)");
+            used[i]->pending_release = true;
+        }
         stats.kernel_launches += 1;
     }
 
     void check_status() {
-        FrameCounters c{};
-        check(cudaMemcpyAsync(&c, d_counters.ptr, sizeof(c), cudaMemcpyDeviceToHost, stream), "cudaMemcpyAsync(status)");
+        int status = 0;
+        check(cudaMemcpyAsync(&status, d_status.ptr, sizeof(status), cudaMemcpyDeviceToHost, stream),
+              "cudaMemcpyAsync(status)");
         check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
-        if (c.status == kStatusRankNotCovered) fail("VNLB CUDA: group_size must cover the effective VNLB rank");
-        if (c.status != 0) fail("VNLB CUDA: device status " + std::to_string(c.status));
+        if (status != 0) {
+            check(cudaMemsetAsync(d_status.ptr, 0, sizeof(int), stream), "cudaMemsetAsync(status)");
+            if (status == kStatusRankNotCovered) fail("VNLB CUDA: group_size must cover the effective VNLB rank");
+            fail("VNLB CUDA: device status " + std::to_string(status));
+        }
     }
 };
 
@@ -825,7 +901,10 @@ int vnlbgpu_render_frame(vnlbgpu_session* session, int n, float* const* planes, 
         std::lock_guard guard(s.lock);
         if (n < 0 || n >= s.frames) vnlbgpu::fail("VNLB CUDA: frame index out of range");
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.require_sources();
+        s.fork();
         s.render_to_device(n, s.d_out_frame.ptr);
+        s.join();
         copy_planes_out(s.d_out_frame.ptr, planes, strides, s.width, s.height, s.channels, s.stream);
         s.check_status();
     });
@@ -836,7 +915,10 @@ int vnlbgpu_render_clip_device(vnlbgpu_session* session, float* device_out) {
         Session& s = session->impl;
         std::lock_guard guard(s.lock);
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.require_sources();
+        s.fork();
         for (int n = 0; n < s.frames; ++n) s.render_to_device(n, device_out + static_cast<size_t>(n) * s.frame_values());
+        s.join();
     });
 }
 
@@ -847,7 +929,10 @@ int vnlbgpu_render_clip_host(vnlbgpu_session* session, float* out) {
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
         if (!s.d_pack.ptr || s.d_pack.count < s.frame_values() * s.frames)
             s.d_pack.allocate(s.frame_values() * s.frames, "cudaMalloc(clip output)");
+        s.require_sources();
+        s.fork();
         for (int n = 0; n < s.frames; ++n) s.render_to_device(n, s.d_pack.ptr + static_cast<size_t>(n) * s.frame_values());
+        s.join();
         vnlbgpu::check(cudaMemcpyAsync(out, s.d_pack.ptr, s.frame_values() * s.frames * sizeof(float),
                                        cudaMemcpyDeviceToHost, s.stream),
                        "cudaMemcpyAsync(clip download)");
@@ -876,9 +961,15 @@ int vnlbgpu_render_stack(vnlbgpu_session* session, int n, float* const* planes, 
         if (n > s.frames - s.Pt) {
             vnlbgpu::check(cudaMemsetAsync(s.d_pack.ptr, 0, packed * sizeof(float), s.stream), "cudaMemsetAsync(stack)");
         } else {
-            const float* stack = s.stack_for(n);
-            vnlbgpu::check(vnlbgpu::launch_pack_stack(stack, s.width, s.height, s.channels, s.slots, s.d_pack.ptr, s.stream),
+            s.fork();
+            Session::CachedStack* c = s.stack_for(n);
+            vnlbgpu::check(cudaStreamWaitEvent(s.stream, c->ready, 0), "cudaStreamWaitEvent(stack ready)");
+            vnlbgpu::check(vnlbgpu::launch_pack_stack(c->data.ptr, s.width, s.height, s.channels, s.slots, s.d_pack.ptr,
+                                                      s.stream),
                            "pack kernel launch");
+            vnlbgpu::check(cudaEventRecord(c->released, s.stream), "cudaEventRecord(stack release)");
+            c->pending_release = true;
+            s.join();
         }
         const int rows = s.slots * 2 * s.height;
         for (int c = 0; c < s.channels; ++c) {
@@ -963,6 +1054,7 @@ int vnlbgpu_set_stream(vnlbgpu_session* session, void* stream) {
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
         s.collect_timing();
         vnlbgpu::check(cudaStreamSynchronize(s.stream), "cudaStreamSynchronize");
+        for (auto& l : s.lanes) vnlbgpu::check(cudaStreamSynchronize(l.stream), "cudaStreamSynchronize");
         s.stream = stream ? static_cast<cudaStream_t>(stream) : s.own_stream;
     });
 }
@@ -995,16 +1087,19 @@ int vnlbgpu_diag_anchor(vnlbgpu_session* session, int anchor, int* grid_xy, int*
         if (anchor < 0 || anchor > s.frames - s.Pt) vnlbgpu::fail("VNLB CUDA: anchor frame out of range");
         vnlbgpu::DeviceArray<float> stack;
         stack.allocate(s.stack_values(), "cudaMalloc(diag stack)");
-        s.compute_anchor(anchor, stack.ptr);
+        s.fork();
+        Session::Lane& lane = s.lanes[0];
+        s.compute_anchor(anchor, stack.ptr, lane);
+        s.join();
         s.check_status();
         vnlbgpu::Grid& grid = s.grid_for(anchor);
         const int G = static_cast<int>(grid.anchors.size());
         *groups = G;
         *max_rows = s.max_rows;
         std::vector<int> counts(G);
-        vnlbgpu::check(cudaMemcpy(counts.data(), s.d_row_counts.ptr, G * sizeof(int), cudaMemcpyDeviceToHost), "copy");
+        vnlbgpu::check(cudaMemcpy(counts.data(), lane.row_counts.ptr, G * sizeof(int), cudaMemcpyDeviceToHost), "copy");
         std::vector<vnlbgpu::MatchRow> mrows(static_cast<size_t>(G) * s.max_rows);
-        vnlbgpu::check(cudaMemcpy(mrows.data(), s.d_rows.ptr, mrows.size() * sizeof(vnlbgpu::MatchRow),
+        vnlbgpu::check(cudaMemcpy(mrows.data(), lane.rows.ptr, mrows.size() * sizeof(vnlbgpu::MatchRow),
                                   cudaMemcpyDeviceToHost),
                        "copy");
         for (int g = 0; g < G && g < grid_capacity; ++g) {
@@ -1017,20 +1112,20 @@ int vnlbgpu_diag_anchor(vnlbgpu_session* session, int anchor, int* grid_xy, int*
             }
         }
         vnlbgpu::FrameCounters c{};
-        vnlbgpu::check(cudaMemcpy(&c, s.d_counters.ptr, sizeof(c), cudaMemcpyDeviceToHost), "copy");
+        vnlbgpu::check(cudaMemcpy(&c, lane.counters.ptr, sizeof(c), cudaMemcpyDeviceToHost), "copy");
         *active_groups = c.active;
         *rows = c.rows;
         std::vector<int> act(c.active);
         if (c.active > 0)
-            vnlbgpu::check(cudaMemcpy(act.data(), s.d_active.ptr, c.active * sizeof(int), cudaMemcpyDeviceToHost), "copy");
+            vnlbgpu::check(cudaMemcpy(act.data(), lane.active.ptr, c.active * sizeof(int), cudaMemcpyDeviceToHost), "copy");
         for (int i = 0; i < c.active && i < active_capacity; ++i) active[i] = act[i];
         std::vector<vnlbgpu::MatchRow> info(c.rows);
         std::vector<float> w(c.rows);
         if (c.rows > 0) {
-            vnlbgpu::check(cudaMemcpy(info.data(), s.d_row_info.ptr, c.rows * sizeof(vnlbgpu::MatchRow),
+            vnlbgpu::check(cudaMemcpy(info.data(), lane.row_info.ptr, c.rows * sizeof(vnlbgpu::MatchRow),
                                       cudaMemcpyDeviceToHost),
                            "copy");
-            vnlbgpu::check(cudaMemcpy(w.data(), s.d_weights.ptr, c.rows * sizeof(float), cudaMemcpyDeviceToHost), "copy");
+            vnlbgpu::check(cudaMemcpy(w.data(), lane.weights.ptr, c.rows * sizeof(float), cudaMemcpyDeviceToHost), "copy");
         }
         for (int r = 0; r < c.rows && r < active_row_capacity; ++r)
             active_rows[r] = vnlbgpu_diag_row{info[r].distance, info[r].x, info[r].y, info[r].frame, w[r]};

@@ -106,6 +106,7 @@ struct FilterLaunch {
     const int* active;
     const int* row_offset;
     FrameCounters* counters;
+    int* status;            // session status word (first error wins), not reset per anchor frame
     // per active group a (intermediates between the three filter kernels)
     float* means;           // [G][2][dim]: model (membership) mean, reconstruction centre
     float* gram;            // [G][Bmax*Bmax]
