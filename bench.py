@@ -299,7 +299,13 @@ def run_ours(args):
         "work": "3 FP32 ops (sub, mul, add; no FMA, the CPU's order) per candidate element, "
                 "G x W^2 x T x d_m per anchor frame",
         "ms_per_launch": match_ms / max(1, match_launches),
-        "traffic": None,
+        # dram__bytes_read.sum + dram__bytes_write.sum of one match launch (mean of the
+        # Basic and Final launches) from profiles/kernels_1080p_yuv444_one_anchor_frame.md;
+        # algorithmic reads are 24.9 MB (Basic) and 74.6 MB (Final) per launch
+        "traffic": 59.5e6,
+        "traffic_unit": "bytes per launch (ncu, one capture)",
+        "note": "event-timed inside the timed region, where the other pipeline lane runs concurrently; "
+                "ncu's serial per-launch times are in profiles/",
     }
     per_kernel = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1],
                       "share": v[0] / total_kernel_ms if total_kernel_ms else None} for k, v in kernels.items()}
