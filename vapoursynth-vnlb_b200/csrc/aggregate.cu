@@ -20,7 +20,8 @@ namespace vnlbgpu {
 namespace {
 
 constexpr int kTileThreads = kTile * kTile;
-constexpr int kEntryCap = 1024;
+constexpr int kTileWarps = kTileThreads / 32;
+constexpr int kMaxGridRows = 64;  // grid rows per collection round
 
 struct Entry {
     int r;     // global row
@@ -28,10 +29,18 @@ struct Entry {
     float w;   // row weight
 };
 
+// One CTA per (16x16 tile, slot), one pixel per thread.  The rows that can
+// cover the tile form one contiguous row range per grid row in reach (reach
+// tables, built per grid); their concatenation is in increasing global row
+// order.  All threads test 256 rows at a time, an ordered block compaction
+// keeps the covering ones in that order, and every thread applies them to
+// its pixel before the next chunk: the CPU's accumulation order, with no
+// atomics and one write per stack value.
 __global__ void __launch_bounds__(kTileThreads) tile_kernel(TileLaunch L) {
-    __shared__ Entry entries[kEntryCap];
-    __shared__ int s_count;
-    __shared__ int s_done;
+    __shared__ Entry entries[kTileThreads];
+    __shared__ int s_rbeg[kMaxGridRows];
+    __shared__ int s_rpre[kMaxGridRows + 1];
+    __shared__ int s_warp[kTileWarps + 1];
     extern __shared__ float window[];
 
     const int tx = blockIdx.x, ty = blockIdx.y, slot = blockIdx.z;
@@ -43,105 +52,97 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(TileLaunch L) {
     const int lane = tid & 31;
     for (int i = tid; i < P * P; i += blockDim.x) window[i] = L.window[i];
 
-    // warp-0 iterator over the grid rows that reach this tile; each grid row
-    // contributes one contiguous range of rows [row_offset[a0], row_offset[a1])
-    const int2 grid_rows = L.tile_grid_rows[ty];
-    int cur_row = grid_rows.x;
-    int cur_r = 0, r_end = 0;  // empty range: the first step loads grid row cur_row
-
     const int px = tx0 + (tid % kTile);
     const int py = ty0 + (tid / kTile);
     float num[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     float wt = 0.0f;
-    __syncthreads();
-
     const int fused_cols = (P == kLanes || P == 2 * kLanes) ? P : (P / kLanes) * kLanes;
-    for (;;) {
-        if (warp == 0) {
-            int count = 0;
-            bool full = false;
-            while (!full) {
-                if (cur_r >= r_end) {
-                    if (cur_row >= grid_rows.y) break;
-                    const int2 anchors = L.tile_anchors[static_cast<size_t>(cur_row) * L.tiles_x + tx];
-                    ++cur_row;
-                    const int a0 = L.active_prefix[anchors.x];
-                    const int a1 = L.active_prefix[anchors.y];
-                    cur_r = L.row_offset[a0];
-                    r_end = L.row_offset[a1];
-                    continue;
+    const int2 grid_rows = L.tile_grid_rows[ty];
+
+    for (int k0 = grid_rows.x; k0 < grid_rows.y; k0 += kMaxGridRows) {
+        const int nk = min(kMaxGridRows, grid_rows.y - k0);
+        __syncthreads();
+        if (tid < nk) {
+            const int2 anchors = L.tile_anchors[static_cast<size_t>(k0 + tid) * L.tiles_x + tx];
+            const int rb = L.row_offset[L.active_prefix[anchors.x]];
+            const int re = L.row_offset[L.active_prefix[anchors.y]];
+            s_rbeg[tid] = rb;
+            s_rpre[tid + 1] = re - rb;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            s_rpre[0] = 0;
+            for (int k = 1; k <= nk; ++k) s_rpre[k] += s_rpre[k - 1];
+        }
+        __syncthreads();
+        const int total = s_rpre[nk];
+        for (int chunk = 0; chunk < total; chunk += kTileThreads) {
+            // test one virtual row per thread
+            const int vrow = chunk + tid;
+            bool hit = false;
+            Entry en;
+            if (vrow < total) {
+                int lo = 0, hi = nk - 1;  // last k with s_rpre[k] <= vrow
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_rpre[mid] <= vrow) lo = mid;
+                    else hi = mid - 1;
                 }
-                const int r = cur_r + lane;
-                int hits = 0;
-                int t_hit = 0;
-                MatchRow m = {0.0f, 0, 0, 0};
-                if (r < r_end) {
-                    m = L.row_info[r];
-                    if (m.x <= tx0 + kTile - 1 && m.x + P - 1 >= tx0 && m.y <= ty0 + kTile - 1 && m.y + P - 1 >= ty0) {
-                        const int t = slot - L.search_bwd + L.anchor_frame - m.frame;
-                        if (t >= 0 && t < L.Pt) {
-                            hits = 1;
-                            t_hit = t;
-                        }
+                const int r = s_rbeg[lo] + (vrow - s_rpre[lo]);
+                const MatchRow m = L.row_info[r];
+                if (m.x <= tx0 + kTile - 1 && m.x + P - 1 >= tx0 && m.y <= ty0 + kTile - 1 && m.y + P - 1 >= ty0) {
+                    const int t = slot - L.search_bwd + L.anchor_frame - m.frame;
+                    if (t >= 0 && t < L.Pt) {
+                        hit = true;
+                        en.r = r;
+                        en.xyt = m.x | (m.y << 14) | (t << 28);
+                        en.w = L.weights[r];
                     }
                 }
-                const unsigned ballot = __ballot_sync(0xffffffffu, hits != 0);
-                const int total = __popc(ballot);
-                if (count + total > kEntryCap) {
-                    full = true;
-                    break;
-                }
-                if (hits) {
-                    Entry en;
-                    en.r = r;
-                    en.xyt = m.x | (m.y << 14) | (t_hit << 28);
-                    en.w = L.weights[r];
-                    entries[count + __popc(ballot & ((1u << lane) - 1u))] = en;
-                }
-                count += total;
-                cur_r += 32;
             }
-            if (lane == 0) {
-                s_count = count;
-                s_done = full ? 0 : 1;
+            // ordered block compaction
+            const unsigned ballot = __ballot_sync(0xffffffffu, hit);
+            if (lane == 0) s_warp[warp + 1] = __popc(ballot);
+            __syncthreads();
+            if (tid == 0) {
+                s_warp[0] = 0;
+                for (int w = 1; w <= kTileWarps; ++w) s_warp[w] += s_warp[w - 1];
             }
-        }
-        __syncthreads();
-        // apply the batch to this thread's pixel, in order
-        const int n = s_count;
-        for (int e = 0; e < n; ++e) {
-            const Entry en = entries[e];
-            const int ex = en.xyt & 0x3fff;
-            const int ey = (en.xyt >> 14) & 0x3fff;
-            const unsigned dx = static_cast<unsigned>(px - ex);
-            const unsigned dy = static_cast<unsigned>(py - ey);
-            if (dx >= static_cast<unsigned>(P) || dy >= static_cast<unsigned>(P)) continue;
-            const int t = en.xyt >> 28;
-            const int pos = (t * P + static_cast<int>(dy)) * P + static_cast<int>(dx);
-            const float* f = L.filtered + static_cast<size_t>(en.r) * L.dim + pos;
-            if (L.coupled && !L.windowed) {
-                const bool fused = static_cast<int>(dx) < fused_cols;
+            __syncthreads();
+            if (hit) entries[s_warp[warp] + __popc(ballot & ((1u << lane) - 1u))] = en;
+            const int n = s_warp[kTileWarps];
+            __syncthreads();
+            // apply, in order, to this thread's pixel
+            for (int e = 0; e < n; ++e) {
+                const Entry x = entries[e];
+                const unsigned dx = static_cast<unsigned>(px - (x.xyt & 0x3fff));
+                const unsigned dy = static_cast<unsigned>(py - ((x.xyt >> 14) & 0x3fff));
+                if (dx >= static_cast<unsigned>(P) || dy >= static_cast<unsigned>(P)) continue;
+                const int t = x.xyt >> 28;
+                const int pos = (t * P + static_cast<int>(dy)) * P + static_cast<int>(dx);
+                const float* f = L.filtered + static_cast<size_t>(x.r) * L.dim + pos;
+                if (L.coupled && !L.windowed) {
+                    const bool fused = static_cast<int>(dx) < fused_cols;
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    if (c >= C) break;
-                    const float x = __ldg(f + c * L.patch_dim);
-                    num[c] = fused ? __fmaf_rn(en.w, x, num[c]) : __fadd_rn(num[c], __fmul_rn(en.w, x));
-                }
-                wt = __fadd_rn(wt, en.w);
-            } else {
-                const float cw = __fmul_rn(en.w, window[dy * P + dx]);
+                    for (int c = 0; c < 4; ++c) {
+                        if (c >= C) break;
+                        const float v = __ldg(f + c * L.patch_dim);
+                        num[c] = fused ? __fmaf_rn(x.w, v, num[c]) : __fadd_rn(num[c], __fmul_rn(x.w, v));
+                    }
+                    wt = __fadd_rn(wt, x.w);
+                } else {
+                    const float cw = __fmul_rn(x.w, window[dy * P + dx]);
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    if (c >= C) break;
-                    const float x = __ldg(f + c * L.patch_dim);
-                    num[c] = __fadd_rn(num[c], __fmul_rn(cw, x));
+                    for (int c = 0; c < 4; ++c) {
+                        if (c >= C) break;
+                        const float v = __ldg(f + c * L.patch_dim);
+                        num[c] = __fadd_rn(num[c], __fmul_rn(cw, v));
+                    }
+                    wt = __fadd_rn(wt, cw);
                 }
-                wt = __fadd_rn(wt, cw);
             }
+            __syncthreads();
         }
-        const bool done = s_done != 0;
-        __syncthreads();
-        if (done) break;
     }
     // write this slot's tile: every pixel, so the stack needs no clearing
     if (px < L.width && py < L.height) {

@@ -36,8 +36,9 @@
 namespace vnlbgpu {
 namespace {
 
-constexpr int kApplyThreads = 128;
+constexpr int kApplyThreads = 256;
 constexpr int kApplyWarps = kApplyThreads / 32;
+constexpr int kRecCols = 8;  // reconstruction columns held in registers per lane (blocks of 256)
 constexpr int kPrepareWarps = 4;
 constexpr float kEigenFloor = 128.0f * FLT_EPSILON;
 
@@ -436,7 +437,7 @@ __host__ __device__ inline ApplyLayout apply_layout(int D, int Bmax, int R, int 
     a.dual = off;    off += static_cast<size_t>(R) * Bmax;
     a.scal = off;    off += 5 * static_cast<size_t>(R);
     a.scores = off;  off += static_cast<size_t>(max_rows);
-    a.scratch = off; off += static_cast<size_t>(warps) * 3 * a.ldb;
+    a.scratch = off; off += static_cast<size_t>(warps) * (2 * a.ldb + R + 1);
     off = (off + 1) & ~static_cast<size_t>(1);
     a.bases = off;   off += 2 * static_cast<size_t>(max_rows);
     a.bytes = off * sizeof(float);
@@ -512,28 +513,29 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
         const float* center_vec = means + D;
         if (R > 0) {
             // centred model rows (compute_mean + center_rows of the first B rows)
-            for (int e = tid; e < B * D; e += kApplyThreads) {
-                const int s = e / D;
-                const int col = e - s * D;
-                X[s * ldx + col] = __fsub_rn(__ldg(model_video + bases[s] + coloff[col]), member_mean[col]);
+            for (int s = warp; s < B; s += kApplyWarps) {
+                const float* src = model_video + bases[s];
+                for (int col = lane; col < D; col += 32)
+                    X[s * ldx + col] = __fsub_rn(__ldg(src + coloff[col]), member_mean[col]);
             }
             __syncthreads();
             // dual -> primal basis (map_dual_eigenvectors_to_basis): one output
-            // per thread, the samples accumulated in order
-            for (int e = tid; e < R * D; e += kApplyThreads) {
-                const int b = e / D;
-                const int col = e - b * D;
-                float acc = 0.0f;
-                if (eig[b] > kEigenFloor) {
-                    const bool fused = fused_column(col, D);
-                    for (int s = 0; s < B; ++s) {
-                        const float x = X[s * ldx + col];
-                        const float w = dual[b * Bmax + s];
-                        acc = fused ? __fmaf_rn(w, x, acc) : __fadd_rn(acc, __fmul_rn(w, x));
+            // per lane, the samples accumulated in order
+            for (int b = warp; b < R; b += kApplyWarps) {
+                const bool live = eig[b] > kEigenFloor;
+                for (int col = lane; col < D; col += 32) {
+                    float acc = 0.0f;
+                    if (live) {
+                        const bool fused = fused_column(col, D);
+                        for (int s = 0; s < B; ++s) {
+                            const float x = X[s * ldx + col];
+                            const float w = dual[b * Bmax + s];
+                            acc = fused ? __fmaf_rn(w, x, acc) : __fadd_rn(acc, __fmul_rn(w, x));
+                        }
+                        acc = __fmul_rn(acc, inv_sqrt[b]);
                     }
-                    acc = __fmul_rn(acc, inv_sqrt[b]);
+                    basis[b * ldb + col] = acc;
                 }
-                basis[b * ldb + col] = acc;
             }
             __syncthreads();
             for (int b = warp; b < R; b += kApplyWarps) {
@@ -572,9 +574,9 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
         // per row: membership score and reconstruction.  In the Basic stage the
         // membership row and the reconstruction row are the same centred noisy
         // row, so its projections serve both.
-        float* u = scratch + warp * 3 * ldb;  // centred membership row
-        float* v = u + ldb;                   // centred noisy row (Final)
-        float* o = v + ldb;                   // reconstruction accumulator
+        float* u = scratch + warp * (2 * ldb + R + 1);  // centred membership row
+        float* v = u + ldb;                             // centred noisy row (Final)
+        float* proj = v + ldb;                          // projections for the reconstruction
         const int j8 = lane & 7;
         const int oct = lane >> 3;
         const float score_scale = __fsqrt_rn(__fmul_rn(2.0f, static_cast<float>(D)));
@@ -588,7 +590,6 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
                 } else {
                     u[col] = __fsub_rn(xn, member_mean[col]);
                 }
-                o[col] = 0.0f;
             }
             __syncwarp();
             float distance = 0.0f, projected = 0.0f, norm2 = 0.0f;
@@ -612,12 +613,7 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
                         distance = __fadd_rn(distance, __fdiv_rn(proj2, denom[ck]));
                         projected = __fadd_rn(projected, proj2);
                     }
-                    if (coef[ck] != 0.0f) {
-                        const float scaled = __fmul_rn(coef[ck], rk);
-                        const float* bc = basis + ck * ldb;
-                        for (int col = lane; col < D; col += 32)
-                            o[col] = add_scaled_elem(o[col], bc[col], scaled, col, D);
-                    }
+                    if (lane == 0) proj[ck] = rk;
                 }
             }
             if (membership_on) {
@@ -626,8 +622,30 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
                 const float score = __fdiv_rn(__fsub_rn(distance, static_cast<float>(D)), score_scale);
                 if (lane == 0) scores[i] = score;
             }
+            __syncwarp();
+            // reconstruction (project_bayes_estimate), components in order,
+            // accumulated in registers over blocks of 32 * kRecCols columns
             float* out = L.filtered + static_cast<size_t>(r0 + i) * D;
-            for (int col = lane; col < D; col += 32) out[col] = __fadd_rn(o[col], center_vec[col]);
+            for (int base = 0; base < D; base += 32 * kRecCols) {
+                float o[kRecCols];
+#pragma unroll
+                for (int j = 0; j < kRecCols; ++j) o[j] = 0.0f;
+                for (int c = 0; c < R; ++c) {
+                    if (coef[c] == 0.0f) continue;
+                    const float scaled = __fmul_rn(coef[c], proj[c]);
+                    const float* bc = basis + c * ldb;
+#pragma unroll
+                    for (int j = 0; j < kRecCols; ++j) {
+                        const int col = base + lane + 32 * j;
+                        if (col < D) o[j] = add_scaled_elem(o[j], bc[col], scaled, col, D);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < kRecCols; ++j) {
+                    const int col = base + lane + 32 * j;
+                    if (col < D) out[col] = __fadd_rn(o[j], center_vec[col]);
+                }
+            }
             __syncwarp();
         }
         __syncthreads();
@@ -705,7 +723,7 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t st
         cudaError_t err = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
         if (err != cudaSuccess) return err;
-        const int ctas = std::min(max_groups, 148 * 12);
+        const int ctas = std::min(max_groups, 148 * 8);
         apply_kernel<<<ctas, kApplyThreads, smem, stream>>>(L);
         if ((err = cudaGetLastError()) != cudaSuccess) return err;
     }
