@@ -130,6 +130,26 @@ int vnlbgpu_render_stack(vnlbgpu_session* session, int n, float* const* planes, 
 int vnlbgpu_aggregate(const float* stacks, const float* source, int width, int height, int frames, int channels,
                       int search_bwd, int search_fwd, int patch_time, int device_id, float* out);
 
+/* vnlb.Aggregate of the single output frame n (0 <= n < frames), from the
+ * same host stacks and source clip as vnlbgpu_aggregate, into host memory
+ * [planes][H][W].  It has no counterpart in the reference.  It allocates
+ * nothing: no cudaMalloc, no cudaFree, no allocating library routine.  It is
+ * for hosts that cannot allocate device memory while serving frames, such as
+ * a frame server that reserves its device memory budget at start-up and
+ * shares the GPU with other filters; there an allocation in the middle of a
+ * clip can fail under memory pressure, and a free waits for the whole device.
+ * The rows pass through a fixed 32 MiB device scratch per device, in bands of
+ * whole rows.  One row of the frame's contributing stacks, source and output
+ * must fit: (contributing stacks * 2 + 2) * planes * width * 4 bytes
+ * <= 32 MiB.  A larger frame is rejected with an error.  The first call on a
+ * device sets up that device's scratch address; make it before any stream
+ * capture begins.  Calls on one device are serialised inside, because calls
+ * whose GPU work overlapped would race on the one scratch.  Returns when the
+ * output is on the host.  Results equal vnlbgpu_aggregate's bit for bit. */
+int vnlbgpu_aggregate_frame_noalloc(const float* stacks, const float* source, int width, int height, int frames,
+                                    int channels, int search_bwd, int search_fwd, int patch_time, int device_id, int n,
+                                    float* out);
+
 int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats);
 
 /* The CUDA stream the session enqueues on (a cudaStream_t), for callers that

@@ -1029,6 +1029,18 @@ int vnlbgpu_aggregate(const float* stacks, const float* source, int width, int h
     });
 }
 
+int vnlbgpu_aggregate_frame_noalloc(const float* stacks, const float* source, int width, int height, int frames,
+                                    int channels, int search_bwd, int search_fwd, int patch_time, int device_id, int n,
+                                    float* out) {
+    // no exception and no host allocation on success: the failure text is
+    // copied into the error string only when there is one
+    const char* failure = vnlbgpu::aggregate_frame_noalloc(stacks, source, width, height, frames, channels,
+                                                           search_bwd, search_fwd, patch_time, device_id, n, out);
+    if (!failure) return 0;
+    vnlbgpu::g_last_error = failure;
+    return -1;
+}
+
 int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats) {
     return guarded([&]() {
         if (!session || !stats) vnlbgpu::fail("VNLB CUDA: null argument");

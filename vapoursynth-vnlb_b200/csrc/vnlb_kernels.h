@@ -178,4 +178,12 @@ cudaError_t launch_aggregate_stacks(const AggregateLaunch& L, cudaStream_t strea
 cudaError_t launch_pack_stack(const float* stack, int width, int height, int channels, int slots,
                               float* out, cudaStream_t stream);
 
+// vnlb.Aggregate of output frame n through a fixed device scratch of
+// kNoAllocScratchBytes per device, with no allocation (aggregate_noalloc.cu).
+// Returns null on success, else the failure text.
+constexpr size_t kNoAllocScratchBytes = static_cast<size_t>(32) << 20;
+const char* aggregate_frame_noalloc(const float* stacks, const float* source, int width, int height, int frames,
+                                    int channels, int search_bwd, int search_fwd, int patch_time, int device_id,
+                                    int n, float* out);
+
 }  // namespace vnlbgpu

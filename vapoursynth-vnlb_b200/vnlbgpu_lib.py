@@ -50,7 +50,8 @@ EXPORTS = [
     "vnlbgpu_last_error", "vnlbgpu_create", "vnlbgpu_destroy", "vnlbgpu_set_frame",
     "vnlbgpu_set_clip_host", "vnlbgpu_set_clip_device", "vnlbgpu_render_frame",
     "vnlbgpu_render_clip_host", "vnlbgpu_render_clip_device", "vnlbgpu_synchronize",
-    "vnlbgpu_render_stack", "vnlbgpu_aggregate", "vnlbgpu_get_stats", "vnlbgpu_stream",
+    "vnlbgpu_render_stack", "vnlbgpu_aggregate", "vnlbgpu_aggregate_frame_noalloc", "vnlbgpu_get_stats",
+    "vnlbgpu_stream",
     "vnlbgpu_set_stream", "vnlbgpu_diag_anchor", "vnlbgpu_diag_kernel_timing",
 ]
 KERNEL_CLASSES = ("match", "paste", "filter", "tiles", "normalize")
@@ -86,6 +87,8 @@ def load() -> ctypes.CDLL:
             lib.vnlbgpu_stream.argtypes = [ctypes.c_void_p]
             lib.vnlbgpu_stream.restype = ctypes.c_void_p
             lib.vnlbgpu_aggregate.argtypes = [ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 8 + [ctypes.c_void_p]
+            lib.vnlbgpu_aggregate_frame_noalloc.argtypes = ([ctypes.c_void_p, ctypes.c_void_p] + [ctypes.c_int] * 9
+                                                            + [ctypes.c_void_p])
             lib.vnlbgpu_diag_anchor.argtypes = [
                 ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                 ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
@@ -232,4 +235,19 @@ def aggregate(stacks: np.ndarray, source: np.ndarray, search_bwd: int, search_fw
     out = np.empty_like(source)
     _check(lib.vnlbgpu_aggregate(stacks.ctypes.data, source.ctypes.data, width, height, frames, channels,
                                  search_bwd, search_fwd, patch_time, device_id, out.ctypes.data))
+    return out
+
+
+def aggregate_frame_noalloc(stacks: np.ndarray, source: np.ndarray, n: int, search_bwd: int, search_fwd: int,
+                            patch_time: int, device_id: int = 0) -> np.ndarray:
+    """vnlb.Aggregate of output frame n alone, through the library's fixed
+    device scratch (no device allocation): [planes][H][W]."""
+    lib = load()
+    stacks = _f32(stacks)
+    source = _f32(source)
+    frames, channels, height, width = source.shape
+    out = np.empty((channels, height, width), np.float32)
+    _check(lib.vnlbgpu_aggregate_frame_noalloc(stacks.ctypes.data, source.ctypes.data, width, height, frames,
+                                               channels, search_bwd, search_fwd, patch_time, device_id, n,
+                                               out.ctypes.data))
     return out
