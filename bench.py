@@ -178,19 +178,60 @@ def run_reference(args):
     return 0
 
 
+# --------------------------------------------------------------------------- ranks
+class RankGroup:
+    """The ranks of one job: one process per GPU under torchrun (RANK,
+    WORLD_SIZE, LOCAL_RANK, MASTER_ADDR/MASTER_PORT from the environment).
+    Each rank denoises its own clip (seeded by its rank), so the data path
+    exchanges nothing; the only collectives are the barriers around the timed
+    regions and the max of the timings.  The GPU run uses backend "nccl" with
+    the rank's device; the same code runs with "gloo" on the CPU."""
+
+    def __init__(self, backend: str = "nccl", device=None, timeout_s: float = 300.0):
+        import torch.distributed as dist
+        self.dist = dist
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = device
+        if self.world > 1:
+            from datetime import timedelta
+            kw = {"device_id": device} if device is not None else {}
+            dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s), **kw)
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, value: float) -> float:
+        """The maximum of `value` over the ranks (every rank gets it)."""
+        if self.world == 1:
+            return float(value)
+        import torch
+        t = torch.tensor([float(value)], dtype=torch.float64, device=self.device or "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def whole_job_rate(world: int, frames_per_step: int, steps: int, max_ms: float) -> float:
+    """Frames/s of the whole job: every rank's frames over the slowest rank's time."""
+    return world * frames_per_step * steps / (max_ms / 1e3)
+
+
 # --------------------------------------------------------------------------- GPU path
 def run_ours(args):
     import torch
-    import torch.distributed as dist
     import vnlbgpu_lib as lib
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    ranks = RankGroup("nccl", torch.device("cuda", local))
+    rank, world = ranks.rank, ranks.world
 
     clean, noisy = synth.make_clip(WIDTH, HEIGHT, FRAMES, PLANES, SIGMA, seed=rank)
     clip_bytes = noisy.nbytes
@@ -226,8 +267,7 @@ def run_ours(args):
     groups0 = sb.stats()["groups"] + sf.stats()["groups"]
     sb.kernel_timing(True)
     sf.kernel_timing(True)
-    if world > 1:
-        dist.barrier()
+    ranks.barrier()
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
@@ -242,11 +282,8 @@ def run_ours(args):
     kb, kf = sb.kernel_timing(False), sf.kernel_timing(False)
     launches = sb.stats()["kernel_launches"] + sf.stats()["kernel_launches"] - launches0
     groups = sb.stats()["groups"] + sf.stats()["groups"] - groups0
-    t = torch.tensor([elapsed_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
-    value = world * FRAMES * args.steps / (max_ms / 1e3)
+    max_ms = ranks.max(elapsed_ms)
+    value = whole_job_rate(world, FRAMES, args.steps, max_ms)
 
     # ---- end to end through the C ABI with pinned host buffers
     h_noisy = torch.from_numpy(noisy).pin_memory()
@@ -261,8 +298,7 @@ def run_ours(args):
         sf.render_clip_into(h_final.data_ptr())
 
     e2e_step()
-    if world > 1:
-        dist.barrier()
+    ranks.barrier()
     torch.cuda.synchronize()
     e2e_steps = max(1, min(args.steps, 5))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -271,10 +307,7 @@ def run_ours(args):
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    te = torch.tensor([e0.elapsed_time(e1)], device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * FRAMES * e2e_steps / (float(te.item()) / 1e3)
+    e2e_value = whole_job_rate(world, FRAMES, e2e_steps, ranks.max(e0.elapsed_time(e1)))
     same = bool(torch.equal(h_final, d_final.cpu()))
 
     # ---- roofline of the dominant kernel class
@@ -335,9 +368,7 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     sb.close()
     sf.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     return 0
 
 
