@@ -146,7 +146,23 @@ __device__ __forceinline__ void task_distances(const float* planes, int plane_va
     for (int q = 0; q < planes_n; ++q) {
         const float* plane = planes + q * plane_values + row0 * rs + col0;
         const float* ref_plane = ref + q * PP * PP;
-        if constexpr (P > 0) {
+        if constexpr (P == kLanes) {
+            // packed pairs: half the FP32 instructions, the same bits
+            float2 rv[P * P / 2];
+#pragma unroll
+            for (int i = 0; i < P * P / 2; ++i) rv[i] = make_float2(ref_plane[2 * i], ref_plane[2 * i + 1]);
+#pragma unroll
+            for (int r = 0; r < kKY + P - 1; ++r) {
+                float2 cv[P / 2];
+#pragma unroll
+                for (int i = 0; i < P / 2; ++i) cv[i] = make_float2(plane[r * rs + 2 * i], plane[r * rs + 2 * i + 1]);
+#pragma unroll
+                for (int j = 0; j < kKY; ++j) {
+                    const int y = r - j;
+                    if (y >= 0 && y < P) dist[j] = row_ssd8_x2(dist[j], rv + y * (P / 2), cv);
+                }
+            }
+        } else if constexpr (P > 0) {
             float rv[P * P];
 #pragma unroll
             for (int i = 0; i < P * P; ++i) rv[i] = ref_plane[i];
@@ -178,7 +194,7 @@ __device__ __forceinline__ void task_distances(const float* planes, int plane_va
 }
 
 template <int P>
-__global__ void __launch_bounds__(256) match_kernel(MatchLaunch L) {
+__global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;

@@ -76,6 +76,54 @@ __device__ __forceinline__ float reduce8(const float v[kLanes]) {
     return __fadd_rn(__fadd_rn(a0, a2), __fadd_rn(a1, a3));
 }
 
+// Packed pairs of FP32 (sm_100 add/sub/mul/fma .f32x2): one instruction
+// computes two independent lanes, each rounded exactly as the scalar
+// instruction with the same rounding mode, so a pairwise rewrite of a scalar
+// sequence gives the same bits with half the FP32 instructions.
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+__device__ __forceinline__ float2 sub2_rn(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+__device__ __forceinline__ float2 fma2_rn(float2 a, float2 b, float2 c) {
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rc, {%6, %7};\n\tfma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
+// Packed square d*d, rounded once.  It is fma(d, d, +0), not mul.rn.f32x2:
+// ptxas contracts a mul.rn.f32x2 whose result feeds an add.rn.f32x2 into one
+// fused multiply-add, even with --fmad=false, which changes the bits (every
+// such mismatch measured on sm_100a equalled the fused result).  A square is
+// never -0, so fma(d, d, +0) = round(d*d) exactly, and nothing fuses it.
+__device__ __forceinline__ float2 sqr2_rn(float2 d) { return fma2_rn(d, d, make_float2(0.0f, 0.0f)); }
+
+// row_ssd<8> on packed pairs: ref and cand hold samples (0,1) (2,3) (4,5)
+// (6,7).  The fold ((v0+v4)+(v2+v6)) + ((v1+v5)+(v3+v7)) of reduce8 is two
+// pair adds (a0,a1) (a2,a3), one pair add (a0+a2, a1+a3) and a scalar add.
+__device__ __forceinline__ float row_ssd8_x2(float distance, const float2 ref[4], const float2 cand[4]) {
+    float2 v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        v[i] = sqr2_rn(sub2_rn(ref[i], cand[i]));
+    }
+    const float2 t = add2_rn(add2_rn(v[0], v[2]), add2_rn(v[1], v[3]));
+    return __fadd_rn(distance, __fadd_rn(t.x, t.y));
+}
+
 // add_squared_row_distance_highway: distance + SSD of one patch row of
 // `count` samples, in the pinned order.  `ref` and `cand` may be any
 // addressable memory (registers after unrolling, shared, global).
