@@ -680,6 +680,370 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// apply, warp per group: the same arithmetic as apply_kernel, register-blocked
+// for D % 32 == 0, rank <= 8 and at most 8 model rows (the shapes of the
+// default parameter sets: 8x8 patches, one or three planes, rank 8, group 8).
+//
+// A lane owns columns lane + 32 jj for the elementwise work (centred model
+// rows in registers, basis columns, the reconstruction and its store); for
+// the dot products octet k = lane / 8 runs the pinned 8-lane chains j = lane
+// % 8 over elements j + 8 m of components k and k + 4 at once, on packed
+// pairs: the basis sits in shared memory as float2 (component p, p + 4), so
+// one 8-byte load and one packed fused multiply-add advance both chains.
+// Per warp (floats): basis [4][D] float2, u[D], v[D], dual [8][8],
+// per-component scalars [5][8], scores[max_rows], row bases[max_rows] (size_t).
+constexpr int kWarpApplyWarps = 4;
+
+struct WarpApplyLayout {
+    int basis, u, v, dual, scal, scores, bases, per_warp;
+};
+
+__host__ __device__ inline WarpApplyLayout warp_apply_layout(int D, int max_rows) {
+    WarpApplyLayout w{};
+    int off = 0;
+    w.basis = off;  off += 8 * D;
+    w.u = off;      off += D;
+    w.v = off;      off += D;
+    w.dual = off;   off += 64;
+    w.scal = off;   off += 5 * 8;
+    w.scores = off; off += max_rows;
+    off = (off + 1) & ~1;
+    w.bases = off;  off += 2 * max_rows;
+    off = (off + 3) & ~3;
+    w.per_warp = off;
+    return w;
+}
+
+__device__ __forceinline__ float2 octet_reduce2(float2 v) {
+    // the reduce8 fold of lanes 8k .. 8k+7 into lane 8k, for both halves
+    v.x = __fadd_rn(v.x, __shfl_down_sync(0xffffffffu, v.x, 4, 8));
+    v.y = __fadd_rn(v.y, __shfl_down_sync(0xffffffffu, v.y, 4, 8));
+    v.x = __fadd_rn(v.x, __shfl_down_sync(0xffffffffu, v.x, 2, 8));
+    v.y = __fadd_rn(v.y, __shfl_down_sync(0xffffffffu, v.y, 2, 8));
+    v.x = __fadd_rn(v.x, __shfl_down_sync(0xffffffffu, v.x, 1, 8));
+    v.y = __fadd_rn(v.y, __shfl_down_sync(0xffffffffu, v.y, 1, 8));
+    return v;
+}
+
+__device__ __forceinline__ float octet_reduce(float v) {
+    v = __fadd_rn(v, __shfl_down_sync(0xffffffffu, v, 4, 8));
+    v = __fadd_rn(v, __shfl_down_sync(0xffffffffu, v, 2, 8));
+    v = __fadd_rn(v, __shfl_down_sync(0xffffffffu, v, 1, 8));
+    return v;
+}
+
+template <int D>
+__global__ void __launch_bounds__(32 * kWarpApplyWarps, 6) apply_warp_kernel(FilterLaunch L) {
+    static_assert(D % 32 == 0, "columns are owned in blocks of 32");
+    constexpr int kCols = D / 32;
+    constexpr int kChain = D / 8;
+    extern __shared__ __align__(16) float sm[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int j8 = lane & 7;
+    const int oct = lane >> 3;
+    const WarpApplyLayout lay = warp_apply_layout(D, L.max_rows);
+    int* coloff = reinterpret_cast<int*>(sm);
+    float* wr = sm + D + warp * lay.per_warp;
+    float2* basis2 = reinterpret_cast<float2*>(wr + lay.basis);
+    const float* basis_f = wr + lay.basis;  // component c, column col at ((c & 3) * D + col) * 2 + (c >> 2)
+    float* u = wr + lay.u;
+    float* v = wr + lay.v;
+    float* dual = wr + lay.dual;
+    float* eig = wr + lay.scal;
+    float* coef = eig + 8;
+    float* denom = coef + 8;
+    float* inv_sqrt = denom + 8;
+    float* terms = inv_sqrt + 8;
+    float* scores = wr + lay.scores;
+    size_t* bases = reinterpret_cast<size_t*>(wr + lay.bases);
+    for (int col = threadIdx.x; col < D; col += blockDim.x) coloff[col] = column_offset(L, col);
+
+    const int Bmax = bmax_of(L);
+    const int R = L.rank;
+    const StageConfig& P = L.cfg;
+    const bool final_stage = L.stage == 1;
+    const float* model_video = final_stage ? L.basic : L.noisy;
+    const bool weights_enabled = P.weight_alpha != 0.0f || P.weight_beta != 0.0f || P.weight_gamma != 0.0f;
+    const float sigma2 = __fmul_rn(__fmul_rn(P.beta, P.sigma), P.sigma);
+    const float model_noise2 = final_stage ? __fmul_rn(__fmul_rn(P.beta, P.sigma_basic), P.sigma_basic) : sigma2;
+    const float match_sigma = final_stage ? P.sigma_basic : P.sigma;
+    const float mem2 = std_max(__fmul_rn(match_sigma, match_sigma),
+                               __fmul_rn(__fmul_rn(P.membership_noise_floor, P.sigma), P.sigma));
+    const bool membership_on = P.weight_beta != 0.0f;
+    const bool need_dm = membership_on || !final_stage;
+    const float score_scale = __fsqrt_rn(__fmul_rn(2.0f, static_cast<float>(D)));
+    const int active_count = L.counters->active;
+    __syncthreads();
+
+    for (int a = blockIdx.x * kWarpApplyWarps + warp; a < active_count; a += gridDim.x * kWarpApplyWarps) {
+        if (L.flags[a] != 0) continue;  // equal groups are done, skipped ones reported
+        const int g = L.active[a];
+        const int S = L.row_counts[g];
+        const MatchRow* rows = L.rows + static_cast<size_t>(g) * L.max_rows;
+        const int r0 = L.row_offset[a];
+        const int B = min(S, L.model_cap);
+        const float* gm = L.means + static_cast<size_t>(a) * 2 * D;
+        float mm[kCols], cc[kCols];
+#pragma unroll
+        for (int jj = 0; jj < kCols; ++jj) {
+            mm[jj] = __ldg(gm + lane + 32 * jj);
+            cc[jj] = __ldg(gm + D + lane + 32 * jj);
+        }
+        for (int i = lane; i < S; i += 32) bases[i] = row_base(L, rows[i]);
+        for (int i = lane; i < R * Bmax; i += 32) {
+            const int b = i / Bmax, s = i - b * Bmax;
+            dual[b * 8 + s] = L.dual[static_cast<size_t>(a) * R * Bmax + i];
+        }
+        if (lane < R) {
+            const int c = lane;
+            const float lambda = L.eig[static_cast<size_t>(a) * R + c];
+            eig[c] = lambda;
+            const float diff = __fsub_rn(lambda, model_noise2);
+            const float signal = diff > 0.0f ? diff : 0.0f;
+            denom[c] = __fadd_rn(signal, mem2);
+            inv_sqrt[c] = lambda > kEigenFloor ? __fdiv_rn(1.0f, __fsqrt_rn(lambda)) : 0.0f;
+            terms[c] = (membership_on && signal > 0.0f) ? cr_log1pf(__fdiv_rn(signal, mem2)) : 0.0f;
+            const float sigma_basic2 = final_stage ? model_noise2 : sigma2;
+            const float threshold = __fmul_rn(P.variance_threshold, sigma2);
+            float variance = lambda;
+            if (sigma_basic2 > 0.0f) variance = __fsub_rn(variance, std_min(variance, sigma_basic2));
+            coef[c] = variance > threshold ? __fdiv_rn(1.0f, __fadd_rn(1.0f, __fdiv_rn(sigma2, variance))) : 0.0f;
+        }
+        __syncwarp();
+
+        if (R > 0) {
+            // dual -> primal basis over blocks of this lane's columns: the
+            // centred model rows of the block in registers, then every
+            // component's samples accumulated in order (all columns fused)
+            float* bf = wr + lay.basis;
+            constexpr int kBlk = kCols % 3 == 0 ? 3 : (kCols % 2 == 0 ? 2 : 1);
+#pragma unroll
+            for (int j0 = 0; j0 < kCols; j0 += kBlk) {
+                float xr[8][kBlk];
+#pragma unroll
+                for (int s = 0; s < 8; ++s) {
+                    if (s < B) {
+                        const float* src = model_video + bases[s];
+#pragma unroll
+                        for (int jj = 0; jj < kBlk; ++jj)
+                            xr[s][jj] = __fsub_rn(__ldg(src + coloff[lane + 32 * (j0 + jj)]), mm[j0 + jj]);
+                    } else {
+#pragma unroll
+                        for (int jj = 0; jj < kBlk; ++jj) xr[s][jj] = 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < 8; ++b) {
+                    if (b >= R) break;
+                    const bool live = eig[b] > kEigenFloor;
+                    float acc[kBlk];
+#pragma unroll
+                    for (int jj = 0; jj < kBlk; ++jj) acc[jj] = 0.0f;
+                    if (live) {
+#pragma unroll
+                        for (int s = 0; s < 8; ++s) {
+                            if (s >= B) break;
+                            const float w = dual[b * 8 + s];
+#pragma unroll
+                            for (int jj = 0; jj < kBlk; ++jj) acc[jj] = __fmaf_rn(w, xr[s][jj], acc[jj]);
+                        }
+                        const float is = inv_sqrt[b];
+#pragma unroll
+                        for (int jj = 0; jj < kBlk; ++jj) acc[jj] = __fmul_rn(acc[jj], is);
+                    }
+#pragma unroll
+                    for (int jj = 0; jj < kBlk; ++jj)
+                        bf[((b & 3) * D + lane + 32 * (j0 + jj)) * 2 + (b >> 2)] = acc[jj];
+                }
+            }
+            __syncwarp();
+            // unit norm: octet k normalises components k and k + 4
+            {
+                float2 nv = make_float2(0.0f, 0.0f);
+                const float2* row = basis2 + oct * D;
+#pragma unroll
+                for (int m = 0; m < kChain; ++m) {
+                    const float2 x = row[j8 + 8 * m];
+                    nv = fma2_rn(x, x, nv);
+                }
+                nv = octet_reduce2(nv);
+                const float n0 = __shfl_sync(0xffffffffu, nv.x, oct * 8);
+                const float n1 = __shfl_sync(0xffffffffu, nv.y, oct * 8);
+                const int c0 = oct, c1 = oct + 4;
+                const bool live0 = c0 < R && eig[c0] > kEigenFloor;
+                const bool live1 = c1 < R && eig[c1] > kEigenFloor;
+                const float s0 = live0 && !(n0 <= kEigenFloor) ? __fdiv_rn(1.0f, __fsqrt_rn(n0)) : 0.0f;
+                const float s1 = live1 && !(n1 <= kEigenFloor) ? __fdiv_rn(1.0f, __fsqrt_rn(n1)) : 0.0f;
+                float2* wrow = basis2 + oct * D;
+#pragma unroll
+                for (int m = 0; m < kChain; ++m) {
+                    float2 x = wrow[j8 + 8 * m];
+                    if (live0) x.x = n0 <= kEigenFloor ? 0.0f : __fmul_rn(x.x, s0);
+                    if (live1) x.y = n1 <= kEigenFloor ? 0.0f : __fmul_rn(x.y, s1);
+                    wrow[j8 + 8 * m] = x;
+                }
+            }
+            __syncwarp();
+        }
+        // group precision and volume, component order (every lane, uniform)
+        float lgw, volume;
+        {
+            float trace = 0.0f, vol = 0.0f;
+            for (int c = 0; c < R; ++c) {
+                const float diff = __fsub_rn(eig[c], model_noise2);
+                const float lambda = diff > 0.0f ? diff : 0.0f;
+                if (lambda > 0.0f) {
+                    trace = __fadd_rn(trace, __fdiv_rn(lambda, __fadd_rn(lambda, sigma2)));
+                    vol = __fadd_rn(vol, terms[c]);
+                }
+            }
+            const float tau = __fadd_rn(
+                __fadd_rn(P.weight_epsilon, __fdiv_rn(static_cast<float>(D), static_cast<float>(B))), trace);
+            lgw = P.weight_alpha == 0.0f ? 0.0f : __fmul_rn(-P.weight_alpha, cr_logf(tau));
+            volume = __fdiv_rn(vol, static_cast<float>(D));
+        }
+
+        // rows: membership score and reconstruction; the next row's samples are
+        // loaded while the current one is reduced
+        float min_score = kInf;
+        float nx[kCols], nb[kCols];
+        if (S > 0) {
+#pragma unroll
+            for (int jj = 0; jj < kCols; ++jj) {
+                const size_t off = bases[0] + coloff[lane + 32 * jj];
+                nx[jj] = __ldg(L.noisy + off);
+                nb[jj] = final_stage ? __ldg(L.basic + off) : 0.0f;
+            }
+        }
+        for (int i = 0; i < S; ++i) {
+#pragma unroll
+            for (int jj = 0; jj < kCols; ++jj) {
+                const int col = lane + 32 * jj;
+                if (final_stage) {
+                    u[col] = __fsub_rn(nb[jj], mm[jj]);
+                    v[col] = __fsub_rn(nx[jj], cc[jj]);
+                } else {
+                    u[col] = __fsub_rn(nx[jj], mm[jj]);
+                }
+            }
+            if (i + 1 < S) {
+#pragma unroll
+                for (int jj = 0; jj < kCols; ++jj) {
+                    const size_t off = bases[i + 1] + coloff[lane + 32 * jj];
+                    nx[jj] = __ldg(L.noisy + off);
+                    nb[jj] = final_stage ? __ldg(L.basic + off) : 0.0f;
+                }
+            }
+            __syncwarp();
+            // octet chains: norm of u, u . basis and (Final) v . basis for
+            // components oct and oct + 4
+            float nrm = 0.0f;
+            float2 pm = make_float2(0.0f, 0.0f), pr = make_float2(0.0f, 0.0f);
+            const float2* brow = basis2 + oct * D;
+#pragma unroll 8
+            for (int m = 0; m < kChain; ++m) {
+                const int e = j8 + 8 * m;
+                const float ue = u[e];
+                if (membership_on) nrm = __fmaf_rn(ue, ue, nrm);
+                if (R > 0) {
+                    const float2 bb = brow[e];
+                    if (need_dm) pm = fma2_rn(make_float2(ue, ue), bb, pm);
+                    if (final_stage) {
+                        const float ve = v[e];
+                        pr = fma2_rn(make_float2(ve, ve), bb, pr);
+                    }
+                }
+            }
+            if (membership_on) nrm = octet_reduce(nrm);
+            if (need_dm) pm = octet_reduce2(pm);
+            if (final_stage) pr = octet_reduce2(pr);
+            // lane c < R gathers component c from its octet leader
+            const int src = 8 * (lane & 3);
+            const bool hi = (lane & 4) != 0;
+            float mk = 0.0f, rk = 0.0f;
+            {
+                const float tx = __shfl_sync(0xffffffffu, pm.x, src);
+                const float ty = __shfl_sync(0xffffffffu, pm.y, src);
+                mk = hi ? ty : tx;
+                if (final_stage) {
+                    const float qx = __shfl_sync(0xffffffffu, pr.x, src);
+                    const float qy = __shfl_sync(0xffffffffu, pr.y, src);
+                    rk = hi ? qy : qx;
+                } else {
+                    rk = mk;
+                }
+            }
+            if (membership_on) {
+                const float norm2 = __shfl_sync(0xffffffffu, nrm, 0);
+                const float proj2 = __fmul_rn(mk, mk);
+                const float q = lane < R ? __fdiv_rn(proj2, denom[lane]) : 0.0f;
+                float distance = 0.0f, projected = 0.0f;
+                for (int c = 0; c < R; ++c) {
+                    distance = __fadd_rn(distance, __shfl_sync(0xffffffffu, q, c));
+                    projected = __fadd_rn(projected, __shfl_sync(0xffffffffu, proj2, c));
+                }
+                const float res = __fsub_rn(norm2, projected);
+                distance = __fadd_rn(distance, __fdiv_rn(res > 0.0f ? res : 0.0f, mem2));
+                const float score = __fdiv_rn(__fsub_rn(distance, static_cast<float>(D)), score_scale);
+                if (lane == 0) scores[i] = score;
+                min_score = std_min(min_score, score);
+            }
+            // reconstruction (project_bayes_estimate), components in order
+            const float scaled = lane < R ? __fmul_rn(coef[lane], rk) : 0.0f;
+            float o[kCols];
+#pragma unroll
+            for (int jj = 0; jj < kCols; ++jj) o[jj] = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                if (c >= R) break;
+                const float sc = __shfl_sync(0xffffffffu, scaled, c);
+                if (coef[c] == 0.0f) continue;
+#pragma unroll
+                for (int jj = 0; jj < kCols; ++jj)
+                    o[jj] = __fmaf_rn(sc, basis_f[((c & 3) * D + lane + 32 * jj) * 2 + (c >> 2)], o[jj]);
+            }
+            float* out = L.filtered + static_cast<size_t>(r0 + i) * D;
+#pragma unroll
+            for (int jj = 0; jj < kCols; ++jj) out[lane + 32 * jj] = __fadd_rn(o[jj], cc[jj]);
+            __syncwarp();
+        }
+        // aggregation weights (accumulate_aggregation_model + finalize)
+        for (int i = lane; i < S; i += 32) {
+            float w = 1.0f;
+            if (weights_enabled) {
+                float lw;
+                if (P.weight_alpha == 0.0f && P.weight_beta == 0.0f) {
+                    lw = 0.0f;
+                } else if (membership_on) {
+                    const float diff = __fsub_rn(scores[i], min_score);
+                    const float membership = __fadd_rn(diff > 0.0f ? diff : 0.0f, volume);
+                    lw = __fadd_rn(0.0f, __fsub_rn(lgw, __fmul_rn(P.weight_beta, membership)));
+                } else {
+                    lw = __fadd_rn(0.0f, lgw);
+                }
+                lw = lw < -80.0f ? -80.0f : (80.0f < lw ? 80.0f : lw);
+                w = cr_expf(lw);
+            }
+            L.weights[r0 + i] = w;
+        }
+        __syncwarp();
+    }
+}
+
+template <int D>
+cudaError_t launch_apply_warp(const FilterLaunch& L, int max_groups, cudaStream_t stream) {
+    const WarpApplyLayout lay = warp_apply_layout(D, L.max_rows);
+    const size_t smem = (static_cast<size_t>(D) + static_cast<size_t>(kWarpApplyWarps) * lay.per_warp) * sizeof(float);
+    cudaError_t err = cudaFuncSetAttribute(apply_warp_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           static_cast<int>(smem));
+    if (err != cudaSuccess) return err;
+    const int ctas = std::max(1, std::min((max_groups + kWarpApplyWarps - 1) / kWarpApplyWarps, 148 * 8));
+    apply_warp_kernel<D><<<ctas, 32 * kWarpApplyWarps, smem, stream>>>(L);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t stream) {
@@ -717,7 +1081,13 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t st
         if ((err = cudaGetLastError()) != cudaSuccess) return err;
     }
     // apply
-    {
+    if (R <= 8 && Bmax <= 8 && (D == 64 || D == 128 || D == 192 || D == 256)) {
+        cudaError_t err = D == 64    ? launch_apply_warp<64>(L, max_groups, stream)
+                          : D == 128 ? launch_apply_warp<128>(L, max_groups, stream)
+                          : D == 192 ? launch_apply_warp<192>(L, max_groups, stream)
+                                     : launch_apply_warp<256>(L, max_groups, stream);
+        if (err != cudaSuccess) return err;
+    } else {
         const ApplyLayout lay = apply_layout(D, Bmax, R, L.max_rows, kApplyWarps);
         const size_t smem = lay.bytes;
         cudaError_t err = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
