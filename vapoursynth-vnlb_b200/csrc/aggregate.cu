@@ -155,6 +155,149 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(TileLaunch L) {
     }
 }
 
+// patch_time 1: a covering row lands in exactly one slot (its frame offset
+// from the anchor frame), so one CTA per tile scans the candidate rows once
+// for all slots (at most kMaxTileSlots) and keeps one accumulator set per
+// slot.  Each (pixel, slot) still sees its rows in increasing global row
+// order: the same sums as tile_kernel.
+constexpr int kMaxTileSlots = 4;
+
+__global__ void __launch_bounds__(kTileThreads) tile_slots_kernel(TileLaunch L) {
+    __shared__ Entry entries[kTileThreads];
+    __shared__ int s_rbeg[kMaxGridRows];
+    __shared__ int s_rpre[kMaxGridRows + 1];
+    __shared__ int s_warp[kTileWarps + 1];
+    extern __shared__ float window[];
+
+    const int tx = blockIdx.x, ty = blockIdx.y;
+    const int tx0 = tx * kTile, ty0 = ty * kTile;
+    const int P = L.P;
+    const int C = L.channels;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+    for (int i = tid; i < P * P; i += blockDim.x) window[i] = L.window[i];
+
+    const int px = tx0 + (tid % kTile);
+    const int py = ty0 + (tid / kTile);
+    float num[kMaxTileSlots][4];
+    float wt[kMaxTileSlots];
+#pragma unroll
+    for (int s = 0; s < kMaxTileSlots; ++s) {
+        wt[s] = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) num[s][c] = 0.0f;
+    }
+    const int fused_cols = (P == kLanes || P == 2 * kLanes) ? P : (P / kLanes) * kLanes;
+    const int2 grid_rows = L.tile_grid_rows[ty];
+    const int slot_base = L.search_bwd - L.anchor_frame;  // slot = frame + slot_base
+
+    for (int k0 = grid_rows.x; k0 < grid_rows.y; k0 += kMaxGridRows) {
+        const int nk = min(kMaxGridRows, grid_rows.y - k0);
+        __syncthreads();
+        if (tid < nk) {
+            const int2 anchors = L.tile_anchors[static_cast<size_t>(k0 + tid) * L.tiles_x + tx];
+            const int rb = L.row_offset[L.active_prefix[anchors.x]];
+            const int re = L.row_offset[L.active_prefix[anchors.y]];
+            s_rbeg[tid] = rb;
+            s_rpre[tid + 1] = re - rb;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            s_rpre[0] = 0;
+            for (int k = 1; k <= nk; ++k) s_rpre[k] += s_rpre[k - 1];
+        }
+        __syncthreads();
+        const int total = s_rpre[nk];
+        for (int chunk = 0; chunk < total; chunk += kTileThreads) {
+            const int vrow = chunk + tid;
+            bool hit = false;
+            Entry en;
+            if (vrow < total) {
+                int lo = 0, hi = nk - 1;  // last k with s_rpre[k] <= vrow
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_rpre[mid] <= vrow) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int r = s_rbeg[lo] + (vrow - s_rpre[lo]);
+                const MatchRow m = L.row_info[r];
+                if (m.x <= tx0 + kTile - 1 && m.x + P - 1 >= tx0 && m.y <= ty0 + kTile - 1 && m.y + P - 1 >= ty0) {
+                    const int slot = m.frame + slot_base;
+                    if (slot >= 0 && slot < L.slots) {
+                        hit = true;
+                        en.r = r;
+                        en.xyt = m.x | (m.y << 14) | (slot << 28);
+                        en.w = L.weights[r];
+                    }
+                }
+            }
+            const unsigned ballot = __ballot_sync(0xffffffffu, hit);
+            if (lane == 0) s_warp[warp + 1] = __popc(ballot);
+            __syncthreads();
+            if (tid == 0) {
+                s_warp[0] = 0;
+                for (int w = 1; w <= kTileWarps; ++w) s_warp[w] += s_warp[w - 1];
+            }
+            __syncthreads();
+            if (hit) entries[s_warp[warp] + __popc(ballot & ((1u << lane) - 1u))] = en;
+            const int n = s_warp[kTileWarps];
+            __syncthreads();
+            for (int e = 0; e < n; ++e) {
+                const Entry x = entries[e];
+                const unsigned dx = static_cast<unsigned>(px - (x.xyt & 0x3fff));
+                const unsigned dy = static_cast<unsigned>(py - ((x.xyt >> 14) & 0x3fff));
+                if (dx >= static_cast<unsigned>(P) || dy >= static_cast<unsigned>(P)) continue;
+                const int slot = x.xyt >> 28;
+                const int pos = static_cast<int>(dy) * P + static_cast<int>(dx);
+                const float* f = L.filtered + static_cast<size_t>(x.r) * L.dim + pos;
+                float val[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) val[c] = c < C ? __ldg(f + c * L.patch_dim) : 0.0f;
+                if (L.coupled && !L.windowed) {
+                    const bool fused = static_cast<int>(dx) < fused_cols;
+#pragma unroll
+                    for (int s = 0; s < kMaxTileSlots; ++s) {
+                        if (s != slot) continue;
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            if (c >= C) break;
+                            num[s][c] = fused ? __fmaf_rn(x.w, val[c], num[s][c])
+                                              : __fadd_rn(num[s][c], __fmul_rn(x.w, val[c]));
+                        }
+                        wt[s] = __fadd_rn(wt[s], x.w);
+                    }
+                } else {
+                    const float cw = __fmul_rn(x.w, window[dy * P + dx]);
+#pragma unroll
+                    for (int s = 0; s < kMaxTileSlots; ++s) {
+                        if (s != slot) continue;
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            if (c >= C) break;
+                            num[s][c] = __fadd_rn(num[s][c], __fmul_rn(cw, val[c]));
+                        }
+                        wt[s] = __fadd_rn(wt[s], cw);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (px < L.width && py < L.height) {
+        const size_t plane = static_cast<size_t>(L.width) * L.height;
+#pragma unroll
+        for (int s = 0; s < kMaxTileSlots; ++s) {
+            if (s >= L.slots) break;
+            float* base = L.stack + static_cast<size_t>(s) * (C + 1) * plane + static_cast<size_t>(py) * L.width + px;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (c < C) base[c * plane] = num[s][c];
+            base[C * plane] = wt[s];
+        }
+    }
+}
+
 __global__ void normalize_kernel(NormalizeLaunch L) {
     const size_t plane = static_cast<size_t>(L.width) * L.height;
     const int C = L.channels;
@@ -217,9 +360,13 @@ cudaError_t launch_aggregate_stacks(const AggregateLaunch& L, cudaStream_t strea
 
 cudaError_t launch_tiles(const TileLaunch& L, cudaStream_t stream) {
     if (L.channels > 4 || L.width >= (1 << 14) || L.height >= (1 << 14) || L.Pt > 7) return cudaErrorInvalidValue;
-    const dim3 grid(L.tiles_x, L.tiles_y, L.slots);
     const size_t smem = static_cast<size_t>(L.P) * L.P * sizeof(float);
-    tile_kernel<<<grid, kTileThreads, smem, stream>>>(L);
+    if (L.Pt == 1 && L.slots <= kMaxTileSlots) {
+        tile_slots_kernel<<<dim3(L.tiles_x, L.tiles_y, 1), kTileThreads, smem, stream>>>(L);
+    } else {
+        const dim3 grid(L.tiles_x, L.tiles_y, L.slots);
+        tile_kernel<<<grid, kTileThreads, smem, stream>>>(L);
+    }
     return cudaGetLastError();
 }
 
