@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
     const int Bmax = bmax_of(L);
     int* coloff = reinterpret_cast<int*>(sm);
     size_t* bases_all = reinterpret_cast<size_t*>(sm + ((D + 3) & ~3));  // kPrepareWarps * max_rows
-    const int ldx = D + 1;  // padded row stride: lanes on different rows hit different banks
+    const int ldx = D + 8;  // padded row stride: octets on different rows hit different banks
     float* X = reinterpret_cast<float*>(bases_all + kPrepareWarps * L.max_rows) +
                (threadIdx.x >> 5) * Bmax * ldx;  // this warp's model rows
     size_t* bases = bases_all + (threadIdx.x >> 5) * L.max_rows;
@@ -247,13 +247,19 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
             const float scale = __fdiv_rn(1.0f, static_cast<float>(B));
             float* gram = L.gram + static_cast<size_t>(a) * Bmax * Bmax;
             const int pairs = B * (B + 1) / 2;
-            for (int e = lane; e < pairs; e += 32) {
+            // octet k takes pair e0 + k; lane j of the octet runs the pinned
+            // chain j (octet_dot8: the same sums as thread_dot8)
+            const int oct = lane >> 3;
+            for (int e0 = 0; e0 < pairs; e0 += 4) {
+                const int e = min(e0 + oct, pairs - 1);
                 int r = 0;
                 while ((r + 1) * (r + 2) / 2 <= e) ++r;
                 const int c = e - r * (r + 1) / 2;
-                const float v = __fmul_rn(scale, thread_dot8(X + r * ldx, X + c * ldx, D));
-                gram[r * B + c] = v;
-                gram[c * B + r] = v;
+                const float v = __fmul_rn(scale, octet_dot8(X + r * ldx, X + c * ldx, D, lane & 7));
+                if ((lane & 7) == 0 && e0 + oct < pairs) {
+                    gram[r * B + c] = v;
+                    gram[c * B + r] = v;
+                }
             }
         }
         if (lane == 0) L.flags[a] = 0;
@@ -265,7 +271,7 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
 // jacobi: topk_symmetric_eigen_jacobi (linalg.cpp:447-519) for many groups per
 // warp.  A group owns a segment of `seg` lanes (a power of two >= its rows,
 // at most 32); lane r of the segment owns matrix rows r, r + seg, ...
-__global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg) {
+__global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg, int ld, int gstride) {
     extern __shared__ __align__(16) float sm[];
     const int Bmax = bmax_of(L);
     const int R = L.rank;
@@ -274,9 +280,9 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg) {
     const int slot = (threadIdx.x >> 5) * groups_per_warp + lane / seg;  // group slot in the CTA
     const int r0 = lane % seg;
     const unsigned seg_mask = seg == 32 ? 0xffffffffu : (((1u << seg) - 1u) << ((lane / seg) * seg));
-    float* m = sm + static_cast<size_t>(slot) * (2 * Bmax * Bmax + Bmax);
-    float* v = m + Bmax * Bmax;
-    int* order = reinterpret_cast<int*>(v + Bmax * Bmax);
+    float* m = sm + static_cast<size_t>(slot) * gstride;
+    float* v = m + Bmax * ld;
+    int* order = reinterpret_cast<int*>(v + Bmax * ld);
     const int active_count = L.counters->active;
     const int slots_per_cta = (blockDim.x >> 5) * groups_per_warp;
     for (int base = blockIdx.x * slots_per_cta; base < active_count; base += gridDim.x * slots_per_cta) {
@@ -293,8 +299,8 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg) {
         for (int r = r0; r < B; r += seg) {
             for (int c = 0; c < B; ++c) {
                 const float x = gram[r * B + c];
-                m[r * Bmax + c] = x;
-                v[r * Bmax + c] = r == c ? 1.0f : 0.0f;
+                m[r * ld + c] = x;
+                v[r * ld + c] = r == c ? 1.0f : 0.0f;
                 mx = std_max(mx, fabsf(x));
             }
         }
@@ -305,7 +311,7 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg) {
             for (int sweep = 0; sweep < 64; ++sweep) {
                 float off = 0.0f;
                 for (int r = r0; r < B; r += seg)
-                    for (int c = r + 1; c < B; ++c) off = std_max(off, fabsf(m[r * Bmax + c]));
+                    for (int c = r + 1; c < B; ++c) off = std_max(off, fabsf(m[r * ld + c]));
                 for (int o = seg / 2; o > 0; o >>= 1) off = fmaxf(off, __shfl_xor_sync(0xffffffffu, off, o));
                 const bool busy = B > 1 && !(off <= threshold);
                 if (!__any_sync(0xffffffffu, busy)) break;
@@ -314,11 +320,11 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg) {
                         bool rot = false;
                         float app = 0.0f, aqq = 0.0f, apq = 0.0f;
                         if (busy && q < B) {
-                            apq = m[p * Bmax + q];
+                            apq = m[p * ld + q];
                             rot = fabsf(apq) > threshold && apq != 0.0f;
                             if (rot) {
-                                app = m[p * Bmax + p];
-                                aqq = m[q * Bmax + q];
+                                app = m[p * ld + p];
+                                aqq = m[q * ld + q];
                             }
                         }
                         __syncwarp();
@@ -333,29 +339,29 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg) {
                             const float s = __fmul_rn(t, c);
                             for (int r = r0; r < B; r += seg) {
                                 if (r != p && r != q) {
-                                    const float arp = m[r * Bmax + p];
-                                    const float arq = m[r * Bmax + q];
+                                    const float arp = m[r * ld + p];
+                                    const float arq = m[r * ld + q];
                                     const float nrp = __fsub_rn(__fmul_rn(c, arp), __fmul_rn(s, arq));
                                     const float nrq = __fadd_rn(__fmul_rn(s, arp), __fmul_rn(c, arq));
-                                    m[r * Bmax + p] = nrp;
-                                    m[p * Bmax + r] = nrp;
-                                    m[r * Bmax + q] = nrq;
-                                    m[q * Bmax + r] = nrq;
+                                    m[r * ld + p] = nrp;
+                                    m[p * ld + r] = nrp;
+                                    m[r * ld + q] = nrq;
+                                    m[q * ld + r] = nrq;
                                 }
-                                const float vrp = v[r * Bmax + p];
-                                const float vrq = v[r * Bmax + q];
-                                v[r * Bmax + p] = __fsub_rn(__fmul_rn(c, vrp), __fmul_rn(s, vrq));
-                                v[r * Bmax + q] = __fadd_rn(__fmul_rn(s, vrp), __fmul_rn(c, vrq));
+                                const float vrp = v[r * ld + p];
+                                const float vrq = v[r * ld + q];
+                                v[r * ld + p] = __fsub_rn(__fmul_rn(c, vrp), __fmul_rn(s, vrq));
+                                v[r * ld + q] = __fadd_rn(__fmul_rn(s, vrp), __fmul_rn(c, vrq));
                                 const float cc = __fmul_rn(c, c), ss = __fmul_rn(s, s);
                                 const float cs2 = __fmul_rn(2.0f, __fmul_rn(c, s));
                                 if (r == p) {
-                                    m[p * Bmax + p] = __fadd_rn(__fsub_rn(__fmul_rn(cc, app), __fmul_rn(cs2, apq)),
+                                    m[p * ld + p] = __fadd_rn(__fsub_rn(__fmul_rn(cc, app), __fmul_rn(cs2, apq)),
                                                                 __fmul_rn(ss, aqq));
-                                    m[p * Bmax + q] = 0.0f;
+                                    m[p * ld + q] = 0.0f;
                                 } else if (r == q) {
-                                    m[q * Bmax + q] = __fadd_rn(__fadd_rn(__fmul_rn(ss, app), __fmul_rn(cs2, apq)),
+                                    m[q * ld + q] = __fadd_rn(__fadd_rn(__fmul_rn(ss, app), __fmul_rn(cs2, apq)),
                                                                 __fmul_rn(cc, aqq));
-                                    m[q * Bmax + p] = 0.0f;
+                                    m[q * ld + p] = 0.0f;
                                 }
                             }
                         }
@@ -367,10 +373,10 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg) {
         // stable sort of the diagonal (descending), canonicalised top-rank
         // eigenvectors (canonicalize_vector_row, linalg.cpp:198-227)
         for (int r = r0; r < B; r += seg) {
-            const float dr = m[r * Bmax + r];
+            const float dr = m[r * ld + r];
             int pos = 0;
             for (int j = 0; j < B; ++j) {
-                const float dj = m[j * Bmax + j];
+                const float dj = m[j * ld + j];
                 if (dj > dr || (j < r && !(dr > dj))) ++pos;
             }
             order[pos] = r;
@@ -381,11 +387,11 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg) {
             float* dual = L.dual + static_cast<size_t>(a) * R * Bmax;
             for (int out = r0; out < R; out += seg) {
                 const int src = order[out];
-                eig[out] = m[src * Bmax + src];
+                eig[out] = m[src * ld + src];
                 float norm2 = 0.0f, best = 0.0f;
                 int pivot = 0;
                 for (int r = 0; r < B; ++r) {
-                    const float x = v[r * Bmax + src];
+                    const float x = v[r * ld + src];
                     norm2 = __fadd_rn(norm2, __fmul_rn(x, x));
                     const float ax = fabsf(x);
                     if (ax > best) {
@@ -397,10 +403,10 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg) {
                 const bool scale = !(norm2 <= FLT_MIN);
                 if (scale) {
                     sc = __fdiv_rn(1.0f, __fsqrt_rn(norm2));
-                    if (v[pivot * Bmax + src] < 0.0f) sc = -sc;
+                    if (v[pivot * ld + src] < 0.0f) sc = -sc;
                 }
                 for (int r = 0; r < B; ++r) {
-                    const float x = v[r * Bmax + src];
+                    const float x = v[r * ld + src];
                     dual[out * Bmax + r] = scale ? __fmul_rn(x, sc) : x;
                 }
             }
@@ -1054,7 +1060,7 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t st
     const size_t colpad = static_cast<size_t>((D + 3) & ~3);
     // prepare
     {
-        const size_t smem = (colpad + static_cast<size_t>(kPrepareWarps) * Bmax * (D + 1)) * sizeof(float) +
+        const size_t smem = (colpad + static_cast<size_t>(kPrepareWarps) * Bmax * (D + 8)) * sizeof(float) +
                             static_cast<size_t>(kPrepareWarps) * L.max_rows * sizeof(size_t);
         cudaError_t err = cudaFuncSetAttribute(prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
@@ -1065,10 +1071,20 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t st
     }
     // jacobi
     if (R > 0) {
+        // a segment of `seg` lanes per group, each lane owning rows r0, r0 + seg,
+        // ...; two rows per lane from 8 rows up, which halves the rotation
+        // parameters every lane recomputes
         int seg = 1;
         while (seg < Bmax && seg < 32) seg <<= 1;
+        if (seg >= 8) seg /= 2;
         seg = std::max(seg, 1);
-        const size_t per_group = static_cast<size_t>(2 * Bmax * Bmax + Bmax) * sizeof(float);
+        // rows padded to Bmax + 1 and groups to gstride floats: for Bmax = 8
+        // (segments of 4, 8 groups per warp, gstride = 4 mod 32) the lanes of
+        // a warp touch 32 distinct banks
+        const int ld = Bmax + 1;
+        int gstride = 2 * Bmax * ld + Bmax;
+        if (seg == 4) gstride += ((4 - gstride % 32) + 32) % 32;
+        const size_t per_group = static_cast<size_t>(gstride) * sizeof(float);
         int warps = 8;
         while (warps > 1 && static_cast<size_t>(warps) * (32 / seg) * per_group > 160 * 1024) warps /= 2;
         const size_t smem = static_cast<size_t>(warps) * (32 / seg) * per_group;
@@ -1077,7 +1093,7 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t st
         if (err != cudaSuccess) return err;
         const int per_cta = warps * (32 / seg);
         const int ctas = std::max(1, std::min((max_groups + per_cta - 1) / per_cta, 148 * 32));
-        jacobi_kernel<<<ctas, 32 * warps, smem, stream>>>(L, seg);
+        jacobi_kernel<<<ctas, 32 * warps, smem, stream>>>(L, seg, ld, gstride);
         if ((err = cudaGetLastError()) != cudaSuccess) return err;
     }
     // apply
