@@ -31,15 +31,21 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
+def build(verbose: bool = False, ptxas_info: bool = False, out: Path | None = None,
+          defines: tuple[str, ...] = ()) -> Path:
+    """Compiles the library to `out` (default lib/libvnlbgpu.so); `defines`
+    are extra -D macros for a variant build."""
+    lib = Path(out) if out else LIB
+    lib.parent.mkdir(parents=True, exist_ok=True)
     LIB_DIR.mkdir(exist_ok=True)
     objs = []
     common = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off",
                      "-I", str(PKG.parent / "include")]
     if ptxas_info:
         common += ["-Xptxas", "-v"]
-    build_dir = PKG / "_build"
-    build_dir.mkdir(exist_ok=True)
+    common += [f"-D{d}" for d in defines]
+    build_dir = PKG / "_build" / ("variant_" + lib.stem if out else "default")
+    build_dir.mkdir(parents=True, exist_ok=True)
     for src in SOURCES:
         obj = build_dir / (Path(src).stem + ".o")
         cmd = [nvcc(), "-c", str(CSRC / src), "-o", str(obj)] + common
@@ -49,9 +55,9 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
         objs.append(str(obj))
-    cmd = [nvcc(), "-shared", "-o", str(LIB)] + ARCH + [*objs, "-cudart", "static"]
+    cmd = [nvcc(), "-shared", "-o", str(lib)] + ARCH + [*objs, "-cudart", "static"]
     subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

@@ -42,32 +42,8 @@ constexpr int kRecCols = 8;  // reconstruction columns held in registers per lan
 constexpr int kPrepareWarps = 4;
 constexpr float kEigenFloor = 128.0f * FLT_EPSILON;
 
-// dot_contiguous_highway, one thread.
-__device__ float thread_dot8(const float* l, const float* r, int count) {
-    float v[kLanes];
-    if (count == kLanes || count == 2 * kLanes) {
-#pragma unroll
-        for (int i = 0; i < kLanes; ++i) v[i] = __fmul_rn(l[i], r[i]);
-        if (count == 2 * kLanes) {
-#pragma unroll
-            for (int i = 0; i < kLanes; ++i) v[i] = __fmaf_rn(l[i + kLanes], r[i + kLanes], v[i]);
-        }
-        return reduce8(v);
-    }
-#pragma unroll
-    for (int i = 0; i < kLanes; ++i) v[i] = 0.0f;
-    int index = 0;
-    for (; index + kLanes <= count; index += kLanes) {
-#pragma unroll
-        for (int i = 0; i < kLanes; ++i) v[i] = __fmaf_rn(l[index + i], r[index + i], v[i]);
-    }
-    float total = reduce8(v);
-    for (; index < count; ++index) total = __fadd_rn(total, __fmul_rn(l[index], r[index]));
-    return total;
-}
-
-// dot_contiguous_highway computed by an octet of lanes (j = lane & 7): lane j
-// owns accumulator j; the fold follows reduce8.  All 8 lanes return the dot.
+// dot_contiguous_highway (the pinned 8-lane order) computed by an octet of
+// lanes (j = lane & 7): lane j owns accumulator j; the fold follows reduce8.  All 8 lanes return the dot.
 // Every lane of the warp must call it.
 __device__ __forceinline__ float octet_dot8(const float* l, const float* r, int count, int j) {
     float v = 0.0f;
@@ -248,7 +224,7 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
             float* gram = L.gram + static_cast<size_t>(a) * Bmax * Bmax;
             const int pairs = B * (B + 1) / 2;
             // octet k takes pair e0 + k; lane j of the octet runs the pinned
-            // chain j (octet_dot8: the same sums as thread_dot8)
+            // chain j (octet_dot8: the pinned 8-lane order)
             const int oct = lane >> 3;
             for (int e0 = 0; e0 < pairs; e0 += 4) {
                 const int e = min(e0 + oct, pairs - 1);
@@ -739,8 +715,14 @@ __device__ __forceinline__ float octet_reduce(float v) {
     return v;
 }
 
+// resident blocks per SM the warp-per-group apply is compiled for (a register
+// budget); a build parameter for comparisons
+#ifndef VNLB_APPLY_MIN_BLOCKS
+#define VNLB_APPLY_MIN_BLOCKS 4
+#endif
+
 template <int D>
-__global__ void __launch_bounds__(32 * kWarpApplyWarps, 6) apply_warp_kernel(FilterLaunch L) {
+__global__ void __launch_bounds__(32 * kWarpApplyWarps, VNLB_APPLY_MIN_BLOCKS) apply_warp_kernel(FilterLaunch L) {
     static_assert(D % 32 == 0, "columns are owned in blocks of 32");
     constexpr int kCols = D / 32;
     constexpr int kChain = D / 8;

@@ -410,8 +410,58 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
         __syncwarp();
     }
     if (!active_warp) return;
+    int S = 0;
+    bool selected_in_warp = false;
     if (fast) {
-        if (lane < s.count) {
+        // select_similar_patches with pairwise distinct buffered distances:
+        // the heap replay below has a unique outcome, computed warp-wide.
+        // partial_sort(first, first + M, first + n) keeps in [0, M) the M
+        // smallest in ascending order; tail slot i (M <= i < n) ends up with
+        // the heap's maximum at the time element i arrived when that element
+        // is smaller (it is swapped in), else with the element itself.
+        const int n = s.count;
+        const unsigned key = lane < n ? reg_d : (0x80000000u | static_cast<unsigned>(lane));
+        const bool tie = __any_sync(0xffffffffu, __popc(__match_any_sync(0xffffffffu, key)) > 1);
+        if (K > 1 && !tie) {
+            const int M = min(K, n);
+            unsigned d = reg_d;
+            int id = reg_id;
+            unsigned cur_max = __reduce_max_sync(0xffffffffu, lane < M ? d : 0u);
+            for (int i = M; i < n; ++i) {
+                const unsigned di = __shfl_sync(0xffffffffu, d, i);
+                const int ii = __shfl_sync(0xffffffffu, id, i);
+                if (di < cur_max) {
+                    const int o = __ffs(__ballot_sync(0xffffffffu, lane < M && d == cur_max)) - 1;
+                    const int oi = __shfl_sync(0xffffffffu, id, o);
+                    if (lane == o) {
+                        d = di;
+                        id = ii;
+                    }
+                    if (lane == i) {
+                        d = cur_max;
+                        id = oi;
+                    }
+                    cur_max = __reduce_max_sync(0xffffffffu, lane < M ? d : 0u);
+                }
+            }
+            // the kept M ascending (distinct: rank = number of smaller ones),
+            // then the tail slots within the threshold, in slot order
+            const float threshold = std_max(L.tau, __uint_as_float(cur_max));
+            int rank = 0;
+            for (int j = 0; j < M; ++j) rank += __shfl_sync(0xffffffffu, d, j) < d ? 1 : 0;
+            const bool keep_tail = lane >= M && lane < n && __uint_as_float(d) <= threshold;
+            const unsigned tail_mask = __ballot_sync(0xffffffffu, keep_tail);
+            if (lane < M) {
+                buf_d[rank] = __uint_as_float(d);
+                buf_i[rank] = id;
+            } else if (keep_tail) {
+                const int pos = M + __popc(tail_mask & ((1u << lane) - 1u));
+                buf_d[pos] = __uint_as_float(d);
+                buf_i[pos] = id;
+            }
+            S = M + __popc(tail_mask);
+            selected_in_warp = true;
+        } else if (lane < n) {
             buf_d[lane] = __uint_as_float(reg_d);
             buf_i[lane] = reg_id;
         }
@@ -419,8 +469,7 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     }
 
     // select_similar_patches (core.cpp:1200-1243): single lane.
-    int S = 0;
-    if (lane == 0) {
+    if (!selected_in_warp && lane == 0) {
         const int n = s.count;
         if (K <= 1) {
             // similar <= 1: the anchor itself (core.cpp:1253-1257)
@@ -446,7 +495,7 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
             S = out;
         }
     }
-    S = __shfl_sync(0xffffffffu, S, 0);
+    if (!selected_in_warp) S = __shfl_sync(0xffffffffu, S, 0);
     __syncwarp();
     MatchRow* rows_out = L.rows + static_cast<size_t>(g) * L.max_rows;
     int nvict = 0;

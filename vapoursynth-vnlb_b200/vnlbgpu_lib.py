@@ -6,12 +6,15 @@ if the library is missing or no CUDA device is usable, every call raises.
 from __future__ import annotations
 
 import ctypes
+import os
 import threading
 from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libvnlbgpu.so"
+# VNLBGPU_LIBRARY names another build of the same library (a variant built for
+# a comparison); unset, the in-tree build is loaded.
+LIB_PATH = Path(os.environ.get("VNLBGPU_LIBRARY") or Path(__file__).resolve().parent / "lib" / "libvnlbgpu.so")
 
 STAGE_BASIC, STAGE_FINAL = 0, 1
 SOURCE_CLIP, SOURCE_REF = 0, 1
