@@ -156,6 +156,35 @@ def test_random_access_and_threads():
         assert np.array_equal(results[n], whole[n])
 
 
+def test_pinned_host_pipeline_matches_pageable():
+    """Pinned host clips go up frame by frame on an upload stream and pinned
+    outputs come down frame by frame while later anchor frames compute; the
+    result must equal the pageable path (whole-clip copies) bit for bit, for
+    Basic and for Final reading both sources, and again after re-uploading."""
+    import torch
+
+    _, noisy = synth.make_clip(96, 64, 7, 3, 20.0, seed=61)
+    p = O.cpu_params(O.BASIC, 20.0, radius=2, patch_time=2, group_size=12, rank=10)
+    pf = O.cpu_params(O.FINAL, 20.0, radius=2, patch_time=2, group_size=12, rank=10, tau=400.0)
+    sb = session_for(lib.STAGE_BASIC, p, noisy)
+    want_b = sb.render_clip()
+    sf = session_for(lib.STAGE_FINAL, pf, noisy, want_b)
+    want_f = sf.render_clip()
+    h_noisy = torch.from_numpy(noisy).pin_memory()
+    h_basic = torch.empty_like(h_noisy).pin_memory()
+    h_final = torch.empty_like(h_noisy).pin_memory()
+    for _ in range(2):
+        sb.set_clip_ptr(lib.SOURCE_CLIP, h_noisy.data_ptr())
+        sb.render_clip_into(h_basic.data_ptr())
+        sf.set_clip_ptr(lib.SOURCE_CLIP, h_noisy.data_ptr())
+        sf.set_clip_ptr(lib.SOURCE_REF, h_basic.data_ptr())
+        sf.render_clip_into(h_final.data_ptr())
+        assert np.array_equal(bits(h_basic.numpy()), bits(want_b))
+        assert np.array_equal(bits(h_final.numpy()), bits(want_f))
+    sb.close()
+    sf.close()
+
+
 def test_aggregate_matches_oracle():
     _, noisy = synth.make_clip(48, 40, 4, 3, 20.0, seed=51)
     p = O.cpu_params(O.BASIC, 20.0, radius=2, patch_time=2, group_size=12, rank=10)

@@ -190,6 +190,18 @@ struct Session {
     cudaEvent_t ev_fork = nullptr;     // main-stream point the lanes start after
     cudaEvent_t ev_lane[kLaneCount] = {nullptr, nullptr};
 
+    // Host transfers run on their own streams so that they overlap the
+    // kernels: each uploaded frame records frame_ready[source][frame], and an
+    // anchor frame's lane waits only for the frames it reads; each output
+    // frame of a whole-clip host render is downloaded as soon as it is
+    // normalised.
+    cudaStream_t upload_stream = nullptr, download_stream = nullptr;
+    cudaEvent_t ev_main = nullptr;      // main-stream point a copy stream starts after
+    cudaEvent_t ev_out = nullptr;       // an output frame is normalised
+    cudaEvent_t ev_download = nullptr;  // the downloads are done
+    std::vector<cudaEvent_t> frame_ready[2];
+    bool frames_async[2] = {false, false};  // the source's frames came through upload_stream
+
     DeviceArray<unsigned long long> d_totals;
     DeviceArray<int> d_status;
     DeviceArray<float> d_window, d_out_frame, d_pack;
@@ -223,6 +235,14 @@ struct Session {
             if (c->ready) cudaEventDestroy(c->ready);
             if (c->released) cudaEventDestroy(c->released);
         }
+        if (upload_stream) cudaStreamSynchronize(upload_stream);
+        if (download_stream) cudaStreamSynchronize(download_stream);
+        for (auto& v : frame_ready)
+            for (cudaEvent_t e : v) cudaEventDestroy(e);
+        for (cudaEvent_t e : {ev_main, ev_out, ev_download})
+            if (e) cudaEventDestroy(e);
+        if (upload_stream) cudaStreamDestroy(upload_stream);
+        if (download_stream) cudaStreamDestroy(download_stream);
         if (ev_fork) cudaEventDestroy(ev_fork);
         for (cudaEvent_t e : ev_lane)
             if (e) cudaEventDestroy(e);
@@ -241,6 +261,27 @@ struct Session {
         for (int i = 0; i < kLaneCount; ++i) {
             check(cudaEventRecord(ev_lane[i], lanes[i].stream), "cudaEventRecord(join)");
             check(cudaStreamWaitEvent(stream, ev_lane[i], 0), "cudaStreamWaitEvent(join)");
+        }
+    }
+
+    // Copies on upload_stream start after everything queued on the main
+    // stream (earlier work may still read the buffer being overwritten).
+    void begin_upload() {
+        check(cudaEventRecord(ev_main, stream), "cudaEventRecord(upload start)");
+        check(cudaStreamWaitEvent(upload_stream, ev_main, 0), "cudaStreamWaitEvent(upload start)");
+    }
+    void frame_uploaded(int source, int frame) {
+        check(cudaEventRecord(frame_ready[source][frame], upload_stream), "cudaEventRecord(frame uploaded)");
+        frames_async[source] = true;
+    }
+    // `s` waits for the uploads of frames [first, last] of every source.
+    void wait_frames(cudaStream_t s, int first, int last) {
+        first = std::max(first, 0);
+        last = std::min(last, frames - 1);
+        for (int src = 0; src < 2; ++src) {
+            if (!frames_async[src]) continue;
+            for (int f = first; f <= last; ++f)
+                check(cudaStreamWaitEvent(s, frame_ready[src][f], 0), "cudaStreamWaitEvent(frame uploaded)");
         }
     }
 
@@ -400,6 +441,14 @@ struct Session {
         check(cudaMemset(d_status.ptr, 0, sizeof(int)), "cudaMemset(status)");
         check(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "cudaEventCreate");
         for (cudaEvent_t& e : ev_lane) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        check(cudaStreamCreateWithFlags(&upload_stream, cudaStreamNonBlocking), "cudaStreamCreate(upload)");
+        check(cudaStreamCreateWithFlags(&download_stream, cudaStreamNonBlocking), "cudaStreamCreate(download)");
+        for (cudaEvent_t* e : {&ev_main, &ev_out, &ev_download})
+            check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+        for (auto& v : frame_ready) {
+            v.assign(frames, nullptr);
+            for (cudaEvent_t& e : v) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        }
         d_out_frame.allocate(frame_values(), "cudaMalloc(output frame)");
         // aggregation window (prepare_aggregation_window, core.cpp:296-324)
         host_window.assign(static_cast<size_t>(P) * P, 1.0f);
@@ -578,6 +627,7 @@ struct Session {
         // schedule (compute_temporal_range / schedule_temporal_range)
         int low, high;
         temporal_range(frames, Pt, params.search_bwd, params.search_fwd, anchor, low, high);
+        wait_frames(ls, low, high + Pt - 1);  // every sample the anchor frame reads
         int schedule[kMaxContributors];
         int schedule_len = 0;
         schedule[schedule_len++] = anchor;
@@ -753,6 +803,7 @@ struct Session {
         }
         for (int i = 0; i < nl.count; ++i)
             check(cudaStreamWaitEvent(stream, used[i]->ready, 0), "cudaStreamWaitEvent(stack ready)");
+        wait_frames(stream, n, n);
         nl.source = clip + static_cast<size_t>(n) * frame_values();
         nl.out = out;
         cudaEvent_t t0 = begin_timed(stream);
@@ -858,8 +909,10 @@ int vnlbgpu_set_frame(vnlbgpu_session* session, int source, int frame, const flo
                 vnlbgpu::fail("VNLB CUDA: unsupported frame stride");
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
         float* base = s.source_buffer(source);
+        s.begin_upload();
         copy_planes_in(base + static_cast<size_t>(frame) * s.frame_values(), planes, strides, s.width, s.height,
-                       s.channels, s.stream);
+                       s.channels, s.upload_stream);
+        s.frame_uploaded(source, frame);
         if (source == VNLBGPU_SOURCE_CLIP) s.clip_ready = true; else s.ref_ready = true;
         s.invalidate();
     });
@@ -871,9 +924,15 @@ int vnlbgpu_set_clip_host(vnlbgpu_session* session, int source, const float* cli
         std::lock_guard guard(s.lock);
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
         float* base = s.source_buffer(source);
-        vnlbgpu::check(cudaMemcpyAsync(base, clip, s.frame_values() * s.frames * sizeof(float), cudaMemcpyHostToDevice,
-                                       s.stream),
-                       "cudaMemcpyAsync(clip upload)");
+        // one copy per frame, so that anchor frames start as their frames land
+        s.begin_upload();
+        const size_t fv = s.frame_values();
+        for (int f = 0; f < s.frames; ++f) {
+            vnlbgpu::check(cudaMemcpyAsync(base + fv * f, clip + fv * f, fv * sizeof(float), cudaMemcpyHostToDevice,
+                                           s.upload_stream),
+                           "cudaMemcpyAsync(clip upload)");
+            s.frame_uploaded(source, f);
+        }
         if (source == VNLBGPU_SOURCE_CLIP) s.clip_ready = true; else s.ref_ready = true;
         s.invalidate();
     });
@@ -886,10 +945,12 @@ int vnlbgpu_set_clip_device(vnlbgpu_session* session, int source, const float* d
         if (source == VNLBGPU_SOURCE_CLIP) {
             s.clip = device_clip;
             s.clip_ready = true;
+            s.frames_async[0] = false;
         } else {
             if (s.stage != 1) vnlbgpu::fail("VNLB CUDA: only the Final stage takes a ref clip");
             s.ref = device_clip;
             s.ref_ready = true;
+            s.frames_async[1] = false;
         }
         s.invalidate();
     });
@@ -930,12 +991,38 @@ int vnlbgpu_render_clip_host(vnlbgpu_session* session, float* out) {
         if (!s.d_pack.ptr || s.d_pack.count < s.frame_values() * s.frames)
             s.d_pack.allocate(s.frame_values() * s.frames, "cudaMalloc(clip output)");
         s.require_sources();
+        // Pinned output: each frame goes down on the download stream as soon
+        // as it is normalised.  Pageable output: a copy into pageable memory
+        // holds the calling thread, so everything is enqueued first and the
+        // clip goes down in one copy at the end.
+        cudaPointerAttributes attr{};
+        const bool pinned = cudaPointerGetAttributes(&attr, out) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+        cudaGetLastError();  // a failed query leaves no sticky error
+        const size_t fv = s.frame_values();
+        if (!pinned) {
+            s.fork();
+            for (int n = 0; n < s.frames; ++n) s.render_to_device(n, s.d_pack.ptr + fv * n);
+            s.join();
+            vnlbgpu::check(cudaMemcpyAsync(out, s.d_pack.ptr, fv * s.frames * sizeof(float), cudaMemcpyDeviceToHost,
+                                           s.stream),
+                           "cudaMemcpyAsync(clip download)");
+            s.check_status();
+            return;
+        }
         s.fork();
-        for (int n = 0; n < s.frames; ++n) s.render_to_device(n, s.d_pack.ptr + static_cast<size_t>(n) * s.frame_values());
+        vnlbgpu::check(cudaEventRecord(s.ev_main, s.stream), "cudaEventRecord(download start)");
+        vnlbgpu::check(cudaStreamWaitEvent(s.download_stream, s.ev_main, 0), "cudaStreamWaitEvent(download start)");
+        for (int n = 0; n < s.frames; ++n) {
+            s.render_to_device(n, s.d_pack.ptr + fv * n);
+            vnlbgpu::check(cudaEventRecord(s.ev_out, s.stream), "cudaEventRecord(frame done)");
+            vnlbgpu::check(cudaStreamWaitEvent(s.download_stream, s.ev_out, 0), "cudaStreamWaitEvent(frame done)");
+            vnlbgpu::check(cudaMemcpyAsync(out + fv * n, s.d_pack.ptr + fv * n, fv * sizeof(float),
+                                           cudaMemcpyDeviceToHost, s.download_stream),
+                           "cudaMemcpyAsync(frame download)");
+        }
         s.join();
-        vnlbgpu::check(cudaMemcpyAsync(out, s.d_pack.ptr, s.frame_values() * s.frames * sizeof(float),
-                                       cudaMemcpyDeviceToHost, s.stream),
-                       "cudaMemcpyAsync(clip download)");
+        vnlbgpu::check(cudaEventRecord(s.ev_download, s.download_stream), "cudaEventRecord(downloads done)");
+        vnlbgpu::check(cudaStreamWaitEvent(s.stream, s.ev_download, 0), "cudaStreamWaitEvent(downloads done)");
         s.check_status();
     });
 }
