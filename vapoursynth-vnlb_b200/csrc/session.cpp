@@ -80,21 +80,13 @@ void temporal_range(int source_frames, int patch_time, int bwd, int fwd, int anc
     high = std::min(max_origin, end - shift);
 }
 
-void spatial_range(int center, int axis, int P, int window, int& low, int& high) {
-    const int max_origin = axis - P;
-    const int half = (window - 1) / 2;
-    const int start = center - half;
-    const int end = center + half;
-    const int shift = std::min(0, start) + std::max(0, end - max_origin);
-    low = std::max(0, start - shift);
-    high = std::min(max_origin, end - shift);
-}
-
 struct Grid {
     std::vector<int2> anchors;
     std::vector<Strip> strips;
+    std::vector<Strip> strips_chosen;  // up to kChosenAnchors anchors per strip (chosen matcher)
     DeviceArray<int2> d_anchors;
     DeviceArray<Strip> d_strips;
+    DeviceArray<Strip> d_strips_chosen;
     DeviceArray<int> d_map;  // [H][W] anchor index or -1
     // stack-tile reach tables (TileLaunch)
     DeviceArray<int2> d_tile_grid_rows;  // [tiles_y]
@@ -114,6 +106,10 @@ struct Session {
     int slots = 0, valid_anchor_frames = 0, max_rows = 0, buffer_cap = 0;
     int max_groups = 0, victim_stride = 0, warps = 8;
     int region_rows = 0, region_stride = 0, region_w_max = 0;
+    // chosen matcher geometry (form == VNLBGPU_FORM_CHOSEN and 8x8 patches)
+    bool chosen = false;
+    int chosen_tiles_x = 0, chosen_rows = 0, chosen_stride = 0, chosen_wy = 0, chosen_shortlist = 0,
+        chosen_pool_cap = 0;
     bool coupled = true;
     int device = 0;
     cudaStream_t stream = nullptr;      // the stream all work is enqueued on
@@ -324,6 +320,7 @@ struct Session {
         require(p.device_id >= 0, "device_id must be non-negative");
         require(p.num_streams >= 1 && p.num_streams <= 32, "num_streams must be in the range 1..32");
         require(p.chunk_size > 0, "chunk_size must be positive");
+        require(p.form == VNLBGPU_FORM_PLAIN || p.form == VNLBGPU_FORM_CHOSEN, "form must be plain (0) or chosen (1)");
     }
 
     void configure(const vnlbgpu_params& p, int w, int h, int n, int c) {
@@ -405,6 +402,23 @@ struct Session {
             if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
         }
         if (warps < 1) fail("VNLB CUDA: the search region of one anchor does not fit in shared memory");
+        // chosen matcher: strips of up to kChosenAnchors anchors, 8-column tiles
+        if (p.form == VNLBGPU_FORM_CHOSEN && chosen_match_supported(P, search_channels * Pt)) {
+            const int sched_max = std::min(frames, p.search_bwd + p.search_fwd + 1);
+            const int cap_eff = static_cast<int>(std::min<long long>(soft_cap, static_cast<long long>(cw0) * ch0 * sched_max));
+            MatchLaunch probe{};
+            probe.P = P;
+            probe.Pt = Pt;
+            probe.search_channels = search_channels;
+            probe.window_rows = chosen_wy = ch0;
+            probe.region_rows = chosen_rows = ch0 + P - 1;
+            probe.tiles_x = chosen_tiles_x = ((kChosenAnchors - 1) * step + cw0 + 7) / 8;
+            probe.region_stride = chosen_stride = 8 * chosen_tiles_x + 8;
+            probe.window_cells = cw0 * ch0;
+            probe.shortlist = chosen_shortlist = std::min(cw0 * ch0, (p.tau > 0.0f ? cap_eff : K) + 16);
+            probe.pool_cap = chosen_pool_cap = sched_max * (chosen_shortlist + 8);
+            chosen = 2 * soft_cap <= cw0 * ch0 && chosen_match_shared_bytes(probe) <= 227 * 1024;
+        }
 
         const size_t G = static_cast<size_t>(max_groups);
         const size_t R = G * max_rows;
@@ -541,6 +555,33 @@ struct Session {
             if (s.region_w > region_w_max) fail("VNLB CUDA: internal error: search region exceeds its reservation");
             grid->strips.push_back(s);
         }
+        if (chosen) {
+            size_t k = 0;
+            while (k < a.size()) {
+                Strip st{};
+                st.first = static_cast<int>(k);
+                st.y = a[k].y;
+                int x0 = INT_MAX, x1 = INT_MIN, count = 0;
+                while (k < a.size() && a[k].y == st.y && count < kChosenAnchors) {
+                    int xl, xh;
+                    spatial_range(a[k].x, width, P, params.search_window, xl, xh);
+                    const int nx0 = std::min(x0, xl), nx1 = std::max(x1, xh);
+                    if (count > 0 && nx1 - nx0 + 1 > 8 * chosen_tiles_x) break;
+                    x0 = nx0;
+                    x1 = nx1;
+                    ++count;
+                    ++k;
+                }
+                st.count = count;
+                st.region_x = x0;  // first candidate column
+                st.region_w = x1 - x0 + 1;
+                grid->strips_chosen.push_back(st);
+            }
+            grid->d_strips_chosen.allocate(grid->strips_chosen.size(), "cudaMalloc(strips)");
+            check(cudaMemcpy(grid->d_strips_chosen.ptr, grid->strips_chosen.data(),
+                             grid->strips_chosen.size() * sizeof(Strip), cudaMemcpyHostToDevice),
+                  "cudaMemcpy(strips)");
+        }
         grid->d_anchors.allocate(a.size(), "cudaMalloc(anchors)");
         grid->d_strips.allocate(grid->strips.size(), "cudaMalloc(strips)");
         check(cudaMemcpy(grid->d_anchors.ptr, a.data(), a.size() * sizeof(int2), cudaMemcpyHostToDevice),
@@ -667,7 +708,18 @@ struct Session {
         m.victim_counts = lane.victim_counts.ptr;
         m.victim_stride = victim_stride;
         cudaEvent_t t0 = begin_timed(ls);
-        check(launch_match(m, static_cast<int>(grid.strips.size()), warps, ls), "match kernel launch");
+        if (chosen) {
+            m.strips = grid.d_strips_chosen.ptr;
+            m.region_rows = chosen_rows;
+            m.region_stride = chosen_stride;
+            m.tiles_x = chosen_tiles_x;
+            m.window_rows = chosen_wy;
+            m.shortlist = chosen_shortlist;
+            m.pool_cap = chosen_pool_cap;
+            check(launch_match_chosen(m, static_cast<int>(grid.strips_chosen.size()), ls), "match kernel launch");
+        } else {
+            check(launch_match(m, static_cast<int>(grid.strips.size()), warps, ls), "match kernel launch");
+        }
         end_timed(kTimedMatch, t0, ls);
 
         check(cudaMemsetAsync(lane.counters.ptr, 0, sizeof(FrameCounters), ls), "cudaMemsetAsync(counters)");

@@ -239,4 +239,15 @@ __host__ __device__ __forceinline__ float cr_log1pf(float x) {
 __host__ __device__ __forceinline__ float std_max(float a, float b) { return (a < b) ? b : a; }
 __host__ __device__ __forceinline__ float std_min(float a, float b) { return (b < a) ? b : a; }
 
+// compute_spatial_range (core.cpp:910-932)
+__host__ __device__ __forceinline__ void spatial_range(int center, int axis, int P, int window, int& low, int& high) {
+    const int max_origin = axis - P;
+    const int half = (window - 1) / 2;
+    const int start = center - half;
+    const int end = center + half;
+    const int shift = min(0, start) + max(0, end - max_origin);
+    low = max(0, start - shift);
+    high = min(max_origin, end - shift);
+}
+
 }  // namespace vnlbgpu

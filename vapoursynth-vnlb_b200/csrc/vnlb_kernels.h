@@ -47,6 +47,11 @@ struct MatchLaunch {
     int window_cells;     // max Wx*Wy
     int buffer_cap;       // match buffer capacity per warp
     int warp_floats;      // shared floats per warp
+    // chosen form (match_chosen.cu)
+    int tiles_x;          // 8-column candidate tiles per strip
+    int window_rows;      // max Wy
+    int shortlist;        // candidates re-ranked exactly per anchor and frame
+    int pool_cap;         // pooled short-list entries per anchor
     // outputs
     MatchRow* rows;       // [G][max_rows]
     int* row_counts;      // [G]
@@ -54,6 +59,45 @@ struct MatchLaunch {
     int* victim_counts;   // [G]
     int victim_stride;
 };
+
+// Chosen form: a CTA of kChosenWarps warps matches up to kChosenAnchors
+// anchors (the 16 rows of a tensor-core tile).  Shared layout in floats:
+// FP32 planes, BF16 planes and their copy shifted by one column (its start
+// 16 banks off the first), candidate norms, approximate distances (the row
+// sums of squares alias them), BF16 and FP32 reference patches, reference
+// norms, windows, and the pooled short lists.
+constexpr int kChosenAnchors = 16;
+constexpr int kChosenWarps = 16;
+
+struct ChosenLayout {
+    int region, ebf, obf, nb, dist, abf, reff, na, win, pool_d, pool_i, pool_n, floats;
+};
+
+__host__ __device__ inline ChosenLayout chosen_layout(int planes_n, int rows, int stride, int tiles_x, int wy,
+                                                      int cells, int kd, int pool_cap) {
+    ChosenLayout l{};
+    const int plane = rows * stride;
+    int off = 0;
+    l.region = off; off += planes_n * plane;
+    l.ebf = off;    off += (planes_n * plane + 1) / 2;
+    off += (48 - (off - l.ebf) % 32) % 32;  // the shifted copy starts 16 banks after the first
+    l.obf = off;    off += (planes_n * plane + 1) / 2 + 1;
+    l.nb = off;     off += wy * 8 * tiles_x;
+    l.dist = off;   off += kChosenAnchors * cells > rows * 8 * tiles_x ? kChosenAnchors * cells : rows * 8 * tiles_x;
+    l.abf = off;    off += kChosenAnchors * kd / 2;
+    l.reff = off;   off += kChosenAnchors * kd;
+    l.na = off;     off += kChosenAnchors;
+    l.win = off;    off += 2 * kChosenAnchors;
+    l.pool_d = off; off += kChosenAnchors * pool_cap;
+    l.pool_i = off; off += kChosenAnchors * pool_cap;
+    l.pool_n = off; off += kChosenAnchors;
+    l.floats = (off + 3) & ~3;
+    return l;
+}
+
+bool chosen_match_supported(int P, int planes_n);
+size_t chosen_match_shared_bytes(const MatchLaunch& L);
+cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t stream);
 
 size_t match_shared_bytes(const MatchLaunch& L, int warps);
 int match_warp_floats(int window_cells, int planes_n, int P, int buffer_cap);

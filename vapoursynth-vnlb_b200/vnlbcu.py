@@ -122,6 +122,15 @@ def parse_parameters(stage: int, clip: np.ndarray, sigma, args: dict) -> lib.Par
     for key, field in (("device_id", "device_id"), ("num_streams", "num_streams"), ("chunk_size", "chunk_size")):
         if key in given:
             p[field] = _int(key, g(key))
+    # matcher form (no reference counterpart): "plain" reproduces the CPU core
+    # bit for bit, "chosen" scores candidates on tensor cores and re-ranks a
+    # short list exactly
+    p["form"] = lib.FORM_PLAIN
+    if "form" in given:
+        forms = {"plain": lib.FORM_PLAIN, "chosen": lib.FORM_CHOSEN}
+        if g("form") not in forms:
+            _err('form must be "plain" or "chosen"')
+        p["form"] = forms[g("form")]
     # default group/rank clamps (cuda_plugin.cpp:482-534)
     default_group = "group_size" not in given
     default_rank = "rank" not in given
@@ -246,7 +255,7 @@ class _Filter:
 _BASIC_ARGS = ("block_size", "block_step", "group_size", "bm_range", "patch_time", "radius", "search_bwd",
                "search_fwd", "rank", "cap_factor", "model_cap_factor", "beta", "tau", "variance_threshold",
                "weight_alpha", "weight_beta", "weight_gamma", "weight_epsilon", "membership_noise_floor", "chroma",
-               "device_id", "num_streams", "chunk_size")
+               "device_id", "num_streams", "chunk_size", "form")
 _FINAL_ARGS = _BASIC_ARGS + ("sigma_basic", "gamma", "flat_areas")
 
 

@@ -17,6 +17,7 @@ import numpy as np
 LIB_PATH = Path(os.environ.get("VNLBGPU_LIBRARY") or Path(__file__).resolve().parent / "lib" / "libvnlbgpu.so")
 
 STAGE_BASIC, STAGE_FINAL = 0, 1
+FORM_PLAIN, FORM_CHOSEN = 0, 1
 SOURCE_CLIP, SOURCE_REF = 0, 1
 
 
@@ -36,6 +37,7 @@ class Params(ctypes.Structure):
         ("weight_epsilon", ctypes.c_float), ("membership_noise_floor", ctypes.c_float),
         ("proc_step", ctypes.c_int), ("flat_areas", ctypes.c_int), ("couple_channels", ctypes.c_int),
         ("device_id", ctypes.c_int), ("num_streams", ctypes.c_int), ("chunk_size", ctypes.c_int),
+        ("form", ctypes.c_int),
     ]
 
 
