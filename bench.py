@@ -329,6 +329,14 @@ def roofline_of(r, steps):
                 # dram__bytes_read.sum + dram__bytes_write.sum of one match launch (mean of the
                 # Basic and Final launches), profiles/kernels_1080p_yuv444_one_anchor_frame.md
                 "traffic": 59.5e6, "traffic_unit": "bytes per launch (ncu, one capture)"}
+    if dominant == "match" and r["form"] == "chosen":
+        flops = 2.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
+        return {"kernel": "match, chosen form (FP32 dot-product distances + exact re-rank)", "bound": "fp32",
+                "achieved": flops / (ms / 1e3) / 1e12, "peak": 2 * FP32_LANE_OPS / 1e12, "unit": "TFLOP/s",
+                "frac": flops / (ms / 1e3) / (2 * FP32_LANE_OPS),
+                "peak_source": "nominal FP32 FMA rate x 2 (MEASURED_PEAKS.json has no FP32 figure)",
+                "work": "2 G C d_m (multiply-adds of all candidate dot products) per anchor frame",
+                "ms_per_launch": ms / max(1, launches), "traffic": None}
     if dominant == "match":
         flops = 2.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
         peak = measured_peak("bf16_tflops", 1590.0)
@@ -372,7 +380,7 @@ def run_ours(args):
     # frames it reads, and the timing events see all of the work
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    forms = ["plain", "chosen"] if args.form == "both" else [args.form]
+    forms = ["plain", "chosen_tc", "chosen"] if args.form == "all" else [args.form]
     results = {f: measure_form(f, args, ranks, stream, noisy, clean, d_noisy, local) for f in forms}
     head = results[forms[-1]]
     per_kernel = {}
@@ -394,7 +402,8 @@ def run_ours(args):
 
     if rank == 0:
         describe = {"plain": "plain (exact, bit-identical to the CPU core)",
-                    "chosen": "chosen (BF16 tensor-core distances, exact FP32 re-rank of a short list)"}
+                    "chosen": "chosen (selection on FP32 dot-product distances, exact FP32 re-rank)",
+                    "chosen_tc": "chosen_tc (selection on BF16 tensor-core distances, exact FP32 re-rank)"}
         config = dict(workload_config(describe[head["form"]]), psnr_db=head["psnr"], kernels=per_kernel,
                       dominant_kernel=roofline["kernel"], e2e_output_matches_device_output=head["same"])
         if "plain" in results and head["form"] != "plain":
@@ -406,9 +415,14 @@ def run_ours(args):
             config["max_abs_vs_plain"] = {
                 s: float(np.max(np.abs(a - b))) for s, a, b in
                 zip(("basic", "final"), head["outputs"], plain["outputs"])}
+        if "chosen_tc" in results and head["form"] != "chosen_tc":
+            tc = results["chosen_tc"]
+            config["chosen_tc_form"] = {"value": tc["value"], "e2e": tc["e2e"], "psnr_db": tc["psnr"],
+                                        "ms_per_step": tc["max_ms"] / args.steps,
+                                        "match_ms_per_step": tc["kernels"]["match"][0] / args.steps}
         line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": head["max_ms"] / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if head["form"] == "plain" else "bf16+f32",
+                "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32" if head["form"] == "chosen_tc" else "f32",
                 "data": "synthetic", "config": config, "roofline": roofline, "cpu_baseline": cpu_baseline,
                 "e2e": {"value": head["e2e"], "unit": UNIT, "h2d_bytes_per_step": 3 * clip_bytes,
                         "d2h_bytes_per_step": 2 * clip_bytes},
@@ -429,7 +443,7 @@ def run_profile_case(args):
     out = []
     for stage in (lib.STAGE_BASIC, lib.STAGE_FINAL):
         import vnlbcu
-        kw = dict(CPU_DEFAULTS, form="chosen" if args.form == "chosen" else "plain")
+        kw = dict(CPU_DEFAULTS, form=args.form if args.form != "all" else "plain")
         if stage == lib.STAGE_FINAL:
             kw.update(tau=400.0, variance_threshold=1.7)
         else:
@@ -451,9 +465,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--form", choices=("both", "plain", "chosen"), default="both",
-                    help="matcher form(s) to time; with both, the chosen form is the headline and the plain form "
-                         "is measured beside it for the speed-up and the PSNR gate")
+    ap.add_argument("--form", choices=("all", "plain", "chosen", "chosen_tc"), default="all",
+                    help="matcher form(s) to time; with all, the chosen form is the headline and the plain and "
+                         "tensor-core forms are measured beside it for the speed-up and the PSNR gate")
     ap.add_argument("--profile-case", action="store_true",
                     help="run only a small case (one anchor frame per stage) for ncu captures")
     args = ap.parse_args()

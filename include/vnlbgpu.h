@@ -80,16 +80,21 @@ typedef struct vnlbgpu_params {
     int device_id;
     int num_streams;       /* accepted like vnlbcu (1..32) */
     int chunk_size;        /* accepted like vnlbcu (> 0) */
-    int form;              /* VNLBGPU_FORM_PLAIN (default) or VNLBGPU_FORM_CHOSEN; no reference counterpart */
+    int form;              /* VNLBGPU_FORM_*; no reference counterpart */
 } vnlbgpu_params;
 
-/* Forms of the matcher.  PLAIN reproduces the reference CPU core bit for bit.
- * CHOSEN scores candidates with BF16 tensor-core dot products, re-ranks a
- * short list per frame with the exact FP32 distance and keeps the CPU's
- * selection rule on it: faster, within a PSNR tolerance of PLAIN rather than
- * bit-identical.  It applies to 8x8 patches; other sizes use PLAIN. */
+/* Forms of the matcher (no reference counterpart).  PLAIN reproduces the
+ * reference CPU core bit for bit.  CHOSEN ranks candidates by the
+ * approximate distance ||a||^2 + ||b||^2 - 2 a.b (FP32 dot products, FP32
+ * norms), runs the CPU's selection on those values, re-computes the exact
+ * FP32 distance of every retained candidate and selects on the exact values:
+ * within a PSNR tolerance of PLAIN rather than bit-identical.  CHOSEN_TC does
+ * the same with the dot products on BF16 tensor cores.  Both apply to 8x8
+ * patches with a buffer of at most 32 patches (group_size * cap_factor) and
+ * group_size <= 32; other configurations run PLAIN. */
 #define VNLBGPU_FORM_PLAIN 0
 #define VNLBGPU_FORM_CHOSEN 1
+#define VNLBGPU_FORM_CHOSEN_TC 2
 
 typedef struct vnlbgpu_session vnlbgpu_session;
 

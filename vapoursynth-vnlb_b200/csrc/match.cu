@@ -183,7 +183,67 @@ __device__ __forceinline__ void task_distances(const float* planes, int plane_va
     }
 }
 
-template <int P>
+// Approximate distances of one lane task for 8x8 patches (chosen form):
+// ||a||^2 + ||b||^2 - 2 a.b, the dot products as packed FP32 multiply-adds
+// (four per patch row and candidate, against 13 instructions for the exact
+// row SSD), the candidate norms from the per-frame norm table, clamped at 0
+// so that the values order like their bit patterns.
+__device__ __forceinline__ void task_distances_approx(const float* planes, int plane_values, int rs, int col0,
+                                                      int row0, const float* ref, int planes_n, float ref_norm,
+                                                      const float* norms, float dist[kKY]) {
+    constexpr int P = kLanes;
+    float2 acc[kKY];
+#pragma unroll
+    for (int j = 0; j < kKY; ++j) acc[j] = make_float2(0.0f, 0.0f);
+    for (int q = 0; q < planes_n; ++q) {
+        const float* plane = planes + q * plane_values + row0 * rs + col0;
+        const float* ref_plane = ref + q * P * P;
+        float2 rv[P * P / 2];
+#pragma unroll
+        for (int i = 0; i < P * P / 2; ++i) rv[i] = make_float2(ref_plane[2 * i], ref_plane[2 * i + 1]);
+#pragma unroll
+        for (int r = 0; r < kKY + P - 1; ++r) {
+            float2 cv[P / 2];
+#pragma unroll
+            for (int i = 0; i < P / 2; ++i) cv[i] = make_float2(plane[r * rs + 2 * i], plane[r * rs + 2 * i + 1]);
+#pragma unroll
+            for (int j = 0; j < kKY; ++j) {
+                const int y = r - j;
+                if (y >= 0 && y < P) {
+#pragma unroll
+                    for (int i = 0; i < P / 2; ++i) acc[j] = fma2_rn(rv[y * (P / 2) + i], cv[i], acc[j]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kKY; ++j)
+        dist[j] = fmaxf(ref_norm + norms[(row0 + j) * rs + col0] - 2.0f * (acc[j].x + acc[j].y), 0.0f);
+}
+
+// Exact SSD of one candidate (the plain form's arithmetic and bits).
+__device__ __forceinline__ float exact_distance8(const float* planes, int plane_values, int rs, int col, int row,
+                                                 const float* ref, int planes_n) {
+    constexpr int P = kLanes;
+    float d = 0.0f;
+    for (int q = 0; q < planes_n; ++q) {
+#pragma unroll
+        for (int r = 0; r < P; ++r) {
+            const float* rr = ref + q * P * P + r * P;
+            const float* cr = planes + q * plane_values + (row + r) * rs + col;
+            float2 a2[P / 2], b2[P / 2];
+#pragma unroll
+            for (int i = 0; i < P / 2; ++i) {
+                a2[i] = make_float2(rr[2 * i], rr[2 * i + 1]);
+                b2[i] = make_float2(cr[2 * i], cr[2 * i + 1]);
+            }
+            d = row_ssd8_x2(d, a2, b2);
+        }
+    }
+    return d;
+}
+
+template <int P, bool kApprox>
 __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
@@ -195,7 +255,11 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     const int plane_values = L.region_rows * L.region_stride;
 
     float* planes = smem;
-    float* warp_base = planes + planes_n * plane_values + warp * L.warp_floats;
+    // chosen form: per-frame norm table of every patch origin in the region,
+    // and the row sums of squares it is built from
+    float* norms = planes + planes_n * plane_values;
+    float* rowsq = norms + (kApprox ? plane_values : 0);
+    float* warp_base = planes + planes_n * plane_values + (kApprox ? 2 * plane_values : 0) + warp * L.warp_floats;
     float* dist = warp_base;                                  // window_cells
     float* ref = dist + L.window_cells;                        // planes_n * P * P
     float* buf_d = ref + planes_n * Pd * Pd;                   // buffer_cap
@@ -232,6 +296,8 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     const bool fast = s.cap <= 32 && K <= 32;
     unsigned reg_d = 0u, reg_top = 0u;  // bits of non-negative distances (0 = empty)
     int reg_id = 0;
+    float ref_norm = 0.0f;   // chosen form: ||reference||^2
+    float reg_exact = 0.0f;  // chosen form: exact distance of this lane's buffer slot
 
     for (int k = 0; k < L.schedule_len; ++k) {
         const int frame = L.schedule[k];
@@ -252,6 +318,30 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
             }
         }
         __syncthreads();
+        if constexpr (kApprox) {
+            const int rs = L.region_stride;
+            for (int i = threadIdx.x; i < rows * (cols - P + 1); i += blockDim.x) {
+                const int r = i / (cols - P + 1);
+                const int cx = i - r * (cols - P + 1);
+                float acc = 0.0f;
+                for (int q = 0; q < planes_n; ++q) {
+                    const float* row = planes + q * plane_values + r * rs + cx;
+#pragma unroll
+                    for (int ii = 0; ii < P; ++ii) acc = fmaf(row[ii], row[ii], acc);
+                }
+                rowsq[r * rs + cx] = acc;
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < (rows - P + 1) * (cols - P + 1); i += blockDim.x) {
+                const int r = i / (cols - P + 1);
+                const int cx = i - r * (cols - P + 1);
+                float acc = 0.0f;
+#pragma unroll
+                for (int rr = 0; rr < P; ++rr) acc += rowsq[(r + rr) * rs + cx];
+                norms[r * rs + cx] = acc;
+            }
+            __syncthreads();
+        }
         if (!active_warp) continue;
         if (k == 0) {
             // Reference patch (anchor frame is scheduled first).
@@ -264,14 +354,25 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
                                 (ax - strip.region_x + px)];
             }
             __syncwarp();
+            if constexpr (kApprox) {
+                float acc = 0.0f;
+                for (int i = lane; i < planes_n * Pd * Pd; i += 32) acc = fmaf(ref[i], ref[i], acc);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                ref_norm = acc;
+            }
         }
         // Distances of all candidates of frame k.
         for (int task = lane; task < tasks; task += 32) {
             const int cx = task % Wx;
             const int gy = task / Wx;
             float d[kKY];
-            task_distances<P>(planes, plane_values, L.region_stride, xl - strip.region_x + cx,
-                              yl - strip.region_y + gy * kKY, ref, planes_n, Pd, d);
+            if constexpr (kApprox)
+                task_distances_approx(planes, plane_values, L.region_stride, xl - strip.region_x + cx,
+                                      yl - strip.region_y + gy * kKY, ref, planes_n, ref_norm, norms, d);
+            else
+                task_distances<P>(planes, plane_values, L.region_stride, xl - strip.region_x + cx,
+                                  yl - strip.region_y + gy * kKY, ref, planes_n, Pd, d);
 #pragma unroll
             for (int j = 0; j < kKY; ++j) {
                 const int cy = gy * kKY + j;
@@ -330,6 +431,17 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
                         if (lane == owner) reg_top = __float_as_uint(d);
                         s.top_front = __uint_as_float(__reduce_max_sync(0xffffffffu, reg_top));
                     }
+                }
+            }
+            if constexpr (kApprox) {
+                // exact FP32 distance of the buffer slots frame k filled, while
+                // frame k is staged: each lane re-ranks its own slot
+                if (lane < s.count && (reg_id >> 20) == k) {
+                    const int cell = reg_id & 0xfffff;
+                    const int cy = cell / Wx;
+                    reg_exact = exact_distance8(planes, plane_values, L.region_stride,
+                                                xl - strip.region_x + (cell - cy * Wx), yl - strip.region_y + cy,
+                                                ref, planes_n);
                 }
             }
             continue;
@@ -402,7 +514,28 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     if (!active_warp) return;
     int S = 0;
     bool selected_in_warp = false;
-    if (fast) {
+    if (kApprox && fast && K > 1) {
+        // chosen form: select_similar_patches on the exact distances of the
+        // buffer -- the K smallest, the threshold max(tau, d_K), the slots
+        // within it, closest first (ties by candidate order), at most the cap
+        const int n = s.count;
+        int rank = 0;
+        for (int j = 0; j < n; ++j) {
+            const float dj = __shfl_sync(0xffffffffu, reg_exact, j);
+            const int ij = __shfl_sync(0xffffffffu, reg_id, j);
+            rank += (dj < reg_exact || (dj == reg_exact && ij < reg_id)) ? 1 : 0;
+        }
+        if (lane < n) {
+            buf_d[rank] = reg_exact;
+            buf_i[rank] = reg_id;
+        }
+        __syncwarp();
+        const int M = min(K, n);
+        const float threshold = std_max(L.tau, buf_d[M - 1]);
+        const int within = __popc(__ballot_sync(0xffffffffu, lane < n && buf_d[lane] <= threshold));
+        S = min(within, min(L.soft_cap, n));
+        selected_in_warp = true;
+    } else if (fast) {
         // select_similar_patches with pairwise distinct buffered distances:
         // the heap replay below has a unique outcome, computed warp-wide.
         // partial_sort(first, first + M, first + n) keeps in [0, M) the M
@@ -549,7 +682,8 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
 }  // namespace
 
 size_t match_shared_bytes(const MatchLaunch& L, int warps) {
-    const size_t planes = static_cast<size_t>(L.search_channels) * L.Pt * L.region_rows * L.region_stride;
+    const size_t plane = static_cast<size_t>(L.region_rows) * L.region_stride;
+    const size_t planes = static_cast<size_t>(L.search_channels) * L.Pt * plane + (L.approx ? 2 * plane : 0);
     return (planes + static_cast<size_t>(warps) * L.warp_floats) * sizeof(float);
 }
 
@@ -569,13 +703,18 @@ cudaError_t launch_match(const MatchLaunch& L, int strips, int warps, cudaStream
         kernel<<<strips, block, smem, stream>>>(L);
         err = cudaGetLastError();
     };
+    if (L.approx) {
+        if (L.P != kLanes) return cudaErrorInvalidValue;
+        launch(match_kernel<8, true>);
+        return err;
+    }
     switch (L.P) {
-        case 4: launch(match_kernel<4>); break;
-        case 5: launch(match_kernel<5>); break;
-        case 6: launch(match_kernel<6>); break;
-        case 7: launch(match_kernel<7>); break;
-        case 8: launch(match_kernel<8>); break;
-        default: launch(match_kernel<0>); break;
+        case 4: launch(match_kernel<4, false>); break;
+        case 5: launch(match_kernel<5, false>); break;
+        case 6: launch(match_kernel<6, false>); break;
+        case 7: launch(match_kernel<7, false>); break;
+        case 8: launch(match_kernel<8, false>); break;
+        default: launch(match_kernel<0, false>); break;
     }
     return err;
 }

@@ -7,28 +7,31 @@
 //   1. approximate distance ||a||^2 + ||b||^2 - 2 a.b for every candidate, the
 //      dot products on BF16 tensor cores (mma.sync m16n8k16, FP32
 //      accumulation), the norms in FP32 from the FP32 samples;
-//   2. per scheduled frame and anchor, the `shortlist` smallest approximate
-//      distances (a bisection on the value, ties broken by candidate order);
-//   3. their exact FP32 SSD in the CPU's arithmetic order (the same bits the
-//      plain form computes for those candidates);
-//   4. select_similar_patches (core.cpp:1200-1243) on the exact distances of
-//      the pooled short lists: the K smallest, the threshold max(tau, d_K),
-//      the rows within it closest first, at most the cap.
+//   2. the CPU's sequential selection (find_similar_patches,
+//      core.cpp:1277-1359: the K-smallest front and the capped buffer) run on
+//      the approximate distances, frame by frame in the CPU's candidate order;
+//   3. the exact FP32 SSD, in the CPU's arithmetic order (the bits the plain
+//      form computes), of every buffer entry a frame brings in, while that
+//      frame is still staged;
+//   4. select_similar_patches (core.cpp:1200-1243) on those exact distances:
+//      the K smallest, the threshold max(tau, d_K), the entries within it,
+//      closest first, at most the cap.
 //
-// Step 4 keeps the rows sorted by (distance, candidate order); the CPU leaves
-// the rows past the K-th in the order its heap replay produces, which only
-// changes the order in which equal-weight contributions are summed.
+// The buffer is the plain form's whenever the approximate distances order the
+// candidates as the exact ones do.  Step 4 keeps the rows sorted by
+// (distance, candidate order); the CPU leaves the rows past the K-th in the
+// order its heap replay produces, which only changes the order in which
+// contributions are summed.
 //
-// Work decomposition.  One CTA takes a strip of up to 16 consecutive anchors
-// of one grid row: the 16 rows of the MMA are the 16 reference patches (K =
-// patch samples, two patch rows per k16 step), the 8 columns of an MMA tile
-// are 8 consecutive candidate positions of one window row.  Every scheduled
-// frame's search region is staged once in shared memory as FP32 (norms and
-// exact re-rank) and as BF16 twice -- as loaded, and shifted left by one
-// column -- so that each lane's pair of B-fragment samples is one aligned
-// 32-bit load whatever the parity of its candidate column.  The candidate
-// columns of the strip are shared by all its anchors; results outside an
-// anchor's window are dropped.
+// Work decomposition.  One CTA takes a strip of up to 8 consecutive anchors
+// of one grid row: rows 0-7 of each m16n8k16 tile are their reference patches
+// (rows 8-15 are zero), K runs over the patch samples two patch rows per k16
+// step, and the 8 columns of a tile are 8 consecutive candidate positions of
+// one window row, shared by all anchors of the strip (results outside an
+// anchor's window are dropped).  Every scheduled frame's search region is
+// staged once in shared memory in FP32 (B fragments are converted to BF16 as
+// they are staged; norms and the exact re-rank read the FP32 samples).  Each
+// warp then takes one anchor through the selection of the frame.
 #include <cuda_bf16.h>
 
 #include "vnlb_kernels.h"
@@ -60,13 +63,14 @@ __device__ __forceinline__ float warp_max_f(float v) {
 }
 
 template <int NCH>  // k16 steps per patch: planes * kPatch / 2
-__global__ void __launch_bounds__(kChosenThreads, 1) match_chosen_kernel(MatchLaunch L) {
+__global__ void __launch_bounds__(kChosenThreads, 2) match_chosen_kernel(MatchLaunch L) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int g = lane >> 2;  // MMA group: fragment row / column
     const int t = lane & 3;
     constexpr int P = kPatch;
+    constexpr int kVals = kChosenMaxCells / 32;
     const Strip strip = L.strips[blockIdx.x];
     const int planes_n = L.search_channels * L.Pt;
     const int kd = planes_n * P * P;
@@ -78,7 +82,7 @@ __global__ void __launch_bounds__(kChosenThreads, 1) match_chosen_kernel(MatchLa
     int yl, yh;
     spatial_range(strip.y, L.height, P, L.search_window, yl, yh);
     const int Wy = yh - yl + 1;
-    const ChosenLayout lay = chosen_layout(planes_n, rows, rs, tiles_x, L.window_rows, L.window_cells, kd, L.pool_cap);
+    const ChosenLayout lay = chosen_layout(planes_n, rows, rs, tiles_x, L.window_rows, L.window_cells, kd);
     float* region = smem + lay.region;
     __nv_bfloat16* ebf = reinterpret_cast<__nv_bfloat16*>(smem + lay.ebf);
     __nv_bfloat16* obf = reinterpret_cast<__nv_bfloat16*>(smem + lay.obf);
@@ -88,11 +92,8 @@ __global__ void __launch_bounds__(kChosenThreads, 1) match_chosen_kernel(MatchLa
     __nv_bfloat16* abf = reinterpret_cast<__nv_bfloat16*>(smem + lay.abf);
     float* reff = smem + lay.reff;
     float* na = smem + lay.na;
-    int* win_xl = reinterpret_cast<int*>(smem + lay.win);
-    int* win_wx = win_xl + kChosenAnchors;
-    float* pool_d = smem + lay.pool_d;
-    int* pool_i = reinterpret_cast<int*>(smem + lay.pool_i);
-    int* pool_n = reinterpret_cast<int*>(smem + lay.pool_n);
+    int* win_lo = reinterpret_cast<int*>(smem + lay.win);  // window columns relative to the strip origin
+    int* win_wx = win_lo + kChosenAnchors;
     const int count = strip.count;
     const int rx0 = strip.region_x;  // first candidate column of the strip
 
@@ -103,34 +104,49 @@ __global__ void __launch_bounds__(kChosenThreads, 1) match_chosen_kernel(MatchLa
             const int2 a = L.anchors[strip.first + m];
             spatial_range(a.x, L.width, P, L.search_window, xl, xh);
         }
-        win_xl[m] = xl;
+        win_lo[m] = xl - rx0;
         win_wx[m] = xh - xl + 1;
-        pool_n[m] = 0;
     }
-    unsigned afrag[NCH][4];
-    const unsigned* e32 = reinterpret_cast<const unsigned*>(ebf);
-    const unsigned* o32 = reinterpret_cast<const unsigned*>(obf);
+    unsigned afrag[NCH][2];  // rows g of the tile (rows g + 8 are zero)
+    int my_lo = 0, my_wx = 0;
+    float my_na = 0.0f;
+    // selection state of this warp's anchor (the plain matcher's WarpSelect)
+    const int K = L.K;
+    struct {
+        int count, cap, worst_idx, top_count;
+        float worst, top_front;
+    } s;
+    s.count = 0;
+    s.cap = min(L.soft_cap, L.search_window * L.search_window * L.schedule_len);
+    s.worst_idx = 0;
+    s.worst = kInf;
+    s.top_count = 0;
+    s.top_front = kInf;
+    unsigned reg_d = 0u, reg_top = 0u;  // bits of non-negative distances
+    int reg_id = 0;
+    float reg_exact = 0.0f;
 
     for (int k = 0; k < L.schedule_len; ++k) {
         const int frame = L.schedule[k];
         __syncthreads();
-        // Stage frame k's planes (channel, t): FP32, BF16, BF16 shifted by one.
+        // Stage frame k's planes (channel, t) in FP32.
         for (int q = 0; q < planes_n; ++q) {
             const int c = q / L.Pt;
             const int tt = q % L.Pt;
             const float* src = L.video + (static_cast<size_t>(frame + tt) * L.channels + c) * L.height *
                                              static_cast<size_t>(L.width);
-            for (int i = threadIdx.x; i < rows * rs; i += kChosenThreads) {
-                const int r = i / rs;
-                const int cx = i - r * rs;
-                const int gx = rx0 + cx;
+            for (int r = warp; r < rows; r += kChosenWarps) {
                 const int gy = yl + r;
-                float v = 0.0f;
-                if (gx < L.width && gy < L.height) v = __ldg(src + static_cast<size_t>(gy) * L.width + gx);
-                region[q * plane + i] = v;
-                const __nv_bfloat16 b = __float2bfloat16_rn(v);
-                ebf[q * plane + i] = b;
-                if (cx > 0) obf[q * plane + i - 1] = b;
+                const float* srow = src + static_cast<size_t>(gy) * L.width;
+                for (int cx = lane; cx < rs; cx += 32) {
+                    const int gx = rx0 + cx;
+                    const float v = gx < L.width && gy < L.height ? __ldg(srow + gx) : 0.0f;
+                    const int i = q * plane + r * rs + cx;
+                    region[i] = v;
+                    const __nv_bfloat16 b = __float2bfloat16_rn(v);
+                    ebf[i] = b;
+                    if (cx > 0) obf[i - 1] = b;
+                }
             }
         }
         __syncthreads();
@@ -153,17 +169,16 @@ __global__ void __launch_bounds__(kChosenThreads, 1) match_chosen_kernel(MatchLa
             }
         }
         // row sums of squares over P columns, all planes (candidate norms)
-        for (int i = threadIdx.x; i < rows * ncols; i += kChosenThreads) {
-            const int r = i / ncols;
-            const int cx = i - r * ncols;
-            float acc = 0.0f;
-            for (int q = 0; q < planes_n; ++q) {
-                const float* row = region + q * plane + r * rs + cx;
+        for (int r = warp; r < rows; r += kChosenWarps)
+            for (int cx = lane; cx < ncols; cx += 32) {
+                float acc = 0.0f;
+                for (int q = 0; q < planes_n; ++q) {
+                    const float* row = region + q * plane + r * rs + cx;
 #pragma unroll
-                for (int ii = 0; ii < P; ++ii) acc = fmaf(row[ii], row[ii], acc);
+                    for (int ii = 0; ii < P; ++ii) acc = fmaf(row[ii], row[ii], acc);
+                }
+                rowsum[r * ncols + cx] = acc;
             }
-            rowsum[i] = acc;
-        }
         __syncthreads();
         if (k == 0) {
             if (warp < kChosenAnchors) {
@@ -177,127 +192,150 @@ __global__ void __launch_bounds__(kChosenThreads, 1) match_chosen_kernel(MatchLa
 #pragma unroll
             for (int cq = 0; cq < NCH; ++cq) {
                 afrag[cq][0] = a32[(g * kd + 16 * cq + 2 * t) >> 1];
-                afrag[cq][1] = a32[((g + 8) * kd + 16 * cq + 2 * t) >> 1];
-                afrag[cq][2] = a32[(g * kd + 16 * cq + 2 * t + 8) >> 1];
-                afrag[cq][3] = a32[((g + 8) * kd + 16 * cq + 2 * t + 8) >> 1];
+                afrag[cq][1] = a32[(g * kd + 16 * cq + 2 * t + 8) >> 1];
             }
+            my_lo = g < count ? win_lo[g] : 1 << 20;
+            my_wx = g < count ? win_wx[g] : 0;
         }
-        for (int i = threadIdx.x; i < Wy * ncols; i += kChosenThreads) {
-            const int y = i / ncols;
-            const int cx = i - y * ncols;
-            float acc = 0.0f;
+        for (int y = warp; y < Wy; y += kChosenWarps)
+            for (int cx = lane; cx < ncols; cx += 32) {
+                float acc = 0.0f;
 #pragma unroll
-            for (int r = 0; r < P; ++r) acc += rowsum[(y + r) * ncols + cx];
-            nb[i] = acc;
-        }
+                for (int r = 0; r < P; ++r) acc += rowsum[(y + r) * ncols + cx];
+                nb[y * ncols + cx] = acc;
+            }
         __syncthreads();
-        // Approximate distances: tile = 16 anchors x 8 candidates of one row.
+        if (k == 0) my_na = na[g];
+        // Approximate distances: tile = 8 anchors (rows g) x 8 candidates of one row.
         {
-            const unsigned* src32 = (g & 1) ? o32 : e32;
-            const int tiles = Wy * tiles_x;
-            for (int tile = warp; tile < tiles; tile += kChosenWarps) {
-                const int y = tile / tiles_x;
-                const int j = tile - y * tiles_x;
-                const int col = 8 * j + g + 2 * t - (g & 1);  // even index into the even or shifted copy
+            // lane pairs (columns c, c + 1) as one aligned 32-bit load: from the
+            // even copy for even c, from the shifted copy (index c - 1) for odd c
+            const unsigned* src32 = reinterpret_cast<const unsigned*>((g & 1) ? obf : ebf);
+            int y = 0, j = warp;  // tile (y, j) = y * tiles_x + j, strided by the warp count
+            while (j >= tiles_x && y < Wy) {
+                j -= tiles_x;
+                ++y;
+            }
+            for (; y < Wy; j += kChosenWarps) {
+                while (j >= tiles_x) {
+                    j -= tiles_x;
+                    ++y;
+                }
+                if (y >= Wy) break;
+                const int base = (y * rs + 8 * j + g + 2 * t - (g & 1)) >> 1;  // 32-bit word of the pair
                 float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
                 for (int cq = 0; cq < NCH; ++cq) {
-                    const int q = cq >> 2;
-                    const int rp = cq & 3;
-                    const int base = q * plane + (y + 2 * rp) * rs + col;
-                    mma_bf16_16816(c, afrag[cq], src32[base >> 1], src32[(base + rs) >> 1]);
+                    const int w = base + (((cq >> 2) * plane + 2 * (cq & 3) * rs) >> 1);
+                    const unsigned a[4] = {afrag[cq][0], 0u, afrag[cq][1], 0u};
+                    mma_bf16_16816(c, a, src32[w], src32[w + (rs >> 1)]);
                 }
+                // this lane's results: anchor g, candidate columns 8j + 2t and + 1
+                const int cx = 8 * j + 2 * t - my_lo;
 #pragma unroll
-                for (int h = 0; h < 4; ++h) {
-                    const int m = g + 8 * (h >> 1);
-                    const int cn = 8 * j + 2 * t + (h & 1);  // candidate column relative to rx0
-                    if (m >= count) continue;
-                    const int cxw = rx0 + cn - win_xl[m];
-                    if (cxw < 0 || cxw >= win_wx[m]) continue;
-                    dist[m * L.window_cells + y * win_wx[m] + cxw] = na[m] + nb[y * ncols + cn] - 2.0f * c[h];
+                for (int h = 0; h < 2; ++h) {
+                    if (cx + h < 0 || cx + h >= my_wx) continue;
+                    dist[g * L.window_cells + y * my_wx + cx + h] =
+                        my_na + nb[y * ncols + 8 * j + 2 * t + h] - 2.0f * c[h];
                 }
             }
         }
         __syncthreads();
-        // Short list of frame k per anchor, exact re-rank.
+        // The CPU's sequential selection over frame k (raster order) on the
+        // approximate distances: the K-smallest front and the capped buffer,
+        // buffer slot i in lane i (the plain matcher's register replay).
         if (warp < count) {
             const int m = warp;
-            const int Wx = win_wx[m];
-            const int n = Wx * Wy;
-            const float* dm = dist + m * L.window_cells;
-            const int want = min(n, L.shortlist);
-            float lo = kInf, hi = -kInf;
-            for (int i = lane; i < n; i += 32) {
-                const float v = dm[i];
-                lo = fminf(lo, v);
-                hi = fmaxf(hi, v);
-            }
-            lo = warp_min_f(lo);
-            hi = warp_max_f(hi);
-            // invariant: at least `want` values are <= hi
-            if (want < n) {
-                for (int it = 0; it < 32; ++it) {
-                    const float mid = lo + 0.5f * (hi - lo);
-                    if (!(mid > lo && mid < hi)) break;
-                    int cnt = 0;
-                    for (int i = lane; i < n; i += 32) cnt += dm[i] <= mid ? 1 : 0;
-                    cnt = __reduce_add_sync(0xffffffffu, cnt);
-                    if (cnt >= want) {
-                        hi = mid;
-                        if (cnt <= want + 8) break;
-                    } else {
-                        lo = mid;
-                    }
-                }
-            }
-            const int budget = L.shortlist + 8;
-            const int np0 = pool_n[m];
-            float* pd = pool_d + m * L.pool_cap + np0;
-            int* pi = pool_i + m * L.pool_cap + np0;
-            int taken = 0;
-            for (int base = 0; base < n && taken < budget; base += 32) {
-                const int i = base + lane;
-                const bool sel = i < n && dm[i] <= hi;
-                const unsigned bal = __ballot_sync(0xffffffffu, sel);
-                const int pos = taken + __popc(bal & ((1u << lane) - 1u));
-                if (sel && pos < budget) {
-                    const int cy = i / Wx;
-                    const int col = win_xl[m] + (i - cy * Wx) - rx0;
-                    float d = 0.0f;
-                    for (int q = 0; q < planes_n; ++q) {
-#pragma unroll
-                        for (int r = 0; r < P; ++r) {
-                            const float* rr = reff + m * kd + q * P * P + r * P;
-                            const float* cr = region + q * plane + (cy + r) * rs + col;
-                            d = row_ssd<P>(d, [&](int ii) { return rr[ii]; }, [&](int ii) { return cr[ii]; });
+            const int cells = win_wx[m] * Wy;
+            const float* dk = dist + m * L.window_cells;
+            for (int base = 0; base < cells; base += 32) {
+                const int idx = base + lane;
+                // approximate distances can dip below zero; clamp so that they
+                // order like their bit patterns
+                const float mine = idx < cells ? fmaxf(dk[idx], 0.0f) : kInf;
+                float limit = s.top_count >= K ? std_max(L.tau, s.top_front) : kInf;
+                if (s.count >= s.cap) limit = std_min(limit, s.worst);
+                unsigned pass = __ballot_sync(0xffffffffu, idx < cells && mine <= limit);
+                while (pass) {
+                    const int src_lane = __ffs(pass) - 1;
+                    pass &= pass - 1;
+                    const float d = __shfl_sync(0xffffffffu, mine, src_lane);
+                    limit = s.top_count >= K ? std_max(L.tau, s.top_front) : kInf;
+                    if (s.count >= s.cap) limit = std_min(limit, s.worst);
+                    if (!(d <= limit)) continue;
+                    const int id = (k << 20) | (base + src_lane);
+                    if (s.count < s.cap) {
+                        if (lane == s.count) {
+                            reg_d = __float_as_uint(d);
+                            reg_id = id;
                         }
+                        s.count++;
+                        if (s.count == s.cap) {
+                            const unsigned w = __reduce_max_sync(0xffffffffu, reg_d);
+                            s.worst_idx = __ffs(__ballot_sync(0xffffffffu, reg_d == w)) - 1;
+                            s.worst = __uint_as_float(w);
+                        }
+                    } else if (d < s.worst) {
+                        if (lane == s.worst_idx) {
+                            reg_d = __float_as_uint(d);
+                            reg_id = id;
+                        }
+                        const unsigned w = __reduce_max_sync(0xffffffffu, reg_d);
+                        s.worst_idx = __ffs(__ballot_sync(0xffffffffu, reg_d == w)) - 1;
+                        s.worst = __uint_as_float(w);
                     }
-                    pd[pos] = d;
-                    pi[pos] = (k << 20) | i;
+                    if (s.top_count < K) {
+                        if (lane == s.top_count) reg_top = __float_as_uint(d);
+                        s.top_count++;
+                        if (s.top_count == K) s.top_front = __uint_as_float(__reduce_max_sync(0xffffffffu, reg_top));
+                    } else if (d < s.top_front) {
+                        const unsigned f = __float_as_uint(s.top_front);
+                        const int owner = __ffs(__ballot_sync(0xffffffffu, lane < K && reg_top == f)) - 1;
+                        if (lane == owner) reg_top = __float_as_uint(d);
+                        s.top_front = __uint_as_float(__reduce_max_sync(0xffffffffu, reg_top));
+                    }
                 }
-                taken = min(budget, taken + __popc(bal));
             }
-            __syncwarp();
-            if (lane == 0) pool_n[m] = np0 + taken;
+            // exact FP32 distance of the buffer entries frame k brought in,
+            // while frame k is staged: each lane re-ranks its own slot
+            if (lane < s.count && (reg_id >> 20) == k) {
+                const int i = reg_id & 0xfffff;
+                const int Wx = win_wx[m];
+                const int cy = i / Wx;
+                const int col = win_lo[m] + (i - cy * Wx);
+                const float* rf = reff + m * kd;
+                float d = 0.0f;
+                for (int q = 0; q < planes_n; ++q) {
+#pragma unroll
+                    for (int r = 0; r < P; ++r) {
+                        const float* rr = rf + q * P * P + r * P;
+                        const float* cr = region + q * plane + (cy + r) * rs + col;
+                        float2 a2[4], b2[4];
+#pragma unroll
+                        for (int ii = 0; ii < 4; ++ii) {
+                            a2[ii] = make_float2(rr[2 * ii], rr[2 * ii + 1]);
+                            b2[ii] = make_float2(cr[2 * ii], cr[2 * ii + 1]);
+                        }
+                        d = row_ssd8_x2(d, a2, b2);
+                    }
+                }
+                reg_exact = d;
+            }
         }
     }
-    __syncthreads();
     if (warp >= count) return;
 
-    // select_similar_patches on the pooled exact distances
+    // select_similar_patches on the exact distances of the buffer: the K
+    // smallest, the threshold max(tau, d_K), the entries within it, closest
+    // first (ties by candidate order), at most the cap
     const int m = warp;
     const int gi = strip.first + m;
     const int2 anchor = L.anchors[gi];
     const int Wx = win_wx[m];
-    const int xl = win_xl[m];
-    const int np = pool_n[m];
-    const float* pd = pool_d + m * L.pool_cap;
-    const int* pi = pool_i + m * L.pool_cap;
-    float* sd = dist + m * L.window_cells;  // sorted pool (free now)
-    int* si = reinterpret_cast<int*>(sd + L.soft_cap);
-    const int K = L.K;
-    const int cap = min(L.soft_cap, L.search_window * L.search_window * L.schedule_len);
-    const int nbuf = min(cap, np);
+    const int xl = win_lo[m] + rx0;
+    float* sd = dist + m * L.window_cells;  // sorted buffer (free now)
+    int* si = reinterpret_cast<int*>(sd + 32);
+    const int n = s.count;
     int S;
     if (K <= 1) {
         // similar <= 1: the anchor itself (core.cpp:1253-1257)
@@ -307,28 +345,21 @@ __global__ void __launch_bounds__(kChosenThreads, 1) match_chosen_kernel(MatchLa
         }
         S = 1;
     } else {
-        for (int i = lane; i < np; i += 32) {
-            const float di = pd[i];
-            const int ii = pi[i];
-            int rank = 0;
-            for (int j = 0; j < np; ++j) {
-                const float dj = pd[j];
-                rank += (dj < di || (dj == di && pi[j] < ii)) ? 1 : 0;
-            }
-            if (rank < nbuf) {
-                sd[rank] = di;
-                si[rank] = ii;
-            }
+        int rank = 0;
+        for (int j = 0; j < n; ++j) {
+            const float dj = __shfl_sync(0xffffffffu, reg_exact, j);
+            const int ij = __shfl_sync(0xffffffffu, reg_id, j);
+            rank += (dj < reg_exact || (dj == reg_exact && ij < reg_id)) ? 1 : 0;
+        }
+        if (lane < n) {
+            sd[rank] = reg_exact;
+            si[rank] = reg_id;
         }
         __syncwarp();
-        const int selected = min(K, nbuf);
+        const int selected = min(K, n);
         const float threshold = std_max(L.tau, sd[selected - 1]);
-        int within = 0;
-        for (int base = 0; base < nbuf; base += 32) {
-            const int i = base + lane;
-            within += __popc(__ballot_sync(0xffffffffu, i < nbuf && sd[i] <= threshold));
-        }
-        S = min(within, min(L.soft_cap, nbuf));
+        const int within = __popc(__ballot_sync(0xffffffffu, lane < n && sd[lane] <= threshold));
+        S = min(within, min(L.soft_cap, n));
     }
     __syncwarp();
     MatchRow* rows_out = L.rows + static_cast<size_t>(gi) * L.max_rows;
@@ -399,7 +430,7 @@ bool chosen_match_supported(int P, int planes_n) {
 size_t chosen_match_shared_bytes(const MatchLaunch& L) {
     const int planes_n = L.search_channels * L.Pt;
     const ChosenLayout lay = chosen_layout(planes_n, L.region_rows, L.region_stride, L.tiles_x, L.window_rows,
-                                           L.window_cells, planes_n * L.P * L.P, L.pool_cap);
+                                           L.window_cells, planes_n * L.P * L.P);
     return static_cast<size_t>(lay.floats) * sizeof(float);
 }
 

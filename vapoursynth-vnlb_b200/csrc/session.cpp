@@ -106,10 +106,12 @@ struct Session {
     int slots = 0, valid_anchor_frames = 0, max_rows = 0, buffer_cap = 0;
     int max_groups = 0, victim_stride = 0, warps = 8;
     int region_rows = 0, region_stride = 0, region_w_max = 0;
-    // chosen matcher geometry (form == VNLBGPU_FORM_CHOSEN and 8x8 patches)
+    // matcher forms: approx (VNLBGPU_FORM_CHOSEN: approximate distances in
+    // the plain matcher's tiling, exact re-rank) and tensor
+    // (VNLBGPU_FORM_CHOSEN_TC: BF16 tensor-core distances, match_chosen.cu)
+    bool approx = false;
     bool chosen = false;
-    int chosen_tiles_x = 0, chosen_rows = 0, chosen_stride = 0, chosen_wy = 0, chosen_shortlist = 0,
-        chosen_pool_cap = 0;
+    int chosen_tiles_x = 0, chosen_rows = 0, chosen_stride = 0, chosen_wy = 0;
     bool coupled = true;
     int device = 0;
     cudaStream_t stream = nullptr;      // the stream all work is enqueued on
@@ -320,7 +322,8 @@ struct Session {
         require(p.device_id >= 0, "device_id must be non-negative");
         require(p.num_streams >= 1 && p.num_streams <= 32, "num_streams must be in the range 1..32");
         require(p.chunk_size > 0, "chunk_size must be positive");
-        require(p.form == VNLBGPU_FORM_PLAIN || p.form == VNLBGPU_FORM_CHOSEN, "form must be plain (0) or chosen (1)");
+        require(p.form == VNLBGPU_FORM_PLAIN || p.form == VNLBGPU_FORM_CHOSEN || p.form == VNLBGPU_FORM_CHOSEN_TC,
+                "form must be plain (0), chosen (1) or chosen_tc (2)");
     }
 
     void configure(const vnlbgpu_params& p, int w, int h, int n, int c) {
@@ -387,6 +390,11 @@ struct Session {
         region_rows = std::min(p.search_window, height - P + 1) + P - 1 + KY - 1;
         const int cw0 = std::min(p.search_window, width - P + 1);
         const int ch0 = std::min(p.search_window, height - P + 1);
+        const int sched_max = std::min(frames, p.search_bwd + p.search_fwd + 1);
+        const long long cap_eff = std::min<long long>(soft_cap, static_cast<long long>(cw0) * ch0 * sched_max);
+        // approximate distances need 8x8 patches and the register replay
+        // (buffer and K front within a warp)
+        approx = p.form == VNLBGPU_FORM_CHOSEN && P == kLanes && cap_eff <= 32 && K <= 32;
         for (warps = 8; warps >= 1; warps /= 2) {
             region_w_max = ((warps - 1) * step + cw0 + P - 1 + 3 + 3) & ~3;
             // stride = 4 (mod 8): the 4 candidate rows of one lane task start 16
@@ -398,14 +406,13 @@ struct Session {
             probe.Pt = Pt;
             probe.region_rows = region_rows;
             probe.region_stride = region_stride;
+            probe.approx = approx ? 1 : 0;
             probe.warp_floats = match_warp_floats(cw0 * ch0, search_channels * Pt, P, buffer_cap);
             if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
         }
         if (warps < 1) fail("VNLB CUDA: the search region of one anchor does not fit in shared memory");
         // chosen matcher: strips of up to kChosenAnchors anchors, 8-column tiles
-        if (p.form == VNLBGPU_FORM_CHOSEN && chosen_match_supported(P, search_channels * Pt)) {
-            const int sched_max = std::min(frames, p.search_bwd + p.search_fwd + 1);
-            const int cap_eff = static_cast<int>(std::min<long long>(soft_cap, static_cast<long long>(cw0) * ch0 * sched_max));
+        if (p.form == VNLBGPU_FORM_CHOSEN_TC && chosen_match_supported(P, search_channels * Pt)) {
             MatchLaunch probe{};
             probe.P = P;
             probe.Pt = Pt;
@@ -415,9 +422,9 @@ struct Session {
             probe.tiles_x = chosen_tiles_x = ((kChosenAnchors - 1) * step + cw0 + 7) / 8;
             probe.region_stride = chosen_stride = 8 * chosen_tiles_x + 8;
             probe.window_cells = cw0 * ch0;
-            probe.shortlist = chosen_shortlist = std::min(cw0 * ch0, (p.tau > 0.0f ? cap_eff : K) + 16);
-            probe.pool_cap = chosen_pool_cap = sched_max * (chosen_shortlist + 8);
-            chosen = 2 * soft_cap <= cw0 * ch0 && chosen_match_shared_bytes(probe) <= 227 * 1024;
+            // the register replay: the buffer and the K front fit in a warp
+            chosen = cap_eff <= 32 && K <= 32 && 64 <= cw0 * ch0 && cw0 * ch0 <= kChosenMaxCells &&
+                     chosen_match_shared_bytes(probe) <= 227 * 1024;
         }
 
         const size_t G = static_cast<size_t>(max_groups);
@@ -701,6 +708,7 @@ struct Session {
         const int chh = std::min(params.search_window, height - P + 1);
         m.window_cells = cw * chh;
         m.buffer_cap = buffer_cap;
+        m.approx = approx ? 1 : 0;
         m.warp_floats = match_warp_floats(m.window_cells, search_channels * Pt, P, buffer_cap);
         m.rows = lane.rows.ptr;
         m.row_counts = lane.row_counts.ptr;
@@ -714,8 +722,6 @@ struct Session {
             m.region_stride = chosen_stride;
             m.tiles_x = chosen_tiles_x;
             m.window_rows = chosen_wy;
-            m.shortlist = chosen_shortlist;
-            m.pool_cap = chosen_pool_cap;
             check(launch_match_chosen(m, static_cast<int>(grid.strips_chosen.size()), ls), "match kernel launch");
         } else {
             check(launch_match(m, static_cast<int>(grid.strips.size()), warps, ls), "match kernel launch");

@@ -47,11 +47,10 @@ struct MatchLaunch {
     int window_cells;     // max Wx*Wy
     int buffer_cap;       // match buffer capacity per warp
     int warp_floats;      // shared floats per warp
-    // chosen form (match_chosen.cu)
+    int approx;           // chosen form in this matcher: approximate distances, exact re-rank
+    // tensor-core form (match_chosen.cu)
     int tiles_x;          // 8-column candidate tiles per strip
     int window_rows;      // max Wy
-    int shortlist;        // candidates re-ranked exactly per anchor and frame
-    int pool_cap;         // pooled short-list entries per anchor
     // outputs
     MatchRow* rows;       // [G][max_rows]
     int* row_counts;      // [G]
@@ -61,26 +60,29 @@ struct MatchLaunch {
 };
 
 // Chosen form: a CTA of kChosenWarps warps matches up to kChosenAnchors
-// anchors (the 16 rows of a tensor-core tile).  Shared layout in floats:
-// FP32 planes, BF16 planes and their copy shifted by one column (its start
-// 16 banks off the first), candidate norms, approximate distances (the row
-// sums of squares alias them), BF16 and FP32 reference patches, reference
-// norms, windows, and the pooled short lists.
-constexpr int kChosenAnchors = 16;
-constexpr int kChosenWarps = 16;
+// anchors (rows of a tensor-core tile; the other 8 rows are zero).  Shared
+// layout in floats: FP32 planes, their BF16 copies, candidate norms,
+// approximate distances (the
+// row sums of squares alias them), BF16 and FP32 reference patches, reference
+// norms and windows.
+constexpr int kChosenAnchors = 8;
+constexpr int kChosenWarps = 8;
+constexpr int kChosenMaxCells = 512;  // window cells per anchor (values a lane holds: 16)
 
 struct ChosenLayout {
-    int region, ebf, obf, nb, dist, abf, reff, na, win, pool_d, pool_i, pool_n, floats;
+    int region, ebf, obf, nb, dist, abf, reff, na, win, floats;
 };
 
 __host__ __device__ inline ChosenLayout chosen_layout(int planes_n, int rows, int stride, int tiles_x, int wy,
-                                                      int cells, int kd, int pool_cap) {
+                                                      int cells, int kd) {
     ChosenLayout l{};
     const int plane = rows * stride;
     int off = 0;
     l.region = off; off += planes_n * plane;
+    // BF16 copies: as loaded, and shifted left by one column (its start 16
+    // banks after the first, so even and odd lanes use disjoint banks)
     l.ebf = off;    off += (planes_n * plane + 1) / 2;
-    off += (48 - (off - l.ebf) % 32) % 32;  // the shifted copy starts 16 banks after the first
+    off += (48 - (off - l.ebf) % 32) % 32;
     l.obf = off;    off += (planes_n * plane + 1) / 2 + 1;
     l.nb = off;     off += wy * 8 * tiles_x;
     l.dist = off;   off += kChosenAnchors * cells > rows * 8 * tiles_x ? kChosenAnchors * cells : rows * 8 * tiles_x;
@@ -88,9 +90,6 @@ __host__ __device__ inline ChosenLayout chosen_layout(int planes_n, int rows, in
     l.reff = off;   off += kChosenAnchors * kd;
     l.na = off;     off += kChosenAnchors;
     l.win = off;    off += 2 * kChosenAnchors;
-    l.pool_d = off; off += kChosenAnchors * pool_cap;
-    l.pool_i = off; off += kChosenAnchors * pool_cap;
-    l.pool_n = off; off += kChosenAnchors;
     l.floats = (off + 3) & ~3;
     return l;
 }

@@ -123,13 +123,14 @@ def parse_parameters(stage: int, clip: np.ndarray, sigma, args: dict) -> lib.Par
         if key in given:
             p[field] = _int(key, g(key))
     # matcher form (no reference counterpart): "plain" reproduces the CPU core
-    # bit for bit, "chosen" scores candidates on tensor cores and re-ranks a
-    # short list exactly
+    # bit for bit; "chosen" selects on approximate distances and re-ranks the
+    # retained candidates exactly; "chosen_tc" computes the approximate
+    # distances on BF16 tensor cores
     p["form"] = lib.FORM_PLAIN
     if "form" in given:
-        forms = {"plain": lib.FORM_PLAIN, "chosen": lib.FORM_CHOSEN}
+        forms = {"plain": lib.FORM_PLAIN, "chosen": lib.FORM_CHOSEN, "chosen_tc": lib.FORM_CHOSEN_TC}
         if g("form") not in forms:
-            _err('form must be "plain" or "chosen"')
+            _err('form must be "plain", "chosen" or "chosen_tc"')
         p["form"] = forms[g("form")]
     # default group/rank clamps (cuda_plugin.cpp:482-534)
     default_group = "group_size" not in given

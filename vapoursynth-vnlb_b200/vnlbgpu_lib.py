@@ -17,7 +17,7 @@ import numpy as np
 LIB_PATH = Path(os.environ.get("VNLBGPU_LIBRARY") or Path(__file__).resolve().parent / "lib" / "libvnlbgpu.so")
 
 STAGE_BASIC, STAGE_FINAL = 0, 1
-FORM_PLAIN, FORM_CHOSEN = 0, 1
+FORM_PLAIN, FORM_CHOSEN, FORM_CHOSEN_TC = 0, 1, 2
 SOURCE_CLIP, SOURCE_REF = 0, 1
 
 
