@@ -328,7 +328,7 @@ def roofline_of(r, steps):
                 "ms_per_launch": ms / max(1, launches),
                 # dram__bytes_read.sum + dram__bytes_write.sum of one match launch (mean of the
                 # Basic and Final launches), profiles/kernels_1080p_yuv444_one_anchor_frame.md
-                "traffic": 59.5e6, "traffic_unit": "bytes per launch (ncu, one capture)"}
+                "traffic": 59.3e6, "traffic_unit": "bytes per launch (ncu, one capture)"}
     if dominant == "match" and r["form"] == "chosen":
         flops = 2.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
         return {"kernel": "match, chosen form (FP32 dot-product distances + exact re-rank)", "bound": "fp32",
