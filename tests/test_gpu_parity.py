@@ -81,6 +81,10 @@ CASES = [
                                               block_step=5)),
     ("yuv_no_weights", 72, 56, 3, 3, 12.0, dict(weight_alpha=0.0, weight_beta=0.0, weight_gamma=0.0)),
     ("yuv_alpha_only", 72, 56, 3, 3, 12.0, dict(weight_beta=0.0, cap_factor=0.0)),
+    # model rows beyond group_size (vnlb.* semantics: model_cap_factor 0 or >= 1)
+    ("yuv_model_cap2_tau", 96, 72, 4, 3, 20.0, dict(tau=800.0, model_cap_factor=2.0)),
+    ("gray_model_cap0", 80, 64, 4, 1, 25.0, dict(group_size=12, rank=10, tau=1500.0, cap_factor=3.0,
+                                                 model_cap_factor=0.0)),
 ]
 
 

@@ -303,8 +303,10 @@ struct Session {
         require(p.rank >= 0, "rank must be non-negative");
         require(std::isfinite(p.similar_cap_factor) && (p.similar_cap_factor == 0.0f || p.similar_cap_factor >= 1.0f),
                 "cap_factor must be zero or at least 1.0");
-        require(std::isfinite(p.model_cap_factor) && p.model_cap_factor == 1.0f,
-                "the CUDA backend currently requires model_cap_factor=1");
+        // vnlb.* semantics (plugin.cpp:409-412); vnlbcu's own check (model_cap_factor = 1) stays in its
+        // argument parser, as in cuda_plugin.cpp
+        require(std::isfinite(p.model_cap_factor) && (p.model_cap_factor == 0.0f || p.model_cap_factor >= 1.0f),
+                "model_cap_factor must be zero or at least 1.0");
         require(std::isfinite(p.beta) && p.beta > 0.0f, "beta must be finite and positive");
         require(std::isfinite(p.tau) && p.tau >= 0.0f, "tau must be finite and non-negative");
         require(std::isfinite(p.variance_threshold), "variance_threshold must be finite");
@@ -360,7 +362,14 @@ struct Session {
         const int cw = std::min(p.search_window, width - P + 1);
         const int ch = std::min(p.search_window, height - P + 1);
         const long long candidates = static_cast<long long>(cw) * ch * temporal;
-        const int basis = static_cast<int>(std::min<long long>(K, candidates));
+        // model rows per group: B = min(S, model cap) with S <= min(soft cap,
+        // candidates) (model_similar_cap, core.cpp:159-172); every group takes
+        // the dual path when the largest B is below the dimension
+        const long long retained_max = std::min<long long>(cap_of(K, p.similar_cap_factor), candidates);
+        const int basis = static_cast<int>(
+            std::min<long long>(std::max<long long>(std::min<long long>(K, candidates),
+                                                    std::min<long long>(cap_of(K, p.model_cap_factor), retained_max)),
+                                retained_max));
         if (basis > 128) fail("VNLB CUDA: the CUDA dual-PCA filter supports at most 128 model samples");
         if (p.rank > basis) fail("VNLB CUDA: rank must not exceed min(group_size, candidate_count)");
         if (!(dim >= 64 && basis < dim))
