@@ -40,7 +40,8 @@ def vnlb_kwargs(p: O.StageParams, stage):
               search_fwd=p.search_fwd, group_size=p.similar, rank=p.rank, cap_factor=p.similar_cap_factor,
               beta=p.beta, tau=float(np.float32(p.tau) * np.float32(65025.0)),
               variance_threshold=p.variance_threshold, weight_alpha=p.weight_alpha, weight_beta=p.weight_beta,
-              weight_gamma=p.weight_gamma, block_step=p.proc_step)
+              weight_gamma=p.weight_gamma, block_step=p.proc_step, model_cap_factor=p.model_cap_factor,
+              chroma=p.couple_channels)
     if stage == lib.STAGE_FINAL:
         kw.update(flat_areas=p.flat_areas, gamma=p.gamma)
     return kw
@@ -85,6 +86,9 @@ CASES = [
     ("yuv_model_cap2_tau", 96, 72, 4, 3, 20.0, dict(tau=800.0, model_cap_factor=2.0)),
     ("gray_model_cap0", 80, 64, 4, 1, 25.0, dict(group_size=12, rank=10, tau=1500.0, cap_factor=3.0,
                                                  model_cap_factor=0.0)),
+    # uncoupled planes (chroma=0): one model per plane, weights combined over the planes
+    ("yuv_uncoupled", 96, 72, 4, 3, 20.0, dict(chroma=0)),
+    ("yuv_uncoupled_tau", 80, 64, 4, 3, 25.0, dict(chroma=0, tau=800.0, group_size=12, rank=10)),
 ]
 
 
@@ -219,7 +223,7 @@ def test_unsupported_configurations_raise():
     with pytest.raises(lib.VNLBError, match="dual-PCA"):
         vnlb.Basic(gray, sigma=10.0, block_size=4, group_size=8, rank=8)  # covariance model (dim 16)
     with pytest.raises(lib.VNLBError, match="chroma=1"):
-        vnlb.Basic(np.zeros((3, 3, 32, 32), np.float32), sigma=10.0, chroma=0)
+        vnlbcu.Basic(np.zeros((3, 3, 32, 32), np.float32), sigma=10.0, chroma=0)  # vnlbcu keeps its rule
 
 
 def test_full_size_anchor_frames_bit_exact():

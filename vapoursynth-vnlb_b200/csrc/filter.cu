@@ -112,7 +112,16 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
     const bool weights_enabled = P.weight_alpha != 0.0f || P.weight_beta != 0.0f || P.weight_gamma != 0.0f;
     const int active_count = L.counters->active;
     const int warps_total = gridDim.x * kPrepareWarps;
-    for (int a = blockIdx.x * kPrepareWarps + (threadIdx.x >> 5); a < active_count; a += warps_total) {
+    // model v = (active group a, model channel mc): one model per group when
+    // the channels are coupled (or the clip has one plane), one per plane
+    // otherwise (transform_vnlb_channel, core.cpp:795-808)
+    const int models = L.models;
+    const size_t hw = static_cast<size_t>(L.height) * L.width;
+    const int RD = L.row_dim;
+    for (int v = blockIdx.x * kPrepareWarps + (threadIdx.x >> 5); v < active_count * models; v += warps_total) {
+        const int a = v / models;
+        const int mc = v - a * models;
+        const size_t cb = mc * hw;  // plane offset of this model's channel
         const int g = L.active[a];
         const int S = L.row_counts[g];
         const MatchRow* rows = L.rows + static_cast<size_t>(g) * L.max_rows;
@@ -120,16 +129,19 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
         const int B = min(S, L.model_cap);
         for (int i = lane; i < S; i += 32) {
             const MatchRow m = rows[i];
-            L.row_info[r0 + i] = m;
-            L.row_group[r0 + i] = a;
+            if (mc == 0) {
+                L.row_info[r0 + i] = m;
+                L.row_group[r0 + i] = a;
+            }
             bases[i] = row_base(L, m);
         }
         __syncwarp();
         // equal group (samples_are_equal / group_is_equal): independent loads
         bool differs = S <= 1;
         if (S > 1) {
-            for (int col = lane; col < D; col += 32) {
-                const float* src = L.noisy + coloff[col];
+            for (int col = lane; col < D * models; col += 32) {
+                const int cm = col / D;  // plane of an uncoupled group (group_is_equal, core.cpp:516-531)
+                const float* src = L.noisy + cm * hw + coloff[col - cm * D];
                 const float v0 = __ldg(src + bases[0]);
                 int i = 1;
                 for (; i + 4 <= S; i += 4) {
@@ -144,8 +156,8 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
             // filtered = input, default aggregation model (core.cpp:253-274)
             for (int i = 0; i < S; ++i) {
                 const size_t b = bases[i];
-                float* out = L.filtered + static_cast<size_t>(r0 + i) * D;
-                for (int col = lane; col < D; col += 32) out[col] = __ldg(L.noisy + b + coloff[col]);
+                float* out = L.filtered + static_cast<size_t>(r0 + i) * RD + mc * D;
+                for (int col = lane; col < D; col += 32) out[col] = __ldg(L.noisy + b + cb + coloff[col]);
             }
             const float tau = __fadd_rn(P.weight_epsilon, __fdiv_rn(static_cast<float>(D), static_cast<float>(B)));
             const float lgw = P.weight_alpha == 0.0f ? 0.0f : __fmul_rn(-P.weight_alpha, cr_logf(tau));
@@ -155,15 +167,16 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
                 lw = lw < -80.0f ? -80.0f : (80.0f < lw ? 80.0f : lw);
                 w = cr_expf(lw);
             }
-            for (int i = lane; i < S; i += 32) L.weights[r0 + i] = w;
-            if (lane == 0) L.flags[a] = kGroupDone;
+            if (mc == 0)
+                for (int i = lane; i < S; i += 32) L.weights[r0 + i] = w;
+            if (lane == 0) L.flags[v] = kGroupDone;
             continue;
         }
         // flat area (Final): mean channel variance of the noisy rows
         bool flat = false;
         if (final_stage && P.flat_areas) {
             const int pd = L.patch_dim;
-            const int channels = D / pd;
+            const int channels = models > 1 ? models : D / pd;
             const int per_channel = pd * S;
             float variance = 0.0f;
             for (int c = 0; c < channels; ++c) {
@@ -171,9 +184,9 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
                 for (int i = 0; i < S; ++i) {
                     const float* src = L.noisy + bases[i];
                     for (int q = lane; q < pd; q += 32) {
-                        const float v = __ldg(src + coloff[c * pd + q]);
-                        sum += static_cast<double>(v);
-                        sum2 += static_cast<double>(v) * static_cast<double>(v);
+                        const float x = __ldg(src + (models > 1 ? c * hw + coloff[q] : coloff[c * pd + q]));
+                        sum += static_cast<double>(x);
+                        sum2 += static_cast<double>(x) * static_cast<double>(x);
                     }
                 }
 #pragma unroll
@@ -192,17 +205,17 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
         if (B < min(D, L.rank)) {
             if (lane == 0) {
                 atomicCAS(L.status, 0, kStatusRankNotCovered);
-                L.flags[a] = kGroupSkip;
+                L.flags[v] = kGroupSkip;
             }
             continue;
         }
         // model rows, means over the first B rows (compute_mean), centring
         for (int s = 0; s < B; ++s) {
             const size_t b = bases[s];
-            for (int col = lane; col < D; col += 32) X[s * ldx + col] = __ldg(model_video + b + coloff[col]);
+            for (int col = lane; col < D; col += 32) X[s * ldx + col] = __ldg(model_video + b + cb + coloff[col]);
         }
         const float inv_b = __fdiv_rn(1.0f, static_cast<float>(B));
-        float* means = L.means + static_cast<size_t>(a) * 2 * D;
+        float* means = L.means + static_cast<size_t>(v) * 2 * D;
         for (int col = lane; col < D; col += 32) {
             float mm = 0.0f;
             for (int s = 0; s < B; ++s) mm = __fadd_rn(mm, X[s * ldx + col]);
@@ -210,7 +223,7 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
             float center = mm;  // Basic: noisy mean; Final flat: basic mean
             if (final_stage && !flat) {
                 float mn = 0.0f;
-                for (int s = 0; s < B; ++s) mn = __fadd_rn(mn, __ldg(L.noisy + bases[s] + coloff[col]));
+                for (int s = 0; s < B; ++s) mn = __fadd_rn(mn, __ldg(L.noisy + bases[s] + cb + coloff[col]));
                 center = __fmul_rn(mn, inv_b);
             }
             means[col] = mm;
@@ -221,7 +234,7 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
         if (L.rank > 0) {
             // dual Gram (compute_gram_centered), one pair per lane
             const float scale = __fdiv_rn(1.0f, static_cast<float>(B));
-            float* gram = L.gram + static_cast<size_t>(a) * Bmax * Bmax;
+            float* gram = L.gram + static_cast<size_t>(v) * Bmax * Bmax;
             const int pairs = B * (B + 1) / 2;
             // octet k takes pair e0 + k; lane j of the octet runs the pinned
             // chain j (octet_dot8: the pinned 8-lane order)
@@ -238,7 +251,7 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
                 }
             }
         }
-        if (lane == 0) L.flags[a] = 0;
+        if (lane == 0) L.flags[v] = 0;
         __syncwarp();
     }
 }
@@ -259,15 +272,15 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg, in
     float* m = sm + static_cast<size_t>(slot) * gstride;
     float* v = m + Bmax * ld;
     int* order = reinterpret_cast<int*>(v + Bmax * ld);
-    const int active_count = L.counters->active;
+    const int models_total = L.counters->active * L.models;
     const int slots_per_cta = (blockDim.x >> 5) * groups_per_warp;
-    for (int base = blockIdx.x * slots_per_cta; base < active_count; base += gridDim.x * slots_per_cta) {
-        const int a = base + slot;
-        bool valid = a < active_count && R > 0;
+    for (int base = blockIdx.x * slots_per_cta; base < models_total; base += gridDim.x * slots_per_cta) {
+        const int a = base + slot;  // model index (group x model channel)
+        bool valid = a < models_total && R > 0;
         int B = 0;
         if (valid) {
             valid = L.flags[a] == 0;
-            B = min(L.row_counts[L.active[a]], L.model_cap);
+            B = min(L.row_counts[L.active[a / L.models]], L.model_cap);
         }
         if (!valid) B = 0;
         const float* gram = L.gram + static_cast<size_t>(max(a, 0)) * Bmax * Bmax;
@@ -392,6 +405,17 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg, in
     }
 }
 
+// One model's term of a row's log weight (accumulate_aggregation_model,
+// core.cpp:326-412): the group weight, minus beta times the membership.
+__device__ __forceinline__ float model_log_weight(const StageConfig& P, bool membership_on, float lgw, float volume,
+                                                  float score, float min_score) {
+    if (P.weight_alpha == 0.0f && P.weight_beta == 0.0f) return 0.0f;
+    if (!membership_on) return lgw;
+    const float diff = __fsub_rn(score, min_score);
+    const float membership = __fadd_rn(diff > 0.0f ? diff : 0.0f, volume);
+    return __fsub_rn(lgw, __fmul_rn(P.weight_beta, membership));
+}
+
 // ---------------------------------------------------------------------------
 // apply: one CTA per group.  Shared layout (floats unless noted):
 //   coloff[D] (int), means[2D], X[B][ldx] centred model rows, basis[R][ldb],
@@ -462,22 +486,27 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
                                __fmul_rn(__fmul_rn(P.membership_noise_floor, P.sigma), P.sigma));
     const bool membership_on = P.weight_beta != 0.0f;
     const int active_count = L.counters->active;
+    const int models = L.models;  // models per group (planes when uncoupled)
+    const size_t hw = static_cast<size_t>(L.height) * L.width;
     __syncthreads();
-    for (int a = blockIdx.x; a < active_count; a += gridDim.x) {
-        if (L.flags[a] != 0) continue;  // uniform: equal groups are done, skipped ones reported
+    for (int mi = blockIdx.x; mi < active_count * models; mi += gridDim.x) {
+        if (L.flags[mi] != 0) continue;  // uniform: equal groups are done, skipped ones reported
+        const int a = mi / models;
+        const int mc = mi - a * models;
         const int g = L.active[a];
         const int S = L.row_counts[g];
         const MatchRow* rows = L.rows + static_cast<size_t>(g) * L.max_rows;
         const int r0 = L.row_offset[a];
         const int B = min(S, L.model_cap);
-        const float* gm = L.means + static_cast<size_t>(a) * 2 * D;
+        const float* gm = L.means + static_cast<size_t>(mi) * 2 * D;
         for (int i = tid; i < 2 * D; i += kApplyThreads) means[i] = gm[i];
-        for (int i = tid; i < R * Bmax; i += kApplyThreads) dual[i] = L.dual[static_cast<size_t>(a) * R * Bmax + i];
-        for (int i = tid; i < S; i += kApplyThreads) bases[i] = row_base(L, rows[i]);
+        for (int i = tid; i < R * Bmax; i += kApplyThreads) dual[i] = L.dual[static_cast<size_t>(mi) * R * Bmax + i];
+        // row bases of this model's plane
+        for (int i = tid; i < S; i += kApplyThreads) bases[i] = row_base(L, rows[i]) + mc * hw;
         // per-component scalars, computed once per group (same operations as
         // the CPU, which recomputes them where it uses them)
         for (int c = tid; c < R; c += kApplyThreads) {
-            const float lambda = L.eig[static_cast<size_t>(a) * R + c];
+            const float lambda = L.eig[static_cast<size_t>(mi) * R + c];
             eig[c] = lambda;
             const float diff = __fsub_rn(lambda, model_noise2);
             const float signal = diff > 0.0f ? diff : 0.0f;
@@ -607,7 +636,7 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
             __syncwarp();
             // reconstruction (project_bayes_estimate), components in order,
             // accumulated in registers over blocks of 32 * kRecCols columns
-            float* out = L.filtered + static_cast<size_t>(r0 + i) * D;
+            float* out = L.filtered + static_cast<size_t>(r0 + i) * L.row_dim + mc * D;
             for (int base = 0; base < D; base += 32 * kRecCols) {
                 float o[kRecCols];
 #pragma unroll
@@ -641,6 +670,13 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
         __syncthreads();
         const float min_score = s_misc[2];
         for (int i = tid; i < S; i += kApplyThreads) {
+            if (models > 1) {
+                // this plane's term of the row's log weight; combine_weights
+                // sums the planes in order and finalises
+                L.logw[static_cast<size_t>(r0 + i) * models + mc] =
+                    model_log_weight(P, membership_on, lgw, volume, scores[i], min_score);
+                continue;
+            }
             float w = 1.0f;
             if (weights_enabled) {
                 float lw;
@@ -763,30 +799,35 @@ __global__ void __launch_bounds__(32 * kWarpApplyWarps, VNLB_APPLY_MIN_BLOCKS) a
     const bool need_dm = membership_on || !final_stage;
     const float score_scale = __fsqrt_rn(__fmul_rn(2.0f, static_cast<float>(D)));
     const int active_count = L.counters->active;
+    const int models = L.models;  // models per group (planes when uncoupled)
+    const size_t hw = static_cast<size_t>(L.height) * L.width;
     __syncthreads();
 
-    for (int a = blockIdx.x * kWarpApplyWarps + warp; a < active_count; a += gridDim.x * kWarpApplyWarps) {
-        if (L.flags[a] != 0) continue;  // equal groups are done, skipped ones reported
+    for (int mi = blockIdx.x * kWarpApplyWarps + warp; mi < active_count * models;
+         mi += gridDim.x * kWarpApplyWarps) {
+        if (L.flags[mi] != 0) continue;  // equal groups are done, skipped ones reported
+        const int a = mi / models;
+        const int mc = mi - a * models;
         const int g = L.active[a];
         const int S = L.row_counts[g];
         const MatchRow* rows = L.rows + static_cast<size_t>(g) * L.max_rows;
         const int r0 = L.row_offset[a];
         const int B = min(S, L.model_cap);
-        const float* gm = L.means + static_cast<size_t>(a) * 2 * D;
+        const float* gm = L.means + static_cast<size_t>(mi) * 2 * D;
         float mm[kCols], cc[kCols];
 #pragma unroll
         for (int jj = 0; jj < kCols; ++jj) {
             mm[jj] = __ldg(gm + lane + 32 * jj);
             cc[jj] = __ldg(gm + D + lane + 32 * jj);
         }
-        for (int i = lane; i < S; i += 32) bases[i] = row_base(L, rows[i]);
+        for (int i = lane; i < S; i += 32) bases[i] = row_base(L, rows[i]) + mc * hw;  // this model's plane
         for (int i = lane; i < R * Bmax; i += 32) {
             const int b = i / Bmax, s = i - b * Bmax;
-            dual[b * 8 + s] = L.dual[static_cast<size_t>(a) * R * Bmax + i];
+            dual[b * 8 + s] = L.dual[static_cast<size_t>(mi) * R * Bmax + i];
         }
         if (lane < R) {
             const int c = lane;
-            const float lambda = L.eig[static_cast<size_t>(a) * R + c];
+            const float lambda = L.eig[static_cast<size_t>(mi) * R + c];
             eig[c] = lambda;
             const float diff = __fsub_rn(lambda, model_noise2);
             const float signal = diff > 0.0f ? diff : 0.0f;
@@ -992,13 +1033,18 @@ __global__ void __launch_bounds__(32 * kWarpApplyWarps, VNLB_APPLY_MIN_BLOCKS) a
                 for (int jj = 0; jj < kCols; ++jj)
                     o[jj] = __fmaf_rn(sc, basis_f[((c & 3) * D + lane + 32 * jj) * 2 + (c >> 2)], o[jj]);
             }
-            float* out = L.filtered + static_cast<size_t>(r0 + i) * D;
+            float* out = L.filtered + static_cast<size_t>(r0 + i) * L.row_dim + mc * D;
 #pragma unroll
             for (int jj = 0; jj < kCols; ++jj) out[lane + 32 * jj] = __fadd_rn(o[jj], cc[jj]);
             __syncwarp();
         }
         // aggregation weights (accumulate_aggregation_model + finalize)
         for (int i = lane; i < S; i += 32) {
+            if (models > 1) {
+                L.logw[static_cast<size_t>(r0 + i) * models + mc] =
+                    model_log_weight(P, membership_on, lgw, volume, scores[i], min_score);
+                continue;
+            }
             float w = 1.0f;
             if (weights_enabled) {
                 float lw;
@@ -1020,6 +1066,31 @@ __global__ void __launch_bounds__(32 * kWarpApplyWarps, VNLB_APPLY_MIN_BLOCKS) a
     }
 }
 
+// Weights of the rows of an uncoupled group: the log-weight terms of its
+// plane models summed in plane order, times 1 / models, clamped and
+// exponentiated (finalize_aggregation_weights, core.cpp:276-294).  Equal
+// groups already hold their default-model weight.
+__global__ void combine_weights_kernel(FilterLaunch L) {
+    const StageConfig& P = L.cfg;
+    const bool weights_enabled = P.weight_alpha != 0.0f || P.weight_beta != 0.0f || P.weight_gamma != 0.0f;
+    const int models = L.models;
+    const float inv_models = __fdiv_rn(1.0f, static_cast<float>(models));
+    const int rows = L.counters->rows;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        const int a = L.row_group[r];
+        if (L.flags[static_cast<size_t>(a) * models] != 0) continue;
+        float w = 1.0f;
+        if (weights_enabled) {
+            float acc = 0.0f;
+            for (int c = 0; c < models; ++c) acc = __fadd_rn(acc, L.logw[static_cast<size_t>(r) * models + c]);
+            float lw = __fmul_rn(acc, inv_models);
+            lw = lw < -80.0f ? -80.0f : (80.0f < lw ? 80.0f : lw);
+            w = cr_expf(lw);
+        }
+        L.weights[r] = w;
+    }
+}
+
 template <int D>
 cudaError_t launch_apply_warp(const FilterLaunch& L, int max_groups, cudaStream_t stream) {
     const WarpApplyLayout lay = warp_apply_layout(D, L.max_rows);
@@ -1034,8 +1105,9 @@ cudaError_t launch_apply_warp(const FilterLaunch& L, int max_groups, cudaStream_
 
 }  // namespace
 
-cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t stream) {
-    if (max_groups <= 0) return cudaSuccess;
+cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t stream) {
+    if (max_groups_in <= 0) return cudaSuccess;
+    const int max_groups = max_groups_in * L.models;  // models to filter at most
     const int D = L.dim;
     const int Bmax = std::min(L.model_cap, L.max_rows);
     const int R = L.rank;
@@ -1094,6 +1166,13 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t st
         const int ctas = std::min(max_groups, 148 * 8);
         apply_kernel<<<ctas, kApplyThreads, smem, stream>>>(L);
         if ((err = cudaGetLastError()) != cudaSuccess) return err;
+    }
+    if (L.models > 1) {
+        const long long rows = static_cast<long long>(max_groups_in) * L.max_rows;
+        const int ctas = static_cast<int>(std::max<long long>(1, std::min<long long>((rows + 255) / 256, 148 * 8)));
+        combine_weights_kernel<<<ctas, 256, 0, stream>>>(L);
+        cudaError_t err = cudaGetLastError();
+        if (err != cudaSuccess) return err;
     }
     return cudaSuccess;
 }

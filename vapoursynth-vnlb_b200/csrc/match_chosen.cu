@@ -50,18 +50,6 @@ __device__ __forceinline__ void mma_bf16_16816(float c[4], const unsigned a[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ float warp_min_f(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
-__device__ __forceinline__ float warp_max_f(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
-}
-
 template <int NCH>  // k16 steps per patch: planes * kPatch / 2
 __global__ void __launch_bounds__(kChosenThreads, 2) match_chosen_kernel(MatchLaunch L) {
     extern __shared__ __align__(16) float smem[];
@@ -70,7 +58,6 @@ __global__ void __launch_bounds__(kChosenThreads, 2) match_chosen_kernel(MatchLa
     const int g = lane >> 2;  // MMA group: fragment row / column
     const int t = lane & 3;
     constexpr int P = kPatch;
-    constexpr int kVals = kChosenMaxCells / 32;
     const Strip strip = L.strips[blockIdx.x];
     const int planes_n = L.search_channels * L.Pt;
     const int kd = planes_n * P * P;

@@ -113,6 +113,8 @@ struct Session {
     bool chosen = false;
     int chosen_tiles_x = 0, chosen_rows = 0, chosen_stride = 0, chosen_wy = 0;
     bool coupled = true;
+    int models = 1;   // filter models per group
+    int row_dim = 0;  // filtered row width (patch_dim * channels)
     int device = 0;
     cudaStream_t stream = nullptr;      // the stream all work is enqueued on
     cudaStream_t own_stream = nullptr;  // created by the session
@@ -180,7 +182,7 @@ struct Session {
         DeviceArray<int> row_counts, victims, victim_counts, active, row_offset, row_group, active_prefix, gflags;
         DeviceArray<int2> active_xy;
         DeviceArray<FrameCounters> counters;
-        DeviceArray<float> filtered, weights, gmeans, gram, eig, dual;
+        DeviceArray<float> filtered, weights, gmeans, gram, eig, dual, logw;
     };
     static constexpr int kLaneCount = 2;
     Lane lanes[kLaneCount];
@@ -319,8 +321,6 @@ struct Session {
         require(std::isfinite(p.membership_noise_floor) && p.membership_noise_floor > 0.0f,
                 "membership_noise_floor must be finite and positive");
         require(p.proc_step >= 0, "block_step must be non-negative; use 0 for auto");
-        require(p.couple_channels != 0 || channels == 1,
-                "the CUDA backend currently requires chroma=1 (coupled channels)");
         require(p.device_id >= 0, "device_id must be non-negative");
         require(p.num_streams >= 1 && p.num_streams <= 32, "num_streams must be in the range 1..32");
         require(p.chunk_size > 0, "chunk_size must be positive");
@@ -348,6 +348,9 @@ struct Session {
         patch_dim = P * P * Pt;
         dim = patch_dim * (p.couple_channels ? channels : 1);
         coupled = p.couple_channels != 0 && channels > 1;
+        // uncoupled planes: one model per plane (transform_vnlb_group, core.cpp:848-870)
+        models = (!coupled && channels > 1) ? channels : 1;
+        row_dim = patch_dim * channels;
         search_channels = stage == 1 ? channels : 1;
         K = p.similar;
         soft_cap = cap_of(K, p.similar_cap_factor);
@@ -441,7 +444,7 @@ struct Session {
         const size_t Bmax = static_cast<size_t>(std::min(model_cap, max_rows));
         size_t free_bytes = 0, total_bytes = 0;
         check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
-        const size_t need = kLaneCount * R * (static_cast<size_t>(dim) * 4 + 4 + sizeof(MatchRow) + 4);
+        const size_t need = kLaneCount * R * (static_cast<size_t>(row_dim) * 4 + 4 + sizeof(MatchRow) + 4);
         if (need > free_bytes / 2)
             fail("VNLB CUDA: the group buffers of one anchor frame do not fit in device memory");
         for (Lane& l : lanes) {
@@ -455,12 +458,14 @@ struct Session {
             l.row_offset.allocate(G + 1, "cudaMalloc(row offsets)");
             l.active_prefix.allocate(G + 1, "cudaMalloc(active prefix)");
             l.counters.allocate(1, "cudaMalloc(counters)");
-            l.filtered.allocate(R * dim, "cudaMalloc(filtered rows)");
-            l.gmeans.allocate(G * 2 * dim, "cudaMalloc(group means)");
-            l.gram.allocate(G * Bmax * Bmax, "cudaMalloc(group Gram)");
-            l.eig.allocate(G * std::max(1, p.rank), "cudaMalloc(group eigenvalues)");
-            l.dual.allocate(G * std::max(1, p.rank) * Bmax, "cudaMalloc(group dual vectors)");
-            l.gflags.allocate(G, "cudaMalloc(group flags)");
+            const size_t M = G * models;  // models: one per group, or one per plane when uncoupled
+            l.filtered.allocate(R * row_dim, "cudaMalloc(filtered rows)");
+            l.gmeans.allocate(M * 2 * dim, "cudaMalloc(group means)");
+            l.gram.allocate(M * Bmax * Bmax, "cudaMalloc(group Gram)");
+            l.eig.allocate(M * std::max(1, p.rank), "cudaMalloc(group eigenvalues)");
+            l.dual.allocate(M * std::max(1, p.rank) * Bmax, "cudaMalloc(group dual vectors)");
+            l.gflags.allocate(M, "cudaMalloc(group flags)");
+            if (models > 1) l.logw.allocate(R * models, "cudaMalloc(row log weights)");
             l.weights.allocate(R, "cudaMalloc(row weights)");
             l.row_info.allocate(R, "cudaMalloc(row info)");
             l.row_group.allocate(R, "cudaMalloc(row groups)");
@@ -771,6 +776,9 @@ struct Session {
         fl.rank = params.rank;
         fl.max_rows = max_rows;
         fl.coupled = coupled ? 1 : 0;
+        fl.models = models;
+        fl.row_dim = row_dim;
+        fl.logw = lane.logw.ptr;
         fl.cfg = cfg;
         fl.rows = lane.rows.ptr;
         fl.row_counts = lane.row_counts.ptr;
@@ -798,7 +806,7 @@ struct Session {
         tl.P = P;
         tl.Pt = Pt;
         tl.patch_dim = patch_dim;
-        tl.dim = dim;
+        tl.dim = row_dim;  // filtered row stride
         tl.slots = slots;
         tl.search_bwd = params.search_bwd;
         tl.anchor_frame = anchor;

@@ -143,6 +143,8 @@ struct FilterLaunch {
     int P, Pt, patch_dim, dim;
     int K, model_cap, rank, max_rows;
     int coupled;            // sample-major (coupled, C > 1) vs group path
+    int models;             // models per group: 1, or the planes of an uncoupled clip
+    int row_dim;            // filtered row width: patch_dim * planes (dim when coupled)
     StageConfig cfg;
     const MatchRow* rows;   // [G][max_rows]
     const int* row_counts;
@@ -150,14 +152,16 @@ struct FilterLaunch {
     const int* row_offset;
     FrameCounters* counters;
     int* status;            // session status word (first error wins), not reset per anchor frame
-    // per active group a (intermediates between the three filter kernels)
+    // per model v = active group a * models + plane (intermediates between the
+    // three filter kernels)
     float* means;           // [G][2][dim]: model (membership) mean, reconstruction centre
     float* gram;            // [G][Bmax*Bmax]
     float* eig;             // [G][rank]
     float* dual;            // [G][rank*Bmax]
     int* flags;             // [G]: kGroupDone / kGroupSkip
     // outputs, indexed by global row r = row_offset[a] + i
-    float* filtered;        // [R][dim]
+    float* filtered;        // [R][row_dim]
+    float* logw;            // [R][models], uncoupled only: each plane model's log-weight term
     float* weights;         // [R]
     MatchRow* row_info;     // [R]
     int* row_group;         // [R] active index of the row's group
