@@ -89,6 +89,11 @@ CASES = [
     # uncoupled planes (chroma=0): one model per plane, weights combined over the planes
     ("yuv_uncoupled", 96, 72, 4, 3, 20.0, dict(chroma=0)),
     ("yuv_uncoupled_tau", 80, 64, 4, 3, 25.0, dict(chroma=0, tau=800.0, group_size=12, rank=10)),
+    # covariance models: dimension below 64 (core.cpp:656-658)
+    ("gray_covariance_p4", 48, 40, 4, 1, 15.0, dict(block_size=4, block_step=2, group_size=12, rank=6, bm_range=3)),
+    ("gray_covariance_p7", 64, 48, 4, 1, 20.0, dict(block_size=7, block_step=4, group_size=16, rank=8)),
+    ("yuv_uncoupled_covariance", 48, 40, 3, 3, 15.0, dict(chroma=0, block_size=4, block_step=2, group_size=10,
+                                                          rank=5, bm_range=3)),
 ]
 
 
@@ -221,7 +226,8 @@ def test_constant_video(planes):
 def test_unsupported_configurations_raise():
     gray = np.zeros((3, 1, 32, 32), np.float32)
     with pytest.raises(lib.VNLBError, match="dual-PCA"):
-        vnlb.Basic(gray, sigma=10.0, block_size=4, group_size=8, rank=8)  # covariance model (dim 16)
+        # vnlbcu keeps its rule min(group_size, candidates) < dimension (here 2 x 2 x 2 = 8)
+        vnlbcu.Basic(gray, sigma=10.0, block_size=2, group_size=8, rank=4)
     with pytest.raises(lib.VNLBError, match="chroma=1"):
         vnlbcu.Basic(np.zeros((3, 3, 32, 32), np.float32), sigma=10.0, chroma=0)  # vnlbcu keeps its rule
 

@@ -232,22 +232,47 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
         }
         __syncwarp();
         if (L.rank > 0) {
-            // dual Gram (compute_gram_centered), one pair per lane
             const float scale = __fdiv_rn(1.0f, static_cast<float>(B));
-            float* gram = L.gram + static_cast<size_t>(v) * Bmax * Bmax;
-            const int pairs = B * (B + 1) / 2;
-            // octet k takes pair e0 + k; lane j of the octet runs the pinned
-            // chain j (octet_dot8: the pinned 8-lane order)
-            const int oct = lane >> 3;
-            for (int e0 = 0; e0 < pairs; e0 += 4) {
-                const int e = min(e0 + oct, pairs - 1);
-                int r = 0;
-                while ((r + 1) * (r + 2) / 2 <= e) ++r;
-                const int c = e - r * (r + 1) / 2;
-                const float v = __fmul_rn(scale, octet_dot8(X + r * ldx, X + c * ldx, D, lane & 7));
-                if ((lane & 7) == 0 && e0 + oct < pairs) {
-                    gram[r * B + c] = v;
-                    gram[c * B + r] = v;
+            float* gram = L.gram + static_cast<size_t>(v) * L.nmax * L.nmax;
+            if (D >= 64 && B < D) {
+                // dual Gram (compute_gram_centered): octet k takes pair e0 + k;
+                // lane j of the octet runs the pinned chain j (octet_dot8)
+                const int pairs = B * (B + 1) / 2;
+                const int oct = lane >> 3;
+                for (int e0 = 0; e0 < pairs; e0 += 4) {
+                    const int e = min(e0 + oct, pairs - 1);
+                    int r = 0;
+                    while ((r + 1) * (r + 2) / 2 <= e) ++r;
+                    const int c = e - r * (r + 1) / 2;
+                    const float val = __fmul_rn(scale, octet_dot8(X + r * ldx, X + c * ldx, D, lane & 7));
+                    if ((lane & 7) == 0 && e0 + oct < pairs) {
+                        gram[r * B + c] = val;
+                        gram[c * B + r] = val;
+                    }
+                }
+            } else {
+                // covariance (compute_covariance_centered, linalg.cpp:378-412):
+                // per sample, row r gets x[r] * x[r..] through
+                // add_scaled_contiguous_highway, fused on the full 8-lane chunks of
+                // the D - r columns it spans; then scaled, both triangles
+                const int entries = D * (D + 1) / 2;
+                for (int e = lane; e < entries; e += 32) {
+                    int r = 0, rem = e;
+                    while (rem >= D - r) {
+                        rem -= D - r;
+                        ++r;
+                    }
+                    const int c = r + rem;
+                    const bool fused = fused_column(rem, D - r);
+                    float acc = 0.0f;
+                    for (int s2 = 0; s2 < B; ++s2) {
+                        const float left = X[s2 * ldx + r];
+                        const float x = X[s2 * ldx + c];
+                        acc = fused ? __fmaf_rn(left, x, acc) : __fadd_rn(acc, __fmul_rn(left, x));
+                    }
+                    const float val = __fmul_rn(acc, scale);
+                    gram[r * D + c] = val;
+                    gram[c * D + r] = val;
                 }
             }
         }
@@ -262,7 +287,8 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
 // at most 32); lane r of the segment owns matrix rows r, r + seg, ...
 __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg, int ld, int gstride) {
     extern __shared__ __align__(16) float sm[];
-    const int Bmax = bmax_of(L);
+    const int N = L.nmax;  // largest matrix dimension (model rows, or the dimension for covariance models)
+    const int D = L.dim;
     const int R = L.rank;
     const int lane = threadIdx.x & 31;
     const int groups_per_warp = 32 / seg;
@@ -270,20 +296,21 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg, in
     const int r0 = lane % seg;
     const unsigned seg_mask = seg == 32 ? 0xffffffffu : (((1u << seg) - 1u) << ((lane / seg) * seg));
     float* m = sm + static_cast<size_t>(slot) * gstride;
-    float* v = m + Bmax * ld;
-    int* order = reinterpret_cast<int*>(v + Bmax * ld);
+    float* v = m + N * ld;
+    int* order = reinterpret_cast<int*>(v + N * ld);
     const int models_total = L.counters->active * L.models;
     const int slots_per_cta = (blockDim.x >> 5) * groups_per_warp;
     for (int base = blockIdx.x * slots_per_cta; base < models_total; base += gridDim.x * slots_per_cta) {
         const int a = base + slot;  // model index (group x model channel)
         bool valid = a < models_total && R > 0;
-        int B = 0;
+        int B = 0;  // matrix dimension: the dual Gram's B, or the covariance's D
         if (valid) {
             valid = L.flags[a] == 0;
-            B = min(L.row_counts[L.active[a / L.models]], L.model_cap);
+            const int Bm = min(L.row_counts[L.active[a / L.models]], L.model_cap);
+            B = (D >= 64 && Bm < D) ? Bm : D;  // use_dual_pca (core.cpp:656-658)
         }
         if (!valid) B = 0;
-        const float* gram = L.gram + static_cast<size_t>(max(a, 0)) * Bmax * Bmax;
+        const float* gram = L.gram + static_cast<size_t>(max(a, 0)) * N * N;
         float mx = 0.0f;
         for (int r = r0; r < B; r += seg) {
             for (int c = 0; c < B; ++c) {
@@ -304,8 +331,8 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg, in
                 for (int o = seg / 2; o > 0; o >>= 1) off = fmaxf(off, __shfl_xor_sync(0xffffffffu, off, o));
                 const bool busy = B > 1 && !(off <= threshold);
                 if (!__any_sync(0xffffffffu, busy)) break;
-                for (int p = 0; p + 1 < Bmax; ++p) {
-                    for (int q = p + 1; q < Bmax; ++q) {
+                for (int p = 0; p + 1 < N; ++p) {
+                    for (int q = p + 1; q < N; ++q) {
                         bool rot = false;
                         float app = 0.0f, aqq = 0.0f, apq = 0.0f;
                         if (busy && q < B) {
@@ -373,7 +400,7 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg, in
         __syncwarp();
         if (valid) {
             float* eig = L.eig + static_cast<size_t>(a) * R;
-            float* dual = L.dual + static_cast<size_t>(a) * R * Bmax;
+            float* dual = L.dual + static_cast<size_t>(a) * R * N;
             for (int out = r0; out < R; out += seg) {
                 const int src = order[out];
                 eig[out] = m[src * ld + src];
@@ -396,7 +423,7 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg, in
                 }
                 for (int r = 0; r < B; ++r) {
                     const float x = v[r * ld + src];
-                    dual[out * Bmax + r] = scale ? __fmul_rn(x, sc) : x;
+                    dual[out * N + r] = scale ? __fmul_rn(x, sc) : x;
                 }
             }
         }
@@ -500,7 +527,10 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
         const int B = min(S, L.model_cap);
         const float* gm = L.means + static_cast<size_t>(mi) * 2 * D;
         for (int i = tid; i < 2 * D; i += kApplyThreads) means[i] = gm[i];
-        for (int i = tid; i < R * Bmax; i += kApplyThreads) dual[i] = L.dual[static_cast<size_t>(mi) * R * Bmax + i];
+        const int N = L.nmax;  // row stride of the eigenvector rows
+        const bool dual_model = D >= 64 && B < D;  // use_dual_pca (core.cpp:656-658)
+        for (int i = tid; i < R * Bmax; i += kApplyThreads)
+            dual[i] = L.dual[static_cast<size_t>(mi) * R * N + (i / Bmax) * N + i % Bmax];
         // row bases of this model's plane
         for (int i = tid; i < S; i += kApplyThreads) bases[i] = row_base(L, rows[i]) + mc * hw;
         // per-component scalars, computed once per group (same operations as
@@ -522,7 +552,14 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
         __syncthreads();
         const float* member_mean = means;
         const float* center_vec = means + D;
-        if (R > 0) {
+        if (R > 0 && !dual_model) {
+            // covariance model: the canonicalised eigenvectors are the basis
+            for (int b = warp; b < R; b += kApplyWarps)
+                for (int col = lane; col < D; col += 32)
+                    basis[b * ldb + col] = L.dual[static_cast<size_t>(mi) * R * N + static_cast<size_t>(b) * N + col];
+            __syncthreads();
+        }
+        if (R > 0 && dual_model) {
             // centred model rows (compute_mean + center_rows of the first B rows)
             for (int s = warp; s < B; s += kApplyWarps) {
                 const float* src = model_video + bases[s];
@@ -1128,15 +1165,16 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
         // a segment of `seg` lanes per group, each lane owning rows r0, r0 + seg,
         // ...; two rows per lane from 8 rows up, which halves the rotation
         // parameters every lane recomputes
+        const int N = L.nmax;  // largest matrix: model rows, or the dimension of covariance models
         int seg = 1;
-        while (seg < Bmax && seg < 32) seg <<= 1;
+        while (seg < N && seg < 32) seg <<= 1;
         if (seg >= 8) seg /= 2;
         seg = std::max(seg, 1);
         // rows padded to Bmax + 1 and groups to gstride floats: for Bmax = 8
         // (segments of 4, 8 groups per warp, gstride = 4 mod 32) the lanes of
         // a warp touch 32 distinct banks
-        const int ld = Bmax + 1;
-        int gstride = 2 * Bmax * ld + Bmax;
+        const int ld = N + 1;
+        int gstride = 2 * N * ld + N;
         if (seg == 4) gstride += ((4 - gstride % 32) + 32) % 32;
         const size_t per_group = static_cast<size_t>(gstride) * sizeof(float);
         int warps = 8;
@@ -1151,7 +1189,7 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
         if ((err = cudaGetLastError()) != cudaSuccess) return err;
     }
     // apply
-    if (R <= 8 && Bmax <= 8 && (D == 64 || D == 128 || D == 192 || D == 256)) {
+    if (R <= 8 && Bmax <= 8 && L.nmax == Bmax && (D == 64 || D == 128 || D == 192 || D == 256)) {
         cudaError_t err = D == 64    ? launch_apply_warp<64>(L, max_groups, stream)
                           : D == 128 ? launch_apply_warp<128>(L, max_groups, stream)
                           : D == 192 ? launch_apply_warp<192>(L, max_groups, stream)

@@ -114,6 +114,8 @@ struct Session {
     int chosen_tiles_x = 0, chosen_rows = 0, chosen_stride = 0, chosen_wy = 0;
     bool coupled = true;
     int models = 1;   // filter models per group
+    bool covariance_possible = false;  // some group takes the dim x dim covariance model
+    int nmax = 0;                      // largest eigen problem of a group
     int row_dim = 0;  // filtered row width (patch_dim * channels)
     int device = 0;
     cudaStream_t stream = nullptr;      // the stream all work is enqueued on
@@ -375,9 +377,9 @@ struct Session {
                                 retained_max));
         if (basis > 128) fail("VNLB CUDA: the CUDA dual-PCA filter supports at most 128 model samples");
         if (p.rank > basis) fail("VNLB CUDA: rank must not exceed min(group_size, candidate_count)");
-        if (!(dim >= 64 && basis < dim))
-            fail("VNLB CUDA: the CUDA backend currently requires the dual-PCA path (min(group_size, "
-                 "candidate_count) must be smaller than the coupled patch dimension, which must be at least 64)");
+        // groups whose model rows reach the dimension, or below dimension 64,
+        // take the covariance model (use_dual_pca, core.cpp:656-658)
+        covariance_possible = !(dim >= 64 && basis < dim);
         if (slots > kMaxContributors || p.search_bwd + p.search_fwd + 1 > kMaxContributors)
             fail("VNLB CUDA: search_bwd + search_fwd + patch_time must be at most 32");
         if (channels > 4) fail("VNLB CUDA: at most four planes are supported");
@@ -442,6 +444,8 @@ struct Session {
         const size_t G = static_cast<size_t>(max_groups);
         const size_t R = G * max_rows;
         const size_t Bmax = static_cast<size_t>(std::min(model_cap, max_rows));
+        nmax = static_cast<int>(covariance_possible ? std::max<size_t>(Bmax, dim) : Bmax);
+        if (nmax > 96) fail("VNLB CUDA: eigen problems above 96 x 96 (model rows or covariance dimension) are not supported");
         size_t free_bytes = 0, total_bytes = 0;
         check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
         const size_t need = kLaneCount * R * (static_cast<size_t>(row_dim) * 4 + 4 + sizeof(MatchRow) + 4);
@@ -459,11 +463,12 @@ struct Session {
             l.active_prefix.allocate(G + 1, "cudaMalloc(active prefix)");
             l.counters.allocate(1, "cudaMalloc(counters)");
             const size_t M = G * models;  // models: one per group, or one per plane when uncoupled
+            const size_t N = static_cast<size_t>(nmax);
             l.filtered.allocate(R * row_dim, "cudaMalloc(filtered rows)");
             l.gmeans.allocate(M * 2 * dim, "cudaMalloc(group means)");
-            l.gram.allocate(M * Bmax * Bmax, "cudaMalloc(group Gram)");
+            l.gram.allocate(M * N * N, "cudaMalloc(group Gram)");
             l.eig.allocate(M * std::max(1, p.rank), "cudaMalloc(group eigenvalues)");
-            l.dual.allocate(M * std::max(1, p.rank) * Bmax, "cudaMalloc(group dual vectors)");
+            l.dual.allocate(M * std::max(1, p.rank) * N, "cudaMalloc(group eigenvectors)");
             l.gflags.allocate(M, "cudaMalloc(group flags)");
             if (models > 1) l.logw.allocate(R * models, "cudaMalloc(row log weights)");
             l.weights.allocate(R, "cudaMalloc(row weights)");
@@ -777,6 +782,7 @@ struct Session {
         fl.max_rows = max_rows;
         fl.coupled = coupled ? 1 : 0;
         fl.models = models;
+        fl.nmax = nmax;
         fl.row_dim = row_dim;
         fl.logw = lane.logw.ptr;
         fl.cfg = cfg;

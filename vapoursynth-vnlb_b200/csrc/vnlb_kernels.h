@@ -144,6 +144,7 @@ struct FilterLaunch {
     int K, model_cap, rank, max_rows;
     int coupled;            // sample-major (coupled, C > 1) vs group path
     int models;             // models per group: 1, or the planes of an uncoupled clip
+    int nmax;               // largest eigen problem: model rows, or dim where a covariance model occurs
     int row_dim;            // filtered row width: patch_dim * planes (dim when coupled)
     StageConfig cfg;
     const MatchRow* rows;   // [G][max_rows]
@@ -155,9 +156,9 @@ struct FilterLaunch {
     // per model v = active group a * models + plane (intermediates between the
     // three filter kernels)
     float* means;           // [G][2][dim]: model (membership) mean, reconstruction centre
-    float* gram;            // [G][Bmax*Bmax]
+    float* gram;            // [G][nmax*nmax]: dual Gram (B x B) or covariance (dim x dim)
     float* eig;             // [G][rank]
-    float* dual;            // [G][rank*Bmax]
+    float* dual;            // [G][rank][nmax]: dual vectors (B long) or covariance eigenvectors (dim long)
     int* flags;             // [G]: kGroupDone / kGroupSkip
     // outputs, indexed by global row r = row_offset[a] + i
     float* filtered;        // [R][row_dim]

@@ -9,8 +9,9 @@ parse_stage_parameters (plugin.cpp:372-449) and parse_temporal_parameters
 per anchor frame a stack frame of height H * 2 * slots per plane, numerator
 rows slot*2H + y and weight rows slot*2H + H + y, the weight repeated in every
 plane.  vnlb.Aggregate divides the summed stacks (render_aggregate_frame,
-plugin.cpp:966-1045).  The GPU path implements the configurations the B200
-kernels cover (coupled channels, dual-PCA model); others raise.
+plugin.cpp:966-1045).  The GPU path implements the CPU core's stage for
+coupled and uncoupled planes, the dual-PCA and the covariance models and any
+model cap; eigen problems above 96 x 96 and MVTools search centres raise.
 """
 from __future__ import annotations
 
