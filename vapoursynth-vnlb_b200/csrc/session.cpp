@@ -111,7 +111,7 @@ struct Session {
     // (VNLBGPU_FORM_CHOSEN_TC: BF16 tensor-core distances, match_chosen.cu)
     bool approx = false;
     bool chosen = false;
-    int chosen_tiles_x = 0, chosen_rows = 0, chosen_stride = 0, chosen_wy = 0;
+    int chosen_tiles_x = 0, chosen_wy = 0, approx_stride = 0;
     bool coupled = true;
     int models = 1;   // filter models per group
     bool covariance_possible = false;  // some group takes the dim x dim covariance model
@@ -185,6 +185,7 @@ struct Session {
         DeviceArray<int2> active_xy;
         DeviceArray<FrameCounters> counters;
         DeviceArray<float> filtered, weights, gmeans, gram, eig, dual, logw;
+        DeviceArray<float> approx;  // tensor-core form: approximate distances [G][approx_stride]
     };
     static constexpr int kLaneCount = 2;
     Lane lanes[kLaneCount];
@@ -425,20 +426,21 @@ struct Session {
             if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
         }
         if (warps < 1) fail("VNLB CUDA: the search region of one anchor does not fit in shared memory");
-        // chosen matcher: strips of up to kChosenAnchors anchors, 8-column tiles
-        if (p.form == VNLBGPU_FORM_CHOSEN_TC && chosen_match_supported(P, search_channels * Pt)) {
+        // tensor-core matcher: strips of up to kChosenAnchors anchors whose
+        // windows lie within kChosenCols candidate columns
+        if (p.form == VNLBGPU_FORM_CHOSEN_TC && chosen_match_supported(P, search_channels * Pt, cw0, ch0)) {
             MatchLaunch probe{};
             probe.P = P;
             probe.Pt = Pt;
             probe.search_channels = search_channels;
             probe.window_rows = chosen_wy = ch0;
-            probe.region_rows = chosen_rows = ch0 + P - 1;
-            probe.tiles_x = chosen_tiles_x = ((kChosenAnchors - 1) * step + cw0 + 7) / 8;
-            probe.region_stride = chosen_stride = 8 * chosen_tiles_x + 8;
+            probe.tiles_x = chosen_tiles_x = kChosenCols / 8;
             probe.window_cells = cw0 * ch0;
-            // the register replay: the buffer and the K front fit in a warp
-            chosen = cap_eff <= 32 && K <= 32 && 64 <= cw0 * ch0 && cw0 * ch0 <= kChosenMaxCells &&
+            // the register replay: the buffer and the K front fit in a warp;
+            // each anchor's distance array doubles as its 32 + 32 sorted rows
+            chosen = cap_eff <= 32 && K <= 32 && 64 <= cw0 * ch0 &&
                      chosen_match_shared_bytes(probe) <= 227 * 1024;
+            approx_stride = sched_max * cw0 * ch0;
         }
 
         const size_t G = static_cast<size_t>(max_groups);
@@ -462,6 +464,7 @@ struct Session {
             l.row_offset.allocate(G + 1, "cudaMalloc(row offsets)");
             l.active_prefix.allocate(G + 1, "cudaMalloc(active prefix)");
             l.counters.allocate(1, "cudaMalloc(counters)");
+            if (chosen) l.approx.allocate(G * approx_stride, "cudaMalloc(approximate distances)");
             const size_t M = G * models;  // models: one per group, or one per plane when uncoupled
             const size_t N = static_cast<size_t>(nmax);
             l.filtered.allocate(R * row_dim, "cudaMalloc(filtered rows)");
@@ -734,12 +737,15 @@ struct Session {
         m.victims = lane.victims.ptr;
         m.victim_counts = lane.victim_counts.ptr;
         m.victim_stride = victim_stride;
+        m.status = d_status.ptr;
         cudaEvent_t t0 = begin_timed(ls);
         if (chosen) {
             m.strips = grid.d_strips_chosen.ptr;
-            m.region_rows = chosen_rows;
-            m.region_stride = chosen_stride;
             m.tiles_x = chosen_tiles_x;
+            m.approx_dist = lane.approx.ptr;
+            m.approx_stride = approx_stride;
+            m.anchor_count = static_cast<int>(grid.anchors.size());
+            m.strip_count = static_cast<int>(grid.strips_chosen.size());
             m.window_rows = chosen_wy;
             check(launch_match_chosen(m, static_cast<int>(grid.strips_chosen.size()), ls), "match kernel launch");
         } else {
@@ -905,6 +911,8 @@ struct Session {
         if (status != 0) {
             check(cudaMemsetAsync(d_status.ptr, 0, sizeof(int), stream), "cudaMemsetAsync(status)");
             if (status == kStatusRankNotCovered) fail("VNLB CUDA: group_size must cover the effective VNLB rank");
+            if (status == kStatusTensorTimeout)
+                fail("VNLB CUDA: the tensor-core matcher timed out waiting for its MMAs");
             fail("VNLB CUDA: device status " + std::to_string(status));
         }
     }

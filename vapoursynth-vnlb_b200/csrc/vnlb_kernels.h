@@ -49,8 +49,13 @@ struct MatchLaunch {
     int warp_floats;      // shared floats per warp
     int approx;           // chosen form in this matcher: approximate distances, exact re-rank
     // tensor-core form (match_chosen.cu)
-    int tiles_x;          // 8-column candidate tiles per strip
+    int tiles_x;          // 8-column candidate blocks per strip
     int window_rows;      // max Wy
+    int* status;          // session status word (kStatus* codes, first error wins)
+    float* approx_dist;   // [anchor][approx_stride] approximate distances (tensor-core form)
+    int approx_stride;    // >= schedule_len * window_cells
+    int anchor_count;     // grid anchors of this anchor frame
+    int strip_count;      // strips of the launch (tensor-core form)
     // outputs
     MatchRow* rows;       // [G][max_rows]
     int* row_counts;      // [G]
@@ -59,42 +64,19 @@ struct MatchLaunch {
     int victim_stride;
 };
 
-// Chosen form: a CTA of kChosenWarps warps matches up to kChosenAnchors
-// anchors (rows of a tensor-core tile; the other 8 rows are zero).  Shared
-// layout in floats: FP32 planes, their BF16 copies, candidate norms,
-// approximate distances (the
-// row sums of squares alias them), BF16 and FP32 reference patches, reference
-// norms and windows.
+// Chosen form on tensor cores (match_chosen.cu): a CTA of kChosenWarps warps
+// matches up to kChosenAnchors consecutive anchors of one grid row whose
+// search windows lie within kChosenCols consecutive candidate columns.  One
+// tcgen05 MMA (M = 128, N = 16, K = 16) covers two candidate rows of those
+// columns against every anchor of the strip, so the window may have at most
+// 2 * 16 rows (16 row pairs of 16 accumulator columns fill kChosenTmemCols).
 constexpr int kChosenAnchors = 8;
 constexpr int kChosenWarps = 8;
-constexpr int kChosenMaxCells = 512;  // window cells per anchor (values a lane holds: 16)
+constexpr int kChosenCols = 64;
+constexpr int kChosenMaxRows = 32;
+constexpr int kChosenTmemCols = 256;
 
-struct ChosenLayout {
-    int region, ebf, obf, nb, dist, abf, reff, na, win, floats;
-};
-
-__host__ __device__ inline ChosenLayout chosen_layout(int planes_n, int rows, int stride, int tiles_x, int wy,
-                                                      int cells, int kd) {
-    ChosenLayout l{};
-    const int plane = rows * stride;
-    int off = 0;
-    l.region = off; off += planes_n * plane;
-    // BF16 copies: as loaded, and shifted left by one column (its start 16
-    // banks after the first, so even and odd lanes use disjoint banks)
-    l.ebf = off;    off += (planes_n * plane + 1) / 2;
-    off += (48 - (off - l.ebf) % 32) % 32;
-    l.obf = off;    off += (planes_n * plane + 1) / 2 + 1;
-    l.nb = off;     off += wy * 8 * tiles_x;
-    l.dist = off;   off += kChosenAnchors * cells > rows * 8 * tiles_x ? kChosenAnchors * cells : rows * 8 * tiles_x;
-    l.abf = off;    off += kChosenAnchors * kd / 2;
-    l.reff = off;   off += kChosenAnchors * kd;
-    l.na = off;     off += kChosenAnchors;
-    l.win = off;    off += 2 * kChosenAnchors;
-    l.floats = (off + 3) & ~3;
-    return l;
-}
-
-bool chosen_match_supported(int P, int planes_n);
+bool chosen_match_supported(int P, int planes_n, int window_w, int window_h);
 size_t chosen_match_shared_bytes(const MatchLaunch& L);
 cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t stream);
 
@@ -112,6 +94,7 @@ struct FrameCounters {
 
 constexpr int kStatusRankNotCovered = 1;  // fewer model rows than the rank
 constexpr int kStatusPasteCapacity = 2;   // too many anchors for the paste kernel
+constexpr int kStatusTensorTimeout = 3;   // an MMA completion wait ran out (tensor-core matcher)
 
 struct PasteLaunch {
     int groups;
