@@ -89,9 +89,11 @@ typedef struct vnlbgpu_params {
  * norms), runs the CPU's selection on those values, re-computes the exact
  * FP32 distance of every retained candidate and selects on the exact values:
  * within a PSNR tolerance of PLAIN rather than bit-identical.  CHOSEN_TC does
- * the same with the dot products on BF16 tensor cores.  Both apply to 8x8
- * patches with a buffer of at most 32 patches (group_size * cap_factor) and
- * group_size <= 32; other configurations run PLAIN. */
+ * the same with the dot products on BF16 tensor cores (tcgen05, FP32
+ * accumulation in tensor memory) and also needs a search window of at most 64
+ * columns by 32 rows.  Both apply to 8x8 patches with a buffer of at most 32
+ * patches (group_size * cap_factor) and group_size <= 32; other
+ * configurations run PLAIN. */
 #define VNLBGPU_FORM_PLAIN 0
 #define VNLBGPU_FORM_CHOSEN 1
 #define VNLBGPU_FORM_CHOSEN_TC 2

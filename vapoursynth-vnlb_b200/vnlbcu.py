@@ -125,7 +125,7 @@ def parse_parameters(stage: int, clip: np.ndarray, sigma, args: dict) -> lib.Par
     # matcher form (no reference counterpart): "plain" reproduces the CPU core
     # bit for bit; "chosen" selects on approximate distances and re-ranks the
     # retained candidates exactly; "chosen_tc" computes the approximate
-    # distances on BF16 tensor cores
+    # distances on BF16 tensor cores (tcgen05, FP32 accumulation)
     p["form"] = lib.FORM_PLAIN
     if "form" in given:
         forms = {"plain": lib.FORM_PLAIN, "chosen": lib.FORM_CHOSEN, "chosen_tc": lib.FORM_CHOSEN_TC}
