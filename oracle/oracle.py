@@ -80,6 +80,48 @@ class StageParams:
         return self.search_bwd + self.search_fwd + self.patch_time
 
 
+class _CFlowGrids(ctypes.Structure):
+    _fields_ = [("present", ctypes.c_int), ("block_size_x", ctypes.c_int), ("block_size_y", ctypes.c_int),
+                ("pel", ctypes.c_int), ("overlap_x", ctypes.c_int), ("overlap_y", ctypes.c_int),
+                ("block_count_x", ctypes.c_int), ("block_count_y", ctypes.c_int),
+                ("usable", ctypes.POINTER(ctypes.c_ubyte)), ("vectors", ctypes.POINTER(ctypes.c_int))]
+
+
+class _CFlow(ctypes.Structure):
+    _fields_ = [("fw", _CFlowGrids), ("bw", _CFlowGrids)]
+
+
+@dataclass(frozen=True)
+class FlowGrids:
+    """One direction of motion vectors (vnlb_flow_grids, oracle/vnlb_oracle.h):
+    the MVTools block geometry, a usable flag per frame and the finest-level
+    vectors [frames][block_count_y][block_count_x][2] in sub-pel units."""
+    block_size_x: int
+    block_size_y: int
+    pel: int
+    overlap_x: int
+    overlap_y: int
+    usable: np.ndarray
+    vectors: np.ndarray
+
+
+def c_flow(fw: FlowGrids | None, bw: FlowGrids | None):
+    """-> (vnlb_flow, the arrays it points into)."""
+    keep = []
+
+    def grids(g):
+        if g is None:
+            return _CFlowGrids()
+        usable = np.ascontiguousarray(g.usable, dtype=np.uint8)
+        vectors = np.ascontiguousarray(g.vectors, dtype=np.int32)
+        keep.extend([usable, vectors])
+        return _CFlowGrids(1, g.block_size_x, g.block_size_y, g.pel, g.overlap_x, g.overlap_y, vectors.shape[2],
+                           vectors.shape[1], usable.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                           vectors.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+
+    return _CFlow(grids(fw), grids(bw)), keep
+
+
 def cpu_params(stage: int, sigma: float, **kw) -> StageParams:
     """The vnlb.Basic / vnlb.Final argument rules of parse_stage_parameters
     (src/vs/plugin.cpp:372-449): 8-bit sigma and tau, radius, bm_range and the
@@ -132,7 +174,8 @@ class Oracle:
 
     def stage_stacks(self, stage: int, params: StageParams, clip: np.ndarray,
                      basic: np.ndarray | None = None, first_anchor: int = 0,
-                     anchor_count: int | None = None, threads: int | None = None):
+                     anchor_count: int | None = None, threads: int | None = None,
+                     flow: tuple[FlowGrids | None, FlowGrids | None] | None = None):
         clip = np.ascontiguousarray(clip, dtype=np.float32)
         frames, channels, height, width = clip.shape
         if basic is not None:
@@ -142,6 +185,13 @@ class Oracle:
         threads = threads or os.cpu_count() or 1
         out = np.zeros((anchor_count, channels, params.slots * 2 * height, width), np.float32)
         cp = params.to_c()
+        if flow is not None:
+            cf, keep = c_flow(*flow)
+            self._check(self._fn("stage_stacks_flow")(
+                ctypes.c_int(stage), ctypes.byref(cp), self._ptr(clip), self._ptr(basic),
+                width, height, frames, channels, first_anchor, anchor_count, threads,
+                ctypes.byref(cf), self._ptr(out)))
+            return out
         self._check(self._fn("stage_stacks")(
             ctypes.c_int(stage), ctypes.byref(cp), self._ptr(clip), self._ptr(basic),
             width, height, frames, channels, first_anchor, anchor_count, threads,
@@ -185,7 +235,7 @@ ROW_DTYPE = [("distance", "f4"), ("x", "i4"), ("y", "i4"), ("frame", "i4"), ("we
 
 
 def anchor_groups(stage: int, params: StageParams, clip: np.ndarray, basic: np.ndarray | None,
-                  anchor: int):
+                  anchor: int, flow: tuple[FlowGrids | None, FlowGrids | None] | None = None):
     """Restatement only: the processed groups of one anchor frame in raster
     order -> (stack, groups [(x, y, S, first)], rows structured array)."""
     o = Oracle("port")
@@ -196,15 +246,17 @@ def anchor_groups(stage: int, params: StageParams, clip: np.ndarray, basic: np.n
     stack = np.zeros((channels, params.slots * 2 * height, width), np.float32)
     cp = params.to_c()
     total = ctypes.c_int()
-    fn = o.lib.vnlboracle_anchor_groups
+    cf, keep = c_flow(*flow) if flow is not None else (None, [])
+    fref = ctypes.byref(cf) if cf is not None else None
+    fn = o.lib.vnlboracle_anchor_groups_flow
     n = fn(ctypes.c_int(stage), ctypes.byref(cp), o._ptr(clip), o._ptr(basic), width, height, frames,
-           channels, anchor, o._ptr(stack), None, 0, None, 0, ctypes.byref(total))
+           channels, anchor, fref, o._ptr(stack), None, 0, None, 0, ctypes.byref(total))
     if n < 0:
         o._check(-1)
     groups = (_Group * max(1, n))()
     matches = (_Match * max(1, total.value))()
     fn(ctypes.c_int(stage), ctypes.byref(cp), o._ptr(clip), o._ptr(basic), width, height, frames, channels,
-       anchor, o._ptr(stack), groups, n, matches, total.value, ctypes.byref(total))
+       anchor, fref, o._ptr(stack), groups, n, matches, total.value, ctypes.byref(total))
     g = [(x.anchor_x, x.anchor_y, x.similar, x.first_match) for x in groups[:n]]
     rows = np.array([(m.distance, m.x, m.y, m.frame, m.weight) for m in matches[:total.value]], dtype=ROW_DTYPE)
     return stack, g, rows

@@ -9,7 +9,11 @@
 //   * vnlbref_aggregate     = render_aggregate_frame (src/vs/plugin.cpp:966-1045)
 //   * vnlbref_chain         = Basic -> Aggregate -> Final(ref) -> Aggregate,
 //                             frames spread over std::threads with one
-//                             workspace per thread, as fmParallel does.
+//                             workspace per thread, as fmParallel does;
+//   * vnlbref_stage_stacks_flow: render_stage_frame with mvfw / mvbw clips,
+//                             the reference's MVToolsVectorGrid objects of the
+//                             anchor's input window handed to its
+//                             MVToolsFlowProvider (plugin.cpp:697-729).
 #include "vnlb_oracle.h"
 
 #include "aggregate/aggregate.hpp"
@@ -70,12 +74,34 @@ int slot_count(const StageParameters& p) {
     return p.search_bwd + p.search_fwd + p.patch_time;
 }
 
+// The reference's grid object of one frame of one direction.
+vnlb::flow::MVToolsVectorGrid make_grid(const vnlb_flow_grids& g, int frame) {
+    vnlb::flow::MVToolsVectorGrid grid;
+    grid.analysis.block_size_x = g.block_size_x;
+    grid.analysis.block_size_y = g.block_size_y;
+    grid.analysis.pel = g.pel;
+    grid.analysis.overlap_x = g.overlap_x;
+    grid.analysis.overlap_y = g.overlap_y;
+    grid.analysis.block_count_x = g.block_count_x;
+    grid.analysis.block_count_y = g.block_count_y;
+    grid.analysis.delta_frame = 1;
+    grid.valid = g.usable[frame] != 0;
+    const std::size_t count = static_cast<std::size_t>(g.block_count_x) * g.block_count_y;
+    grid.vectors.resize(count);
+    const int* v = g.vectors + static_cast<std::size_t>(frame) * count * 2;
+    for (std::size_t i = 0; i < count; ++i) {
+        grid.vectors[i].x = v[2 * i];
+        grid.vectors[i].y = v[2 * i + 1];
+    }
+    return grid;
+}
+
 // render_stage_frame (src/vs/plugin.cpp:616-758) without VapourSynth: the
 // local frame window is [range.first, range.last] of the whole clip.
 void stage_stack(int stage, const StageParameters& parameters,
                  const float* clip, const float* basic, int width, int height,
                  int frames, int channels, int anchor_frame, float* stack,
-                 StageWorkspace& workspace) {
+                 StageWorkspace& workspace, const vnlb_flow* flow = nullptr) {
     const VideoGeometry full{width, height, frames, channels, 0, frames};
     const auto layout = vnlb::aggregate::make_contribution_layout(
         full, parameters.search_bwd, parameters.search_fwd,
@@ -114,17 +140,42 @@ void stage_stack(int stage, const StageParameters& parameters,
                               range.first, frames};
     const ConstVideoView clip_view(
         std::span<const ConstPlaneView>(clip_planes), local);
-    const vnlb::flow::SameLocationProvider flow;
+    if (flow != nullptr && (flow->fw.present || flow->bw.present)) {
+        // build_mvtools_grid_window + MVToolsFlowProvider(mvfw, mvbw)
+        std::vector<vnlb::flow::MVToolsVectorGrid> fw, bw;
+        std::vector<const vnlb::flow::MVToolsVectorGrid*> fw_ptrs, bw_ptrs;
+        for (int f = range.first; f <= range.last; ++f) {
+            if (flow->fw.present) fw.push_back(make_grid(flow->fw, f));
+            if (flow->bw.present) bw.push_back(make_grid(flow->bw, f));
+        }
+        for (auto& g : fw) fw_ptrs.push_back(&g);
+        for (auto& g : bw) bw_ptrs.push_back(&g);
+        const vnlb::flow::MVToolsFlowProvider provider(
+            std::span<const vnlb::flow::MVToolsVectorGrid* const>(fw_ptrs.data(), fw_ptrs.size()), range.first,
+            std::span<const vnlb::flow::MVToolsVectorGrid* const>(bw_ptrs.data(), bw_ptrs.size()), range.first);
+        if (stage == VNLB_STAGE_BASIC) {
+            vnlb::core::process_basic_anchor_mvtools(clip_view, anchor_frame, parameters, provider, contributions,
+                                                     workspace);
+        } else {
+            const ConstVideoView ref_view(std::span<const ConstPlaneView>(ref_planes), local);
+            vnlb::core::process_final_anchor_mvtools(clip_view, ref_view, anchor_frame, parameters, provider,
+                                                     contributions, workspace);
+        }
+        return;
+    }
+    const vnlb::flow::SameLocationProvider flow_same;
+    const auto& flow_provider = flow_same;
     if (stage == VNLB_STAGE_BASIC) {
         vnlb::core::process_basic_anchor_no_flow(clip_view, anchor_frame,
-                                                 parameters, flow,
+                                                 parameters, flow_provider,
                                                  contributions, workspace);
     } else {
         const ConstVideoView ref_view(
             std::span<const ConstPlaneView>(ref_planes), local);
         vnlb::core::process_final_anchor_no_flow(clip_view, ref_view,
-                                                 anchor_frame, parameters, flow,
-                                                 contributions, workspace);
+                                                 anchor_frame, parameters,
+                                                 flow_provider, contributions,
+                                                 workspace);
     }
 }
 
@@ -241,6 +292,27 @@ int vnlbref_stage_stacks(int stage, const vnlb_stage_params* params,
                                         frames, channels, first_anchor + index,
                                         stacks + stack_values * index,
                                         workspace);
+                        });
+    });
+}
+
+int vnlbref_stage_stacks_flow(int stage, const vnlb_stage_params* params,
+                              const float* clip, const float* basic, int width,
+                              int height, int frames, int channels,
+                              int first_anchor, int anchor_count, int threads,
+                              const vnlb_flow* flow, float* stacks) {
+    return guarded([&]() {
+        const StageParameters p = to_core(*params);
+        vnlb::core::validate_stage_configuration(
+            VideoGeometry{width, height, frames, channels, 0, frames}, p);
+        const std::size_t stack_values = static_cast<std::size_t>(channels) *
+                                         slot_count(p) * 2 * height * width;
+        parallel_frames(anchor_count, threads,
+                        [&](int index, StageWorkspace& workspace) {
+                            stage_stack(stage, p, clip, basic, width, height,
+                                        frames, channels, first_anchor + index,
+                                        stacks + stack_values * index,
+                                        workspace, flow);
                         });
     });
 }

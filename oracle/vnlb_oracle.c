@@ -283,6 +283,7 @@ static void partial_sort_matches(match* a, int middle, int last) {
 /* Workspace.                                                                 */
 typedef struct workspace {
     vnlb_stage_params p;
+    const vnlb_flow* flow;    /* flow-guided search centres, or NULL */
     int stage;
     int width, height, source_frames, channels;
     int patch_area, patch_dim, estimator_dim, max_similar;
@@ -482,6 +483,53 @@ static float candidate_distance(const workspace* w, const video* src, int channe
     return distance;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Flow-guided search centres: MVToolsVectorGrid::nearest_vector
+ * (src/flow/flow.hpp:72-120), round_subpixel_to_pixel (flow.hpp:183-191) and
+ * MVToolsFlowProvider::center_for (flow.hpp:341-389).                        */
+static int nearest_block_index(int coordinate, int first_center, int step, int count) {
+    if (count <= 1) return 0;
+    const int shifted = coordinate - first_center;
+    const int index = shifted >= 0 ? (shifted + step / 2) / step : -((-shifted + step / 2) / step);
+    return index < 0 ? 0 : (index > count - 1 ? count - 1 : index);
+}
+
+static int round_subpixel(int value, int pel) {
+    if (pel <= 1) return value;
+    return value >= 0 ? (value + pel / 2) / pel : -((-value + pel / 2) / pel);
+}
+
+/* One frame of the walk: the centre moves by the grid's nearest vector to the
+ * patch centre, rounded to whole pixels, then is clamped to the frame. */
+static void flow_step(const vnlb_flow_grids* g, int frame, int patch_center, int width, int height, int* cx,
+                      int* cy) {
+    if (!g->present || !g->usable[frame] || g->pel <= 0 || g->block_size_x <= 0 || g->block_size_y <= 0 ||
+        g->block_count_x <= 0 || g->block_count_y <= 0)
+        return;
+    const int step_x = imax(1, g->block_size_x - imax(0, g->overlap_x));
+    const int step_y = imax(1, g->block_size_y - imax(0, g->overlap_y));
+    const int bx = nearest_block_index(*cx + patch_center, g->block_size_x / 2, step_x, g->block_count_x);
+    const int by = nearest_block_index(*cy + patch_center, g->block_size_y / 2, step_y, g->block_count_y);
+    const int* v = g->vectors + (((size_t)frame * g->block_count_y + by) * g->block_count_x + bx) * 2;
+    *cx += round_subpixel(v[0], g->pel);
+    *cy += round_subpixel(v[1], g->pel);
+    if (width > 0) *cx = imin(imax(*cx, 0), width - 1);
+    if (height > 0) *cy = imin(imax(*cy, 0), height - 1);
+}
+
+/* The search centre of anchor (ax, ay) of frame af in candidate frame cf. */
+static void flow_center(const workspace* w, int ax, int ay, int af, int cf, int* cx, int* cy) {
+    *cx = ax;
+    *cy = ay;
+    if (!w->flow || cf == af) return;
+    const int patch_center = imax(0, w->p.patch_size / 2);
+    if (cf < af) {
+        for (int f = af; f > cf; --f) flow_step(&w->flow->fw, f, patch_center, w->width, w->height, cx, cy);
+    } else {
+        for (int f = af; f < cf; ++f) flow_step(&w->flow->bw, f, patch_center, w->width, w->height, cx, cy);
+    }
+}
+
 static int find_similar(workspace* w, const video* src, int channels, int ax, int ay, int af) {
     const vnlb_stage_params* p = &w->p;
     if (p->similar <= 1) {
@@ -505,9 +553,10 @@ static int find_similar(workspace* w, const video* src, int channels, int ax, in
     w->top_count = 0;
     for (int s = 0; s < scheduled; ++s) {
         const int cf = schedule[s];
-        int xl, xh, yl, yh;
-        spatial_range(p, ax, w->width, &xl, &xh);
-        spatial_range(p, ay, w->height, &yl, &yh);
+        int xl, xh, yl, yh, ccx, ccy;
+        flow_center(w, ax, ay, af, cf, &ccx, &ccy);
+        spatial_range(p, ccx, w->width, &xl, &xh);
+        spatial_range(p, ccy, w->height, &yl, &yh);
         for (int cy = yl; cy <= yh; ++cy)
             for (int cx = xl; cx <= xh; ++cx) {
                 const float limit = distance_limit(w, &b);
@@ -1049,6 +1098,7 @@ static int process_anchor_frame(workspace* w, const video* noisy, const video* b
 typedef struct job {
     int stage;
     const vnlb_stage_params* p;
+    const vnlb_flow* flow;
     video noisy, basic;
     int first_anchor, anchor_count;
     float* stacks;
@@ -1066,6 +1116,7 @@ static void* worker(void* arg) {
         pthread_mutex_lock(&j->lock); j->status = -1; pthread_mutex_unlock(&j->lock);
         return NULL;
     }
+    w.flow = j->flow;
     for (;;) {
         pthread_mutex_lock(&j->lock);
         const int index = j->status == 0 ? j->next++ : j->anchor_count;
@@ -1082,15 +1133,19 @@ static void* worker(void* arg) {
     return NULL;
 }
 
-int vnlboracle_stage_stacks(int stage, const vnlb_stage_params* params, const float* clip, const float* basic,
-                            int width, int height, int frames, int channels, int first_anchor, int anchor_count,
-                            int threads, float* stacks) {
+/* vnlb.Basic / vnlb.Final stacks of anchor frames first_anchor .. + count - 1,
+ * with flow-guided search centres when flow is not NULL (process_*_anchor_
+ * mvtools, src/core/core.cpp:2095-2109). */
+int vnlboracle_stage_stacks_flow(int stage, const vnlb_stage_params* params, const float* clip, const float* basic,
+                                 int width, int height, int frames, int channels, int first_anchor, int anchor_count,
+                                 int threads, const vnlb_flow* flow, float* stacks) {
     if (validate(params, width, height, frames, channels) != 0) return -1;
     if (stage == VNLB_STAGE_FINAL && basic == NULL) return fail("VNLB: ref must be a video node");
     job j;
     memset(&j, 0, sizeof(j));
     j.stage = stage;
     j.p = params;
+    j.flow = flow;
     j.noisy = (video){clip, width, height, frames, channels};
     j.basic = (video){basic, width, height, frames, channels};
     j.first_anchor = first_anchor;
@@ -1109,6 +1164,13 @@ int vnlboracle_stage_stacks(int stage, const vnlb_stage_params* params, const fl
     return j.status;
 }
 
+int vnlboracle_stage_stacks(int stage, const vnlb_stage_params* params, const float* clip, const float* basic,
+                            int width, int height, int frames, int channels, int first_anchor, int anchor_count,
+                            int threads, float* stacks) {
+    return vnlboracle_stage_stacks_flow(stage, params, clip, basic, width, height, frames, channels, first_anchor,
+                                        anchor_count, threads, NULL, stacks);
+}
+
 int vnlboracle_stage_stack(int stage, const vnlb_stage_params* params, const float* clip, const float* basic,
                            int width, int height, int frames, int channels, int anchor_frame, float* stack) {
     return vnlboracle_stage_stacks(stage, params, clip, basic, width, height, frames, channels, anchor_frame, 1, 1,
@@ -1118,14 +1180,16 @@ int vnlboracle_stage_stack(int stage, const vnlb_stage_params* params, const flo
 /* Same as vnlboracle_stage_stack, and also reports every processed group in
  * raster order: its anchor, its rows (CPU row order) and their weights.
  * Returns the number of groups (which may exceed group_capacity), or -1. */
-int vnlboracle_anchor_groups(int stage, const vnlb_stage_params* params, const float* clip, const float* basic,
-                             int width, int height, int frames, int channels, int anchor_frame, float* stack,
-                             vnlb_group_record* groups, int group_capacity, vnlb_match_record* matches,
-                             int match_capacity, int* match_total) {
+int vnlboracle_anchor_groups_flow(int stage, const vnlb_stage_params* params, const float* clip,
+                                  const float* basic, int width, int height, int frames, int channels,
+                                  int anchor_frame, const vnlb_flow* flow, float* stack, vnlb_group_record* groups,
+                                  int group_capacity, vnlb_match_record* matches, int match_capacity,
+                                  int* match_total) {
     if (validate(params, width, height, frames, channels) != 0) return -1;
     workspace w;
     memset(&w, 0, sizeof(w));
     if (ws_prepare(&w, stage, params, width, height, frames, channels) != 0) return -1;
+    w.flow = flow;
     const video noisy = {clip, width, height, frames, channels};
     const video ref = {basic, width, height, frames, channels};
     const stack_view sv = {stack, width, height, channels,
@@ -1136,6 +1200,14 @@ int vnlboracle_anchor_groups(int stage, const vnlb_stage_params* params, const f
     if (status != 0) return -1;
     if (match_total) *match_total = sink.match_count;
     return sink.group_count;
+}
+
+int vnlboracle_anchor_groups(int stage, const vnlb_stage_params* params, const float* clip, const float* basic,
+                             int width, int height, int frames, int channels, int anchor_frame, float* stack,
+                             vnlb_group_record* groups, int group_capacity, vnlb_match_record* matches,
+                             int match_capacity, int* match_total) {
+    return vnlboracle_anchor_groups_flow(stage, params, clip, basic, width, height, frames, channels, anchor_frame,
+                                         NULL, stack, groups, group_capacity, matches, match_capacity, match_total);
 }
 
 /* Matches of one anchor alone (no paste mask), rows in CPU order. */

@@ -76,6 +76,26 @@ typedef struct vnlb_match_record {
     float weight;     /* final aggregation weight of the row */
 } vnlb_match_record;
 
+/* Motion vectors of the flow-guided search: the vnlb plugin's optional
+ * mvfw / mvbw clips (MVTools delta-1 vectors, finest level), as
+ * MVToolsVectorGrid holds them (src/flow/flow.hpp:37-120).  One block
+ * geometry per direction; per frame a usable flag (the vectors parsed valid
+ * and the source frame is not a scene change, src/vs/plugin.cpp:476-485,
+ * 507-525) and block_count_y x block_count_x vectors (x, y) in sub-pel
+ * units.  MVToolsFlowProvider (flow.hpp:321-429) walks the mvfw grids toward
+ * earlier candidate frames and the mvbw grids toward later ones. */
+typedef struct vnlb_flow_grids {
+    int present;  /* the clip was given */
+    int block_size_x, block_size_y, pel, overlap_x, overlap_y, block_count_x, block_count_y;
+    const unsigned char* usable; /* [frames] */
+    const int* vectors;          /* [frames][block_count_y][block_count_x][2] */
+} vnlb_flow_grids;
+
+typedef struct vnlb_flow {
+    vnlb_flow_grids fw; /* mvfw */
+    vnlb_flow_grids bw; /* mvbw */
+} vnlb_flow;
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,6 +16,14 @@ ref_outputs.npz
     Basic -> Aggregate -> Final -> Aggregate chain of the vnlb plugin).  They
     pin the C restatement and the GPU path bit for bit without the reference
     sources being present.
+
+flow_outputs.npz
+    The same with the vnlb plugin's mvfw / mvbw MVTools clips: seeded random
+    vectors, some frames invalid or marked as scene changes
+    (tests/mvtools_blobs.py), and the aggregated Basic and Final outputs of the
+    reference's flow-guided search (process_*_anchor_mvtools; the Basic ->
+    Aggregate -> Final -> Aggregate chain).  The clips and vectors are
+    regenerated from the seeds by tests/mvtools_blobs.flow_case.
 """
 from __future__ import annotations
 
@@ -29,8 +37,10 @@ import numpy as np
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT / "oracle"))
 sys.path.insert(0, str(ROOT / "vapoursynth-vnlb_b200"))
+sys.path.insert(0, str(ROOT / "tests"))
 
 import oracle as O  # noqa: E402
+import mvtools_blobs as M  # noqa: E402
 import synth  # noqa: E402
 
 REFERENCE = Path("/root/reference")
@@ -83,8 +93,28 @@ def ref_outputs():
     np.savez_compressed(OUT / "ref_outputs.npz", meta=json.dumps(meta), **arrays)
 
 
+def flow_outputs():
+    o = O.Oracle("ref")
+    arrays, meta = {}, {}
+    for case in M.FLOW_CASES:
+        name, w, h, f, planes, sigma, seed, kw, fw_spec, bw_spec = case
+        noisy, fw, bw = M.flow_case(*case)
+        flow = (M.flow_grids(fw), M.flow_grids(bw))
+        bp = O.cpu_params(O.BASIC, sigma, **kw)
+        fp = O.cpu_params(O.FINAL, sigma, **kw)
+        bs = o.stage_stacks(O.BASIC, bp, noisy, flow=flow)
+        basic = o.aggregate(bs, noisy, bp.search_bwd, bp.search_fwd, bp.patch_time)
+        fs = o.stage_stacks(O.FINAL, fp, noisy, basic, flow=flow)
+        final = o.aggregate(fs, noisy, fp.search_bwd, fp.search_fwd, fp.patch_time)
+        arrays[f"{name}/basic"] = basic
+        arrays[f"{name}/final"] = final
+        meta[name] = {"sigma": sigma, "kwargs": kw}
+    np.savez_compressed(OUT / "flow_outputs.npz", meta=json.dumps(meta), **arrays)
+
+
 if __name__ == "__main__":
     reference_cases()
     ref_outputs()
-    for p in ("reference_cases.npz", "ref_outputs.npz"):
+    flow_outputs()
+    for p in ("reference_cases.npz", "ref_outputs.npz", "flow_outputs.npz"):
         print(p, (OUT / p).stat().st_size, "bytes")
