@@ -177,6 +177,43 @@ void* vnlbgpu_stream(vnlbgpu_session* session);
  * ordered after the Basic frames it reads. */
 int vnlbgpu_set_stream(vnlbgpu_session* session, void* stream);
 
+/* Flow-guided search: the vnlb plugin's optional mvfw / mvbw clips (MVTools
+ * delta-1 vectors; the reference's vnlbcu has no such search).
+ *
+ *   parse_mvtools_analysis (src/flow/flow.hpp:193-250)  vnlbgpu_parse_mvtools_analysis
+ *   parse_mvtools_vectors  (flow.hpp:252-318)           vnlbgpu_parse_mvtools_vectors
+ *   read_mvtools_analysis_from_node + validate_mvtools_clip
+ *     (src/vs/plugin.cpp:429-474, 881-899)              vnlbgpu_set_mvtools_analysis
+ *   cache_mvtools_grid (plugin.cpp:507-525)             vnlbgpu_set_mvtools_frame
+ *   MVToolsFlowProvider::center_for (flow.hpp:341-389)  the search centres of
+ *                                                       every render that follows
+ *
+ * direction 0 is mvfw (MVTools isb=False), walked toward earlier candidate
+ * frames; 1 is mvbw (isb=True), walked toward later ones.  The two parsers
+ * need no device and no session: parse_analysis reads the 21 32-bit fields of
+ * an MVTools_MVAnalysisData frame property; parse_vectors the finest level of
+ * an MVTools_vectors property, *valid its valid flag, xy up to capacity
+ * (x, y) pairs, *count their number.  set_mvtools_analysis takes the
+ * direction's analysis data (the property of the vector clip's frame 0) and
+ * checks it against the clip; set_mvtools_frame then takes frame n's
+ * MVTools_vectors property and whether the source clip's frame n marks a scene
+ * change (_SceneChangePrev or Scenechange for mvfw, _SceneChangeNext for mvbw),
+ * which makes the frame's vectors unusable.  Frames never given are unusable.
+ * With any flow set, the session runs the plain matcher (the chosen forms
+ * need windows centred on the anchor). */
+typedef struct vnlbgpu_mvtools_analysis {
+    int block_size_x, block_size_y, pel, level_count, delta_frame, backwards, width, height;
+    int overlap_x, overlap_y, block_count_x, block_count_y, bits_per_sample;
+    int chroma_ratio_x, chroma_ratio_y, padding_x, padding_y;
+} vnlbgpu_mvtools_analysis;
+
+int vnlbgpu_parse_mvtools_analysis(const void* data, size_t size, vnlbgpu_mvtools_analysis* out);
+int vnlbgpu_parse_mvtools_vectors(const void* data, size_t size, const vnlbgpu_mvtools_analysis* analysis,
+                                  int* valid, int* xy, size_t capacity, size_t* count);
+int vnlbgpu_set_mvtools_analysis(vnlbgpu_session* session, int direction, const void* data, size_t size);
+int vnlbgpu_set_mvtools_frame(vnlbgpu_session* session, int direction, int frame, const void* vectors,
+                              size_t size, int scene_change);
+
 #ifdef __cplusplus
 }
 #endif

@@ -243,12 +243,20 @@ __device__ __forceinline__ float exact_distance8(const float* planes, int plane_
     return d;
 }
 
-template <int P, bool kApprox>
+template <int P, bool kApprox, bool kFlow>  // kFlow: search centres from L.centers
 __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const Strip strip = L.strips[blockIdx.x];
+    Strip strip;
+    if constexpr (kFlow) {  // flow-guided search: one anchor per CTA, regions set per frame
+        strip.first = blockIdx.x;
+        strip.count = 1;
+        strip.y = L.anchors[blockIdx.x].y;
+        strip.region_x = strip.region_y = strip.region_w = strip.region_h = 0;
+    } else {
+        strip = L.strips[blockIdx.x];
+    }
     const int Pd = L.P;
     const int Cs = L.search_channels;
     const int planes_n = Cs * L.Pt;
@@ -280,6 +288,7 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     const int Wy = yh - yl + 1;
     const int cells = Wx * Wy;
     const int tasks = Wx * ((Wy + kKY - 1) / kKY);
+    int rx0 = strip.region_x, ry0 = strip.region_y, rw = strip.region_w, rh = strip.region_h;
 
     WarpSelect s;
     s.count = 0;
@@ -301,15 +310,26 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
 
     for (int k = 0; k < L.schedule_len; ++k) {
         const int frame = L.schedule[k];
+        if constexpr (kFlow) {
+            // the window of frame k around the anchor's search centre there
+            // (same size as the anchor-centred one)
+            const int2 c = L.centers[static_cast<size_t>(strip.first) * L.schedule_len + k];
+            spatial_range(c.x, L.width, Pd, L.search_window, xl, xh);
+            spatial_range(c.y, L.height, Pd, L.search_window, yl, yh);
+            rx0 = xl & ~3;
+            ry0 = yl;
+            rw = xh + Pd - rx0;
+            rh = yh - yl + Pd;
+        }
         __syncthreads();
         // Stage the strip's region of every plane (channel, t) of frame k.
-        const int rows = strip.region_h;
-        const int cols = strip.region_w;
+        const int rows = rh;
+        const int cols = rw;
         for (int q = 0; q < planes_n; ++q) {
             const int c = q / L.Pt;
             const int t = q % L.Pt;
             const float* src = L.video + ((static_cast<size_t>(frame + t) * L.channels + c) * L.height +
-                                          strip.region_y) * static_cast<size_t>(L.width) + strip.region_x;
+                                          ry0) * static_cast<size_t>(L.width) + rx0;
             float* dst = planes + q * plane_values;
             for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
                 const int r = i / cols;
@@ -350,8 +370,7 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
                 const int rem = i - q * Pd * Pd;
                 const int py = rem / Pd;
                 const int px = rem - py * Pd;
-                ref[i] = planes[q * plane_values + (ay - strip.region_y + py) * L.region_stride +
-                                (ax - strip.region_x + px)];
+                ref[i] = planes[q * plane_values + (ay - ry0 + py) * L.region_stride + (ax - rx0 + px)];
             }
             __syncwarp();
             if constexpr (kApprox) {
@@ -368,11 +387,11 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
             const int gy = task / Wx;
             float d[kKY];
             if constexpr (kApprox)
-                task_distances_approx(planes, plane_values, L.region_stride, xl - strip.region_x + cx,
-                                      yl - strip.region_y + gy * kKY, ref, planes_n, ref_norm, norms, d);
+                task_distances_approx(planes, plane_values, L.region_stride, xl - rx0 + cx, yl - ry0 + gy * kKY, ref,
+                                      planes_n, ref_norm, norms, d);
             else
-                task_distances<P>(planes, plane_values, L.region_stride, xl - strip.region_x + cx,
-                                  yl - strip.region_y + gy * kKY, ref, planes_n, Pd, d);
+                task_distances<P>(planes, plane_values, L.region_stride, xl - rx0 + cx, yl - ry0 + gy * kKY, ref,
+                                  planes_n, Pd, d);
 #pragma unroll
             for (int j = 0; j < kKY; ++j) {
                 const int cy = gy * kKY + j;
@@ -439,9 +458,8 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
                 if (lane < s.count && (reg_id >> 20) == k) {
                     const int cell = reg_id & 0xfffff;
                     const int cy = cell / Wx;
-                    reg_exact = exact_distance8(planes, plane_values, L.region_stride,
-                                                xl - strip.region_x + (cell - cy * Wx), yl - strip.region_y + cy,
-                                                ref, planes_n);
+                    reg_exact = exact_distance8(planes, plane_values, L.region_stride, xl - rx0 + (cell - cy * Wx),
+                                                yl - ry0 + cy, ref, planes_n);
                 }
             }
             continue;
@@ -634,8 +652,15 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
             const int kk = id >> 20;
             const int cell = id & 0xfffff;
             const int cy = cell / Wx;
-            m.x = xl + (cell - cy * Wx);
-            m.y = yl + cy;
+            int fxl = xl, fyl = yl;
+            if constexpr (kFlow) {  // frame kk's window
+                const int2 c = L.centers[static_cast<size_t>(g) * L.schedule_len + kk];
+                int hi;
+                spatial_range(c.x, L.width, Pd, L.search_window, fxl, hi);
+                spatial_range(c.y, L.height, Pd, L.search_window, fyl, hi);
+            }
+            m.x = fxl + (cell - cy * Wx);
+            m.y = fyl + cy;
             m.frame = L.schedule[kk];
         }
         rows_out[i] = m;
@@ -679,7 +704,66 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     if (lane == 0) L.victim_counts[g] = min(nvict, L.victim_stride);
 }
 
+// Flow-guided search centres: MVToolsVectorGrid::nearest_vector
+// (src/flow/flow.hpp:72-120), round_subpixel_to_pixel (flow.hpp:183-191) and
+// MVToolsFlowProvider::center_for (flow.hpp:341-389).  The centre starts at
+// the anchor and walks frame by frame toward the candidate frame (mvfw grids
+// toward earlier frames, mvbw toward later ones): each usable grid moves it
+// by the vector of the block nearest to the patch centre, rounded to whole
+// pixels, then it is clamped to the frame.
+__device__ __forceinline__ int nearest_block_index(int coordinate, int first_center, int step, int count) {
+    if (count <= 1) return 0;
+    const int shifted = coordinate - first_center;
+    const int index = shifted >= 0 ? (shifted + step / 2) / step : -((-shifted + step / 2) / step);
+    return min(max(index, 0), count - 1);
+}
+
+__device__ __forceinline__ int round_subpixel(int value, int pel) {
+    if (pel <= 1) return value;
+    return value >= 0 ? (value + pel / 2) / pel : -((-value + pel / 2) / pel);
+}
+
+__device__ __forceinline__ void flow_step(const FlowGridsDevice& g, int frame, int patch_center, int width,
+                                          int height, int& cx, int& cy) {
+    if (!g.present || !g.usable[frame] || g.pel <= 0 || g.block_size_x <= 0 || g.block_size_y <= 0 ||
+        g.block_count_x <= 0 || g.block_count_y <= 0)
+        return;
+    const int step_x = max(1, g.block_size_x - max(0, g.overlap_x));
+    const int step_y = max(1, g.block_size_y - max(0, g.overlap_y));
+    const int bx = nearest_block_index(cx + patch_center, g.block_size_x / 2, step_x, g.block_count_x);
+    const int by = nearest_block_index(cy + patch_center, g.block_size_y / 2, step_y, g.block_count_y);
+    const int2 v = g.vectors[(static_cast<size_t>(frame) * g.block_count_y + by) * g.block_count_x + bx];
+    cx += round_subpixel(v.x, g.pel);
+    cy += round_subpixel(v.y, g.pel);
+    if (width > 0) cx = min(max(cx, 0), width - 1);
+    if (height > 0) cy = min(max(cy, 0), height - 1);
+}
+
+__global__ void centers_kernel(CentersLaunch L) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.anchor_count * L.schedule_len) return;
+    const int g = i / L.schedule_len;
+    const int k = i - g * L.schedule_len;
+    const int af = L.anchor_frame;
+    const int cf = L.schedule[k];
+    int cx = L.anchors[g].x, cy = L.anchors[g].y;
+    const int patch_center = max(0, L.P / 2);
+    if (cf < af) {
+        for (int f = af; f > cf; --f) flow_step(L.fw, f, patch_center, L.width, L.height, cx, cy);
+    } else {
+        for (int f = af; f < cf; ++f) flow_step(L.bw, f, patch_center, L.width, L.height, cx, cy);
+    }
+    L.centers[i] = make_int2(cx, cy);
+}
+
 }  // namespace
+
+cudaError_t launch_centers(const CentersLaunch& L, cudaStream_t stream) {
+    const int n = L.anchor_count * L.schedule_len;
+    if (n <= 0) return cudaSuccess;
+    centers_kernel<<<(n + 255) / 256, 256, 0, stream>>>(L);
+    return cudaGetLastError();
+}
 
 size_t match_shared_bytes(const MatchLaunch& L, int warps) {
     const size_t plane = static_cast<size_t>(L.region_rows) * L.region_stride;
@@ -703,18 +787,30 @@ cudaError_t launch_match(const MatchLaunch& L, int strips, int warps, cudaStream
         kernel<<<strips, block, smem, stream>>>(L);
         err = cudaGetLastError();
     };
+    if (L.centers) {  // flow-guided search: one anchor (one warp) per CTA
+        if (L.approx || warps != 1) return cudaErrorInvalidValue;
+        switch (L.P) {
+            case 4: launch(match_kernel<4, false, true>); break;
+            case 5: launch(match_kernel<5, false, true>); break;
+            case 6: launch(match_kernel<6, false, true>); break;
+            case 7: launch(match_kernel<7, false, true>); break;
+            case 8: launch(match_kernel<8, false, true>); break;
+            default: launch(match_kernel<0, false, true>); break;
+        }
+        return err;
+    }
     if (L.approx) {
         if (L.P != kLanes) return cudaErrorInvalidValue;
-        launch(match_kernel<8, true>);
+        launch(match_kernel<8, true, false>);
         return err;
     }
     switch (L.P) {
-        case 4: launch(match_kernel<4, false>); break;
-        case 5: launch(match_kernel<5, false>); break;
-        case 6: launch(match_kernel<6, false>); break;
-        case 7: launch(match_kernel<7, false>); break;
-        case 8: launch(match_kernel<8, false>); break;
-        default: launch(match_kernel<0, false>); break;
+        case 4: launch(match_kernel<4, false, false>); break;
+        case 5: launch(match_kernel<5, false, false>); break;
+        case 6: launch(match_kernel<6, false, false>); break;
+        case 7: launch(match_kernel<7, false, false>); break;
+        case 8: launch(match_kernel<8, false, false>); break;
+        default: launch(match_kernel<0, false, false>); break;
     }
     return err;
 }

@@ -17,16 +17,24 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "../../include/vnlbgpu.h"
 #include "../../include/vnlbgpu_diag.h"
+#include "mvtools.h"
 #include "vnlb_kernels.h"
 
 namespace vnlbgpu {
 namespace {
 
 thread_local std::string g_last_error;
+
+}  // namespace
+
+void set_last_error(const std::string& message) { g_last_error = message; }
+
+namespace {
 
 struct Failure : std::runtime_error {
     using std::runtime_error::runtime_error;
@@ -91,6 +99,9 @@ struct Grid {
     // stack-tile reach tables (TileLaunch)
     DeviceArray<int2> d_tile_grid_rows;  // [tiles_y]
     DeviceArray<int2> d_tile_anchors;    // [grid rows][tiles_x]
+    // the same for the flow-guided search, built for flow_reach (x, y)
+    DeviceArray<int2> d_flow_grid_rows, d_flow_anchors;
+    int2 flow_reach = make_int2(-1, -1);
 };
 
 }  // namespace
@@ -106,6 +117,8 @@ struct Session {
     int slots = 0, valid_anchor_frames = 0, max_rows = 0, buffer_cap = 0;
     int max_groups = 0, victim_stride = 0, warps = 8;
     int region_rows = 0, region_stride = 0, region_w_max = 0;
+    int flow_stride = 0;  // row stride of the one-anchor regions of the flow-guided search
+    int sched_max = 0;    // most scheduled frames of an anchor frame
     // matcher forms: approx (VNLBGPU_FORM_CHOSEN: approximate distances in
     // the plain matcher's tiling, exact re-rank) and tensor
     // (VNLBGPU_FORM_CHOSEN_TC: BF16 tensor-core distances, match_chosen.cu)
@@ -183,6 +196,7 @@ struct Session {
     struct Lane {
         cudaStream_t stream = nullptr;
         DeviceArray<MatchRow> rows, row_info;
+        DeviceArray<int2> centers;  // flow-guided search: [anchor][scheduled frame]
         DeviceArray<int> row_counts, victims, victim_counts, active, row_offset, row_group, active_prefix, gflags;
         DeviceArray<int2> active_xy;
         DeviceArray<FrameCounters> counters;
@@ -407,7 +421,7 @@ struct Session {
         region_rows = std::min(p.search_window, height - P + 1) + P - 1 + KY - 1;
         const int cw0 = std::min(p.search_window, width - P + 1);
         const int ch0 = std::min(p.search_window, height - P + 1);
-        const int sched_max = std::min(frames, p.search_bwd + p.search_fwd + 1);
+        sched_max = std::min(frames, p.search_bwd + p.search_fwd + 1);
         const long long cap_eff = std::min<long long>(soft_cap, static_cast<long long>(cw0) * ch0 * sched_max);
         // approximate distances need 8x8 patches and the register replay
         // (buffer and K front within a warp)
@@ -428,6 +442,10 @@ struct Session {
             if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
         }
         if (warps < 1) fail("VNLB CUDA: the search region of one anchor does not fit in shared memory");
+        // one-anchor regions (flow-guided search): the window plus the patch,
+        // from a column rounded down to a multiple of 4
+        flow_stride = (cw0 + P - 1 + 3 + 3) & ~3;
+        while (flow_stride % 8 != 4) ++flow_stride;
         // tensor-core matcher: strips of up to kChosenAnchors anchors whose
         // windows lie within kChosenCols candidate columns
         if (p.form == VNLBGPU_FORM_CHOSEN_TC && chosen_match_supported(P, search_channels * Pt, cw0, ch0)) {
@@ -527,6 +545,46 @@ struct Session {
         }
     }
 
+    // Stack-tile reach tables of an anchor grid: per tile row the grid rows,
+    // and per (grid row, tile column) the anchors, whose matches can cover
+    // the tile when every match lies within (reach_x, reach_y) of its anchor.
+    void build_reach_tables(const std::vector<int2>& a, int reach_x, int reach_y, DeviceArray<int2>& d_rows,
+                            DeviceArray<int2>& d_anchors) {
+        std::vector<int> row_y, row_first;
+        for (size_t j = 0; j < a.size(); ++j)
+            if (j == 0 || a[j].y != a[j - 1].y) {
+                row_y.push_back(a[j].y);
+                row_first.push_back(static_cast<int>(j));
+            }
+        row_first.push_back(static_cast<int>(a.size()));
+        const int rows_n = static_cast<int>(row_y.size());
+        const int tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
+        std::vector<int2> tgr(tiles_y), tan(static_cast<size_t>(rows_n) * tiles_x);
+        for (int ty = 0; ty < tiles_y; ++ty) {
+            const int lo = ty * kTile - (P - 1) - reach_y, hi = ty * kTile + kTile - 1 + reach_y;
+            int k0 = 0;
+            while (k0 < rows_n && row_y[k0] < lo) ++k0;
+            int k1 = k0;
+            while (k1 < rows_n && row_y[k1] <= hi) ++k1;
+            tgr[ty] = make_int2(k0, k1);
+        }
+        for (int k = 0; k < rows_n; ++k)
+            for (int tx = 0; tx < tiles_x; ++tx) {
+                const int lo = tx * kTile - (P - 1) - reach_x, hi = tx * kTile + kTile - 1 + reach_x;
+                int j0 = row_first[k];
+                while (j0 < row_first[k + 1] && a[j0].x < lo) ++j0;
+                int j1 = j0;
+                while (j1 < row_first[k + 1] && a[j1].x <= hi) ++j1;
+                tan[static_cast<size_t>(k) * tiles_x + tx] = make_int2(j0, j1);
+            }
+        d_rows.allocate(tgr.size(), "cudaMalloc(tile rows)");
+        d_anchors.allocate(tan.size(), "cudaMalloc(tile anchors)");
+        check(cudaMemcpy(d_rows.ptr, tgr.data(), tgr.size() * sizeof(int2), cudaMemcpyHostToDevice),
+              "cudaMemcpy(tile rows)");
+        check(cudaMemcpy(d_anchors.ptr, tan.data(), tan.size() * sizeof(int2), cudaMemcpyHostToDevice),
+              "cudaMemcpy(tile anchors)");
+    }
+
     // staggered anchor grid (reference_processing_mask_selected, core.cpp:934-950)
     std::vector<int2> build_anchor_list(int phase_key) const {
         std::vector<int2> out;
@@ -622,42 +680,8 @@ struct Session {
               "cudaMemcpy(strips)");
         // reach tables: a match lies within search_window - 1 of its anchor on
         // each axis, so a stack tile gathers from the anchors in that reach
-        {
-            std::vector<int> row_y, row_first;
-            for (size_t j = 0; j < a.size(); ++j)
-                if (j == 0 || a[j].y != a[j - 1].y) {
-                    row_y.push_back(a[j].y);
-                    row_first.push_back(static_cast<int>(j));
-                }
-            row_first.push_back(static_cast<int>(a.size()));
-            const int rows_n = static_cast<int>(row_y.size());
-            const int reach = params.search_window - 1;
-            const int tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
-            std::vector<int2> tgr(tiles_y), tan(static_cast<size_t>(rows_n) * tiles_x);
-            for (int ty = 0; ty < tiles_y; ++ty) {
-                const int lo = ty * kTile - (P - 1) - reach, hi = ty * kTile + kTile - 1 + reach;
-                int k0 = 0;
-                while (k0 < rows_n && row_y[k0] < lo) ++k0;
-                int k1 = k0;
-                while (k1 < rows_n && row_y[k1] <= hi) ++k1;
-                tgr[ty] = make_int2(k0, k1);
-            }
-            for (int k = 0; k < rows_n; ++k)
-                for (int tx = 0; tx < tiles_x; ++tx) {
-                    const int lo = tx * kTile - (P - 1) - reach, hi = tx * kTile + kTile - 1 + reach;
-                    int j0 = row_first[k];
-                    while (j0 < row_first[k + 1] && a[j0].x < lo) ++j0;
-                    int j1 = j0;
-                    while (j1 < row_first[k + 1] && a[j1].x <= hi) ++j1;
-                    tan[static_cast<size_t>(k) * tiles_x + tx] = make_int2(j0, j1);
-                }
-            grid->d_tile_grid_rows.allocate(tgr.size(), "cudaMalloc(tile rows)");
-            grid->d_tile_anchors.allocate(tan.size(), "cudaMalloc(tile anchors)");
-            check(cudaMemcpy(grid->d_tile_grid_rows.ptr, tgr.data(), tgr.size() * sizeof(int2), cudaMemcpyHostToDevice),
-                  "cudaMemcpy(tile rows)");
-            check(cudaMemcpy(grid->d_tile_anchors.ptr, tan.data(), tan.size() * sizeof(int2), cudaMemcpyHostToDevice),
-                  "cudaMemcpy(tile anchors)");
-        }
+        build_reach_tables(a, params.search_window - 1, params.search_window - 1, grid->d_tile_grid_rows,
+                           grid->d_tile_anchors);
         grid->d_map.allocate(plane(), "cudaMalloc(anchor map)");
         check(cudaMemsetAsync(grid->d_map.ptr, 0xff, plane() * sizeof(int), stream), "cudaMemsetAsync(anchor map)");
         check(launch_anchor_map(grid->d_anchors.ptr, static_cast<int>(a.size()), width, grid->d_map.ptr, stream),
@@ -669,9 +693,101 @@ struct Session {
         return ref_grid;
     }
 
-    void require_sources() const {
+    void require_sources() {
         if (!clip_ready) fail("VNLB CUDA: clip frames were not provided");
         if (stage == 1 && !ref_ready) fail("VNLB CUDA: ref frames were not provided");
+        sync_flow();
+    }
+
+    // Flow-guided search (vnlbgpu_set_mvtools_*): per direction, 0 = mvfw,
+    // 1 = mvbw, the analysis data and every frame's finest vectors and usable
+    // flag, copied to the device before the next render that reads them.
+    struct Flow {
+        bool present = false;
+        bool dirty = false;
+        vnlbgpu_mvtools_analysis analysis{};
+        std::vector<unsigned char> usable;  // [frames]
+        std::vector<int2> vectors;          // [frames][block_count_y][block_count_x]
+        DeviceArray<unsigned char> d_usable;
+        DeviceArray<int2> d_vectors;
+    };
+    Flow flow[2];
+
+    bool flow_on() const { return flow[0].present || flow[1].present; }
+
+    // A bound on how far a search centre moves from its anchor: a walk crosses
+    // at most search_bwd + search_fwd frames (the temporal window shifts at
+    // the clip's ends), each moving the centre by at most the largest rounded
+    // vector of a usable grid of that frame; clamping only shortens it.  A
+    // match then lies within search_window - 1 plus this bound of its anchor.
+    int2 flow_reach = make_int2(0, 0);
+
+    void update_flow_reach() {
+        int walk = params.search_bwd + params.search_fwd;
+        std::vector<int> mx, my;
+        for (const Flow& f : flow) {
+            if (!f.present) continue;
+            const size_t count = static_cast<size_t>(f.analysis.block_count_x) * f.analysis.block_count_y;
+            const int pel = f.analysis.pel;
+            auto rounded = [pel](int v) {
+                const int a = v < 0 ? -v : v;
+                return pel <= 1 ? a : (a + pel / 2) / pel;
+            };
+            for (int fr = 0; fr < frames; ++fr) {
+                int bx = 0, by = 0;
+                if (f.usable[static_cast<size_t>(fr)])
+                    for (size_t i = 0; i < count; ++i) {
+                        const int2 v = f.vectors[static_cast<size_t>(fr) * count + i];
+                        bx = std::max(bx, rounded(v.x));
+                        by = std::max(by, rounded(v.y));
+                    }
+                mx.push_back(bx);
+                my.push_back(by);
+            }
+        }
+        auto bound = [walk](std::vector<int> m, int cap) {
+            std::sort(m.begin(), m.end(), std::greater<int>());
+            long long s = 0;
+            for (int i = 0; i < walk && i < static_cast<int>(m.size()); ++i) s += m[static_cast<size_t>(i)];
+            return static_cast<int>(std::min<long long>(s, cap));
+        };
+        flow_reach = make_int2(bound(mx, width - 1), bound(my, height - 1));
+    }
+
+    void sync_flow() {
+        if (!flow[0].dirty && !flow[1].dirty) return;
+        // earlier renders may still read the device copies
+        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize(flow)");
+        for (Flow& f : flow) {
+            if (!f.dirty) continue;
+            if (f.d_usable.count != f.usable.size()) f.d_usable.allocate(f.usable.size(), "cudaMalloc(flow flags)");
+            if (f.d_vectors.count != f.vectors.size())
+                f.d_vectors.allocate(f.vectors.size(), "cudaMalloc(flow vectors)");
+            check(cudaMemcpy(f.d_usable.ptr, f.usable.data(), f.usable.size(), cudaMemcpyHostToDevice),
+                  "cudaMemcpy(flow flags)");
+            check(cudaMemcpy(f.d_vectors.ptr, f.vectors.data(), f.vectors.size() * sizeof(int2),
+                             cudaMemcpyHostToDevice),
+                  "cudaMemcpy(flow vectors)");
+            f.dirty = false;
+        }
+        update_flow_reach();
+    }
+
+    FlowGridsDevice flow_device(int direction) const {
+        FlowGridsDevice g{};
+        const Flow& f = flow[direction];
+        if (!f.present) return g;
+        g.present = 1;
+        g.block_size_x = f.analysis.block_size_x;
+        g.block_size_y = f.analysis.block_size_y;
+        g.pel = f.analysis.pel;
+        g.overlap_x = f.analysis.overlap_x;
+        g.overlap_y = f.analysis.overlap_y;
+        g.block_count_x = f.analysis.block_count_x;
+        g.block_count_y = f.analysis.block_count_y;
+        g.usable = f.d_usable.ptr;
+        g.vectors = f.d_vectors.ptr;
+        return g;
     }
 
     float* source_buffer(int source) {
@@ -741,7 +857,30 @@ struct Session {
         m.victim_stride = victim_stride;
         m.status = d_status.ptr;
         cudaEvent_t t0 = begin_timed(ls);
-        if (chosen) {
+        if (flow_on()) {
+            // flow-guided search (plain matcher, one anchor per CTA): the
+            // search centre of every anchor in every scheduled frame first
+            if (!lane.centers.ptr)
+                lane.centers.allocate(static_cast<size_t>(max_groups) * sched_max, "cudaMalloc(search centres)");
+            CentersLaunch cl{};
+            cl.fw = flow_device(0);
+            cl.bw = flow_device(1);
+            cl.anchors = grid.d_anchors.ptr;
+            cl.anchor_count = G;
+            for (int i = 0; i < schedule_len; ++i) cl.schedule[i] = schedule[i];
+            cl.schedule_len = schedule_len;
+            cl.anchor_frame = anchor;
+            cl.width = width;
+            cl.height = height;
+            cl.P = P;
+            cl.centers = lane.centers.ptr;
+            check(launch_centers(cl, ls), "centers kernel launch");
+            stats.kernel_launches += 1;
+            m.centers = lane.centers.ptr;
+            m.approx = 0;
+            m.region_stride = flow_stride;
+            check(launch_match(m, G, 1, ls), "match kernel launch");
+        } else if (chosen) {
             m.strips = grid.d_strips_chosen.ptr;
             m.tiles_x = chosen_tiles_x;
             m.approx_dist = lane.approx.ptr;
@@ -837,6 +976,17 @@ struct Session {
         tl.tiles_y = (height + kTile - 1) / kTile;
         tl.tile_grid_rows = grid.d_tile_grid_rows.ptr;
         tl.tile_anchors = grid.d_tile_anchors.ptr;
+        if (flow_on()) {
+            // matches of the flow-guided search lie further from their anchors
+            const int2 reach = make_int2(params.search_window - 1 + flow_reach.x,
+                                         params.search_window - 1 + flow_reach.y);
+            if (grid.flow_reach.x != reach.x || grid.flow_reach.y != reach.y) {
+                build_reach_tables(grid.anchors, reach.x, reach.y, grid.d_flow_grid_rows, grid.d_flow_anchors);
+                grid.flow_reach = reach;
+            }
+            tl.tile_grid_rows = grid.d_flow_grid_rows.ptr;
+            tl.tile_anchors = grid.d_flow_anchors.ptr;
+        }
         t0 = begin_timed(ls);
         check(launch_tiles(tl, ls), "tile kernel launch");
         end_timed(kTimedTiles, t0, ls);
@@ -1217,6 +1367,67 @@ int vnlbgpu_aggregate_frame_noalloc(const float* stacks, const float* source, in
     if (!failure) return 0;
     vnlbgpu::g_last_error = failure;
     return -1;
+}
+
+int vnlbgpu_set_mvtools_analysis(vnlbgpu_session* session, int direction, const void* data, size_t size) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        if (direction != 0 && direction != 1) vnlbgpu::fail("VNLB: MVTools direction must be 0 (mvfw) or 1 (mvbw)");
+        if (!data) vnlbgpu::fail("VNLB: null argument");
+        const std::string name = direction == 0 ? "mvfw" : "mvbw";
+        vnlbgpu_mvtools_analysis a{};
+        try {
+            a = vnlbgpu::mvtools::parse_analysis(data, size);
+        } catch (const std::invalid_argument& e) {
+            vnlbgpu::fail(std::string("VNLB: ") + e.what());
+        }
+        // validate_mvtools_clip (src/vs/plugin.cpp:452-474)
+        if (a.width != s.width || a.height != s.height)
+            vnlbgpu::fail("VNLB: " + name + " analysis dimensions must match clip");
+        if (a.delta_frame != 1) vnlbgpu::fail("VNLB: " + name + " must use MVTools delta=1 vectors");
+        if ((a.backwards != 0) != (direction == 1))
+            vnlbgpu::fail(direction == 1 ? "VNLB: mvbw must be generated with isb=True"
+                                         : "VNLB: mvfw must be generated with isb=False");
+        Session::Flow& f = s.flow[direction];
+        f.present = true;
+        f.analysis = a;
+        f.usable.assign(static_cast<size_t>(s.frames), 0);
+        f.vectors.assign(static_cast<size_t>(s.frames) * a.block_count_x * a.block_count_y, make_int2(0, 0));
+        f.dirty = true;
+        s.invalidate();
+    });
+}
+
+int vnlbgpu_set_mvtools_frame(vnlbgpu_session* session, int direction, int frame, const void* vectors, size_t size,
+                              int scene_change) {
+    return guarded([&]() {
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        if (direction != 0 && direction != 1) vnlbgpu::fail("VNLB: MVTools direction must be 0 (mvfw) or 1 (mvbw)");
+        if (!vectors) vnlbgpu::fail("VNLB: null argument");
+        Session::Flow& f = s.flow[direction];
+        if (!f.present)
+            vnlbgpu::fail(std::string("VNLB: the ") + (direction == 0 ? "mvfw" : "mvbw") +
+                          " analysis data must be set before its frames");
+        if (frame < 0 || frame >= s.frames) vnlbgpu::fail("VNLB CUDA: frame index out of range");
+        std::vector<int> xy;
+        bool valid = false;
+        try {
+            valid = vnlbgpu::mvtools::parse_vectors(vectors, size, f.analysis, xy);
+        } catch (const std::invalid_argument& e) {
+            vnlbgpu::fail(std::string("VNLB: ") + e.what());
+        }
+        // cache_mvtools_grid (plugin.cpp:507-525): a scene change in the source
+        // clip makes the frame's grid invalid
+        const size_t count = static_cast<size_t>(f.analysis.block_count_x) * f.analysis.block_count_y;
+        f.usable[static_cast<size_t>(frame)] = valid && !scene_change ? 1 : 0;
+        for (size_t i = 0; i < count; ++i)
+            f.vectors[static_cast<size_t>(frame) * count + i] = valid ? make_int2(xy[2 * i], xy[2 * i + 1])
+                                                                     : make_int2(0, 0);
+        f.dirty = true;
+        s.invalidate();
+    });
 }
 
 int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats) {

@@ -52,6 +52,11 @@ struct MatchLaunch {
     int tiles_x;          // 8-column candidate blocks per strip
     int window_rows;      // max Wy
     int* status;          // session status word (kStatus* codes, first error wins)
+    // flow-guided search (plain matcher): the search centre of every anchor in
+    // every scheduled frame, [anchor][schedule_len]; null = the anchor itself.
+    // With centres, a CTA is one warp and one anchor, and the region it stages
+    // follows the anchor's window frame by frame.
+    const int2* centers;
     float* approx_dist;   // [anchor][approx_stride] approximate distances (tensor-core form)
     int approx_stride;    // >= schedule_len * window_cells
     int anchor_count;     // grid anchors of this anchor frame
@@ -79,6 +84,29 @@ constexpr int kChosenTmemCols = 256;
 bool chosen_match_supported(int P, int planes_n, int window_w, int window_h);
 size_t chosen_match_shared_bytes(const MatchLaunch& L);
 cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t stream);
+
+// One direction of MVTools motion vectors on the device (mvfw or mvbw).
+struct FlowGridsDevice {
+    int present;
+    int block_size_x, block_size_y, pel, overlap_x, overlap_y, block_count_x, block_count_y;
+    const unsigned char* usable;  // [frames]
+    const int2* vectors;          // [frames][block_count_y][block_count_x], sub-pel units
+};
+
+// Search centres of one anchor frame (MVToolsFlowProvider::center_for,
+// src/flow/flow.hpp:341-389), one thread per anchor and scheduled frame.
+struct CentersLaunch {
+    FlowGridsDevice fw, bw;
+    const int2* anchors;
+    int anchor_count;
+    int schedule[kMaxContributors];
+    int schedule_len;
+    int anchor_frame;
+    int width, height, P;
+    int2* centers;  // [anchor][schedule_len]
+};
+
+cudaError_t launch_centers(const CentersLaunch& L, cudaStream_t stream);
 
 size_t match_shared_bytes(const MatchLaunch& L, int warps);
 int match_warp_floats(int window_cells, int planes_n, int P, int buffer_cap);

@@ -10,8 +10,16 @@ per anchor frame a stack frame of height H * 2 * slots per plane, numerator
 rows slot*2H + y and weight rows slot*2H + H + y, the weight repeated in every
 plane.  vnlb.Aggregate divides the summed stacks (render_aggregate_frame,
 plugin.cpp:966-1045).  The GPU path implements the CPU core's stage for
-coupled and uncoupled planes, the dual-PCA and the covariance models and any
-model cap; eigen problems above 96 x 96 and MVTools search centres raise.
+coupled and uncoupled planes, the dual-PCA and the covariance models, any
+model cap and the MVTools-guided search centres (mvfw / mvbw); eigen problems
+above 96 x 96 raise.
+
+MVTools clips: VapourSynth hands the plugin frames whose properties carry the
+vectors; here `mvfw` and `mvbw` are sequences of those property mappings, one
+per frame ("MVTools_MVAnalysisData", "MVTools_vectors" as bytes), and
+`clip_props` the source clip's per-frame property mappings, of which the
+scene-change flags are read (_SceneChangePrev or Scenechange for mvfw,
+_SceneChangeNext for mvbw; src/vs/plugin.cpp:476-485).
 """
 from __future__ import annotations
 
@@ -150,8 +158,37 @@ _STAGE_ARGS = ("block_size", "block_step", "group_size", "bm_range", "patch_time
                "weight_alpha", "weight_beta", "weight_gamma", "weight_epsilon", "membership_noise_floor", "chroma")
 
 
+def _set_flow(session, clip, mvfw, mvbw, clip_props):
+    """read_mvtools_analysis_from_node + validate_mvtools_clip (plugin.cpp:
+    429-474, 881-899) and cache_mvtools_grid (:507-525) for every frame."""
+    frames = clip.shape[0]
+    props = list(clip_props) if clip_props is not None else [{}] * frames
+    if len(props) != frames:
+        _err("clip_props must hold one property mapping per frame")
+    for direction, name, vectors in ((lib.MVFW, "mvfw", mvfw), (lib.MVBW, "mvbw", mvbw)):
+        if vectors is None:
+            continue
+        vectors = list(vectors)
+        if len(vectors) != frames:
+            _err(f"{name} frame count must match clip")
+        try:
+            session.set_mvtools_analysis(direction, vectors[0]["MVTools_MVAnalysisData"])
+        except KeyError:
+            _err(f"{name} frames carry no MVTools_MVAnalysisData")
+        for n in range(frames):
+            if direction == lib.MVBW:
+                scene = bool(props[n].get("_SceneChangeNext", 0))
+            else:
+                scene = bool(props[n].get("_SceneChangePrev", 0)) or bool(props[n].get("Scenechange", 0))
+            try:
+                data = vectors[n]["MVTools_vectors"]
+            except KeyError:
+                _err(f"{name} frame {n} carries no MVTools_vectors")
+            session.set_mvtools_frame(direction, n, data, scene)
+
+
 class _StageFilter:
-    def __init__(self, stage, clip, ref, sigma, kwargs, allowed):
+    def __init__(self, stage, clip, ref, sigma, kwargs, allowed, mvfw=None, mvbw=None, clip_props=None):
         unknown = set(kwargs) - set(allowed)
         if unknown:
             raise TypeError(f"unexpected argument(s): {', '.join(sorted(unknown))}")
@@ -168,6 +205,8 @@ class _StageFilter:
         self.session.set_clip(lib.SOURCE_CLIP, self.clip)
         if stage == lib.STAGE_FINAL:
             self.session.set_clip(lib.SOURCE_REF, ref)
+        if mvfw is not None or mvbw is not None:
+            _set_flow(self.session, self.clip, mvfw, mvbw, clip_props)
         self.slots = self.p["search_bwd"] + self.p["search_fwd"] + self.p["patch_time"]
 
     def get_frame(self, n: int) -> np.ndarray:
@@ -177,18 +216,18 @@ class _StageFilter:
         return np.stack([self.get_frame(n) for n in range(self.clip.shape[0])])
 
 
-def Basic(clip, sigma=None, **kwargs) -> np.ndarray:
+def Basic(clip, sigma=None, mvfw=None, mvbw=None, clip_props=None, **kwargs) -> np.ndarray:
     """vnlb.Basic: contribution stacks [frames, planes, slots*2*H, W]."""
-    return _StageFilter(lib.STAGE_BASIC, clip, None, sigma, kwargs, _STAGE_ARGS).render()
+    return _StageFilter(lib.STAGE_BASIC, clip, None, sigma, kwargs, _STAGE_ARGS, mvfw, mvbw, clip_props).render()
 
 
-def Final(clip, ref=None, sigma=None, **kwargs) -> np.ndarray:
+def Final(clip, ref=None, sigma=None, mvfw=None, mvbw=None, clip_props=None, **kwargs) -> np.ndarray:
     """vnlb.Final: contribution stacks of the Final stage matched on `ref`."""
     clip = _clip(clip)
     if not isinstance(ref, np.ndarray) or ref.shape != clip.shape or ref.dtype != np.float32:
         _err("ref clip properties must match input clip")
     return _StageFilter(lib.STAGE_FINAL, clip, ref, sigma, kwargs,
-                        _STAGE_ARGS + ("sigma_basic", "gamma", "flat_areas")).render()
+                        _STAGE_ARGS + ("sigma_basic", "gamma", "flat_areas"), mvfw, mvbw, clip_props).render()
 
 
 def Aggregate(clip, src=None, patch_time=None, radius=None, search_bwd=None, search_fwd=None) -> np.ndarray:

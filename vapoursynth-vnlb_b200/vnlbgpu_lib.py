@@ -46,6 +46,17 @@ class Stats(ctypes.Structure):
                 ("anchor_frames", "groups", "active_groups", "rows", "kernel_launches")]
 
 
+class MVToolsAnalysis(ctypes.Structure):
+    """vnlbgpu_mvtools_analysis: MVToolsAnalysisData (src/flow/flow.hpp:37-55)."""
+    _fields_ = [(name, ctypes.c_int) for name in (
+        "block_size_x", "block_size_y", "pel", "level_count", "delta_frame", "backwards", "width", "height",
+        "overlap_x", "overlap_y", "block_count_x", "block_count_y", "bits_per_sample", "chroma_ratio_x",
+        "chroma_ratio_y", "padding_x", "padding_y")]
+
+
+MVFW, MVBW = 0, 1
+
+
 class DiagRow(ctypes.Structure):
     _fields_ = [("distance", ctypes.c_float), ("x", ctypes.c_int), ("y", ctypes.c_int),
                 ("frame", ctypes.c_int), ("weight", ctypes.c_float)]
@@ -58,6 +69,8 @@ EXPORTS = [
     "vnlbgpu_render_stack", "vnlbgpu_aggregate", "vnlbgpu_aggregate_frame_noalloc", "vnlbgpu_get_stats",
     "vnlbgpu_stream",
     "vnlbgpu_set_stream", "vnlbgpu_diag_anchor", "vnlbgpu_diag_kernel_timing",
+    "vnlbgpu_parse_mvtools_analysis", "vnlbgpu_parse_mvtools_vectors", "vnlbgpu_set_mvtools_analysis",
+    "vnlbgpu_set_mvtools_frame",
 ]
 KERNEL_CLASSES = ("match", "paste", "filter", "tiles", "normalize")
 
@@ -102,6 +115,15 @@ def load() -> ctypes.CDLL:
             lib.vnlbgpu_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.vnlbgpu_diag_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                        ctypes.c_void_p]
+            lib.vnlbgpu_parse_mvtools_analysis.argtypes = [ctypes.c_char_p, ctypes.c_size_t,
+                                                           ctypes.POINTER(MVToolsAnalysis)]
+            lib.vnlbgpu_parse_mvtools_vectors.argtypes = [
+                ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(MVToolsAnalysis), ctypes.POINTER(ctypes.c_int),
+                ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+            lib.vnlbgpu_set_mvtools_analysis.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p,
+                                                         ctypes.c_size_t]
+            lib.vnlbgpu_set_mvtools_frame.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
+                                                      ctypes.c_size_t, ctypes.c_int]
             _lib = lib
     return _lib
 
@@ -115,8 +137,37 @@ def _f32(a: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
+def parse_mvtools_analysis(data: bytes) -> MVToolsAnalysis:
+    """parse_mvtools_analysis (flow.hpp:193-250) of an MVTools_MVAnalysisData
+    property; host only, no device needed."""
+    out = MVToolsAnalysis()
+    _check(load().vnlbgpu_parse_mvtools_analysis(bytes(data), len(data), ctypes.byref(out)))
+    return out
+
+
+def parse_mvtools_vectors(data: bytes, analysis: MVToolsAnalysis):
+    """parse_mvtools_vectors (flow.hpp:252-318) of an MVTools_vectors property:
+    (valid, int32 array [count, 2] of the finest level's vectors)."""
+    valid, count = ctypes.c_int(), ctypes.c_size_t()
+    cap = analysis.block_count_x * analysis.block_count_y
+    xy = np.zeros((max(cap, 1), 2), np.int32)
+    _check(load().vnlbgpu_parse_mvtools_vectors(bytes(data), len(data), ctypes.byref(analysis), ctypes.byref(valid),
+                                                xy.ctypes.data, cap, ctypes.byref(count)))
+    return bool(valid.value), xy[:count.value]
+
+
 class Session:
     """One configured stage (Basic or Final) over one clip geometry."""
+
+    def set_mvtools_analysis(self, direction: int, data: bytes):
+        """The mvfw (MVFW) or mvbw (MVBW) clip's MVTools_MVAnalysisData."""
+        _check(load().vnlbgpu_set_mvtools_analysis(self.handle, direction, bytes(data), len(data)))
+
+    def set_mvtools_frame(self, direction: int, frame: int, vectors: bytes, scene_change: bool = False):
+        """Frame `frame`'s MVTools_vectors of that clip, and whether the source
+        clip's frame marks a scene change."""
+        _check(load().vnlbgpu_set_mvtools_frame(self.handle, direction, frame, bytes(vectors), len(vectors),
+                                                1 if scene_change else 0))
 
     def __init__(self, params: Params, width: int, height: int, frames: int, channels: int):
         self.lib = load()
