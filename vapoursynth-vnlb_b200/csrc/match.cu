@@ -248,15 +248,7 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     extern __shared__ __align__(16) float smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    Strip strip;
-    if constexpr (kFlow) {  // flow-guided search: one anchor per CTA, regions set per frame
-        strip.first = blockIdx.x;
-        strip.count = 1;
-        strip.y = L.anchors[blockIdx.x].y;
-        strip.region_x = strip.region_y = strip.region_w = strip.region_h = 0;
-    } else {
-        strip = L.strips[blockIdx.x];
-    }
+    const Strip strip = L.strips[blockIdx.x];
     const int Pd = L.P;
     const int Cs = L.search_channels;
     const int planes_n = Cs * L.Pt;
@@ -308,18 +300,50 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
     float ref_norm = 0.0f;   // chosen form: ||reference||^2
     float reg_exact = 0.0f;  // chosen form: exact distance of this lane's buffer slot
 
-    for (int k = 0; k < L.schedule_len; ++k) {
+    // Flow-guided search: every warp's window of frame k lies around its
+    // anchor's search centre there (same size as the anchor-centred one).  The
+    // strip's warps are taken in passes; a pass stages the bounding box of the
+    // windows of its warps, grown in warp order while it fits the reservation
+    // (region_w_max columns, region_rows rows), so a strip whose anchors move
+    // alike stages frame k once.  pending = warps still to search frame k.
+    __shared__ int2 window_origin[kFlow ? 8 : 1];
+    unsigned pending = 0u;
+    unsigned group = 0xffffffffu;  // warps searching in this pass
+    for (int k = 0; k < L.schedule_len; k += pending == 0u ? 1 : 0) {
         const int frame = L.schedule[k];
         if constexpr (kFlow) {
-            // the window of frame k around the anchor's search centre there
-            // (same size as the anchor-centred one)
-            const int2 c = L.centers[static_cast<size_t>(strip.first) * L.schedule_len + k];
-            spatial_range(c.x, L.width, Pd, L.search_window, xl, xh);
-            spatial_range(c.y, L.height, Pd, L.search_window, yl, yh);
-            rx0 = xl & ~3;
-            ry0 = yl;
-            rw = xh + Pd - rx0;
-            rh = yh - yl + Pd;
+            if (pending == 0u) {
+                __syncthreads();  // the previous frame's passes are done with the table
+                if (active_warp) {
+                    const int2 c = L.centers[static_cast<size_t>(g) * L.schedule_len + k];
+                    spatial_range(c.x, L.width, Pd, L.search_window, xl, xh);
+                    spatial_range(c.y, L.height, Pd, L.search_window, yl, yh);
+                    if (lane == 0) window_origin[warp] = make_int2(xl, yl);
+                }
+                __syncthreads();
+                pending = (1u << strip.count) - 1u;
+            }
+            const int w0 = __ffs(pending) - 1;
+            int2 o = window_origin[w0];
+            int x0 = o.x & ~3, x1 = o.x + Wx - 1 + Pd - 1, y0 = o.y, y1 = o.y + Wy - 1 + Pd - 1;
+            group = 1u << w0;
+            for (int w = w0 + 1; w < strip.count; ++w) {
+                if (!((pending >> w) & 1u)) continue;
+                o = window_origin[w];
+                const int nx0 = min(x0, o.x & ~3), nx1 = max(x1, o.x + Wx - 1 + Pd - 1);
+                const int ny0 = min(y0, o.y), ny1 = max(y1, o.y + Wy - 1 + Pd - 1);
+                if (nx1 - nx0 + 1 > L.region_w_max || ny1 - ny0 + kKY > L.region_rows) continue;
+                x0 = nx0;
+                x1 = nx1;
+                y0 = ny0;
+                y1 = ny1;
+                group |= 1u << w;
+            }
+            pending &= ~group;
+            rx0 = x0;
+            ry0 = y0;
+            rw = x1 - x0 + 1;
+            rh = y1 - y0 + 1;
         }
         __syncthreads();
         // Stage the strip's region of every plane (channel, t) of frame k.
@@ -362,7 +386,7 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
             }
             __syncthreads();
         }
-        if (!active_warp) continue;
+        if (!active_warp || !((group >> warp) & 1u)) continue;
         if (k == 0) {
             // Reference patch (anchor frame is scheduled first).
             for (int i = lane; i < planes_n * Pd * Pd; i += 32) {
@@ -787,8 +811,8 @@ cudaError_t launch_match(const MatchLaunch& L, int strips, int warps, cudaStream
         kernel<<<strips, block, smem, stream>>>(L);
         err = cudaGetLastError();
     };
-    if (L.centers) {  // flow-guided search: one anchor (one warp) per CTA
-        if (L.approx || warps != 1) return cudaErrorInvalidValue;
+    if (L.centers) {  // flow-guided search: windows around per-frame search centres
+        if (L.approx || warps > 8) return cudaErrorInvalidValue;
         switch (L.P) {
             case 4: launch(match_kernel<4, false, true>); break;
             case 5: launch(match_kernel<5, false, true>); break;

@@ -117,7 +117,9 @@ struct Session {
     int slots = 0, valid_anchor_frames = 0, max_rows = 0, buffer_cap = 0;
     int max_groups = 0, victim_stride = 0, warps = 8;
     int region_rows = 0, region_stride = 0, region_w_max = 0;
-    int flow_stride = 0;  // row stride of the one-anchor regions of the flow-guided search
+    // region reservation of the flow-guided search: the strip's plus room for
+    // anchors of one strip that move apart
+    int flow_region_rows = 0, flow_region_stride = 0, flow_region_w_max = 0;
     int sched_max = 0;    // most scheduled frames of an anchor frame
     // matcher forms: approx (VNLBGPU_FORM_CHOSEN: approximate distances in
     // the plain matcher's tiling, exact re-rank) and tensor
@@ -442,10 +444,21 @@ struct Session {
             if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
         }
         if (warps < 1) fail("VNLB CUDA: the search region of one anchor does not fit in shared memory");
-        // one-anchor regions (flow-guided search): the window plus the patch,
-        // from a column rounded down to a multiple of 4
-        flow_stride = (cw0 + P - 1 + 3 + 3) & ~3;
-        while (flow_stride % 8 != 4) ++flow_stride;
+        // flow-guided search: the strips' reservation widened by up to 16
+        // columns and 8 rows while the shared memory allows
+        for (int slack = 16; slack >= 0; slack -= 4) {
+            flow_region_w_max = region_w_max + slack;
+            flow_region_rows = region_rows + slack / 2;
+            flow_region_stride = flow_region_w_max;
+            while (flow_region_stride % 8 != 4) ++flow_region_stride;
+            MatchLaunch probe{};
+            probe.search_channels = search_channels;
+            probe.Pt = Pt;
+            probe.region_rows = flow_region_rows;
+            probe.region_stride = flow_region_stride;
+            probe.warp_floats = match_warp_floats(cw0 * ch0, search_channels * Pt, P, buffer_cap);
+            if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
+        }
         // tensor-core matcher: strips of up to kChosenAnchors anchors whose
         // windows lie within kChosenCols candidate columns
         if (p.form == VNLBGPU_FORM_CHOSEN_TC && chosen_match_supported(P, search_channels * Pt, cw0, ch0)) {
@@ -858,8 +871,8 @@ struct Session {
         m.status = d_status.ptr;
         cudaEvent_t t0 = begin_timed(ls);
         if (flow_on()) {
-            // flow-guided search (plain matcher, one anchor per CTA): the
-            // search centre of every anchor in every scheduled frame first
+            // flow-guided search (plain matcher, the strips' warps in passes):
+            // the search centre of every anchor in every scheduled frame first
             if (!lane.centers.ptr)
                 lane.centers.allocate(static_cast<size_t>(max_groups) * sched_max, "cudaMalloc(search centres)");
             CentersLaunch cl{};
@@ -878,8 +891,10 @@ struct Session {
             stats.kernel_launches += 1;
             m.centers = lane.centers.ptr;
             m.approx = 0;
-            m.region_stride = flow_stride;
-            check(launch_match(m, G, 1, ls), "match kernel launch");
+            m.region_rows = flow_region_rows;
+            m.region_stride = flow_region_stride;
+            m.region_w_max = flow_region_w_max;
+            check(launch_match(m, static_cast<int>(grid.strips.size()), warps, ls), "match kernel launch");
         } else if (chosen) {
             m.strips = grid.d_strips_chosen.ptr;
             m.tiles_x = chosen_tiles_x;

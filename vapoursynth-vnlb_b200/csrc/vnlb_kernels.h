@@ -44,6 +44,7 @@ struct MatchLaunch {
     const int* anchor_map;  // [H][W] anchor index or -1
     int region_rows;      // shared rows per plane (incl. padding)
     int region_stride;    // shared row stride in floats
+    int region_w_max;     // widest region a pass may stage (flow-guided search)
     int window_cells;     // max Wx*Wy
     int buffer_cap;       // match buffer capacity per warp
     int warp_floats;      // shared floats per warp
@@ -54,8 +55,8 @@ struct MatchLaunch {
     int* status;          // session status word (kStatus* codes, first error wins)
     // flow-guided search (plain matcher): the search centre of every anchor in
     // every scheduled frame, [anchor][schedule_len]; null = the anchor itself.
-    // With centres, a CTA is one warp and one anchor, and the region it stages
-    // follows the anchor's window frame by frame.
+    // With centres, each frame's region is the bounding box of the strip's
+    // windows around their centres, staged in passes when it does not fit.
     const int2* centers;
     float* approx_dist;   // [anchor][approx_stride] approximate distances (tensor-core form)
     int approx_stride;    // >= schedule_len * window_cells
