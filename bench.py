@@ -12,6 +12,13 @@ this path.  The plain GPU form computes bit-identical output to the reference
 CPU core.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--params cpu|vnlbcu]
+
+`--params vnlbcu` runs the same clip with vnlbcu's own defaults instead (block
+7, automatic step 3, group 16, bm_range 13, radius 1, patch_time 2, rank 15:
+estimator dimension 294, about 230k groups per anchor frame), plain form only
+(the chosen matchers need 8x8 patches and at most 32 retained rows), without
+the CPU sample.
 
 Under torchrun every rank (one GPU each) denoises its own clip (weak scaling,
 no collective on the data path); rank 0 prints one JSON line.  `value` is
@@ -50,7 +57,18 @@ CPU_DEFAULTS = dict(block_size=8, block_step=8, group_size=8, bm_range=9, radius
 FP32_LANE_OPS = 148 * 128 * 1.965e9
 
 
+# parameter set of the run: "cpu" (the CPU core's defaults, the headline) or
+# "vnlbcu" (vnlbcu's own defaults, a secondary row)
+PARAMS = "cpu"
+
+
 def workload_config(form: str) -> dict:
+    if PARAMS == "vnlbcu":
+        return {"workload": "vnlbcu.Basic+Final 1920x1080 YUV444PS 16 frames sigma 20, vnlbcu default parameters",
+                "form": form, "width": WIDTH, "height": HEIGHT, "frames_per_clip": FRAMES, "planes": PLANES,
+                "sigma": SIGMA, "params": dict(block_size=7, block_step=3, group_size=16, bm_range=13, radius=1,
+                                               patch_time=2, rank=15, cap_factor=4.0),
+                "l2": "inputs larger than L2 (398 MB clip per rank)"}
     return {"workload": "vnlbcu.Basic+Final 1920x1080 YUV444PS 16 frames sigma 20, CPU-default parameter set",
             "form": form, "width": WIDTH, "height": HEIGHT, "frames_per_clip": FRAMES, "planes": PLANES,
             "sigma": SIGMA, "params": CPU_DEFAULTS, "l2": "inputs larger than L2 (398 MB clip per rank)"}
@@ -60,6 +78,8 @@ def stage_params(stage: int, form: str = "plain"):
     import vnlbgpu_lib as lib
     import vnlbcu
     clip_shape = np.empty((FRAMES, PLANES, HEIGHT, WIDTH), np.float32)  # shape only for the parser
+    if PARAMS == "vnlbcu":
+        return vnlbcu.parse_parameters(stage, clip_shape, SIGMA, dict(form=form))
     kw = dict(CPU_DEFAULTS, form=form)
     if stage == lib.STAGE_FINAL:
         kw.update(tau=400.0, variance_threshold=1.7, flat_areas=1, weight_alpha=1.0, weight_beta=0.5,
@@ -160,6 +180,10 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if PARAMS != "cpu":
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU sample is defined for the CPU-default "
+                          "parameter set only (run without --params)"}), flush=True)
+        return 0
     _, kind, threads, fraction, step, sample = cpu_reference_sample()
     for _ in range(args.warmup):
         step()
@@ -255,6 +279,7 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
     psnr = {"noisy": synth.psnr(noisy, clean), "basic": synth.psnr(basic_out, clean),
             "final": synth.psnr(final_out, clean)}
     stats0 = [sb.stats(), sf.stats()]
+    lanes = {"basic": stats0[0]["pipeline_lanes"], "final": stats0[1]["pipeline_lanes"]}
     sb.kernel_timing(True)
     sf.kernel_timing(True)
     ranks.barrier()
@@ -305,7 +330,7 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
     sf.close()
     kernels = {k: (kb[k][0] + kf[k][0], kb[k][1] + kf[k][1]) for k in kb}
     return {"form": form, "value": value, "max_ms": max_ms, "e2e": e2e_value, "same": same, "psnr": psnr,
-            "kernels": kernels, "stats": delta, "clocks": clocks.summary(), "bp": bp, "outputs": (basic_out, final_out)}
+            "kernels": kernels, "stats": delta, "lanes": lanes, "clocks": clocks.summary(), "bp": bp, "outputs": (basic_out, final_out)}
 
 
 def roofline_of(r, steps, which=None):
@@ -331,7 +356,8 @@ def roofline_of(r, steps, which=None):
                 "ms_per_launch": ms / max(1, launches),
                 # dram__bytes_read.sum + dram__bytes_write.sum of one match launch (mean of the
                 # Basic and Final launches), profiles/kernels_1080p_yuv444_one_anchor_frame.md
-                "traffic": 59.3e6, "traffic_unit": "bytes per launch (ncu, one capture)"}
+                "traffic": 59.3e6 if PARAMS == "cpu" else None,
+                "traffic_unit": "bytes per launch (ncu, one capture)"}
     if dominant == "match" and r["form"] == "chosen":
         flops = 2.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
         return {"kernel": "match, chosen form (FP32 dot-product distances + exact re-rank)", "bound": "fp32",
@@ -385,6 +411,8 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     forms = ["plain", "chosen", "chosen_tc"] if args.form == "all" else [args.form]
+    if PARAMS == "vnlbcu":
+        forms = ["plain"]
     results = {f: measure_form(f, args, ranks, stream, noisy, clean, d_noisy, local) for f in forms}
     head = results[forms[-1]]
     per_kernel = {}
@@ -395,7 +423,7 @@ def run_ours(args):
     roofline = roofline_of(head, args.steps)
 
     cpu_baseline = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and PARAMS == "cpu":
         _, kind, threads, fraction, cstep, sample = cpu_reference_sample()
         cstep()
         c0 = time.perf_counter()
@@ -409,7 +437,8 @@ def run_ours(args):
                     "chosen": "chosen (selection on FP32 dot-product distances, exact FP32 re-rank)",
                     "chosen_tc": "chosen_tc (selection on BF16 tcgen05 tensor-core distances, exact FP32 re-rank)"}
         config = dict(workload_config(describe[head["form"]]), psnr_db=head["psnr"], kernels=per_kernel,
-                      dominant_kernel=roofline["kernel"], e2e_output_matches_device_output=head["same"])
+                      dominant_kernel=roofline["kernel"], e2e_output_matches_device_output=head["same"],
+                      pipeline_lanes=head["lanes"])
         if "plain" in results and head["form"] != "plain":
             plain = results["plain"]
             config["plain_form"] = {"value": plain["value"], "e2e": plain["e2e"], "psnr_db": plain["psnr"],
@@ -441,21 +470,29 @@ def run_ours(args):
 
 def run_profile_case(args):
     """A small case for ncu: one Basic and one Final anchor frame of a
-    3-frame 1920x1080 YUV444PS clip (the workload's frame size and
-    parameters), each stage launching every kernel class once."""
+    3-frame YUV444PS clip (the workload's frame size unless --profile-size
+    gives a smaller one, and its parameters), each stage launching every
+    kernel class once."""
     import vnlbgpu_lib as lib
 
-    _, noisy = synth.make_clip(WIDTH, HEIGHT, 3, PLANES, SIGMA, seed=0)
-    shape = np.empty((3, PLANES, HEIGHT, WIDTH), np.float32)
+    width, height = WIDTH, HEIGHT
+    if args.profile_size:
+        width, height = (int(v) for v in args.profile_size.lower().split("x"))
+    _, noisy = synth.make_clip(width, height, 3, PLANES, SIGMA, seed=0)
+    shape = np.empty((3, PLANES, height, width), np.float32)
     out = []
     for stage in (lib.STAGE_BASIC, lib.STAGE_FINAL):
         import vnlbcu
-        kw = dict(CPU_DEFAULTS, form=args.form if args.form != "all" else "plain")
-        if stage == lib.STAGE_FINAL:
-            kw.update(tau=400.0, variance_threshold=1.7)
+        form = args.form if args.form != "all" else "plain"
+        if PARAMS == "vnlbcu":
+            kw = dict(form=form)
         else:
-            kw.update(variance_threshold=1.1)
-        s = lib.Session(vnlbcu.parse_parameters(stage, shape, SIGMA, kw), WIDTH, HEIGHT, 3, PLANES)
+            kw = dict(CPU_DEFAULTS, form=form)
+            if stage == lib.STAGE_FINAL:
+                kw.update(tau=400.0, variance_threshold=1.7)
+            else:
+                kw.update(variance_threshold=1.1)
+        s = lib.Session(vnlbcu.parse_parameters(stage, shape, SIGMA, kw), width, height, 3, PLANES)
         s.set_clip(lib.SOURCE_CLIP, noisy)
         if stage == lib.STAGE_FINAL:
             s.set_clip(lib.SOURCE_REF, noisy)
@@ -478,7 +515,13 @@ def main():
                          "gate")
     ap.add_argument("--profile-case", action="store_true",
                     help="run only a small case (one anchor frame per stage) for ncu captures")
+    ap.add_argument("--profile-size", default=None, metavar="WxH",
+                    help="frame size of the profile case (default: the workload's 1920x1080)")
+    ap.add_argument("--params", choices=("cpu", "vnlbcu"), default="cpu",
+                    help="parameter set: the CPU core's defaults (the headline) or vnlbcu's own defaults")
     args = ap.parse_args()
+    global PARAMS
+    PARAMS = args.params
     if args.profile_case:
         return run_profile_case(args)
     if args.impl == "reference":

@@ -92,33 +92,53 @@ __device__ __forceinline__ size_t row_base(const FilterLaunch& L, const MatchRow
 __device__ __forceinline__ int bmax_of(const FilterLaunch& L) { return min(L.model_cap, L.max_rows); }
 
 // ---------------------------------------------------------------------------
-// prepare: one warp per group.
+// prepare: W warps per group.  W = 1 runs four groups per CTA, one per warp;
+// W = 4 gives a CTA to one group, for model rows too large for four copies in
+// shared memory to leave room for more than a few warps per SM (block 7,
+// patch_time 2, YUV: 16 rows of 294 values).  Every value is computed in the
+// same order either way: the column sums and the centring by the thread that
+// owns the column, each Gram pair by one octet of lanes, each channel's
+// flat-area sums by one warp.
+template <int W>
 __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunch L) {
+    constexpr int kGroups = kPrepareWarps / W;  // groups per CTA
+    constexpr int kT = 32 * W;                  // threads per group
     extern __shared__ __align__(16) float sm[];
+    __shared__ double s_sums[2 * 4];            // flat-area sums per channel (W > 1)
     const int D = L.dim;
     const int Bmax = bmax_of(L);
     int* coloff = reinterpret_cast<int*>(sm);
-    size_t* bases_all = reinterpret_cast<size_t*>(sm + ((D + 3) & ~3));  // kPrepareWarps * max_rows
+    size_t* bases_all = reinterpret_cast<size_t*>(sm + ((D + 3) & ~3));  // kGroups * max_rows
     const int ldx = D + 8;  // padded row stride: octets on different rows hit different banks
-    float* X = reinterpret_cast<float*>(bases_all + kPrepareWarps * L.max_rows) +
-               (threadIdx.x >> 5) * Bmax * ldx;  // this warp's model rows
-    size_t* bases = bases_all + (threadIdx.x >> 5) * L.max_rows;
+    const int slot = threadIdx.x / kT;          // this group's slot in the CTA
+    const int t = threadIdx.x - slot * kT;      // thread within the group
+    float* X = reinterpret_cast<float*>(bases_all + kGroups * L.max_rows) + slot * Bmax * ldx;  // model rows
+    size_t* bases = bases_all + slot * L.max_rows;
     for (int col = threadIdx.x; col < D; col += blockDim.x) coloff[col] = column_offset(L, col);
     __syncthreads();
     const int lane = threadIdx.x & 31;
+    const int gwarp = t >> 5;  // warp within the group
+    auto group_sync = [] {
+        if constexpr (W == 1) __syncwarp();
+        else __syncthreads();
+    };
+    auto group_any = [](bool p) -> bool {
+        if constexpr (W == 1) return __any_sync(0xffffffffu, p);
+        else return __syncthreads_or(p) != 0;
+    };
     const StageConfig& P = L.cfg;
     const bool final_stage = L.stage == 1;
     const float* model_video = final_stage ? L.basic : L.noisy;
     const bool weights_enabled = P.weight_alpha != 0.0f || P.weight_beta != 0.0f || P.weight_gamma != 0.0f;
     const int active_count = L.counters->active;
-    const int warps_total = gridDim.x * kPrepareWarps;
     // model v = (active group a, model channel mc): one model per group when
     // the channels are coupled (or the clip has one plane), one per plane
     // otherwise (transform_vnlb_channel, core.cpp:795-808)
     const int models = L.models;
     const size_t hw = static_cast<size_t>(L.height) * L.width;
     const int RD = L.row_dim;
-    for (int v = blockIdx.x * kPrepareWarps + (threadIdx.x >> 5); v < active_count * models; v += warps_total) {
+    for (int v = blockIdx.x * kGroups + slot; v < active_count * models; v += gridDim.x * kGroups) {
+        group_sync();  // the previous group is done with bases and X
         const int a = v / models;
         const int mc = v - a * models;
         const size_t cb = mc * hw;  // plane offset of this model's channel
@@ -127,7 +147,7 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
         const MatchRow* rows = L.rows + static_cast<size_t>(g) * L.max_rows;
         const int r0 = L.row_offset[a];
         const int B = min(S, L.model_cap);
-        for (int i = lane; i < S; i += 32) {
+        for (int i = t; i < S; i += kT) {
             const MatchRow m = rows[i];
             if (mc == 0) {
                 L.row_info[r0 + i] = m;
@@ -135,11 +155,11 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
             }
             bases[i] = row_base(L, m);
         }
-        __syncwarp();
+        group_sync();
         // equal group (samples_are_equal / group_is_equal): independent loads
         bool differs = S <= 1;
         if (S > 1) {
-            for (int col = lane; col < D * models; col += 32) {
+            for (int col = t; col < D * models; col += kT) {
                 const int cm = col / D;  // plane of an uncoupled group (group_is_equal, core.cpp:516-531)
                 const float* src = L.noisy + cm * hw + coloff[col - cm * D];
                 const float v0 = __ldg(src + bases[0]);
@@ -152,12 +172,12 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
                 for (; i < S; ++i) differs |= __ldg(src + bases[i]) != v0;
             }
         }
-        if (!__any_sync(0xffffffffu, differs)) {
+        if (!group_any(differs)) {
             // filtered = input, default aggregation model (core.cpp:253-274)
             for (int i = 0; i < S; ++i) {
                 const size_t b = bases[i];
                 float* out = L.filtered + static_cast<size_t>(r0 + i) * RD + mc * D;
-                for (int col = lane; col < D; col += 32) out[col] = __ldg(L.noisy + b + cb + coloff[col]);
+                for (int col = t; col < D; col += kT) out[col] = __ldg(L.noisy + b + cb + coloff[col]);
             }
             const float tau = __fadd_rn(P.weight_epsilon, __fdiv_rn(static_cast<float>(D), static_cast<float>(B)));
             const float lgw = P.weight_alpha == 0.0f ? 0.0f : __fmul_rn(-P.weight_alpha, cr_logf(tau));
@@ -168,25 +188,29 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
                 w = cr_expf(lw);
             }
             if (mc == 0)
-                for (int i = lane; i < S; i += 32) L.weights[r0 + i] = w;
-            if (lane == 0) L.flags[v] = kGroupDone;
+                for (int i = t; i < S; i += kT) L.weights[r0 + i] = w;
+            if (t == 0) L.flags[v] = kGroupDone;
             continue;
         }
-        // flat area (Final): mean channel variance of the noisy rows
+        // flat area (Final): mean channel variance of the noisy rows; one warp
+        // sums a channel (lane-strided, then a fixed shuffle tree)
         bool flat = false;
         if (final_stage && P.flat_areas) {
             const int pd = L.patch_dim;
             const int channels = models > 1 ? models : D / pd;
             const int per_channel = pd * S;
             float variance = 0.0f;
-            for (int c = 0; c < channels; ++c) {
+            for (int c0 = 0; c0 < channels; c0 += W) {
+                const int c = c0 + gwarp;
                 double sum = 0.0, sum2 = 0.0;
-                for (int i = 0; i < S; ++i) {
-                    const float* src = L.noisy + bases[i];
-                    for (int q = lane; q < pd; q += 32) {
-                        const float x = __ldg(src + (models > 1 ? c * hw + coloff[q] : coloff[c * pd + q]));
-                        sum += static_cast<double>(x);
-                        sum2 += static_cast<double>(x) * static_cast<double>(x);
+                if (c < channels) {
+                    for (int i = 0; i < S; ++i) {
+                        const float* src = L.noisy + bases[i];
+                        for (int q = lane; q < pd; q += 32) {
+                            const float x = __ldg(src + (models > 1 ? c * hw + coloff[q] : coloff[c * pd + q]));
+                            sum += static_cast<double>(x);
+                            sum2 += static_cast<double>(x) * static_cast<double>(x);
+                        }
                     }
                 }
 #pragma unroll
@@ -194,43 +218,61 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
                     sum += __shfl_xor_sync(0xffffffffu, sum, o);
                     sum2 += __shfl_xor_sync(0xffffffffu, sum2, o);
                 }
-                if (per_channel > 1) {
-                    const double count = static_cast<double>(per_channel);
-                    variance = __fadd_rn(variance, static_cast<float>((sum2 - (sum * sum / count)) / (count - 1.0)));
+                if constexpr (W > 1) {
+                    if (lane == 0 && c < channels) {
+                        s_sums[2 * gwarp] = sum;
+                        s_sums[2 * gwarp + 1] = sum2;
+                    }
+                    group_sync();
                 }
+                // the channels of this round in order
+                for (int k = 0; k < W && c0 + k < channels; ++k) {
+                    double ks = sum, ks2 = sum2;
+                    if constexpr (W > 1) {
+                        ks = s_sums[2 * k];
+                        ks2 = s_sums[2 * k + 1];
+                    }
+                    if (per_channel > 1) {
+                        const double count = static_cast<double>(per_channel);
+                        variance = __fadd_rn(variance, static_cast<float>((ks2 - (ks * ks / count)) / (count - 1.0)));
+                    }
+                }
+                if constexpr (W > 1) group_sync();
             }
             if (per_channel > 1) variance = __fdiv_rn(variance, static_cast<float>(channels));
             flat = variance < __fmul_rn(__fmul_rn(P.sigma, P.sigma), P.gamma);
         }
         if (B < min(D, L.rank)) {
-            if (lane == 0) {
+            if (t == 0) {
                 atomicCAS(L.status, 0, kStatusRankNotCovered);
                 L.flags[v] = kGroupSkip;
             }
             continue;
         }
         // model rows, means over the first B rows (compute_mean), centring
-        for (int s = 0; s < B; ++s) {
-            const size_t b = bases[s];
-            for (int col = lane; col < D; col += 32) X[s * ldx + col] = __ldg(model_video + b + cb + coloff[col]);
+        for (int e = t; e < B * D; e += kT) {
+            const int s2 = e / D;
+            const int col = e - s2 * D;
+            X[s2 * ldx + col] = __ldg(model_video + bases[s2] + cb + coloff[col]);
         }
+        group_sync();
         const float inv_b = __fdiv_rn(1.0f, static_cast<float>(B));
         float* means = L.means + static_cast<size_t>(v) * 2 * D;
-        for (int col = lane; col < D; col += 32) {
+        for (int col = t; col < D; col += kT) {
             float mm = 0.0f;
-            for (int s = 0; s < B; ++s) mm = __fadd_rn(mm, X[s * ldx + col]);
+            for (int s2 = 0; s2 < B; ++s2) mm = __fadd_rn(mm, X[s2 * ldx + col]);
             mm = __fmul_rn(mm, inv_b);
             float center = mm;  // Basic: noisy mean; Final flat: basic mean
             if (final_stage && !flat) {
                 float mn = 0.0f;
-                for (int s = 0; s < B; ++s) mn = __fadd_rn(mn, __ldg(L.noisy + bases[s] + cb + coloff[col]));
+                for (int s2 = 0; s2 < B; ++s2) mn = __fadd_rn(mn, __ldg(L.noisy + bases[s2] + cb + coloff[col]));
                 center = __fmul_rn(mn, inv_b);
             }
             means[col] = mm;
             means[D + col] = center;
-            for (int s = 0; s < B; ++s) X[s * ldx + col] = __fsub_rn(X[s * ldx + col], mm);
+            for (int s2 = 0; s2 < B; ++s2) X[s2 * ldx + col] = __fsub_rn(X[s2 * ldx + col], mm);
         }
-        __syncwarp();
+        group_sync();
         if (L.rank > 0) {
             const float scale = __fdiv_rn(1.0f, static_cast<float>(B));
             float* gram = L.gram + static_cast<size_t>(v) * L.nmax * L.nmax;
@@ -238,8 +280,8 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
                 // dual Gram (compute_gram_centered): octet k takes pair e0 + k;
                 // lane j of the octet runs the pinned chain j (octet_dot8)
                 const int pairs = B * (B + 1) / 2;
-                const int oct = lane >> 3;
-                for (int e0 = 0; e0 < pairs; e0 += 4) {
+                const int oct = t >> 3;
+                for (int e0 = 0; e0 < pairs; e0 += kT / 8) {
                     const int e = min(e0 + oct, pairs - 1);
                     int r = 0;
                     while ((r + 1) * (r + 2) / 2 <= e) ++r;
@@ -256,7 +298,7 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
                 // add_scaled_contiguous_highway, fused on the full 8-lane chunks of
                 // the D - r columns it spans; then scaled, both triangles
                 const int entries = D * (D + 1) / 2;
-                for (int e = lane; e < entries; e += 32) {
+                for (int e = t; e < entries; e += kT) {
                     int r = 0, rem = e;
                     while (rem >= D - r) {
                         rem -= D - r;
@@ -276,8 +318,7 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
                 }
             }
         }
-        if (lane == 0) L.flags[v] = 0;
-        __syncwarp();
+        if (t == 0) L.flags[v] = 0;
     }
 }
 
@@ -1149,15 +1190,20 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
     const int Bmax = std::min(L.model_cap, L.max_rows);
     const int R = L.rank;
     const size_t colpad = static_cast<size_t>((D + 3) & ~3);
-    // prepare
+    // prepare: a warp per group while a group's model rows take at most
+    // 8 KB of shared memory, else a CTA per group
     {
-        const size_t smem = (colpad + static_cast<size_t>(kPrepareWarps) * Bmax * (D + 8)) * sizeof(float) +
-                            static_cast<size_t>(kPrepareWarps) * L.max_rows * sizeof(size_t);
-        cudaError_t err = cudaFuncSetAttribute(prepare_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        const size_t rows_bytes = static_cast<size_t>(Bmax) * (D + 8) * sizeof(float);
+        const bool wide = rows_bytes > 8 * 1024;
+        const int groups_per_cta = wide ? 1 : kPrepareWarps;
+        const size_t smem = (colpad + static_cast<size_t>(groups_per_cta) * Bmax * (D + 8)) * sizeof(float) +
+                            static_cast<size_t>(groups_per_cta) * L.max_rows * sizeof(size_t);
+        auto kernel = wide ? prepare_kernel<kPrepareWarps> : prepare_kernel<1>;
+        cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
         if (err != cudaSuccess) return err;
-        const int ctas = std::min((max_groups + kPrepareWarps - 1) / kPrepareWarps, 148 * 16);
-        prepare_kernel<<<ctas, 32 * kPrepareWarps, smem, stream>>>(L);
+        const int ctas = std::min((max_groups + groups_per_cta - 1) / groups_per_cta, 148 * 16);
+        kernel<<<ctas, 32 * kPrepareWarps, smem, stream>>>(L);
         if ((err = cudaGetLastError()) != cudaSuccess) return err;
     }
     // jacobi

@@ -173,7 +173,7 @@ struct Session {
     void collect_timing() {
         if (timed.empty()) return;
         check(cudaStreamSynchronize(stream), "cudaStreamSynchronize(timing)");
-        for (Lane& l : lanes) check(cudaStreamSynchronize(l.stream), "cudaStreamSynchronize(timing)");
+        for (int i = 0; i < lane_count; ++i) check(cudaStreamSynchronize(lanes[i].stream), "cudaStreamSynchronize(timing)");
         for (const Timed& t : timed) {
             float ms = 0.0f;
             check(cudaEventElapsedTime(&ms, t.start, t.stop), "cudaEventElapsedTime");
@@ -194,7 +194,9 @@ struct Session {
     // with its own stream and scratch, so that one anchor frame's serial
     // paste-mask walk and latency-bound kernels overlap the others' kernels
     // (1080p YUV444 Basic+Final: 220 fps with 2 lanes, 225 with 3, 231 with 4,
-    // no further gain for the plain form with 6 or 8).
+    // no further gain for the plain form with 6 or 8).  A session takes fewer
+    // lanes when their group buffers would take more than half of the free
+    // device memory, so that a Basic session leaves room for its Final.
     struct Lane {
         cudaStream_t stream = nullptr;
         DeviceArray<MatchRow> rows, row_info;
@@ -205,11 +207,12 @@ struct Session {
         DeviceArray<float> filtered, weights, gmeans, gram, eig, dual, logw;
         DeviceArray<float> approx;  // tensor-core form: approximate distances [G][approx_stride]
     };
-    static constexpr int kLaneCount = 4;
-    Lane lanes[kLaneCount];
+    static constexpr int kMaxLanes = 4;
+    Lane lanes[kMaxLanes];
+    int lane_count = kMaxLanes;        // lanes in use (allocated): 1..kMaxLanes
     int next_lane = 0;
     cudaEvent_t ev_fork = nullptr;     // main-stream point the lanes start after
-    cudaEvent_t ev_lane[kLaneCount] = {};
+    cudaEvent_t ev_lane[kMaxLanes] = {};
 
     // Host transfers run on their own streams so that they overlap the
     // kernels: each uploaded frame records frame_ready[source][frame], and an
@@ -275,11 +278,11 @@ struct Session {
     // Lanes start after everything enqueued so far on the main stream ...
     void fork() {
         check(cudaEventRecord(ev_fork, stream), "cudaEventRecord(fork)");
-        for (Lane& l : lanes) check(cudaStreamWaitEvent(l.stream, ev_fork, 0), "cudaStreamWaitEvent(fork)");
+        for (int i = 0; i < lane_count; ++i) check(cudaStreamWaitEvent(lanes[i].stream, ev_fork, 0), "cudaStreamWaitEvent(fork)");
     }
     // ... and the main stream continues after everything the lanes did.
     void join() {
-        for (int i = 0; i < kLaneCount; ++i) {
+        for (int i = 0; i < lane_count; ++i) {
             check(cudaEventRecord(ev_lane[i], lanes[i].stream), "cudaEventRecord(join)");
             check(cudaStreamWaitEvent(stream, ev_lane[i], 0), "cudaStreamWaitEvent(join)");
         }
@@ -483,10 +486,20 @@ struct Session {
         if (nmax > 96) fail("VNLB CUDA: eigen problems above 96 x 96 (model rows or covariance dimension) are not supported");
         size_t free_bytes = 0, total_bytes = 0;
         check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
-        const size_t need = kLaneCount * R * (static_cast<size_t>(row_dim) * 4 + 4 + sizeof(MatchRow) + 4);
-        if (need > free_bytes / 2)
-            fail("VNLB CUDA: the group buffers of one anchor frame do not fit in device memory");
-        for (Lane& l : lanes) {
+        const size_t M = G * models;  // models: one per group, or one per plane when uncoupled
+        const size_t N = static_cast<size_t>(nmax);
+        const size_t rank1 = static_cast<size_t>(std::max(1, p.rank));
+        // bytes of one lane's buffers, as allocated below
+        const size_t lane_bytes =
+            G * max_rows * sizeof(MatchRow) + G * (6 * sizeof(int) + sizeof(int2) + victim_stride * sizeof(int)) +
+            (chosen ? G * static_cast<size_t>(approx_stride) * sizeof(float) : 0) +
+            R * (static_cast<size_t>(row_dim) + 1 + (models > 1 ? models : 0)) * sizeof(float) +
+            R * (sizeof(MatchRow) + sizeof(int)) +
+            M * (2 * static_cast<size_t>(dim) + N * N + rank1 + rank1 * N) * sizeof(float) + M * sizeof(int);
+        lane_count = static_cast<int>(std::min<size_t>(kMaxLanes, free_bytes / 2 / std::max<size_t>(lane_bytes, 1)));
+        if (lane_count < 1) fail("VNLB CUDA: the group buffers of one anchor frame do not fit in device memory");
+        for (int li = 0; li < lane_count; ++li) {
+            Lane& l = lanes[li];
             check(cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking), "cudaStreamCreate(lane)");
             l.rows.allocate(G * max_rows, "cudaMalloc(match rows)");
             l.row_counts.allocate(G, "cudaMalloc(row counts)");
@@ -498,8 +511,6 @@ struct Session {
             l.active_prefix.allocate(G + 1, "cudaMalloc(active prefix)");
             l.counters.allocate(1, "cudaMalloc(counters)");
             if (chosen) l.approx.allocate(G * approx_stride, "cudaMalloc(approximate distances)");
-            const size_t M = G * models;  // models: one per group, or one per plane when uncoupled
-            const size_t N = static_cast<size_t>(nmax);
             l.filtered.allocate(R * row_dim, "cudaMalloc(filtered rows)");
             l.gmeans.allocate(M * 2 * dim, "cudaMalloc(group means)");
             l.gram.allocate(M * N * N, "cudaMalloc(group Gram)");
@@ -548,7 +559,7 @@ struct Session {
         d_window.allocate(host_window.size(), "cudaMalloc(window)");
         check(cudaMemcpy(d_window.ptr, host_window.data(), host_window.size() * sizeof(float), cudaMemcpyHostToDevice),
               "cudaMemcpy(window)");
-        const int cache_size = slots + kLaneCount;  // every contributor of a frame, plus the lanes' work in flight
+        const int cache_size = slots + lane_count;  // every contributor of a frame, plus the lanes' work in flight
         for (int i = 0; i < cache_size; ++i) {
             auto entry = std::make_unique<CachedStack>();
             entry->data.allocate(stack_values(), "cudaMalloc(contribution stack)");
@@ -1024,7 +1035,7 @@ struct Session {
         victim->anchor = anchor;
         victim->last_use = ++use_clock;
         const int li = next_lane;
-        next_lane = (next_lane + 1) % kLaneCount;
+        next_lane = (next_lane + 1) % lane_count;
         Lane& lane = lanes[li];
         if (victim->pending_release)  // its previous contents are still being read
             check(cudaStreamWaitEvent(lane.stream, victim->released, 0), "cudaStreamWaitEvent(stack release)");
@@ -1457,6 +1468,7 @@ int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats) {
         vnlbgpu::check(cudaStreamSynchronize(s.stream), "cudaStreamSynchronize");
         s.stats.active_groups = static_cast<long long>(totals[0]);
         s.stats.rows = static_cast<long long>(totals[1]);
+        s.stats.pipeline_lanes = s.lane_count;
         *stats = s.stats;
     });
 }
@@ -1470,7 +1482,8 @@ int vnlbgpu_set_stream(vnlbgpu_session* session, void* stream) {
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
         s.collect_timing();
         vnlbgpu::check(cudaStreamSynchronize(s.stream), "cudaStreamSynchronize");
-        for (auto& l : s.lanes) vnlbgpu::check(cudaStreamSynchronize(l.stream), "cudaStreamSynchronize");
+        for (int i = 0; i < s.lane_count; ++i)
+            vnlbgpu::check(cudaStreamSynchronize(s.lanes[i].stream), "cudaStreamSynchronize");
         s.stream = stream ? static_cast<cudaStream_t>(stream) : s.own_stream;
     });
 }

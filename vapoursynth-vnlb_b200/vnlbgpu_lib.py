@@ -43,7 +43,7 @@ class Params(ctypes.Structure):
 
 class Stats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_longlong) for name in
-                ("anchor_frames", "groups", "active_groups", "rows", "kernel_launches")]
+                ("anchor_frames", "groups", "active_groups", "rows", "kernel_launches", "pipeline_lanes")]
 
 
 class MVToolsAnalysis(ctypes.Structure):
