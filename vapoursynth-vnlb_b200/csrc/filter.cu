@@ -491,39 +491,75 @@ __device__ __forceinline__ float model_log_weight(const StageConfig& P, bool mem
 //   per-warp scratch (3 rows of ldb), row bases[max_rows] (size_t).
 // Row strides are padded (ldx = D + 1, ldb = D + 8) so that lanes reading
 // different rows at the same column hit different banks.
+// Row tiles of the tiled row loop: kTileRows rows per warp, at most
+// kTileComps components, and per row the folded dot products in kTileSlots
+// floats (membership dots [0, 16), reconstruction dots [16, 32), norm at 32).
+constexpr int kTileRows = 2;
+constexpr int kTileComps = 16;
+constexpr int kTileSlots = 33;
+
 struct ApplyLayout {
-    int D, Bmax, R, ldx, ldb, colpad;
-    size_t means, X, basis, dual, scal, scores, scratch, bases, bytes;
+    int D, Bmax, R, ldx, ldb, ldu, colpad;
+    size_t means, X, basis, dual, scal, scores, scratch, tile_floats, bases, bytes;
 };
 
-__host__ __device__ inline ApplyLayout apply_layout(int D, int Bmax, int R, int max_rows, int warps) {
+// tiled: the row loop of apply_kernel<true>, whose per-warp row tiles (the
+// centred rows at stride ldu = 8 mod 32, and the Final stage's noisy rows)
+// share their space with the model rows X, which are dead by then.
+__host__ __device__ inline ApplyLayout apply_layout(int D, int Bmax, int R, int max_rows, int warps,
+                                                    bool tiled = false, bool final_stage = false) {
     ApplyLayout a{};
     a.D = D;
     a.Bmax = Bmax;
     a.R = R;
     a.ldx = D + 1;
-    a.ldb = D + 8;
+    a.ldu = ((D + 23) & ~31) + 8;  // smallest stride >= D that is 8 mod 32
+    // basis rows: the tiled loop reads four components at one column, 8 banks apart
+    a.ldb = tiled ? a.ldu : D + 8;
     a.colpad = (D + 3) & ~3;
     size_t off = static_cast<size_t>(a.colpad);
     a.means = off;   off += 2 * static_cast<size_t>(D);
-    a.X = off;       off += static_cast<size_t>(Bmax) * a.ldx;
+    if (!tiled) {
+        a.X = off;   off += static_cast<size_t>(Bmax) * a.ldx;
+    }
     a.basis = off;   off += static_cast<size_t>(R) * a.ldb;
     a.dual = off;    off += static_cast<size_t>(R) * Bmax;
     a.scal = off;    off += 5 * static_cast<size_t>(R);
     a.scores = off;  off += static_cast<size_t>(max_rows);
-    a.scratch = off; off += static_cast<size_t>(warps) * (2 * a.ldb + R + 1);
+    a.scratch = off;
+    if (tiled) {
+        a.tile_floats = static_cast<size_t>(final_stage ? 2 : 1) * kTileRows * a.ldu + kTileRows * kTileSlots;
+        a.X = off;
+        const size_t tiles = static_cast<size_t>(warps) * a.tile_floats;
+        const size_t model = static_cast<size_t>(Bmax) * a.ldx;
+        off += tiles > model ? tiles : model;
+    } else {
+        off += static_cast<size_t>(warps) * (2 * a.ldb + R + 1);
+    }
     off = (off + 1) & ~static_cast<size_t>(1);
     a.bases = off;   off += 2 * static_cast<size_t>(max_rows);
     a.bytes = off * sizeof(float);
     return a;
 }
 
-__global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
+// The pinned 8-lane fold of an octet's chains as an xor butterfly: every lane
+// of the octet ends with ((v0 + v4) + (v2 + v6)) + ((v1 + v5) + (v3 + v7)),
+// the same additions as reduce8 (each one commutative).
+__device__ __forceinline__ float octet_fold(float v) {
+    v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, 4));
+    v = __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, 2));
+    return __fadd_rn(v, __shfl_xor_sync(0xffffffffu, v, 1));
+}
+
+// kTiled: rows in tiles of kTileRows per warp (rank <= kTileComps, dimension
+// above 16), else one row per warp with the components four at a time.
+template <bool kTiled>
+__global__ void __launch_bounds__(kApplyThreads, 3) apply_kernel(FilterLaunch L) {
     extern __shared__ __align__(16) float sm[];
     const int D = L.dim;
     const int Bmax = bmax_of(L);
     const int R = L.rank;
-    const ApplyLayout lay = apply_layout(D, Bmax, R, L.max_rows, kApplyWarps);
+    const ApplyLayout lay = apply_layout(D, Bmax, R, L.max_rows, kApplyWarps, kTiled, L.stage == 1);
     const int ldx = lay.ldx, ldb = lay.ldb;
     int* coloff = reinterpret_cast<int*>(sm);
     float* means = sm + lay.means;  // membership mean, reconstruction centre
@@ -660,82 +696,238 @@ __global__ void __launch_bounds__(kApplyThreads) apply_kernel(FilterLaunch L) {
         __syncthreads();
         const float lgw = s_misc[0];
         const float volume = s_misc[1];
-        // per row: membership score and reconstruction.  In the Basic stage the
-        // membership row and the reconstruction row are the same centred noisy
-        // row, so its projections serve both.
-        float* u = scratch + warp * (2 * ldb + R + 1);  // centred membership row
-        float* v = u + ldb;                             // centred noisy row (Final)
-        float* proj = v + ldb;                          // projections for the reconstruction
-        const int j8 = lane & 7;
-        const int oct = lane >> 3;
-        const float score_scale = __fsqrt_rn(__fmul_rn(2.0f, static_cast<float>(D)));
-        for (int i = warp; i < S; i += kApplyWarps) {
-            const size_t b = bases[i];
-            for (int col = lane; col < D; col += 32) {
-                const float xn = __ldg(L.noisy + b + coloff[col]);
-                if (final_stage) {
-                    u[col] = __fsub_rn(__ldg(L.basic + b + coloff[col]), member_mean[col]);
-                    v[col] = __fsub_rn(xn, center_vec[col]);
-                } else {
-                    u[col] = __fsub_rn(xn, member_mean[col]);
-                }
-            }
-            __syncwarp();
-            float distance = 0.0f, projected = 0.0f, norm2 = 0.0f;
-            // pass over c0 = -1 (norm), 0, 4, ...: octet k computes component c0 + k
-            for (int c0 = membership_on ? -1 : 0; c0 < R; c0 += 4) {
-                const int c = min(c0 + oct, R - 1);
-                const float dm = (membership_on || !final_stage) ? octet_dot8(u, c < 0 ? u : basis + c * ldb, D, j8)
-                                                                 : 0.0f;
-                const float dr = final_stage ? octet_dot8(v, basis + max(c, 0) * ldb, D, j8) : dm;
-                for (int k = 0; k < 4; ++k) {
-                    const int ck = c0 + k;
-                    const float mk = __shfl_sync(0xffffffffu, dm, k * 8);
-                    const float rk = __shfl_sync(0xffffffffu, dr, k * 8);
-                    if (ck >= R) break;
-                    if (ck < 0) {
-                        norm2 = mk;
-                        continue;
+        if constexpr (kTiled) {
+            // Rows in tiles of kTileRows per warp.  Lane (j, g) runs the pinned
+            // chain j (elements j + 8m) of both tile rows against components
+            // g, g + 4, g + 8 and g + 12, so one basis load feeds the membership
+            // and the reconstruction chains of two rows; octet_fold folds the
+            // chains, and one lane per (row, dot) adds the unfused tail
+            // (dot_contiguous_highway: the operations of octet_dot8).
+            float* U = scratch + warp * lay.tile_floats;  // centred membership rows
+            float* V = U + kTileRows * lay.ldu;            // centred noisy rows (Final)
+            float* res = U + (final_stage ? 2 : 1) * kTileRows * lay.ldu;  // [row][kTileSlots]
+            const int ldu = lay.ldu;
+            const int j = lane & 7;
+            const int grp = lane >> 3;
+            const int full = D / kLanes;
+            const float score_scale = __fsqrt_rn(__fmul_rn(2.0f, static_cast<float>(D)));
+            for (int t0 = warp * kTileRows; t0 < S; t0 += kApplyWarps * kTileRows) {
+                const int nrows = min(kTileRows, S - t0);
+                for (int r = 0; r < nrows; ++r) {
+                    const size_t b = bases[t0 + r];
+                    for (int col = lane; col < D; col += 32) {
+                        const float xn = __ldg(L.noisy + b + coloff[col]);
+                        if (final_stage) {
+                            U[r * ldu + col] = __fsub_rn(__ldg(L.basic + b + coloff[col]), member_mean[col]);
+                            V[r * ldu + col] = __fsub_rn(xn, center_vec[col]);
+                        } else {
+                            U[r * ldu + col] = __fsub_rn(xn, member_mean[col]);
+                        }
                     }
-                    if (membership_on) {
+                }
+                __syncwarp();
+                const int r1 = nrows > 1 ? 1 : 0;  // a missing second row repeats the first
+                float am[kTileRows][4], ar[kTileRows][4], an[kTileRows];
+#pragma unroll
+                for (int r = 0; r < kTileRows; ++r) {
+                    an[r] = 0.0f;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) am[r][k] = ar[r][k] = 0.0f;
+                }
+                for (int m = 0; m < full; ++m) {
+                    const int col = j + kLanes * m;
+                    const float u0 = U[col], u1 = U[r1 * ldu + col];
+                    an[0] = __fmaf_rn(u0, u0, an[0]);
+                    an[1] = __fmaf_rn(u1, u1, an[1]);
+                    if (final_stage) {
+                        const float v0 = V[col], v1 = V[r1 * ldu + col];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (grp + 4 * k < R) {
+                                const float bv = basis[(grp + 4 * k) * ldb + col];
+                                am[0][k] = __fmaf_rn(u0, bv, am[0][k]);
+                                am[1][k] = __fmaf_rn(u1, bv, am[1][k]);
+                                ar[0][k] = __fmaf_rn(v0, bv, ar[0][k]);
+                                ar[1][k] = __fmaf_rn(v1, bv, ar[1][k]);
+                            }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (grp + 4 * k < R) {
+                                const float bv = basis[(grp + 4 * k) * ldb + col];
+                                am[0][k] = __fmaf_rn(u0, bv, am[0][k]);
+                                am[1][k] = __fmaf_rn(u1, bv, am[1][k]);
+                            }
+                    }
+                }
+                // fold; lane j of octet grp stores (row j / 4, component grp + 4 (j % 4))
+#pragma unroll
+                for (int r = 0; r < kTileRows; ++r) {
+                    an[r] = octet_fold(an[r]);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        am[r][k] = octet_fold(am[r][k]);
+                        if (final_stage) ar[r][k] = octet_fold(ar[r][k]);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < kTileRows; ++r)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (j == 4 * r + k && grp + 4 * k < R) {
+                            res[r * kTileSlots + grp + 4 * k] = am[r][k];
+                            if (final_stage) res[r * kTileSlots + 16 + grp + 4 * k] = ar[r][k];
+                        }
+                if (lane < kTileRows) res[lane * kTileSlots + 32] = lane == 0 ? an[0] : an[1];
+                __syncwarp();
+                if (full * kLanes < D) {
+                    // the unfused tail of each dot: lane -> (row, slot)
+                    for (int e = lane; e < kTileRows * kTileSlots; e += 32) {
+                        const int r = e / kTileSlots;
+                        const int slot = e - r * kTileSlots;
+                        const bool norm = slot == 32;
+                        const bool recon = slot >= 16 && !norm;
+                        const int c = norm ? 0 : (recon ? slot - 16 : slot);
+                        if (r >= nrows || (!norm && (c >= R || (recon && !final_stage)))) continue;
+                        const float* l = (recon ? V : U) + r * ldu;
+                        const float* rgt = norm ? U + r * ldu : basis + c * ldb;
+                        float total = res[e];
+                        for (int idx = full * kLanes; idx < D; ++idx)
+                            total = __fadd_rn(total, __fmul_rn(l[idx], rgt[idx]));
+                        res[e] = total;
+                    }
+                    __syncwarp();
+                }
+                // membership score of each row, components in order
+                if (lane < nrows && membership_on) {
+                    const float* rr = res + lane * kTileSlots;
+                    float distance = 0.0f, projected = 0.0f;
+                    for (int ck = 0; ck < R; ++ck) {
+                        const float mk = rr[ck];
                         const float proj2 = __fmul_rn(mk, mk);
                         distance = __fadd_rn(distance, __fdiv_rn(proj2, denom[ck]));
                         projected = __fadd_rn(projected, proj2);
                     }
-                    if (lane == 0) proj[ck] = rk;
+                    const float resid = __fsub_rn(rr[32], projected);
+                    distance = __fadd_rn(distance, __fdiv_rn(resid > 0.0f ? resid : 0.0f, mem2));
+                    scores[t0 + lane] = __fdiv_rn(__fsub_rn(distance, static_cast<float>(D)), score_scale);
                 }
-            }
-            if (membership_on) {
-                const float res = __fsub_rn(norm2, projected);
-                distance = __fadd_rn(distance, __fdiv_rn(res > 0.0f ? res : 0.0f, mem2));
-                const float score = __fdiv_rn(__fsub_rn(distance, static_cast<float>(D)), score_scale);
-                if (lane == 0) scores[i] = score;
-            }
-            __syncwarp();
-            // reconstruction (project_bayes_estimate), components in order,
-            // accumulated in registers over blocks of 32 * kRecCols columns
-            float* out = L.filtered + static_cast<size_t>(r0 + i) * L.row_dim + mc * D;
-            for (int base = 0; base < D; base += 32 * kRecCols) {
-                float o[kRecCols];
+                // reconstruction (project_bayes_estimate) of the tile's rows,
+                // components in order, in registers over blocks of 32 * kRecCols
+                const int proj_slot = final_stage ? 16 : 0;
+                for (int base = 0; base < D; base += 32 * kRecCols) {
+                    float o[kTileRows][kRecCols];
 #pragma unroll
-                for (int j = 0; j < kRecCols; ++j) o[j] = 0.0f;
-                for (int c = 0; c < R; ++c) {
-                    if (coef[c] == 0.0f) continue;
-                    const float scaled = __fmul_rn(coef[c], proj[c]);
-                    const float* bc = basis + c * ldb;
+                    for (int r = 0; r < kTileRows; ++r)
+#pragma unroll
+                        for (int jj = 0; jj < kRecCols; ++jj) o[r][jj] = 0.0f;
+                    for (int c = 0; c < R; ++c) {
+                        const float cf = coef[c];
+                        if (cf == 0.0f) continue;
+                        const float sc0 = __fmul_rn(cf, res[proj_slot + c]);
+                        const float sc1 = __fmul_rn(cf, res[kTileSlots + proj_slot + c]);
+                        const float* bc = basis + c * ldb;
+#pragma unroll
+                        for (int jj = 0; jj < kRecCols; ++jj) {
+                            const int col = base + lane + 32 * jj;
+                            if (col < D) {
+                                const float bv = bc[col];
+                                o[0][jj] = add_scaled_elem(o[0][jj], bv, sc0, col, D);
+                                o[1][jj] = add_scaled_elem(o[1][jj], bv, sc1, col, D);
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < kTileRows; ++r) {
+                        if (r >= nrows) break;
+                        float* out = L.filtered + static_cast<size_t>(r0 + t0 + r) * L.row_dim + mc * D;
+#pragma unroll
+                        for (int jj = 0; jj < kRecCols; ++jj) {
+                            const int col = base + lane + 32 * jj;
+                            if (col < D) out[col] = __fadd_rn(o[r][jj], center_vec[col]);
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        } else {
+            // per row: membership score and reconstruction.  In the Basic stage the
+            // membership row and the reconstruction row are the same centred noisy
+            // row, so its projections serve both.
+            float* u = scratch + warp * (2 * ldb + R + 1);  // centred membership row
+            float* v = u + ldb;                             // centred noisy row (Final)
+            float* proj = v + ldb;                          // projections for the reconstruction
+            const int j8 = lane & 7;
+            const int oct = lane >> 3;
+            const float score_scale = __fsqrt_rn(__fmul_rn(2.0f, static_cast<float>(D)));
+            for (int i = warp; i < S; i += kApplyWarps) {
+                const size_t b = bases[i];
+                for (int col = lane; col < D; col += 32) {
+                    const float xn = __ldg(L.noisy + b + coloff[col]);
+                    if (final_stage) {
+                        u[col] = __fsub_rn(__ldg(L.basic + b + coloff[col]), member_mean[col]);
+                        v[col] = __fsub_rn(xn, center_vec[col]);
+                    } else {
+                        u[col] = __fsub_rn(xn, member_mean[col]);
+                    }
+                }
+                __syncwarp();
+                float distance = 0.0f, projected = 0.0f, norm2 = 0.0f;
+                // pass over c0 = -1 (norm), 0, 4, ...: octet k computes component c0 + k
+                for (int c0 = membership_on ? -1 : 0; c0 < R; c0 += 4) {
+                    const int c = min(c0 + oct, R - 1);
+                    const float dm = (membership_on || !final_stage) ? octet_dot8(u, c < 0 ? u : basis + c * ldb, D, j8)
+                                                                     : 0.0f;
+                    const float dr = final_stage ? octet_dot8(v, basis + max(c, 0) * ldb, D, j8) : dm;
+                    for (int k = 0; k < 4; ++k) {
+                        const int ck = c0 + k;
+                        const float mk = __shfl_sync(0xffffffffu, dm, k * 8);
+                        const float rk = __shfl_sync(0xffffffffu, dr, k * 8);
+                        if (ck >= R) break;
+                        if (ck < 0) {
+                            norm2 = mk;
+                            continue;
+                        }
+                        if (membership_on) {
+                            const float proj2 = __fmul_rn(mk, mk);
+                            distance = __fadd_rn(distance, __fdiv_rn(proj2, denom[ck]));
+                            projected = __fadd_rn(projected, proj2);
+                        }
+                        if (lane == 0) proj[ck] = rk;
+                    }
+                }
+                if (membership_on) {
+                    const float res = __fsub_rn(norm2, projected);
+                    distance = __fadd_rn(distance, __fdiv_rn(res > 0.0f ? res : 0.0f, mem2));
+                    const float score = __fdiv_rn(__fsub_rn(distance, static_cast<float>(D)), score_scale);
+                    if (lane == 0) scores[i] = score;
+                }
+                __syncwarp();
+                // reconstruction (project_bayes_estimate), components in order,
+                // accumulated in registers over blocks of 32 * kRecCols columns
+                float* out = L.filtered + static_cast<size_t>(r0 + i) * L.row_dim + mc * D;
+                for (int base = 0; base < D; base += 32 * kRecCols) {
+                    float o[kRecCols];
+#pragma unroll
+                    for (int j = 0; j < kRecCols; ++j) o[j] = 0.0f;
+                    for (int c = 0; c < R; ++c) {
+                        if (coef[c] == 0.0f) continue;
+                        const float scaled = __fmul_rn(coef[c], proj[c]);
+                        const float* bc = basis + c * ldb;
+#pragma unroll
+                        for (int j = 0; j < kRecCols; ++j) {
+                            const int col = base + lane + 32 * j;
+                            if (col < D) o[j] = add_scaled_elem(o[j], bc[col], scaled, col, D);
+                        }
+                    }
 #pragma unroll
                     for (int j = 0; j < kRecCols; ++j) {
                         const int col = base + lane + 32 * j;
-                        if (col < D) o[j] = add_scaled_elem(o[j], bc[col], scaled, col, D);
+                        if (col < D) out[col] = __fadd_rn(o[j], center_vec[col]);
                     }
                 }
-#pragma unroll
-                for (int j = 0; j < kRecCols; ++j) {
-                    const int col = base + lane + 32 * j;
-                    if (col < D) out[col] = __fadd_rn(o[j], center_vec[col]);
-                }
+                __syncwarp();
             }
-            __syncwarp();
         }
         __syncthreads();
         // aggregation weights (accumulate_aggregation_model + finalize)
@@ -1242,13 +1434,17 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
                                      : launch_apply_warp<256>(L, max_groups, stream);
         if (err != cudaSuccess) return err;
     } else {
-        const ApplyLayout lay = apply_layout(D, Bmax, R, L.max_rows, kApplyWarps);
+        // tiled rows for rank <= kTileComps above dimension 16 (the special
+        // 8- and 16-element dot orders stay with the row-per-warp loop)
+        const bool tiled = R >= 1 && R <= kTileComps && D > 16;
+        const ApplyLayout lay = apply_layout(D, Bmax, R, L.max_rows, kApplyWarps, tiled, L.stage == 1);
         const size_t smem = lay.bytes;
-        cudaError_t err = cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        auto kernel = tiled ? apply_kernel<true> : apply_kernel<false>;
+        cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                static_cast<int>(smem));
         if (err != cudaSuccess) return err;
         const int ctas = std::min(max_groups, 148 * 8);
-        apply_kernel<<<ctas, kApplyThreads, smem, stream>>>(L);
+        kernel<<<ctas, kApplyThreads, smem, stream>>>(L);
         if ((err = cudaGetLastError()) != cudaSuccess) return err;
     }
     if (L.models > 1) {

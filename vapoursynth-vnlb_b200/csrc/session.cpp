@@ -207,7 +207,10 @@ struct Session {
         DeviceArray<float> filtered, weights, gmeans, gram, eig, dual, logw;
         DeviceArray<float> approx;  // tensor-core form: approximate distances [G][approx_stride]
     };
-    static constexpr int kMaxLanes = 4;
+#ifndef VNLB_MAX_LANES
+#define VNLB_MAX_LANES 4  // a build parameter for comparisons
+#endif
+    static constexpr int kMaxLanes = VNLB_MAX_LANES;
     Lane lanes[kMaxLanes];
     int lane_count = kMaxLanes;        // lanes in use (allocated): 1..kMaxLanes
     int next_lane = 0;
