@@ -25,7 +25,7 @@ constexpr int kMaxGridRows = 64;  // grid rows per collection round
 
 struct Entry {
     int r;     // global row
-    int xyt;   // x | y << 14 | t << 28
+    int xyt;   // x | y << 14 | layer (tile_kernel) or slot (tile_slots_kernel) << 28
     float w;   // row weight
 };
 
@@ -155,13 +155,15 @@ __global__ void __launch_bounds__(kTileThreads) tile_kernel(TileLaunch L) {
     }
 }
 
-// patch_time 1: a covering row lands in exactly one slot (its frame offset
-// from the anchor frame), so one CTA per tile scans the candidate rows once
-// for all slots (at most kMaxTileSlots) and keeps one accumulator set per
-// slot.  Each (pixel, slot) still sees its rows in increasing global row
-// order: the same sums as tile_kernel.
+// All slots in one scan: a covering row's temporal layer t lands in slot
+// s0 + t, s0 its frame's offset in the window, so one CTA per tile scans the
+// candidate rows once for all slots (at most kMaxTileSlots) and keeps one
+// accumulator set per slot.  Each (pixel, slot) still sees its rows in
+// increasing global row order: the same sums as tile_kernel.  kLayers: the
+// patch spans more than one frame (patch_time > 1).
 constexpr int kMaxTileSlots = 4;
 
+template <bool kLayers>
 __global__ void __launch_bounds__(kTileThreads) tile_slots_kernel(TileLaunch L) {
     __shared__ Entry entries[kTileThreads];
     __shared__ int s_rbeg[kMaxGridRows];
@@ -223,11 +225,15 @@ __global__ void __launch_bounds__(kTileThreads) tile_slots_kernel(TileLaunch L) 
                 const int r = s_rbeg[lo] + (vrow - s_rpre[lo]);
                 const MatchRow m = L.row_info[r];
                 if (m.x <= tx0 + kTile - 1 && m.x + P - 1 >= tx0 && m.y <= ty0 + kTile - 1 && m.y + P - 1 >= ty0) {
+                    // slot of layer 0; with several layers it may lie before the
+                    // window (the temporal windows shift at the clip's ends)
+                    // while a later layer lands in it, so it is stored + 8
                     const int slot = m.frame + slot_base;
-                    if (slot >= 0 && slot < L.slots) {
+                    if (slot >= (kLayers ? 1 - L.Pt : 0) && slot < L.slots) {
                         hit = true;
                         en.r = r;
-                        en.xyt = m.x | (m.y << 14) | (slot << 28);
+                        en.xyt = static_cast<int>(static_cast<unsigned>(m.x) | (static_cast<unsigned>(m.y) << 14) |
+                                                  (static_cast<unsigned>(kLayers ? slot + 8 : slot) << 28));
                         en.w = L.weights[r];
                     }
                 }
@@ -248,36 +254,40 @@ __global__ void __launch_bounds__(kTileThreads) tile_slots_kernel(TileLaunch L) 
                 const unsigned dx = static_cast<unsigned>(px - (x.xyt & 0x3fff));
                 const unsigned dy = static_cast<unsigned>(py - ((x.xyt >> 14) & 0x3fff));
                 if (dx >= static_cast<unsigned>(P) || dy >= static_cast<unsigned>(P)) continue;
-                const int slot = x.xyt >> 28;
-                const int pos = static_cast<int>(dy) * P + static_cast<int>(dx);
-                const float* f = L.filtered + static_cast<size_t>(x.r) * L.dim + pos;
-                float val[4];
+                const int slot0 = static_cast<int>(static_cast<unsigned>(x.xyt) >> 28) - (kLayers ? 8 : 0);
+                const int t_end = kLayers ? min(L.Pt, L.slots - slot0) : 1;
+                for (int t = kLayers ? max(0, -slot0) : 0; t < t_end; ++t) {
+                    const int slot = slot0 + t;
+                    const int pos = (t * P + static_cast<int>(dy)) * P + static_cast<int>(dx);
+                    const float* f = L.filtered + static_cast<size_t>(x.r) * L.dim + pos;
+                    float val[4];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) val[c] = c < C ? __ldg(f + c * L.patch_dim) : 0.0f;
-                if (L.coupled && !L.windowed) {
-                    const bool fused = static_cast<int>(dx) < fused_cols;
+                    for (int c = 0; c < 4; ++c) val[c] = c < C ? __ldg(f + c * L.patch_dim) : 0.0f;
+                    if (L.coupled && !L.windowed) {
+                        const bool fused = static_cast<int>(dx) < fused_cols;
 #pragma unroll
-                    for (int s = 0; s < kMaxTileSlots; ++s) {
-                        if (s != slot) continue;
+                        for (int s = 0; s < kMaxTileSlots; ++s) {
+                            if (s != slot) continue;
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) {
-                            if (c >= C) break;
-                            num[s][c] = fused ? __fmaf_rn(x.w, val[c], num[s][c])
-                                              : __fadd_rn(num[s][c], __fmul_rn(x.w, val[c]));
+                            for (int c = 0; c < 4; ++c) {
+                                if (c >= C) break;
+                                num[s][c] = fused ? __fmaf_rn(x.w, val[c], num[s][c])
+                                                  : __fadd_rn(num[s][c], __fmul_rn(x.w, val[c]));
+                            }
+                            wt[s] = __fadd_rn(wt[s], x.w);
                         }
-                        wt[s] = __fadd_rn(wt[s], x.w);
-                    }
-                } else {
-                    const float cw = __fmul_rn(x.w, window[dy * P + dx]);
+                    } else {
+                        const float cw = __fmul_rn(x.w, window[dy * P + dx]);
 #pragma unroll
-                    for (int s = 0; s < kMaxTileSlots; ++s) {
-                        if (s != slot) continue;
+                        for (int s = 0; s < kMaxTileSlots; ++s) {
+                            if (s != slot) continue;
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) {
-                            if (c >= C) break;
-                            num[s][c] = __fadd_rn(num[s][c], __fmul_rn(cw, val[c]));
+                            for (int c = 0; c < 4; ++c) {
+                                if (c >= C) break;
+                                num[s][c] = __fadd_rn(num[s][c], __fmul_rn(cw, val[c]));
+                            }
+                            wt[s] = __fadd_rn(wt[s], cw);
                         }
-                        wt[s] = __fadd_rn(wt[s], cw);
                     }
                 }
             }
@@ -361,8 +371,9 @@ cudaError_t launch_aggregate_stacks(const AggregateLaunch& L, cudaStream_t strea
 cudaError_t launch_tiles(const TileLaunch& L, cudaStream_t stream) {
     if (L.channels > 4 || L.width >= (1 << 14) || L.height >= (1 << 14) || L.Pt > 7) return cudaErrorInvalidValue;
     const size_t smem = static_cast<size_t>(L.P) * L.P * sizeof(float);
-    if (L.Pt == 1 && L.slots <= kMaxTileSlots) {
-        tile_slots_kernel<<<dim3(L.tiles_x, L.tiles_y, 1), kTileThreads, smem, stream>>>(L);
+    if (L.slots <= kMaxTileSlots) {
+        if (L.Pt == 1) tile_slots_kernel<false><<<dim3(L.tiles_x, L.tiles_y, 1), kTileThreads, smem, stream>>>(L);
+        else tile_slots_kernel<true><<<dim3(L.tiles_x, L.tiles_y, 1), kTileThreads, smem, stream>>>(L);
     } else {
         const dim3 grid(L.tiles_x, L.tiles_y, L.slots);
         tile_kernel<<<grid, kTileThreads, smem, stream>>>(L);

@@ -250,10 +250,17 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
             continue;
         }
         // model rows, means over the first B rows (compute_mean), centring
-        for (int e = t; e < B * D; e += kT) {
-            const int s2 = e / D;
-            const int col = e - s2 * D;
-            X[s2 * ldx + col] = __ldg(model_video + bases[s2] + cb + coloff[col]);
+        if constexpr (W == 1) {
+            for (int s2 = 0; s2 < B; ++s2) {
+                const size_t b = bases[s2];
+                for (int col = lane; col < D; col += 32) X[s2 * ldx + col] = __ldg(model_video + b + cb + coloff[col]);
+            }
+        } else {
+            for (int e = t; e < B * D; e += kT) {
+                const int s2 = e / D;
+                const int col = e - s2 * D;
+                X[s2 * ldx + col] = __ldg(model_video + bases[s2] + cb + coloff[col]);
+            }
         }
         group_sync();
         const float inv_b = __fdiv_rn(1.0f, static_cast<float>(B));
