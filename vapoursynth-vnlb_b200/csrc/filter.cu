@@ -1434,7 +1434,10 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
         if ((err = cudaGetLastError()) != cudaSuccess) return err;
     }
     // apply
-    if (R <= 8 && Bmax <= 8 && L.nmax == Bmax && (D == 64 || D == 128 || D == 192 || D == 256)) {
+#ifndef VNLB_APPLY_WARP
+#define VNLB_APPLY_WARP 1  // the warp-per-group apply for its shapes; a build parameter for comparisons
+#endif
+    if (VNLB_APPLY_WARP && R <= 8 && Bmax <= 8 && L.nmax == Bmax && (D == 64 || D == 128 || D == 192 || D == 256)) {
         cudaError_t err = D == 64    ? launch_apply_warp<64>(L, max_groups, stream)
                           : D == 128 ? launch_apply_warp<128>(L, max_groups, stream)
                           : D == 192 ? launch_apply_warp<192>(L, max_groups, stream)
