@@ -383,7 +383,13 @@ def roofline_of(r, steps, which=None):
     return {"kernel": "group filter (prepare + Jacobi + apply)", "bound": "fp32",
             "achieved": flops / (ms / 1e3) / 1e12, "peak": 2 * FP32_LANE_OPS / 1e12, "unit": "TFLOP/s",
             "frac": flops / (ms / 1e3) / (2 * FP32_LANE_OPS),
-            "peak_source": "nominal FP32 FMA rate x 2", "ms_per_launch": ms / max(1, launches), "traffic": None}
+            "peak_source": "nominal FP32 FMA rate x 2", "ms_per_launch": ms / max(1, launches),
+            # dram__bytes_read.sum + dram__bytes_write.sum of prepare + Jacobi + apply for one
+            # anchor frame (mean of Basic 412.8 MB and Final 596.2 MB),
+            # profiles/kernels_1080p_yuv444_one_anchor_frame.md; about 180 GB/s over the
+            # event-timed filter, so the class is bound by latency, not by HBM
+            "traffic": 504.5e6 if PARAMS == "cpu" else None,
+            "traffic_unit": "bytes per anchor frame (ncu, one capture)"}
 
 
 def measured_peak(key: str, fallback: float) -> float:
