@@ -102,6 +102,8 @@ FLOW_CASES = [
     ("yuv_fw_pel4_overlap0", 40, 32, 5, 3, 20.0, 22, dict(radius=2, block_step=4, bm_range=4), (16, 0, 4, 9),
      None),
     ("gray_bw_pel1_far", 48, 40, 5, 1, 15.0, 23, dict(radius=1, bm_range=3, block_step=4), None, (8, 2, 1, 12)),
+    ("yuv_fw_bw_patch_time2", 40, 32, 5, 3, 20.0, 24,
+     dict(radius=1, block_size=7, patch_time=2, block_step=3, bm_range=4), (8, 4, 2, 3), (8, 4, 2, 3)),
 ]
 
 

@@ -175,11 +175,11 @@ def gpu_chain(case):
     noisy, fw, bw = M.flow_case(*case)
     flow = dict(mvfw=M.props(fw, w, h) if fw else None, mvbw=M.props(bw, w, h) if bw else None,
                 clip_props=M.clip_props(fw, bw, f))
-    radius = kw.get("radius", 1)
+    layout = dict(radius=kw.get("radius", 1), patch_time=kw.get("patch_time", 1))  # the stacks' slots
     stacks = vnlb.Basic(noisy, sigma=sigma, **kw, **flow)
-    basic = vnlb.Aggregate(stacks, src=noisy, radius=radius)
+    basic = vnlb.Aggregate(stacks, src=noisy, **layout)
     stacks = vnlb.Final(noisy, ref=basic, sigma=sigma, **kw, **flow)
-    return basic, vnlb.Aggregate(stacks, src=noisy, radius=radius)
+    return basic, vnlb.Aggregate(stacks, src=noisy, **layout)
 
 
 @pytest.mark.gpu
