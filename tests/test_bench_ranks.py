@@ -65,3 +65,27 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
 
     assert bench.run_reference(Args()) == 0
     assert capsys.readouterr().out == ""
+
+
+def test_parameter_sets_of_the_bench(monkeypatch):
+    """The headline passes the CPU core's defaults explicitly; --params vnlbcu
+    takes vnlbcu's own (block 7, automatic step 3, group 16, bm_range 13,
+    patch_time 2, rank 15; cuda_plugin.cpp:380-403) for both stages."""
+    import vnlbgpu_lib as lib
+
+    monkeypatch.setattr(bench, "PARAMS", "cpu")
+    b = bench.stage_params(lib.STAGE_BASIC)
+    assert (b.patch_size, b.proc_step, b.similar, b.search_window, b.patch_time, b.rank) == (8, 8, 8, 19, 1, 8)
+    monkeypatch.setattr(bench, "PARAMS", "vnlbcu")
+    for stage in (lib.STAGE_BASIC, lib.STAGE_FINAL):
+        p = bench.stage_params(stage)
+        assert (p.patch_size, p.proc_step, p.similar, p.search_window, p.patch_time, p.rank) == (7, 3, 16, 27, 2, 15)
+    assert bench.workload_config("plain")["params"]["block_size"] == 7
+
+
+def test_reference_arm_refuses_the_vnlbcu_parameter_set(monkeypatch, capsys):
+    monkeypatch.setattr(bench, "PARAMS", "vnlbcu")
+    monkeypatch.delenv("RANK", raising=False)
+    assert bench.run_reference(None) == 0
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and "unavailable" in line
