@@ -106,7 +106,7 @@ typedef struct vnlbgpu_stats {
     long long active_groups;   /* groups filtered (after the paste mask) */
     long long rows;            /* retained rows filtered and aggregated */
     long long kernel_launches; /* kernels this session launched */
-    long long pipeline_lanes;  /* anchor frames the session keeps in flight (1-4, fewer
+    long long pipeline_lanes;  /* anchor frames the session keeps in flight (1-8, fewer
                                   when their group buffers would exceed half of the free
                                   device memory at create time) */
 } vnlbgpu_stats;

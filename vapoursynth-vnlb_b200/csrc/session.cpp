@@ -193,8 +193,8 @@ struct Session {
     // Pipeline lanes: consecutive anchor frames go round the lanes, each lane
     // with its own stream and scratch, so that one anchor frame's serial
     // paste-mask walk and latency-bound kernels overlap the others' kernels
-    // (1080p YUV444 Basic+Final: 220 fps with 2 lanes, 225 with 3, 231 with 4,
-    // no further gain for the plain form with 6 or 8).  A session takes fewer
+    // (1080p YUV444 Basic+Final, plain / tensor-core matcher: 220 / 224 fps
+    // with 2 lanes, 231 / 237 with 4, 232 / 239 with 8).  A session takes fewer
     // lanes when their group buffers would take more than half of the free
     // device memory, so that a Basic session leaves room for its Final.
     struct Lane {
@@ -208,7 +208,7 @@ struct Session {
         DeviceArray<float> approx;  // tensor-core form: approximate distances [G][approx_stride]
     };
 #ifndef VNLB_MAX_LANES
-#define VNLB_MAX_LANES 4  // a build parameter for comparisons
+#define VNLB_MAX_LANES 8  // a build parameter for comparisons
 #endif
     static constexpr int kMaxLanes = VNLB_MAX_LANES;
     Lane lanes[kMaxLanes];
