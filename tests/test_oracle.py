@@ -46,6 +46,10 @@ def test_port_equals_reference_golden(golden):
     (1, dict(block_size=4, patch_time=2, bm_range=3, radius=6, group_size=40, rank=16, beta=3.0, block_step=2)),
     (3, dict(cap_factor=0.0, tau=900.0)),
     (3, dict(weight_alpha=0.0, weight_beta=0.0, weight_gamma=0.0)),
+    (3, dict(chroma=0, block_size=7, patch_time=2, block_step=3, bm_range=4, group_size=16, rank=8)),
+    (1, dict(block_size=10, patch_time=2, block_step=5, bm_range=4, group_size=16, rank=15)),
+    (1, dict(patch_time=2, radius=2, block_step=4, bm_range=4, group_size=16, rank=16, tau=400.0)),
+    (3, dict(model_cap_factor=2.0, cap_factor=4.0, tau=600.0, group_size=8, rank=8)),
 ])
 def test_port_equals_reference_build(planes, kw):
     _, noisy = synth.make_clip(56, 40, 4, planes, 18.0, seed=21)
