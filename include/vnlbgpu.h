@@ -163,8 +163,13 @@ int vnlbgpu_aggregate(const float* stacks, const float* source, int width, int h
  * <= 32 MiB.  A larger frame is rejected with an error.  The first call on a
  * device sets up that device's scratch address; make it before any stream
  * capture begins.  Calls on one device are serialised inside, because calls
- * whose GPU work overlapped would race on the one scratch.  Returns when the
- * output is on the host.  Results equal vnlbgpu_aggregate's bit for bit. */
+ * whose GPU work overlapped would race on the one scratch; an error return
+ * comes only after the call's queued work has drained.  Every call queues its
+ * copies and kernel on the legacy default stream, so it waits for the
+ * caller's blocking streams on that device and must not run while one of them
+ * is being captured.  device_id is current during the call; the caller's
+ * current device is put back before it returns.  Returns when the output is
+ * on the host.  Results equal vnlbgpu_aggregate's bit for bit. */
 int vnlbgpu_aggregate_frame_noalloc(const float* stacks, const float* source, int width, int height, int frames,
                                     int channels, int search_bwd, int search_fwd, int patch_time, int device_id, int n,
                                     float* out);

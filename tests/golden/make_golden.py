@@ -28,6 +28,7 @@ flow_outputs.npz
 from __future__ import annotations
 
 import json
+import os
 import sys
 import tomllib
 from pathlib import Path
@@ -43,7 +44,7 @@ import oracle as O  # noqa: E402
 import mvtools_blobs as M  # noqa: E402
 import synth  # noqa: E402
 
-REFERENCE = Path("/root/reference")
+REFERENCE = Path(os.environ.get("VNLB_REFERENCE", "/root/reference"))
 OUT = Path(__file__).resolve().parent
 
 # (name, width, height, frames, planes, sigma, seed, shared kwargs, basic extra, final extra)

@@ -56,3 +56,13 @@ def test_rejects_a_row_larger_than_the_scratch():
         lib.aggregate_frame_noalloc(stacks, source, 0, 0, 0, 1)
     with pytest.raises(lib.VNLBError, match="outside the clip"):
         lib.aggregate_frame_noalloc(stacks[:, :, :, :16], source[:, :, :, :16], 1, 0, 0, 1)
+
+
+def test_rejects_a_device_or_slot_count_outside_its_limits():
+    stacks = np.zeros((1, 1, 2, 16), np.float32)
+    source = np.zeros((1, 1, 1, 16), np.float32)
+    with pytest.raises(lib.VNLBError, match="outside the 64 devices"):
+        lib.aggregate_frame_noalloc(stacks, source, 0, 0, 0, 1, device_id=64)
+    # search_bwd + search_fwd + patch_time = 33 slots
+    with pytest.raises(lib.VNLBError, match="at most 32 contribution slots"):
+        lib.aggregate_frame_noalloc(stacks, source, 0, 16, 16, 1)

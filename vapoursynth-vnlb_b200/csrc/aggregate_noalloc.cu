@@ -24,7 +24,16 @@
 //
 // Races: there is one scratch per device.  Calls whose GPU work overlapped
 // would race on it.  This file prevents that by holding a per-device host
-// lock from the set-up until the call's stream work has finished.
+// lock from the set-up until the call's stream work has finished, on the
+// error paths too: once a copy or the kernel has been queued, an error return
+// first drains the stream.
+//
+// Stream: every call queues its copies and kernel on the legacy default
+// stream.  So a call waits for the caller's blocking streams on that device,
+// and it must not run while one of them is being captured.
+//
+// Current device: the call makes device_id current while it runs and puts
+// back the caller's current device before it returns.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -62,6 +71,17 @@ const char* cuda_message(const char* what, cudaError_t status) {
                   cudaGetErrorString(status));
     return g_noalloc_message;
 }
+
+// Puts back the calling thread's current device on every return path.
+struct DeviceRestore {
+    int previous = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
+    }
+    ~DeviceRestore() {
+        if (previous >= 0) cudaSetDevice(previous);
+    }
+};
 
 struct BandLaunch {
     int width, rows, channels, count;
@@ -119,6 +139,7 @@ const char* aggregate_frame_noalloc(const float* stacks, const float* source, in
     const int band_rows = static_cast<int>(std::min<size_t>(height, kNoAllocScratchFloats / row_floats));
 
     std::lock_guard<std::mutex> guard(g_noalloc_lock[device_id]);
+    DeviceRestore restore;  // destroyed before the lock is released
     cudaError_t status = cudaSetDevice(device_id);
     if (status != cudaSuccess) return cuda_message("cudaSetDevice", status);
     if (!g_noalloc_ptr[device_id]) {
@@ -129,6 +150,12 @@ const char* aggregate_frame_noalloc(const float* stacks, const float* source, in
     }
     float* scratch = g_noalloc_ptr[device_id];
     const cudaStream_t stream = nullptr;  // legacy default stream, as the whole-clip aggregate uses
+    // An error after work was queued: wait for that work before the lock is
+    // released, so that no later call overwrites a scratch still in use.
+    auto drained = [stream](const char* what, cudaError_t error) {
+        cudaStreamSynchronize(stream);
+        return cuda_message(what, error);
+    };
 
     const size_t plane = static_cast<size_t>(width) * height;
     const size_t stack_values = plane * channels * slots * 2;
@@ -147,9 +174,9 @@ const char* aggregate_frame_noalloc(const float* stacks, const float* source, in
                 const float* weight_rows = num_rows + plane;
                 float* dst = scratch + (static_cast<size_t>(k) * channels + c) * 2 * band;
                 status = cudaMemcpyAsync(dst, num_rows, bytes, cudaMemcpyHostToDevice, stream);
-                if (status != cudaSuccess) return cuda_message("cudaMemcpyAsync(stack band)", status);
+                if (status != cudaSuccess) return drained("cudaMemcpyAsync(stack band)", status);
                 status = cudaMemcpyAsync(dst + band, weight_rows, bytes, cudaMemcpyHostToDevice, stream);
-                if (status != cudaSuccess) return cuda_message("cudaMemcpyAsync(stack band)", status);
+                if (status != cudaSuccess) return drained("cudaMemcpyAsync(stack band)", status);
             }
         }
         float* src_band = scratch + static_cast<size_t>(count) * channels * 2 * band;
@@ -158,18 +185,18 @@ const char* aggregate_frame_noalloc(const float* stacks, const float* source, in
             const float* src = source + plane * channels * n + static_cast<size_t>(c) * plane +
                                static_cast<size_t>(y0) * width;
             status = cudaMemcpyAsync(src_band + c * band, src, bytes, cudaMemcpyHostToDevice, stream);
-            if (status != cudaSuccess) return cuda_message("cudaMemcpyAsync(source band)", status);
+            if (status != cudaSuccess) return drained("cudaMemcpyAsync(source band)", status);
         }
         BandLaunch L{width, rows, channels, count, scratch};
         const size_t total = band * channels;
         const int blocks = static_cast<int>(std::min<size_t>((total + 255) / 256, 148 * 16));
         aggregate_band_kernel<<<blocks, 256, 0, stream>>>(L);
         status = cudaGetLastError();
-        if (status != cudaSuccess) return cuda_message("aggregate band kernel launch", status);
+        if (status != cudaSuccess) return drained("aggregate band kernel launch", status);
         for (int c = 0; c < channels; ++c) {
             float* dst = out + static_cast<size_t>(c) * plane + static_cast<size_t>(y0) * width;
             status = cudaMemcpyAsync(dst, out_band + c * band, bytes, cudaMemcpyDeviceToHost, stream);
-            if (status != cudaSuccess) return cuda_message("cudaMemcpyAsync(output band)", status);
+            if (status != cudaSuccess) return drained("cudaMemcpyAsync(output band)", status);
         }
     }
     // the output is on the host, and the scratch free for the next call, once
