@@ -25,7 +25,12 @@ no collective on the data path); rank 0 prints one JSON line.  `value` is
 measured with the clip already resident in HBM; `e2e` goes through the C ABI
 with pinned host buffers, the plugin's copies inside the timed region (clip
 up for Basic and for Final -- Final's copy issued first, it does not depend on
-Basic -- Basic frames down, Basic frames up for Final, Final frames down).  `--impl reference` times the reference CPU implementation
+Basic -- Basic frames down, Basic frames up for Final, Final frames down).
+`config.e2e_frame_path` is the same metric through the per-frame plugin path
+(vnlbgpu_render_frame_window from eight frame threads per stage, pageable
+host frames, a long clip through bounded source stores).  The roofline is
+taken from one more step with one pipeline lane per session, so that each
+timed launch runs alone.  `--impl reference` times the reference CPU implementation
 (oracle/_ref, the reference's own sources; the C restatement if that build is
 absent) on a bounded sample of the same workload on the host cores.
 """
@@ -326,72 +331,248 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
     torch.cuda.synchronize()
     e2e_value = whole_job_rate(ranks.world, FRAMES, e2e_steps, ranks.max(e0.elapsed_time(e1)))
     same = bool(torch.equal(h_final, d_final.cpu()))
+
+    # One more device-resident step with one pipeline lane per session: the
+    # anchor frames' kernels then run one after another, so each launch's
+    # event-timed duration is that of the kernel alone (the roofline's
+    # denominator); the timed steps above overlap up to eight lanes.
+    for s in (sb, sf):
+        s.set_lanes(1)
+    step()
+    torch.cuda.synchronize()
+    sb.kernel_timing(True)
+    sf.kernel_timing(True)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    step()
+    s1.record(stream)
+    torch.cuda.synchronize()
+    kb1, kf1 = sb.kernel_timing(False), sf.kernel_timing(False)
+    stats2 = [sb.stats(), sf.stats()]
+    serial_stats = {k: sum(stats2[i][k] - stats1[i][k] for i in range(2)) for k in stats0[0]}
+    for s in (sb, sf):
+        s.set_lanes(0)
     sb.close()
     sf.close()
     kernels = {k: (kb[k][0] + kf[k][0], kb[k][1] + kf[k][1]) for k in kb}
+    serial = {"kernels": {k: (kb1[k][0] + kf1[k][0], kb1[k][1] + kf1[k][1]) for k in kb1},
+              "ms_per_step": s0.elapsed_time(s1), "stats": serial_stats}
     return {"form": form, "value": value, "max_ms": max_ms, "e2e": e2e_value, "same": same, "psnr": psnr,
-            "kernels": kernels, "stats": delta, "lanes": lanes, "clocks": clocks.summary(), "bp": bp, "outputs": (basic_out, final_out)}
+            "kernels": kernels, "stats": delta, "lanes": lanes, "clocks": clocks.summary(), "bp": bp,
+            "serial": serial, "outputs": (basic_out, final_out)}
+
+
+def measure_frame_path(form, args, ranks, noisy, local, threads=8):
+    """End to end through the per-frame drop-in path, as a VapourSynth script
+    runs vnlbcu.Basic into vnlbcu.Final: `threads` frame threads per stage
+    call vnlbgpu_render_frame_window with pageable host frames (one array per
+    plane) and pageable outputs.  The clip is the workload's 16 frames played
+    back and forth, (warmup + steps) * 16 frames per rank, so that every step
+    is 16 new output frames of a long clip (the sessions' source stores and
+    stack caches are bounded; frames already on the device are not copied
+    again).  Under torchrun the ranks split this one clip by
+    vnlbgpu_shard_plan: each renders its block of Final frames, the Basic
+    frames they read and nothing else, with no exchange between ranks.  A
+    Final frame starts once the Basic frames of its source window are out.
+
+    Two phases on the same sessions: the first warmup * 16 Final frames (and
+    the Basic frames they read), untimed; then the timed phase, every
+    remaining Basic and Final frame, from a synchronised start with all
+    threads idle to the last Final frame on the host: wall time, max over
+    ranks.  The timed phase therefore holds all the work of its frames,
+    including the ramp at its start."""
+    import torch
+    import vnlbgpu_lib as lib
+
+    warm = max(1, args.warmup)
+    per_rank = FRAMES * (warm + args.steps)
+    total = per_rank * ranks.world
+    frames = [[noisy[(f % FRAMES) if (f // FRAMES) % 2 == 0 else FRAMES - 1 - f % FRAMES][c] for c in range(PLANES)]
+              for f in range(FRAMES * 2)]
+
+    def src(f):
+        return frames[f % (2 * FRAMES)]
+
+    bp, fp = stage_params(lib.STAGE_BASIC, form), stage_params(lib.STAGE_FINAL, form)
+    for p in (bp, fp):
+        p.device_id = local
+        p.num_streams = threads
+    plan = lib.shard_plan(total, ranks.world, ranks.rank, (bp.search_bwd, bp.search_fwd, bp.patch_time),
+                          (fp.search_bwd, fp.search_fwd, fp.patch_time))
+    (o0, o1), (b0, b1) = plan["out"], plan["basic"]
+    sb = lib.Session(bp, WIDTH, HEIGHT, total, PLANES)
+    sf = lib.Session(fp, WIDTH, HEIGHT, total, PLANES)
+    ring = 48  # Basic outputs kept for Final; Basic runs at most ring - 16 frames ahead
+    basic_out = [np.empty((PLANES, HEIGHT, WIDTH), np.float32) for _ in range(ring)]
+    final_out = [np.empty((PLANES, HEIGHT, WIDTH), np.float32) for _ in range(threads)]
+    cond = threading.Condition()
+    basic_done = set()
+    state = {"final_done": o0}  # Final frames below this index are all out
+
+    def run_phase(f_first, f_last):
+        """Final frames f_first..f_last and the Basic frames they read that
+        are not out yet."""
+        need0 = sf.required_source_range(f_first)[0]
+        need1 = sf.required_source_range(f_last)[1]
+        todo_b = [m for m in range(max(b0, need0), min(b1, need1) + 1) if m not in basic_done]
+        st = {"b": 0, "f": f_first, "error": None, "finished": set()}
+
+        def basic_worker():
+            try:
+                while True:
+                    with cond:
+                        if st["b"] >= len(todo_b) or st["error"]:
+                            return
+                        n = todo_b[st["b"]]
+                        st["b"] += 1
+                        while n - state["final_done"] >= ring - 16 and not st["error"]:
+                            cond.wait()
+                    first, last = sb.required_source_range(n)
+                    sb.render_frame_window(n, [src(f) for f in range(first, last + 1)], first=first,
+                                           out=basic_out[n % ring])
+                    with cond:
+                        basic_done.add(n)
+                        cond.notify_all()
+            except Exception as e:  # noqa: BLE001 - re-raised below
+                with cond:
+                    st["error"] = e
+                    cond.notify_all()
+
+        def final_worker(slot):
+            try:
+                while True:
+                    with cond:
+                        n = st["f"]
+                        if n > f_last or st["error"]:
+                            return
+                        st["f"] += 1
+                    first, last = sf.required_source_range(n)
+                    with cond:
+                        while not all(f in basic_done for f in range(first, last + 1)) and not st["error"]:
+                            cond.wait()
+                    refs = [[basic_out[f % ring][c] for c in range(PLANES)] for f in range(first, last + 1)]
+                    sf.render_frame_window(n, [src(f) for f in range(first, last + 1)], refs, first=first,
+                                           out=final_out[slot])
+                    with cond:
+                        st["finished"].add(n)
+                        while state["final_done"] in st["finished"]:
+                            state["final_done"] += 1
+                        cond.notify_all()
+            except Exception as e:  # noqa: BLE001
+                with cond:
+                    st["error"] = e
+                    cond.notify_all()
+
+        pool = [threading.Thread(target=basic_worker) for _ in range(threads)]
+        pool += [threading.Thread(target=final_worker, args=(i,)) for i in range(threads)]
+        for t in pool:
+            t.start()
+        for t in pool:
+            t.join()
+        if st["error"]:
+            raise st["error"]
+        return len(todo_b)
+
+    warm_last = min(o1, o0 + FRAMES * warm - 1)
+    run_phase(o0, warm_last)
+    torch.cuda.synchronize()
+    ranks.barrier()
+    t0 = time.perf_counter()
+    basic_frames = run_phase(warm_last + 1, o1)
+    torch.cuda.synchronize()
+    seconds = ranks.max(time.perf_counter() - t0)
+    timed = o1 - warm_last
+    st_b, st_f = sb.stats(), sf.stats()
+    sb.close()
+    sf.close()
+    return {"value": ranks.world * timed / seconds,
+            "threads_per_stage": threads, "clip_frames": total, "timed_final_frames_per_rank": timed,
+            "timed_basic_frames_per_rank": basic_frames,
+            "shard": {"out": plan["out"], "basic": plan["basic"], "source": plan["source"]},
+            "source_slots": {"basic": st_b["source_slots"], "final": st_f["source_slots"]},
+            "anchor_frames": {"basic": st_b["anchor_frames"], "final": st_f["anchor_frames"]},
+            "source_uploads": {"basic": st_b["source_uploads"], "final": st_f["source_uploads"]},
+            "pipeline_lanes": {"basic": st_b["pipeline_lanes"], "final": st_f["pipeline_lanes"]}}
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of each
+# kernel class, from one ncu capture of the profile case at the workload's
+# frame size (python bench.py --profile-case: one Basic and one Final anchor
+# frame of a 3-frame 1920x1080 YUV444PS clip, CPU-default parameters), mean of
+# the Basic and Final launches; the filter class sums prepare, Jacobi and
+# apply.  None where no capture of the current kernels exists.
+TRAFFIC_PER_LAUNCH = {
+    ("cpu", "match/plain"): 59.3e6,
+    ("cpu", "filter"): 504.5e6,
+}
+TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none "
+                  "python bench.py --profile-case --form plain")
 
 
 def roofline_of(r, steps, which=None):
     """Roofline of the dominant kernel class of one measured form (or of the
-    class `which`)."""
-    kernels, st, bp = r["kernels"], r["stats"], r["bp"]
+    class `which`), from the one-lane step: algorithmic work per launch over
+    the mean event-timed duration of a launch running alone."""
+    serial = r["serial"]
+    kernels, st, bp = serial["kernels"], serial["stats"], r["bp"]
     dominant = which or max(("match", "filter"), key=lambda k: kernels[k][0])
-    window = bp.search_window
-    temporal = bp.search_bwd + bp.search_fwd + 1
+    ms, launches = kernels[dominant]
+    launches = max(1, launches)
+    ms_launch = ms / launches
+    anchor_frames = max(1, st["anchor_frames"])  # one match and one filter call per anchor frame and stage
+    groups_per_frame = st["groups"] / anchor_frames
+    window, temporal = bp.search_window, min(3, bp.search_bwd + bp.search_fwd + 1)
     dm_basic = bp.patch_size ** 2 * bp.patch_time
     dm_final = dm_basic * PLANES
-    groups_per_stage = st["groups"] / 2
-    ms, launches = kernels[dominant]
+    # per launch: a launch is one anchor frame of one stage; Basic and Final
+    # launches alternate, so a mean launch has the mean match dimension
+    dm_mean = 0.5 * (dm_basic + dm_final)
+    common = {"ms_per_launch": ms_launch, "launches": launches,
+              "timing": "CUDA events around each launch in a step with one pipeline lane per session (kernels "
+                        "serialised), mean over the launches of the step",
+              "serial_step_ms": serial["ms_per_step"]}
+    traffic = TRAFFIC_PER_LAUNCH.get((PARAMS, dominant if dominant == "filter" else "match/" + r["form"]))
+    if traffic is not None:
+        common.update(traffic=traffic, traffic_unit="DRAM bytes per launch (ncu, one capture of the profile case)",
+                      traffic_source=TRAFFIC_SOURCE)
+    else:
+        common.update(traffic=None)
     if dominant == "match" and r["form"] == "plain":
-        ops = 3.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
-        return {"kernel": "match (exact FP32 SSD + CPU-order selection)", "bound": "fp32",
-                "achieved": ops / (ms / 1e3) / 1e12, "peak": FP32_LANE_OPS / 1e12, "unit": "TFLOP/s",
-                "frac": ops / (ms / 1e3) / FP32_LANE_OPS,
-                "peak_source": "nominal FP32 lane-op rate 148 SM x 128 x 1.965 GHz (MEASURED_PEAKS.json has no "
-                               "FP32 figure)",
-                "work": "3 FP32 ops (sub, mul, add; no FMA, the CPU's order) per candidate element, "
-                        "G x W^2 x T x d_m per anchor frame",
-                "ms_per_launch": ms / max(1, launches),
-                # dram__bytes_read.sum + dram__bytes_write.sum of one match launch (mean of the
-                # Basic and Final launches), profiles/kernels_1080p_yuv444_one_anchor_frame.md
-                "traffic": 59.3e6 if PARAMS == "cpu" else None,
-                "traffic_unit": "bytes per launch (ncu, one capture)"}
+        ops = 3.0 * groups_per_frame * window * window * temporal * dm_mean
+        return dict(common, kernel="match (exact FP32 SSD + selection replay)", bound="fp32",
+                    achieved=ops / (ms_launch / 1e3) / 1e12, peak=FP32_LANE_OPS / 1e12, unit="TFLOP/s",
+                    frac=ops / (ms_launch / 1e3) / FP32_LANE_OPS,
+                    peak_source="nominal FP32 lane-op rate 148 SM x 128 x 1.965 GHz (MEASURED_PEAKS.json has no "
+                                "FP32 figure)",
+                    work="3 FP32 ops (sub, mul, add; no FMA, the CPU's order) per candidate element: G x W^2 x T x "
+                         "d_m per launch (one anchor frame of one stage)")
     if dominant == "match" and r["form"] == "chosen":
-        flops = 2.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
-        return {"kernel": "match, chosen form (FP32 dot-product distances + exact re-rank)", "bound": "fp32",
-                "achieved": flops / (ms / 1e3) / 1e12, "peak": 2 * FP32_LANE_OPS / 1e12, "unit": "TFLOP/s",
-                "frac": flops / (ms / 1e3) / (2 * FP32_LANE_OPS),
-                "peak_source": "nominal FP32 FMA rate x 2 (MEASURED_PEAKS.json has no FP32 figure)",
-                "work": "2 G C d_m (multiply-adds of all candidate dot products) per anchor frame",
-                "ms_per_launch": ms / max(1, launches), "traffic": None}
+        flops = 2.0 * groups_per_frame * window * window * temporal * dm_mean
+        return dict(common, kernel="match, chosen form (FP32 dot-product distances + exact re-rank)", bound="fp32",
+                    achieved=flops / (ms_launch / 1e3) / 1e12, peak=2 * FP32_LANE_OPS / 1e12, unit="TFLOP/s",
+                    frac=flops / (ms_launch / 1e3) / (2 * FP32_LANE_OPS),
+                    peak_source="nominal FP32 FMA rate x 2 (MEASURED_PEAKS.json has no FP32 figure)",
+                    work="2 G C d_m (multiply-adds of all candidate dot products) per launch")
     if dominant == "match":
-        flops = 2.0 * groups_per_stage * window * window * temporal * (dm_basic + dm_final)
-        # the matcher runs inside a long step: the sustained GEMM figure
-        peak = measured_peak("bf16_tflops_sustained", 1400.0)
-        return {"kernel": "match, chosen_tc form (tcgen05 BF16 distances into tensor memory, selection on them, "
-                          "exact FP32 re-rank)",
-                "bound": "tensor", "achieved": flops / (ms / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
-                "frac": flops / (ms / 1e3) / 1e12 / peak,
-                "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if peak != 1400.0
-                               else "fallback 1.4 PFLOP/s sustained (of fallback)",
-                "work": "2 G C d_m (algorithmic multiply-adds of all candidate distances) per anchor frame",
-                "ms_per_launch": ms / max(1, launches), "traffic": None}
+        flops = 2.0 * groups_per_frame * window * window * temporal * dm_mean
+        peak = measured_peak("bf16_tflops", 1590.0)  # the kernel is timed alone: the burst figure
+        return dict(common, kernel="match, chosen_tc form (tcgen05 BF16 distances into tensor memory, selection on "
+                                   "them, exact FP32 re-rank)",
+                    bound="tensor", achieved=flops / (ms_launch / 1e3) / 1e12, peak=peak, unit="TFLOP/s",
+                    frac=flops / (ms_launch / 1e3) / 1e12 / peak,
+                    peak_source="MEASURED_PEAKS.json bf16_tflops, burst (of measured)" if peak != 1590.0
+                                else "fallback 1.59 PFLOP/s (of fallback)",
+                    work="2 G C d_m (algorithmic multiply-adds of all candidate distances) per launch")
     # filter: Gram, basis, projections and reconstruction (FP32, exact)
     D, B, rk = dm_final, bp.similar, bp.rank
-    act, rows = st["active_groups"], st["rows"]
+    act, rows = st["active_groups"] / anchor_frames, st["rows"] / anchor_frames
     flops = act * (B * (B + 1) * D + 2 * rk * B * D) + rows * 2 * rk * D * 2.5
-    return {"kernel": "group filter (prepare + Jacobi + apply)", "bound": "fp32",
-            "achieved": flops / (ms / 1e3) / 1e12, "peak": 2 * FP32_LANE_OPS / 1e12, "unit": "TFLOP/s",
-            "frac": flops / (ms / 1e3) / (2 * FP32_LANE_OPS),
-            "peak_source": "nominal FP32 FMA rate x 2", "ms_per_launch": ms / max(1, launches),
-            # dram__bytes_read.sum + dram__bytes_write.sum of prepare + Jacobi + apply for one
-            # anchor frame (mean of Basic 412.8 MB and Final 596.2 MB),
-            # profiles/kernels_1080p_yuv444_one_anchor_frame.md; about 180 GB/s over the
-            # event-timed filter, so the class is bound by latency, not by HBM
-            "traffic": 504.5e6 if PARAMS == "cpu" else None,
-            "traffic_unit": "bytes per anchor frame (ncu, one capture)"}
+    return dict(common, kernel="group filter (prepare + Jacobi + apply), one call per anchor frame and stage",
+                bound="fp32", achieved=flops / (ms_launch / 1e3) / 1e12, peak=2 * FP32_LANE_OPS / 1e12,
+                unit="TFLOP/s", frac=flops / (ms_launch / 1e3) / (2 * FP32_LANE_OPS),
+                peak_source="nominal FP32 FMA rate x 2 (MEASURED_PEAKS.json has no FP32 figure)",
+                work="Gram B(B+1)D + basis 2rBD per active group, projection and reconstruction 5rD per "
+                     "retained row, per call")
 
 
 def measured_peak(key: str, fallback: float) -> float:
@@ -423,6 +604,9 @@ def run_ours(args):
         forms = ["plain"]
     results = {f: measure_form(f, args, ranks, stream, noisy, clean, d_noisy, local) for f in forms}
     head = results[forms[-1]]
+    frame_path = None
+    if not args.no_frame_path:
+        frame_path = measure_frame_path(head["form"], args, ranks, noisy, local)
     per_kernel = {}
     total_kernel_ms = sum(v[0] for v in head["kernels"].values())
     for k, v in head["kernels"].items():
@@ -464,6 +648,11 @@ def run_ours(args):
                                    "match_ms_per_step": other["kernels"]["match"][0] / args.steps}
         if head["form"] != "plain" and not roofline["kernel"].startswith("match"):
             config["match_roofline"] = roofline_of(head, args.steps, which="match")
+        if frame_path is not None:
+            config["e2e_frame_path"] = dict(
+                frame_path, unit=UNIT, h2d_bytes_per_step=3 * clip_bytes, d2h_bytes_per_step=2 * clip_bytes,
+                api="vnlbgpu_render_frame_window per output frame (the plugin's getFrame), pageable host frames, "
+                    "frame threads per stage = num_streams; wall time, synchronised")
         line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": head["max_ms"] / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32" if head["form"] == "chosen_tc" else "f32",
@@ -517,6 +706,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-frame-path", action="store_true",
+                    help="skip the end-to-end run through the per-frame path (vnlbgpu_render_frame_window)")
     ap.add_argument("--form", choices=("all", "plain", "chosen", "chosen_tc"), default="all",
                     help="matcher form(s) to time; with all, the tensor-core form (chosen_tc) is the headline "
                          "and the plain and FP32 chosen forms are measured beside it for the speed-up and the PSNR "

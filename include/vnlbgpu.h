@@ -15,9 +15,11 @@
  *   CudaFilterFree (cuda_plugin.cpp:2022-2036)       vnlbgpu_destroy
  *   upload_source_misses (cuda_plugin.cpp:           vnlbgpu_set_frame,
  *     1291-1361), noisy/basic FrameCache               vnlbgpu_set_clip_host,
- *                                                      vnlbgpu_set_clip_device
- *   render_frame (cuda_plugin.cpp:1635-1864) =       vnlbgpu_render_frame
- *     vnlbcu.Basic / vnlbcu.Final getFrame
+ *     (src/cuda/frame_cache.cpp:120-537)               vnlbgpu_set_clip_device
+ *   required_source_range (cuda_plugin.cpp:846-858)  vnlbgpu_required_source_range
+ *   render_frame (cuda_plugin.cpp:1635-1864) =       vnlbgpu_render_frame_window,
+ *     vnlbcu.Basic / vnlbcu.Final getFrame,            vnlbgpu_render_frame
+ *     with fetch_frames + upload_source_misses
  *   render_stage_frame (src/vs/plugin.cpp:616-758)   vnlbgpu_render_stack
  *     = vnlb.Basic / vnlb.Final getFrame
  *   render_aggregate_frame (plugin.cpp:966-1045)     vnlbgpu_aggregate
@@ -30,8 +32,12 @@
  * vnlbgpu_last_error() on the calling thread.  No C++ exception crosses this
  * boundary.  Sizes are in samples (float32); strides are in bytes, as
  * VapourSynth's getStride reports them.  A session is safe to call from
- * several threads (calls are serialised inside); results match the reference
- * CPU core bit for bit for the plain form (see the parity tests).
+ * several threads.  Per-frame calls (set_frame, render_frame,
+ * render_frame_window) each lease one of num_streams workers and queue their
+ * GPU work under the session's lock, then wait for it with the lock released,
+ * so up to num_streams of them overlap on the GPU; the other calls hold the
+ * lock until they return.  Results match the reference CPU core bit for bit
+ * for the plain form (see the parity tests).
  */
 #ifndef VNLBGPU_H
 #define VNLBGPU_H
@@ -109,32 +115,73 @@ typedef struct vnlbgpu_stats {
     long long pipeline_lanes;  /* anchor frames the session keeps in flight (1-8, fewer
                                   when their group buffers would exceed half of the free
                                   device memory at create time) */
+    long long source_slots;    /* frames each source store holds on the device */
+    long long source_uploads;  /* source frames copied to the device */
 } vnlbgpu_stats;
 
 const char* vnlbgpu_last_error(void);
 
 /* Validates the parameters for a clip of `frames` frames of width x height
- * with 1 (GrayS) or 3 (YUV444PS) planes and reserves device memory. */
+ * with 1 (GrayS) or 3 (YUV444PS) planes and reserves device memory.  No
+ * device memory is sized by `frames`: the group buffers follow the frame
+ * size, the contribution stacks number slots + lanes + num_streams - 1, and
+ * each source store holds min(frames, source window + num_streams - 1)
+ * frames, the source window being 2 * (search_bwd + search_fwd + patch_time
+ * - 1) + 1 frames (derive_geometry's max_source_window,
+ * cuda_plugin.cpp:761-773), until a whole clip is given. */
 int vnlbgpu_create(const vnlbgpu_params* params, int width, int height, int frames, int channels,
                    vnlbgpu_session** out);
 void vnlbgpu_destroy(vnlbgpu_session* session);
 
-/* Sources.  set_frame copies one frame from per-plane host pointers with byte
- * strides; set_clip_host copies a whole clip laid out [frames][planes][H][W];
+/* Sources.  Frames are immutable, as VapourSynth's are: a frame index names
+ * the same samples for the session's life.
+ *
+ * set_frame copies one frame from per-plane host pointers with byte strides
+ * into the source's store on the device, unless that frame is there already;
+ * the store is a ring, so a frame can push out the frame a store's capacity
+ * before or after it.  set_clip_host copies a whole clip laid out
+ * [frames][planes][H][W] and makes the stores hold every frame;
  * set_clip_device makes the session read a caller-owned device buffer of that
- * layout (no copy; it must stay valid while the session uses it). */
+ * layout (no copy; it must stay valid while the session uses it).  The two
+ * whole-clip calls drop the cached contribution stacks. */
 int vnlbgpu_set_frame(vnlbgpu_session* session, int source, int frame, const float* const* planes,
                       const ptrdiff_t* strides);
 int vnlbgpu_set_clip_host(vnlbgpu_session* session, int source, const float* clip);
 int vnlbgpu_set_clip_device(vnlbgpu_session* session, int source, const float* device_clip);
 
-/* vnlbcu.Basic / vnlbcu.Final: the denoised output frame n (aggregated), into
- * per-plane host pointers with byte strides. */
+/* The source frames [*first, *last] that output frame n may read: the union
+ * of its contributing anchor frames' shifted temporal windows plus
+ * patch_time - 1 (required_source_range, cuda_plugin.cpp:846-858).  A plugin
+ * requests these frames in its arInitial step. */
+int vnlbgpu_required_source_range(vnlbgpu_session* session, int n, int* first, int* last);
+
+/* vnlbcu.Basic / vnlbcu.Final getFrame (render_frame, cuda_plugin.cpp:
+ * 1635-1864): the denoised output frame n (aggregated), into per-plane host
+ * pointers with byte strides.  The call gives the source frames first ..
+ * first + count - 1, normally the required source range: clip_planes and
+ * clip_strides hold count * planes entries, frame-major (frame first + i,
+ * plane c at i * planes + c), and ref_planes / ref_strides the same for the
+ * Final stage's ref clip (NULL for Basic).  Frames not on the device yet are
+ * copied through pinned staging; the frames are held until the call's reads
+ * are queued, so concurrent calls cannot push out one another's frames.
+ * count must not exceed the store's frames (vnlbgpu_stats.source_slots).
+ * Anchor frames whose contribution stacks are cached are not recomputed. */
+int vnlbgpu_render_frame_window(vnlbgpu_session* session, int n, int first, int count,
+                                const float* const* clip_planes, const ptrdiff_t* clip_strides,
+                                const float* const* ref_planes, const ptrdiff_t* ref_strides, float* const* planes,
+                                const ptrdiff_t* strides);
+
+/* The same output frame from the frames already on the device (given by
+ * set_frame or a whole-clip call); raises naming the first frame it needs
+ * that is not. */
 int vnlbgpu_render_frame(vnlbgpu_session* session, int n, float* const* planes, const ptrdiff_t* strides);
 
-/* Whole clip in one call, [frames][planes][H][W], into host or device memory.
- * The device form enqueues on the session's stream and returns without
- * waiting; vnlbgpu_synchronize waits and reports device-side errors. */
+/* Whole clip in one call, [frames][planes][H][W], into host or device memory;
+ * every frame of the sources must be on the device (a whole-clip source, or
+ * a clip no longer than the stores).  The device form enqueues on the
+ * session's stream and returns without waiting; vnlbgpu_synchronize waits and
+ * reports device-side errors.  The host form allocates a device buffer of the
+ * whole output clip. */
 int vnlbgpu_render_clip_host(vnlbgpu_session* session, float* out);
 int vnlbgpu_render_clip_device(vnlbgpu_session* session, float* device_out);
 int vnlbgpu_synchronize(vnlbgpu_session* session);
@@ -173,6 +220,23 @@ int vnlbgpu_aggregate(const float* stacks, const float* source, int width, int h
 int vnlbgpu_aggregate_frame_noalloc(const float* stacks, const float* source, int width, int height, int frames,
                                     int channels, int search_bwd, int search_fwd, int patch_time, int device_id, int n,
                                     float* out);
+
+/* One clip over several GPUs, one process per GPU, no exchange between them
+ * (the reference has one device per filter, cuda_plugin.cpp:476; this is the
+ * partition of its per-frame dependencies).  Output frames [0, frames) are
+ * split into `world` contiguous blocks; rank `rank` renders Final frames
+ * [out[0], out[1]] (-1, -1 when its block is empty).  Final frame n reads the
+ * Basic frames and source frames of its required source range, and Basic
+ * frame m reads the source frames of its own: so the rank also renders Basic
+ * frames [basic[0], basic[1]], the union of its Final frames' ranges, and
+ * needs source frames [source[0], source[1]], the union of those Basic
+ * frames' ranges.  Each rank runs its own sessions over the whole clip's
+ * frame count through the per-frame calls, so the temporal windows are the
+ * whole clip's and the blocks joined equal the one-GPU output bit for bit.
+ * Host only: needs no device. */
+int vnlbgpu_shard_plan(int frames, int world, int rank, int basic_search_bwd, int basic_search_fwd,
+                       int basic_patch_time, int final_search_bwd, int final_search_fwd, int final_patch_time,
+                       int out[2], int basic[2], int source[2]);
 
 int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats);
 

@@ -40,6 +40,12 @@ int vnlbgpu_diag_anchor(vnlbgpu_session* session, int anchor, int* grid_xy, int*
  * Timing brackets each launch with CUDA events on the session's stream. */
 int vnlbgpu_diag_kernel_timing(vnlbgpu_session* session, int enable, double* ms, long long* launches);
 
+/* Limits the pipeline lanes the session uses to min(lanes, the lanes it
+ * allocated) after waiting for its queued work; lanes <= 0 restores them all.
+ * With one lane the anchor frames' kernels run one after another, so the
+ * per-kernel times above are those of each kernel alone. */
+int vnlbgpu_diag_set_lanes(vnlbgpu_session* session, int lanes);
+
 #ifdef __cplusplus
 }
 #endif

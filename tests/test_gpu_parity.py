@@ -94,6 +94,12 @@ CASES = [
     ("gray_covariance_p7", 64, 48, 4, 1, 20.0, dict(block_size=7, block_step=4, group_size=16, rank=8)),
     ("yuv_uncoupled_covariance", 48, 40, 3, 3, 15.0, dict(chroma=0, block_size=4, block_step=2, group_size=10,
                                                           rank=5, bm_range=3)),
+    # the reference's large-model profiles (tests/vs/integration_cuda.py:380-398, 436-448): 100 and 60 model
+    # rows of dimension 294 (block 7, patch_time 2, YUV), rank 39
+    ("yuv_k100_rank39", 64, 56, 3, 3, 8.0, dict(block_size=7, group_size=100, rank=39, cap_factor=1.0, bm_range=13,
+                                                patch_time=2, block_step=16, radius=0, variance_threshold=2.7)),
+    ("yuv_k60_rank39", 64, 56, 3, 3, 8.0, dict(block_size=7, group_size=60, rank=39, cap_factor=1.0, bm_range=13,
+                                               patch_time=2, block_step=16, radius=0, variance_threshold=1.8)),
 ]
 
 
@@ -230,6 +236,9 @@ def test_unsupported_configurations_raise():
         vnlbcu.Basic(gray, sigma=10.0, block_size=2, group_size=8, rank=4)
     with pytest.raises(lib.VNLBError, match="chroma=1"):
         vnlbcu.Basic(np.zeros((3, 3, 32, 32), np.float32), sigma=10.0, chroma=0)  # vnlbcu keeps its rule
+    with pytest.raises(lib.VNLBError, match="at most 128 model samples"):
+        # derive_geometry's limit (cuda_plugin.cpp:43, 730): 130 model rows of dimension 294
+        vnlbcu.Basic(np.zeros((3, 3, 64, 64), np.float32), sigma=10.0, group_size=130, rank=20, cap_factor=1.0)
 
 
 def test_full_size_anchor_frames_bit_exact():

@@ -41,6 +41,7 @@ constexpr int kApplyWarps = kApplyThreads / 32;
 constexpr int kRecCols = 8;  // reconstruction columns held in registers per lane (blocks of 256)
 constexpr int kPrepareWarps = 4;
 constexpr float kEigenFloor = 128.0f * FLT_EPSILON;
+constexpr size_t kFilterSharedLimit = 227 * 1024;  // dynamic shared memory of one CTA on sm_100
 
 // dot_contiguous_highway (the pinned 8-lane order) computed by an octet of
 // lanes (j = lane & 7): lane j owns accumulator j; the fold follows reduce8.  All 8 lanes return the dot.
@@ -86,7 +87,7 @@ __device__ __forceinline__ int column_offset(const FilterLaunch& L, int col) {
 }
 
 __device__ __forceinline__ size_t row_base(const FilterLaunch& L, const MatchRow& m) {
-    return (static_cast<size_t>(m.frame) * L.channels * L.height + m.y) * static_cast<size_t>(L.width) + m.x;
+    return (static_cast<size_t>(m.frame % L.ring) * L.channels * L.height + m.y) * static_cast<size_t>(L.width) + m.x;
 }
 
 __device__ __forceinline__ int bmax_of(const FilterLaunch& L) { return min(L.model_cap, L.max_rows); }
@@ -526,9 +527,6 @@ __host__ __device__ inline ApplyLayout apply_layout(int D, int Bmax, int R, int 
     a.colpad = (D + 3) & ~3;
     size_t off = static_cast<size_t>(a.colpad);
     a.means = off;   off += 2 * static_cast<size_t>(D);
-    if (!tiled) {
-        a.X = off;   off += static_cast<size_t>(Bmax) * a.ldx;
-    }
     a.basis = off;   off += static_cast<size_t>(R) * a.ldb;
     a.dual = off;    off += static_cast<size_t>(R) * Bmax;
     a.scal = off;    off += 5 * static_cast<size_t>(R);
@@ -541,7 +539,12 @@ __host__ __device__ inline ApplyLayout apply_layout(int D, int Bmax, int R, int 
         const size_t model = static_cast<size_t>(Bmax) * a.ldx;
         off += tiles > model ? tiles : model;
     } else {
-        off += static_cast<size_t>(warps) * (2 * a.ldb + R + 1);
+        // the centred model rows are read only while the basis is built,
+        // before any warp uses its row scratch: they share the space
+        a.X = off;
+        const size_t rows = static_cast<size_t>(warps) * (2 * a.ldb + R + 1);
+        const size_t model = static_cast<size_t>(Bmax) * a.ldx;
+        off += rows > model ? rows : model;
     }
     off = (off + 1) & ~static_cast<size_t>(1);
     a.bases = off;   off += 2 * static_cast<size_t>(max_rows);
@@ -1368,6 +1371,29 @@ __global__ void combine_weights_kernel(FilterLaunch L) {
     }
 }
 
+// Segment width, row stride and per-group floats of the Jacobi kernel for
+// matrices up to N x N.  A segment of `seg` lanes per group, each lane owning
+// rows r0, r0 + seg, ...; two rows per lane from 8 rows up, which halves the
+// rotation parameters every lane recomputes.  Rows are padded to N + 1 and
+// groups to gstride floats: for N = 8 (segments of 4, 8 groups per warp,
+// gstride = 4 mod 32) the lanes of a warp touch 32 distinct banks.  Wider
+// segments when a warp's groups would not fit in shared memory (N > 119: one
+// group per warp).
+struct JacobiShape {
+    int seg, ld, gstride;
+};
+JacobiShape jacobi_shape(int N) {
+    int seg = 1;
+    while (seg < N && seg < 32) seg <<= 1;
+    if (seg >= 8) seg /= 2;
+    seg = std::max(seg, 1);
+    const int ld = N + 1;
+    int gstride = 2 * N * ld + N;
+    if (seg == 4) gstride += ((4 - gstride % 32) + 32) % 32;
+    while (seg < 32 && static_cast<size_t>(32 / seg) * gstride * sizeof(float) > kFilterSharedLimit) seg <<= 1;
+    return JacobiShape{seg, ld, gstride};
+}
+
 template <int D>
 cudaError_t launch_apply_warp(const FilterLaunch& L, int max_groups, cudaStream_t stream) {
     const WarpApplyLayout lay = warp_apply_layout(D, L.max_rows);
@@ -1381,6 +1407,26 @@ cudaError_t launch_apply_warp(const FilterLaunch& L, int max_groups, cudaStream_
 }
 
 }  // namespace
+
+size_t filter_shared_bytes(const FilterLaunch& L) {
+    const int D = L.dim;
+    const int Bmax = std::min(L.model_cap, L.max_rows);
+    const int R = L.rank;
+    const size_t colpad = static_cast<size_t>((D + 3) & ~3);
+    const size_t rows_bytes = static_cast<size_t>(Bmax) * (D + 8) * sizeof(float);
+    const int groups_per_cta = rows_bytes > 8 * 1024 ? 1 : kPrepareWarps;
+    size_t need = (colpad + static_cast<size_t>(groups_per_cta) * Bmax * (D + 8)) * sizeof(float) +
+                  static_cast<size_t>(groups_per_cta) * L.max_rows * sizeof(size_t);
+    if (R > 0) {
+        const JacobiShape js = jacobi_shape(L.nmax);
+        need = std::max(need, static_cast<size_t>(32 / js.seg) * js.gstride * sizeof(float));
+    }
+    const bool tiled = R >= 1 && R <= kTileComps && D > 16;
+    need = std::max(need, apply_layout(D, Bmax, R, L.max_rows, kApplyWarps, tiled, L.stage == 1).bytes);
+    return need;
+}
+
+size_t filter_shared_limit() { return kFilterSharedLimit; }
 
 cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t stream) {
     if (max_groups_in <= 0) return cudaSuccess;
@@ -1411,16 +1457,8 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
         // ...; two rows per lane from 8 rows up, which halves the rotation
         // parameters every lane recomputes
         const int N = L.nmax;  // largest matrix: model rows, or the dimension of covariance models
-        int seg = 1;
-        while (seg < N && seg < 32) seg <<= 1;
-        if (seg >= 8) seg /= 2;
-        seg = std::max(seg, 1);
-        // rows padded to Bmax + 1 and groups to gstride floats: for Bmax = 8
-        // (segments of 4, 8 groups per warp, gstride = 4 mod 32) the lanes of
-        // a warp touch 32 distinct banks
-        const int ld = N + 1;
-        int gstride = 2 * N * ld + N;
-        if (seg == 4) gstride += ((4 - gstride % 32) + 32) % 32;
+        const JacobiShape js = jacobi_shape(N);
+        const int seg = js.seg, ld = js.ld, gstride = js.gstride;
         const size_t per_group = static_cast<size_t>(gstride) * sizeof(float);
         int warps = 8;
         while (warps > 1 && static_cast<size_t>(warps) * (32 / seg) * per_group > 160 * 1024) warps /= 2;

@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
         for (int q = 0; q < planes_n; ++q) {
             const int c = q / L.Pt;
             const int t = q % L.Pt;
-            const float* src = L.video + ((static_cast<size_t>(frame + t) * L.channels + c) * L.height +
+            const float* src = L.video + ((static_cast<size_t>(frame % L.ring + t) * L.channels + c) * L.height +
                                           ry0) * static_cast<size_t>(L.width) + rx0;
             float* dst = planes + q * plane_values;
             for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {

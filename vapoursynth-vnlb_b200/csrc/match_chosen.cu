@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                     int2 a = make_int2(0, 0);
                     if (n < count) a = L.anchors[strip.first + n];
                     const float* anchor_frame =
-                        L.video + static_cast<size_t>(L.schedule[0]) * L.channels * plane_values;
+                        L.video + static_cast<size_t>(L.schedule[0] % L.ring) * L.channels * plane_values;
 #pragma unroll
                     for (int j = 0; j < PLANES; ++j) {
                         const int e = 2 * (lane + 32 * j);
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
 #pragma unroll
                     for (int q = 0; q < PLANES; ++q) {
                         const int c = q / L.Pt, tt = q % L.Pt;
-                        const float* src = L.video + (static_cast<size_t>(frame + tt) * L.channels + c) * plane_values +
+                        const float* src = L.video + (static_cast<size_t>(frame % L.ring + tt) * L.channels + c) * plane_values +
                                            static_cast<size_t>(row_in ? gy : 0) * L.width;
                         s[q][0] = row_in && x0 < L.width ? __ldg(src + x0) : 0.0f;
                         s[q][1] = row_in && x0 + 32 < L.width ? __ldg(src + x0 + 32) : 0.0f;
@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
     const int cells = Wx * (yh - yl + 1);
     const size_t plane_values = static_cast<size_t>(L.height) * L.width;
     const float* approx = L.approx_dist + static_cast<size_t>(gi) * L.approx_stride;
-    const float* anchor_frame = L.video + static_cast<size_t>(L.schedule[0]) * L.channels * plane_values;
+    const float* anchor_frame = L.video + static_cast<size_t>(L.schedule[0] % L.ring) * L.channels * plane_values;
 
     // selection state (the plain matcher's WarpSelect)
     const int K = L.K;
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
             const int c = q / L.Pt, t = q % L.Pt;
             const float* rp = anchor_frame + (static_cast<size_t>(t) * L.channels + c) * plane_values +
                               static_cast<size_t>(anchor.y) * L.width + anchor.x;
-            const float* cp = L.video + (static_cast<size_t>(frame + t) * L.channels + c) * plane_values +
+            const float* cp = L.video + (static_cast<size_t>(frame % L.ring + t) * L.channels + c) * plane_values +
                               static_cast<size_t>(yl + cy) * L.width + col;
             // the candidate's samples first (all loads in flight), the
             // reference rows (one address for the whole warp) as they are used

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -136,6 +137,7 @@ struct Session {
     cudaStream_t stream = nullptr;      // the stream all work is enqueued on
     cudaStream_t own_stream = nullptr;  // created by the session
     vnlbgpu_stats stats{};
+    long long stats_uploads = 0;  // source frames copied to the device
 
     // optional per-kernel timing: (category, start, stop) event triples
     bool timing = false;
@@ -172,8 +174,7 @@ struct Session {
     }
     void collect_timing() {
         if (timed.empty()) return;
-        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize(timing)");
-        for (int i = 0; i < lane_count; ++i) check(cudaStreamSynchronize(lanes[i].stream), "cudaStreamSynchronize(timing)");
+        drain();
         for (const Timed& t : timed) {
             float ms = 0.0f;
             check(cudaEventElapsedTime(&ms, t.start, t.stop), "cudaEventElapsedTime");
@@ -185,10 +186,161 @@ struct Session {
         timed.clear();
     }
 
-    DeviceArray<float> own_clip, own_ref;
-    const float* clip = nullptr;
-    const float* ref = nullptr;
-    bool clip_ready = false, ref_ready = false;
+    // Events recording reads (of a source frame or a stack), shared by every
+    // place that refers to the same read and recycled when the last goes.
+    std::vector<cudaEvent_t> read_event_pool;
+    using ReadEvent = std::shared_ptr<CUevent_st>;
+    ReadEvent record_read(cudaStream_t on) {
+        cudaEvent_t e;
+        if (!read_event_pool.empty()) {
+            e = read_event_pool.back();
+            read_event_pool.pop_back();
+        } else {
+            check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        }
+        check(cudaEventRecord(e, on), "cudaEventRecord(read)");
+        return ReadEvent(e, [this](cudaEvent_t x) { read_event_pool.push_back(x); });
+    }
+    // `on` waits for every recorded read, which are then forgotten.
+    void wait_reads(cudaStream_t on, std::vector<ReadEvent>& reads) {
+        for (const ReadEvent& r : reads) check(cudaStreamWaitEvent(on, r.get(), 0), "cudaStreamWaitEvent(read)");
+        reads.clear();
+    }
+    // Drops reads that have finished, so that the list of a long-lived frame
+    // slot or stack stays short.
+    static void prune_reads(std::vector<ReadEvent>& reads) {
+        if (reads.size() < 16) return;
+        reads.erase(std::remove_if(reads.begin(), reads.end(),
+                                   [](const ReadEvent& r) { return cudaEventQuery(r.get()) == cudaSuccess; }),
+                    reads.end());
+        cudaGetLastError();  // cudaErrorNotReady is not sticky, but leaves nothing behind either
+    }
+
+    // Source frames on the device (the reference's noisy and basic
+    // FrameCaches, src/cuda/frame_cache.cpp:120-537).  Frame f of a source
+    // lives in slot f % ring of a store of ring + patch_time - 1 frame slots;
+    // the last patch_time - 1 slots repeat the first ones, so that a patch's
+    // patch_time consecutive frames are consecutive slots (MatchLaunch).  A
+    // session starts with ring = min(frames, source window + num_streams - 1),
+    // the source window being 2 (search_bwd + search_fwd + patch_time - 1) + 1
+    // frames, the most one output frame reads (derive_geometry's
+    // max_source_window, cuda_plugin.cpp:761-773).  A whole-clip source
+    // (vnlbgpu_set_clip_host / vnlbgpu_set_clip_device) makes ring = frames.
+    // Frames are immutable, like VapourSynth's: giving a frame that is already
+    // on the device copies nothing.
+    struct FrameSlot {
+        int frame = -1;       // frame held (-1: none)
+        int pins = 0;         // calls that hold the slot between claiming it and queueing their reads
+        bool filling = false; // claimed, its copy not queued yet
+        bool copied = false;  // `ready` marks the copy that filled it
+        cudaEvent_t ready = nullptr;
+        std::vector<ReadEvent> reads;  // queued work that reads the held frame
+    };
+    struct SourceStore {
+        DeviceArray<float> own;          // ring (+ patch_time - 1) frame slots
+        const float* base = nullptr;     // own.ptr, or a caller's whole device clip
+        bool borrowed = false;           // base is the caller's: every frame resident, nothing tracked
+        std::vector<FrameSlot> slots;    // [ring]
+    };
+    SourceStore store[2];
+    int ring = 0;
+    int source_window = 0;  // frames one output frame may read
+    const float* clip = nullptr;  // store[0].base
+    const float* ref = nullptr;   // store[1].base
+
+    int sources() const { return stage == 1 ? 2 : 1; }
+
+    // (Re)allocates a source's own store for `ring` slots, dropping its frames.
+    void reset_store(int source) {
+        SourceStore& st = store[source];
+        const int mirror = ring < frames ? Pt - 1 : 0;
+        if (!st.own.ptr || st.own.count != frame_values() * static_cast<size_t>(ring + mirror)) {
+            st.own.release();
+            st.own.allocate(frame_values() * static_cast<size_t>(ring + mirror), "cudaMalloc(source frames)");
+        }
+        st.base = st.own.ptr;
+        st.borrowed = false;
+        if (static_cast<int>(st.slots.size()) != ring) {
+            for (FrameSlot& sl : st.slots)
+                if (sl.ready) cudaEventDestroy(sl.ready);
+            st.slots.clear();
+            st.slots.resize(static_cast<size_t>(ring));
+            for (FrameSlot& sl : st.slots)
+                check(cudaEventCreateWithFlags(&sl.ready, cudaEventDisableTiming), "cudaEventCreate(frame slot)");
+        }
+        for (FrameSlot& sl : st.slots) {
+            sl.frame = -1;
+            sl.pins = 0;
+            sl.filling = false;
+            sl.copied = false;
+            sl.reads.clear();
+        }
+        if (source == VNLBGPU_SOURCE_CLIP) clip = st.base; else ref = st.base;
+    }
+
+    // Whole clips: every frame gets its own slot.  Waits for all queued work.
+    void make_whole() {
+        if (ring == frames) return;
+        drain();
+        ring = frames;
+        for (int src = 0; src < 2; ++src)
+            if (store[src].own.ptr && !store[src].borrowed) reset_store(src);
+        invalidate();
+    }
+
+    bool resident(int source, int f) const {
+        const SourceStore& st = store[source];
+        if (st.borrowed) return true;
+        if (!st.base) return false;
+        const FrameSlot& sl = st.slots[static_cast<size_t>(f % ring)];
+        return sl.frame == f;
+    }
+    const float* frame_ptr(int source, int f) const {
+        return store[source].base + static_cast<size_t>(f % ring) * frame_values();
+    }
+
+    // Queues the copy of frame f of a source from a contiguous host frame
+    // [planes][H][W] into its slot on `on`, after every queued read of the
+    // slot's previous frame.
+    void queue_copy(int source, int f, const float* host_frame, cudaStream_t on);
+
+    // `on` waits for the copies of frames [first, last] of every source the
+    // stage reads; each must be on the device.
+    void wait_frames(cudaStream_t on, int first, int last) {
+        first = std::max(first, 0);
+        last = std::min(last, frames - 1);
+        for (int src = 0; src < sources(); ++src) {
+            SourceStore& st = store[src];
+            if (st.borrowed) continue;
+            for (int f = first; f <= last; ++f) {
+                FrameSlot& sl = st.slots[static_cast<size_t>(f % ring)];
+                if (sl.frame != f || sl.filling) fail(missing_frame_message(src, f));
+                if (sl.copied) check(cudaStreamWaitEvent(on, sl.ready, 0), "cudaStreamWaitEvent(frame copied)");
+            }
+        }
+    }
+    // Records that work queued on `on` reads frames [first, last] (sources
+    // as wait_frames), so that no copy overwrites them before it is done.
+    void read_frames(cudaStream_t on, int first, int last, int only_source = -1) {
+        first = std::max(first, 0);
+        last = std::min(last, frames - 1);
+        ReadEvent r;
+        for (int src = 0; src < sources(); ++src) {
+            if (only_source >= 0 && src != only_source) continue;
+            SourceStore& st = store[src];
+            if (st.borrowed) continue;
+            if (!r) r = record_read(on);
+            for (int f = first; f <= last; ++f) {
+                FrameSlot& sl = st.slots[static_cast<size_t>(f % ring)];
+                prune_reads(sl.reads);
+                sl.reads.push_back(r);
+            }
+        }
+    }
+    std::string missing_frame_message(int source, int f) const {
+        return "VNLB CUDA: frame " + std::to_string(f) + " of " + (source == 0 ? "clip" : "ref") +
+               " is not on the device (give it with vnlbgpu_set_frame or vnlbgpu_render_frame_window)";
+    }
 
     // Pipeline lanes: consecutive anchor frames go round the lanes, each lane
     // with its own stream and scratch, so that one anchor frame's serial
@@ -212,60 +364,87 @@ struct Session {
 #endif
     static constexpr int kMaxLanes = VNLB_MAX_LANES;
     Lane lanes[kMaxLanes];
-    int lane_count = kMaxLanes;        // lanes in use (allocated): 1..kMaxLanes
+    int lane_count = kMaxLanes;        // lanes in use: 1..lanes_allocated
+    int lanes_allocated = kMaxLanes;   // lanes with streams and buffers
     int next_lane = 0;
     cudaEvent_t ev_fork = nullptr;     // main-stream point the lanes start after
     cudaEvent_t ev_lane[kMaxLanes] = {};
 
-    // Host transfers run on their own streams so that they overlap the
-    // kernels: each uploaded frame records frame_ready[source][frame], and an
-    // anchor frame's lane waits only for the frames it reads; each output
-    // frame of a whole-clip host render is downloaded as soon as it is
-    // normalised.
+    // Whole-clip host transfers run on their own streams so that they overlap
+    // the kernels: an anchor frame's lane waits only for the copies of the
+    // frames it reads; each output frame of a whole-clip host render is
+    // downloaded as soon as it is normalised.
     cudaStream_t upload_stream = nullptr, download_stream = nullptr;
     cudaEvent_t ev_main = nullptr;      // main-stream point a copy stream starts after
     cudaEvent_t ev_out = nullptr;       // an output frame is normalised
     cudaEvent_t ev_download = nullptr;  // the downloads are done
-    std::vector<cudaEvent_t> frame_ready[2];
-    bool frames_async[2] = {false, false};  // the source's frames came through upload_stream
+
+    // Per-frame calls (vnlbgpu_render_frame, vnlbgpu_render_frame_window,
+    // vnlbgpu_set_frame) each lease one of num_streams workers, like the
+    // reference's WorkerPool (cuda_plugin.cpp:1117-1199): a stream, an output
+    // frame on the device and pinned host staging.  A call queues its work
+    // under the session lock and waits for it with the lock released, so
+    // calls from several threads overlap on the GPU.
+    struct Worker {
+        cudaStream_t stream = nullptr;
+        DeviceArray<float> out;           // one output frame
+        float* host_out = nullptr;        // pinned, one frame
+        int* host_status = nullptr;       // pinned
+        std::vector<float*> staging;      // pinned frames for source copies
+        std::vector<cudaEvent_t> staged;  // the device copy out of staging[i] is done
+        std::vector<bool> staged_used;
+        cudaEvent_t done = nullptr;
+        bool busy = false;
+    };
+    std::vector<std::unique_ptr<Worker>> workers;
+    std::condition_variable changed;  // a worker was released, a slot filled or unpinned
+    int staging_slots = 2;
 
     DeviceArray<unsigned long long> d_totals;
     DeviceArray<int> d_status;
     DeviceArray<float> d_window, d_out_frame, d_pack;
     std::map<int, std::unique_ptr<Grid>> grids;
 
-    // contribution stack cache (anchor -> stack), capacity >= slots.  `ready`
-    // is recorded on the producing lane, `released` on the main stream after
-    // the last normalisation that read the stack.
+    // Contribution stack cache (anchor -> stack), the reference's contribution
+    // FrameCache (cuda_plugin.cpp:1530-1605): slots + lanes + num_streams - 1
+    // stacks.  `ready` is recorded on the producing lane; `reads` are the
+    // queued normalisations and packs that read the stack.
     struct CachedStack {
         int anchor = -1;
         long long last_use = 0;
         DeviceArray<float> data;
         cudaEvent_t ready = nullptr;
-        cudaEvent_t released = nullptr;
-        bool pending_release = false;
+        std::vector<ReadEvent> reads;
     };
     std::vector<std::unique_ptr<CachedStack>> cache;
     long long use_clock = 0;
     std::vector<float> host_window;
 
     ~Session() {
-        if (stream) cudaStreamSynchronize(stream);
-        for (Lane& l : lanes)
-            if (l.stream) cudaStreamSynchronize(l.stream);
+        drain();
         for (const Timed& t : timed) {
             cudaEventDestroy(t.start);
             cudaEventDestroy(t.stop);
         }
         for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
         for (auto& c : cache) {
+            c->reads.clear();
             if (c->ready) cudaEventDestroy(c->ready);
-            if (c->released) cudaEventDestroy(c->released);
         }
-        if (upload_stream) cudaStreamSynchronize(upload_stream);
-        if (download_stream) cudaStreamSynchronize(download_stream);
-        for (auto& v : frame_ready)
-            for (cudaEvent_t e : v) cudaEventDestroy(e);
+        for (SourceStore& st : store)
+            for (FrameSlot& sl : st.slots) {
+                sl.reads.clear();
+                if (sl.ready) cudaEventDestroy(sl.ready);
+            }
+        for (cudaEvent_t e : read_event_pool) cudaEventDestroy(e);
+        for (auto& w : workers) {
+            if (w->stream) cudaStreamDestroy(w->stream);
+            if (w->host_out) cudaFreeHost(w->host_out);
+            if (w->host_status) cudaFreeHost(w->host_status);
+            for (float* p : w->staging) cudaFreeHost(p);
+            for (cudaEvent_t e : w->staged) cudaEventDestroy(e);
+            if (w->done) cudaEventDestroy(w->done);
+        }
         for (cudaEvent_t e : {ev_main, ev_out, ev_download})
             if (e) cudaEventDestroy(e);
         if (upload_stream) cudaStreamDestroy(upload_stream);
@@ -278,37 +457,28 @@ struct Session {
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 
-    // Lanes start after everything enqueued so far on the main stream ...
-    void fork() {
-        check(cudaEventRecord(ev_fork, stream), "cudaEventRecord(fork)");
+    // Waits for everything the session queued on any of its streams.
+    void drain() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (Lane& l : lanes)
+            if (l.stream) cudaStreamSynchronize(l.stream);
+        for (auto& w : workers)
+            if (w->stream) cudaStreamSynchronize(w->stream);
+        if (upload_stream) cudaStreamSynchronize(upload_stream);
+        if (download_stream) cudaStreamSynchronize(download_stream);
+    }
+
+    // Lanes start after everything enqueued so far on `from` ...
+    void fork(cudaStream_t from) {
+        check(cudaEventRecord(ev_fork, from), "cudaEventRecord(fork)");
         for (int i = 0; i < lane_count; ++i) check(cudaStreamWaitEvent(lanes[i].stream, ev_fork, 0), "cudaStreamWaitEvent(fork)");
     }
+    void fork() { fork(stream); }
     // ... and the main stream continues after everything the lanes did.
     void join() {
         for (int i = 0; i < lane_count; ++i) {
             check(cudaEventRecord(ev_lane[i], lanes[i].stream), "cudaEventRecord(join)");
             check(cudaStreamWaitEvent(stream, ev_lane[i], 0), "cudaStreamWaitEvent(join)");
-        }
-    }
-
-    // Copies on upload_stream start after everything queued on the main
-    // stream (earlier work may still read the buffer being overwritten).
-    void begin_upload() {
-        check(cudaEventRecord(ev_main, stream), "cudaEventRecord(upload start)");
-        check(cudaStreamWaitEvent(upload_stream, ev_main, 0), "cudaStreamWaitEvent(upload start)");
-    }
-    void frame_uploaded(int source, int frame) {
-        check(cudaEventRecord(frame_ready[source][frame], upload_stream), "cudaEventRecord(frame uploaded)");
-        frames_async[source] = true;
-    }
-    // `s` waits for the uploads of frames [first, last] of every source.
-    void wait_frames(cudaStream_t s, int first, int last) {
-        first = std::max(first, 0);
-        last = std::min(last, frames - 1);
-        for (int src = 0; src < 2; ++src) {
-            if (!frames_async[src]) continue;
-            for (int f = first; f <= last; ++f)
-                check(cudaStreamWaitEvent(s, frame_ready[src][f], 0), "cudaStreamWaitEvent(frame uploaded)");
         }
     }
 
@@ -486,7 +656,21 @@ struct Session {
         const size_t R = G * max_rows;
         const size_t Bmax = static_cast<size_t>(std::min(model_cap, max_rows));
         nmax = static_cast<int>(covariance_possible ? std::max<size_t>(Bmax, dim) : Bmax);
-        if (nmax > 96) fail("VNLB CUDA: eigen problems above 96 x 96 (model rows or covariance dimension) are not supported");
+        if (nmax > 128) fail("VNLB CUDA: eigen problems above 128 x 128 (model rows or covariance dimension) are not supported");
+        {
+            FilterLaunch probe{};
+            probe.dim = dim;
+            probe.rank = p.rank;
+            probe.nmax = nmax;
+            probe.model_cap = model_cap;
+            probe.max_rows = max_rows;
+            probe.stage = stage;
+            const size_t need = filter_shared_bytes(probe);
+            if (need > filter_shared_limit())
+                fail("VNLB CUDA: the group filter needs " + std::to_string(need / 1024) +
+                     " KB of shared memory per block at this dimension, rank and model size (at most " +
+                     std::to_string(filter_shared_limit() / 1024) + " KB)");
+        }
         size_t free_bytes = 0, total_bytes = 0;
         check(cudaMemGetInfo(&free_bytes, &total_bytes), "cudaMemGetInfo");
         const size_t M = G * models;  // models: one per group, or one per plane when uncoupled
@@ -501,6 +685,7 @@ struct Session {
             M * (2 * static_cast<size_t>(dim) + N * N + rank1 + rank1 * N) * sizeof(float) + M * sizeof(int);
         lane_count = static_cast<int>(std::min<size_t>(kMaxLanes, free_bytes / 2 / std::max<size_t>(lane_bytes, 1)));
         if (lane_count < 1) fail("VNLB CUDA: the group buffers of one anchor frame do not fit in device memory");
+        lanes_allocated = lane_count;
         for (int li = 0; li < lane_count; ++li) {
             Lane& l = lanes[li];
             check(cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking), "cudaStreamCreate(lane)");
@@ -535,11 +720,17 @@ struct Session {
         check(cudaStreamCreateWithFlags(&download_stream, cudaStreamNonBlocking), "cudaStreamCreate(download)");
         for (cudaEvent_t* e : {&ev_main, &ev_out, &ev_download})
             check(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
-        for (auto& v : frame_ready) {
-            v.assign(frames, nullptr);
-            for (cudaEvent_t& e : v) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
-        }
-        d_out_frame.allocate(frame_values(), "cudaMalloc(output frame)");
+        // source window and frame stores (derive_geometry, cuda_plugin.cpp:761-773;
+        // initialize_cuda's source slots, :1878-1884)
+        source_window = static_cast<int>(std::min<long long>(
+            frames, 2LL * (p.search_bwd + p.search_fwd + p.patch_time - 1) + 1));
+        ring = std::min(frames, source_window + p.num_streams - 1);
+        workers.resize(static_cast<size_t>(p.num_streams));
+        for (auto& w : workers) w = std::make_unique<Worker>();
+        // pinned staging per worker: 64 MiB of frames, at least two
+        staging_slots = static_cast<int>(std::clamp<size_t>((static_cast<size_t>(64) << 20) /
+                                                                (frame_values() * sizeof(float)),
+                                                            2, static_cast<size_t>(2 * source_window)));
         // aggregation window (prepare_aggregation_window, core.cpp:296-324)
         host_window.assign(static_cast<size_t>(P) * P, 1.0f);
         if (!(p.weight_gamma == 0.0f || P <= 1)) {
@@ -562,12 +753,13 @@ struct Session {
         d_window.allocate(host_window.size(), "cudaMalloc(window)");
         check(cudaMemcpy(d_window.ptr, host_window.data(), host_window.size() * sizeof(float), cudaMemcpyHostToDevice),
               "cudaMemcpy(window)");
-        const int cache_size = slots + lane_count;  // every contributor of a frame, plus the lanes' work in flight
+        // every contributor of a frame, the lanes' work in flight and the
+        // frames of concurrent per-frame calls
+        const int cache_size = std::min(valid_anchor_frames + lane_count, slots + lane_count + p.num_streams - 1);
         for (int i = 0; i < cache_size; ++i) {
             auto entry = std::make_unique<CachedStack>();
             entry->data.allocate(stack_values(), "cudaMalloc(contribution stack)");
             check(cudaEventCreateWithFlags(&entry->ready, cudaEventDisableTiming), "cudaEventCreate");
-            check(cudaEventCreateWithFlags(&entry->released, cudaEventDisableTiming), "cudaEventCreate");
             cache.push_back(std::move(entry));
         }
     }
@@ -721,8 +913,8 @@ struct Session {
     }
 
     void require_sources() {
-        if (!clip_ready) fail("VNLB CUDA: clip frames were not provided");
-        if (stage == 1 && !ref_ready) fail("VNLB CUDA: ref frames were not provided");
+        if (!clip) fail("VNLB CUDA: clip frames were not provided");
+        if (stage == 1 && !ref) fail("VNLB CUDA: ref frames were not provided");
         sync_flow();
     }
 
@@ -784,7 +976,7 @@ struct Session {
     void sync_flow() {
         if (!flow[0].dirty && !flow[1].dirty) return;
         // earlier renders may still read the device copies
-        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize(flow)");
+        drain();
         for (Flow& f : flow) {
             if (!f.dirty) continue;
             if (f.d_usable.count != f.usable.size()) f.d_usable.allocate(f.usable.size(), "cudaMalloc(flow flags)");
@@ -817,20 +1009,92 @@ struct Session {
         return g;
     }
 
-    float* source_buffer(int source) {
-        if (source == VNLBGPU_SOURCE_CLIP) {
-            if (!own_clip.ptr) own_clip.allocate(frame_values() * frames, "cudaMalloc(clip)");
-            clip = own_clip.ptr;
-            return own_clip.ptr;
-        }
-        if (stage != 1) fail("VNLB CUDA: only the Final stage takes a ref clip");
-        if (!own_ref.ptr) own_ref.allocate(frame_values() * frames, "cudaMalloc(ref)");
-        ref = own_ref.ptr;
-        return own_ref.ptr;
+    // The store a source's frames go to, allocated on first use.
+    SourceStore& store_for(int source) {
+        if (source != VNLBGPU_SOURCE_CLIP && source != VNLBGPU_SOURCE_REF)
+            fail("VNLB CUDA: source must be clip (0) or ref (1)");
+        if (source == VNLBGPU_SOURCE_REF && stage != 1) fail("VNLB CUDA: only the Final stage takes a ref clip");
+        SourceStore& st = store[source];
+        if (st.borrowed) fail("VNLB CUDA: this source reads a caller-owned device clip; give frames there");
+        if (!st.own.ptr) reset_store(source);
+        return st;
     }
 
     void invalidate() {
         for (auto& c : cache) c->anchor = -1;
+    }
+
+    // The source frames anchor frame a reads: its shifted temporal window and
+    // the patch_time - 1 frames after it (anchor_source_range,
+    // cuda_plugin.cpp:825-844).
+    void anchor_frames(int a, int& first, int& last) const {
+        int low, high;
+        temporal_range(frames, Pt, params.search_bwd, params.search_fwd, a, low, high);
+        first = low;
+        last = high + Pt - 1;
+    }
+    // contributing_anchors (cuda_plugin.cpp:809-823)
+    void contributors(int n, int& first, int& last) const {
+        first = std::max(0, n - (params.search_fwd + Pt - 1));
+        last = std::min(valid_anchor_frames - 1, n + params.search_bwd);
+    }
+    // required_source_range (cuda_plugin.cpp:846-858): what output frame n may read
+    void required_range(int n, int& first, int& last) const {
+        first = last = n;
+        int a0, a1;
+        contributors(n, a0, a1);
+        for (int a = a0; a <= a1; ++a) {
+            int f0, f1;
+            anchor_frames(a, f0, f1);
+            first = std::min(first, f0);
+            last = std::max(last, f1);
+        }
+    }
+    CachedStack* cached(int anchor) {
+        for (auto& c : cache)
+            if (c->anchor == anchor) return c.get();
+        return nullptr;
+    }
+
+    // Before queueing output frame n (or, with stack_only, anchor frame n's
+    // stack): is a frame it reads still being copied by another call?  Throws
+    // when one is not on the device at all.
+    bool frames_pending(int n, bool stack_only = false) {
+        auto check_range = [&](int f0, int f1, int only) {
+            bool pending = false;
+            for (int src = 0; src < sources(); ++src) {
+                if (only >= 0 && src != only) continue;
+                const SourceStore& st = store[src];
+                if (st.borrowed) continue;
+                if (!st.base) fail(src == 0 ? "VNLB CUDA: clip frames were not provided"
+                                            : "VNLB CUDA: ref frames were not provided");
+                for (int f = std::max(f0, 0); f <= std::min(f1, frames - 1); ++f) {
+                    const FrameSlot& sl = st.slots[static_cast<size_t>(f % ring)];
+                    if (sl.frame != f) fail(missing_frame_message(src, f));
+                    pending |= sl.filling;
+                }
+            }
+            return pending;
+        };
+        bool pending = false;
+        if (stack_only) {
+            if (!cached(n)) {
+                int f0, f1;
+                anchor_frames(n, f0, f1);
+                pending |= check_range(f0, f1, -1);
+            }
+            return pending;
+        }
+        pending |= check_range(n, n, VNLBGPU_SOURCE_CLIP);  // the fallback samples
+        int a0, a1;
+        contributors(n, a0, a1);
+        for (int a = a0; a <= a1; ++a) {
+            if (cached(a)) continue;
+            int f0, f1;
+            anchor_frames(a, f0, f1);
+            pending |= check_range(f0, f1, -1);
+        }
+        return pending;
     }
 
     // One anchor frame on one lane: match -> paste mask -> filter -> stack
@@ -842,7 +1106,7 @@ struct Session {
         // schedule (compute_temporal_range / schedule_temporal_range)
         int low, high;
         temporal_range(frames, Pt, params.search_bwd, params.search_fwd, anchor, low, high);
-        wait_frames(ls, low, high + Pt - 1);  // every sample the anchor frame reads
+        wait_frames(ls, low, high + Pt - 1);  // every sample the anchor frame reads is on the device
         int schedule[kMaxContributors];
         int schedule_len = 0;
         schedule[schedule_len++] = anchor;
@@ -855,6 +1119,7 @@ struct Session {
         m.height = height;
         m.channels = channels;
         m.frames = frames;
+        m.ring = ring;
         m.search_channels = search_channels;
         m.P = P;
         m.Pt = Pt;
@@ -944,6 +1209,7 @@ struct Session {
         FilterLaunch fl{};
         fl.noisy = clip;
         fl.basic = ref;
+        fl.ring = ring;
         fl.width = width;
         fl.height = height;
         fl.channels = channels;
@@ -1019,6 +1285,7 @@ struct Session {
         t0 = begin_timed(ls);
         check(launch_tiles(tl, ls), "tile kernel launch");
         end_timed(kTimedTiles, t0, ls);
+        read_frames(ls, low, high + Pt - 1);
         stats.anchor_frames += 1;
         stats.groups += G;
         stats.kernel_launches += params.rank > 0 ? 6 : 5;
@@ -1027,32 +1294,31 @@ struct Session {
     // The stack of `anchor`, computed on the next lane when not cached.  The
     // returned slot's `ready` event marks the end of its production.
     CachedStack* stack_for(int anchor, int* lane_used = nullptr) {
-        for (auto& c : cache)
-            if (c->anchor == anchor) {
-                c->last_use = ++use_clock;
-                return c.get();
-            }
+        if (CachedStack* c = cached(anchor)) {
+            c->last_use = ++use_clock;
+            return c;
+        }
         CachedStack* victim = cache.front().get();
         for (auto& c : cache)
             if (c->last_use < victim->last_use) victim = c.get();
-        victim->anchor = anchor;
-        victim->last_use = ++use_clock;
         const int li = next_lane;
         next_lane = (next_lane + 1) % lane_count;
         Lane& lane = lanes[li];
-        if (victim->pending_release)  // its previous contents are still being read
-            check(cudaStreamWaitEvent(lane.stream, victim->released, 0), "cudaStreamWaitEvent(stack release)");
-        victim->pending_release = false;
+        wait_reads(lane.stream, victim->reads);  // its previous contents may still be read
+        victim->anchor = -1;                     // until the work below is queued
         compute_anchor(anchor, victim->data.ptr, lane);
         check(cudaEventRecord(victim->ready, lane.stream), "cudaEventRecord(stack ready)");
+        victim->anchor = anchor;
+        victim->last_use = ++use_clock;
         if (lane_used) *lane_used = li;
         return victim;
     }
 
     // vnlbcu.Basic/Final frame n: normalise over the contributing anchors
     // (contributing_anchors, cuda_plugin.cpp:809-823; render_aggregate_frame
-    // order: anchors first..last).  Call between fork() and join().
-    void render_to_device(int n, float* out) {
+    // order: anchors first..last), on `on`.  The lanes' hazards are ordered by
+    // events, so `on` can be the main stream or a worker's.
+    void render_to_device(int n, float* out, cudaStream_t on) {
         const int first = std::max(0, n - (params.search_fwd + Pt - 1));
         const int last = std::min(frames - 1, n + params.search_bwd);
         NormalizeLaunch nl{};
@@ -1070,18 +1336,67 @@ struct Session {
             ++nl.count;
         }
         for (int i = 0; i < nl.count; ++i)
-            check(cudaStreamWaitEvent(stream, used[i]->ready, 0), "cudaStreamWaitEvent(stack ready)");
-        wait_frames(stream, n, n);
-        nl.source = clip + static_cast<size_t>(n) * frame_values();
-        nl.out = out;
-        cudaEvent_t t0 = begin_timed(stream);
-        check(launch_normalize(nl, stream), "normalize kernel launch");
-        end_timed(kTimedNormalize, t0, stream);
-        for (int i = 0; i < nl.count; ++i) {
-            check(cudaEventRecord(used[i]->released, stream), "cudaEventRecord(stack release)");
-            used[i]->pending_release = true;
+            check(cudaStreamWaitEvent(on, used[i]->ready, 0), "cudaStreamWaitEvent(stack ready)");
+        if (!store[0].borrowed) {
+            const FrameSlot& sl = store[0].slots[static_cast<size_t>(n % ring)];
+            if (sl.frame != n || sl.filling) fail(missing_frame_message(0, n));
+            if (sl.copied) check(cudaStreamWaitEvent(on, sl.ready, 0), "cudaStreamWaitEvent(frame copied)");
         }
+        nl.source = frame_ptr(VNLBGPU_SOURCE_CLIP, n);
+        nl.out = out;
+        cudaEvent_t t0 = begin_timed(on);
+        check(launch_normalize(nl, on), "normalize kernel launch");
+        end_timed(kTimedNormalize, t0, on);
+        ReadEvent r = record_read(on);
+        for (int i = 0; i < nl.count; ++i) {
+            prune_reads(used[i]->reads);
+            used[i]->reads.push_back(r);
+        }
+        read_frames(on, n, n, VNLBGPU_SOURCE_CLIP);
         stats.kernel_launches += 1;
+    }
+    void render_to_device(int n, float* out) { render_to_device(n, out, stream); }
+
+    // Leases a worker, waiting while all num_streams are busy; its stream,
+    // buffers and pinned staging are made on first use.
+    Worker& acquire_worker(std::unique_lock<std::mutex>& lk) {
+        for (;;) {
+            for (auto& wp : workers) {
+                Worker& w = *wp;
+                if (w.busy) continue;
+                w.busy = true;
+                try {
+                    if (!w.stream) {
+                        check(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking), "cudaStreamCreate(worker)");
+                        check(cudaEventCreateWithFlags(&w.done, cudaEventDisableTiming), "cudaEventCreate");
+                    }
+                    if (!w.out.ptr) w.out.allocate(frame_values(), "cudaMalloc(output frame)");
+                    if (!w.host_out)
+                        check(cudaMallocHost(reinterpret_cast<void**>(&w.host_out), frame_values() * sizeof(float)),
+                              "cudaMallocHost(output frame)");
+                    if (!w.host_status)
+                        check(cudaMallocHost(reinterpret_cast<void**>(&w.host_status), sizeof(int)),
+                              "cudaMallocHost(status)");
+                } catch (...) {
+                    w.busy = false;
+                    throw;
+                }
+                return w;
+            }
+            changed.wait(lk);
+        }
+    }
+    // Makes a worker's first `count` pinned staging frames.
+    void ensure_staging(Worker& w, int count) {
+        while (static_cast<int>(w.staging.size()) < count) {
+            float* p = nullptr;
+            check(cudaMallocHost(reinterpret_cast<void**>(&p), frame_values() * sizeof(float)), "cudaMallocHost(staging)");
+            w.staging.push_back(p);
+            cudaEvent_t e;
+            check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+            w.staged.push_back(e);
+            w.staged_used.push_back(false);
+        }
     }
 
     void check_status() {
@@ -1098,6 +1413,157 @@ struct Session {
         }
     }
 };
+
+void Session::queue_copy(int source, int f, const float* host_frame, cudaStream_t on) {
+    SourceStore& st = store[source];
+    const int j = f % ring;
+    FrameSlot& sl = st.slots[static_cast<size_t>(j)];
+    wait_reads(on, sl.reads);  // the previous frame's readers
+    const size_t bytes = frame_values() * sizeof(float);
+    float* dst = st.own.ptr + static_cast<size_t>(j) * frame_values();
+    check(cudaMemcpyAsync(dst, host_frame, bytes, cudaMemcpyHostToDevice, on), "cudaMemcpyAsync(frame upload)");
+    if (ring < frames && j < Pt - 1)  // the slots after the last repeat the first ones
+        check(cudaMemcpyAsync(st.own.ptr + static_cast<size_t>(ring + j) * frame_values(), dst, bytes,
+                              cudaMemcpyDeviceToDevice, on),
+              "cudaMemcpyAsync(frame mirror)");
+    check(cudaEventRecord(sl.ready, on), "cudaEventRecord(frame copied)");
+    sl.frame = f;
+    sl.copied = true;
+    sl.filling = false;
+    stats_uploads += 1;
+}
+
+namespace {
+
+// A leased worker, given back (under the session lock) when it goes out of
+// scope.  Declare it before the call's unique_lock, so that the lock is
+// released first.
+struct WorkerLease {
+    Session& s;
+    Session::Worker* w = nullptr;
+    explicit WorkerLease(Session& session) : s(session) {}
+    WorkerLease(const WorkerLease&) = delete;
+    WorkerLease& operator=(const WorkerLease&) = delete;
+    ~WorkerLease() {
+        if (!w) return;
+        std::lock_guard guard(s.lock);
+        w->busy = false;
+        s.changed.notify_all();
+    }
+};
+
+// The source frames one call gives (vnlbgpu_render_frame_window,
+// vnlbgpu_set_frame): claimed all at once (the reference's atomic window
+// acquisition, FrameCache::acquire), copied through the worker's pinned
+// staging, and held until the call's reads are queued.  Frames already on the
+// device are only held.
+struct FrameClaim {
+    struct Given {
+        int source, frame;
+        const float* const* planes;
+        const ptrdiff_t* strides;
+    };
+    Session& s;
+    std::vector<Given> given;
+    std::vector<size_t> fills;  // indices into `given` this call copies
+    bool held = false;
+    explicit FrameClaim(Session& session) : s(session) {}
+    FrameClaim(const FrameClaim&) = delete;
+    FrameClaim& operator=(const FrameClaim&) = delete;
+    ~FrameClaim() {
+        if (!held) return;
+        std::lock_guard guard(s.lock);
+        release_locked();
+    }
+
+    Session::FrameSlot& slot(const Given& g) {
+        return s.store[g.source].slots[static_cast<size_t>(g.frame % s.ring)];
+    }
+
+    // Waits until no frame of `given` needs a slot that another call holds
+    // for a different frame, then holds them all.
+    void take(std::unique_lock<std::mutex>& lk) {
+        for (const Given& g : given) s.store_for(g.source);
+        for (;;) {
+            bool conflict = false;
+            for (const Given& g : given) {
+                const Session::FrameSlot& sl = slot(g);
+                if (sl.frame != g.frame && sl.pins > 0) conflict = true;
+            }
+            if (!conflict) break;
+            s.changed.wait(lk);
+        }
+        for (size_t i = 0; i < given.size(); ++i) {
+            Session::FrameSlot& sl = slot(given[i]);
+            sl.pins += 1;
+            if (sl.frame != given[i].frame) {
+                sl.frame = given[i].frame;
+                sl.copied = false;
+                sl.filling = true;
+                fills.push_back(i);
+            }
+        }
+        held = true;
+    }
+
+    // Copies the claimed frames: host copies into pinned staging with the
+    // lock released, device copies queued on the worker's stream under it.
+    void copy(std::unique_lock<std::mutex>& lk, Session::Worker& w) {
+        const int W = s.width, H = s.height, C = s.channels;
+        const size_t plane = static_cast<size_t>(W) * H;
+        for (size_t i0 = 0; i0 < fills.size(); i0 += static_cast<size_t>(s.staging_slots)) {
+            const size_t i1 = std::min(fills.size(), i0 + static_cast<size_t>(s.staging_slots));
+            s.ensure_staging(w, static_cast<int>(i1 - i0));
+            lk.unlock();
+            for (size_t i = i0; i < i1; ++i) {
+                const size_t k = i - i0;
+                // the device copy out of this staging frame's previous contents
+                if (w.staged_used[k]) vnlbgpu::check(cudaEventSynchronize(w.staged[k]), "cudaEventSynchronize(staging)");
+                const Given& g = given[fills[i]];
+                float* dst = w.staging[k];
+                for (int c = 0; c < C; ++c) {
+                    const char* src = reinterpret_cast<const char*>(g.planes[c]);
+                    float* d = dst + static_cast<size_t>(c) * plane;
+                    if (g.strides[c] == static_cast<ptrdiff_t>(W * sizeof(float))) {
+                        std::memcpy(d, src, plane * sizeof(float));
+                    } else {
+                        for (int y = 0; y < H; ++y)
+                            std::memcpy(d + static_cast<size_t>(y) * W, src + static_cast<size_t>(y) * g.strides[c],
+                                        static_cast<size_t>(W) * sizeof(float));
+                    }
+                }
+            }
+            lk.lock();
+            for (size_t i = i0; i < i1; ++i) {
+                const Given& g = given[fills[i]];
+                s.queue_copy(g.source, g.frame, w.staging[i - i0], w.stream);
+                const size_t k = i - i0;
+                vnlbgpu::check(cudaEventRecord(w.staged[k], w.stream), "cudaEventRecord(staging)");
+                w.staged_used[k] = true;
+            }
+            s.changed.notify_all();
+        }
+    }
+
+    // Under the session lock: stop holding the frames; a claimed frame whose
+    // copy was never queued leaves its slot empty.
+    void release_locked() {
+        if (!held) return;
+        for (size_t i : fills) {
+            Session::FrameSlot& sl = slot(given[i]);
+            if (sl.filling && sl.frame == given[i].frame) {
+                sl.filling = false;
+                sl.frame = -1;
+                sl.copied = false;
+            }
+        }
+        for (const Given& g : given) slot(g).pins -= 1;
+        held = false;
+        s.changed.notify_all();
+    }
+};
+
+}  // namespace
 
 }  // namespace vnlbgpu
 
@@ -1119,29 +1585,6 @@ template <typename Fn> int guarded(Fn&& fn) {
     } catch (...) {
         vnlbgpu::g_last_error = "VNLB CUDA: unknown failure";
         return -1;
-    }
-}
-
-void copy_planes_in(float* device_frame, const float* const* planes, const ptrdiff_t* strides, int width,
-                    int height, int channels, cudaStream_t stream) {
-    for (int c = 0; c < channels; ++c) {
-        vnlbgpu::check(cudaMemcpy2DAsync(device_frame + static_cast<size_t>(c) * width * height,
-                                         static_cast<size_t>(width) * sizeof(float), planes[c],
-                                         static_cast<size_t>(strides[c]), static_cast<size_t>(width) * sizeof(float),
-                                         height, cudaMemcpyHostToDevice, stream),
-                       "cudaMemcpy2DAsync(frame upload)");
-    }
-}
-
-void copy_planes_out(const float* device_frame, float* const* planes, const ptrdiff_t* strides, int width,
-                     int height, int channels, cudaStream_t stream) {
-    for (int c = 0; c < channels; ++c) {
-        vnlbgpu::check(cudaMemcpy2DAsync(planes[c], static_cast<size_t>(strides[c]),
-                                         device_frame + static_cast<size_t>(c) * width * height,
-                                         static_cast<size_t>(width) * sizeof(float),
-                                         static_cast<size_t>(width) * sizeof(float), height, cudaMemcpyDeviceToHost,
-                                         stream),
-                       "cudaMemcpy2DAsync(frame download)");
     }
 }
 
@@ -1171,20 +1614,22 @@ void vnlbgpu_destroy(vnlbgpu_session* session) {
 int vnlbgpu_set_frame(vnlbgpu_session* session, int source, int frame, const float* const* planes,
                       const ptrdiff_t* strides) {
     return guarded([&]() {
+        if (!session || !planes || !strides) vnlbgpu::fail("VNLB CUDA: null argument");
         Session& s = session->impl;
-        std::lock_guard guard(s.lock);
+        vnlbgpu::WorkerLease lease(s);
+        vnlbgpu::FrameClaim claim(s);
+        std::unique_lock lk(s.lock);
         if (frame < 0 || frame >= s.frames) vnlbgpu::fail("VNLB CUDA: frame index out of range");
         for (int c = 0; c < s.channels; ++c)
             if (strides[c] < static_cast<ptrdiff_t>(s.width * sizeof(float)))
                 vnlbgpu::fail("VNLB CUDA: unsupported frame stride");
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
-        float* base = s.source_buffer(source);
-        s.begin_upload();
-        copy_planes_in(base + static_cast<size_t>(frame) * s.frame_values(), planes, strides, s.width, s.height,
-                       s.channels, s.upload_stream);
-        s.frame_uploaded(source, frame);
-        if (source == VNLBGPU_SOURCE_CLIP) s.clip_ready = true; else s.ref_ready = true;
-        s.invalidate();
+        s.store_for(source);
+        lease.w = &s.acquire_worker(lk);
+        claim.given.push_back({source, frame, planes, strides});
+        claim.take(lk);
+        claim.copy(lk, *lease.w);
+        claim.release_locked();
     });
 }
 
@@ -1193,17 +1638,20 @@ int vnlbgpu_set_clip_host(vnlbgpu_session* session, int source, const float* cli
         Session& s = session->impl;
         std::lock_guard guard(s.lock);
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
-        float* base = s.source_buffer(source);
-        // one copy per frame, so that anchor frames start as their frames land
-        s.begin_upload();
-        const size_t fv = s.frame_values();
-        for (int f = 0; f < s.frames; ++f) {
-            vnlbgpu::check(cudaMemcpyAsync(base + fv * f, clip + fv * f, fv * sizeof(float), cudaMemcpyHostToDevice,
-                                           s.upload_stream),
-                           "cudaMemcpyAsync(clip upload)");
-            s.frame_uploaded(source, f);
+        if (source == VNLBGPU_SOURCE_CLIP || source == VNLBGPU_SOURCE_REF) {
+            if (source == VNLBGPU_SOURCE_REF && s.stage != 1) vnlbgpu::fail("VNLB CUDA: only the Final stage takes a ref clip");
+            for (const auto& sl : s.store[source].slots)
+                if (sl.pins > 0) vnlbgpu::fail("VNLB CUDA: a whole clip cannot replace frames that calls in flight hold");
         }
-        if (source == VNLBGPU_SOURCE_CLIP) s.clip_ready = true; else s.ref_ready = true;
+        s.make_whole();
+        if (s.store[source].borrowed) {  // was a caller's device clip: take an own store again
+            s.store[source].borrowed = false;
+            s.store[source].base = nullptr;
+        }
+        s.store_for(source);
+        // one copy per frame, so that anchor frames start as their frames land
+        const size_t fv = s.frame_values();
+        for (int f = 0; f < s.frames; ++f) s.queue_copy(source, f, clip + fv * f, s.upload_stream);
         s.invalidate();
     });
 }
@@ -1212,41 +1660,148 @@ int vnlbgpu_set_clip_device(vnlbgpu_session* session, int source, const float* d
     return guarded([&]() {
         Session& s = session->impl;
         std::lock_guard guard(s.lock);
-        if (source == VNLBGPU_SOURCE_CLIP) {
-            s.clip = device_clip;
-            s.clip_ready = true;
-            s.frames_async[0] = false;
-        } else {
-            if (s.stage != 1) vnlbgpu::fail("VNLB CUDA: only the Final stage takes a ref clip");
-            s.ref = device_clip;
-            s.ref_ready = true;
-            s.frames_async[1] = false;
-        }
+        if (source != VNLBGPU_SOURCE_CLIP && source != VNLBGPU_SOURCE_REF)
+            vnlbgpu::fail("VNLB CUDA: source must be clip (0) or ref (1)");
+        if (source == VNLBGPU_SOURCE_REF && s.stage != 1) vnlbgpu::fail("VNLB CUDA: only the Final stage takes a ref clip");
+        for (const auto& sl : s.store[source].slots)
+            if (sl.pins > 0) vnlbgpu::fail("VNLB CUDA: a whole clip cannot replace frames that calls in flight hold");
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.make_whole();
+        s.drain();
+        Session::SourceStore& st = s.store[source];
+        st.own.release();
+        st.slots.clear();
+        st.borrowed = true;
+        st.base = device_clip;
+        if (source == VNLBGPU_SOURCE_CLIP) s.clip = device_clip; else s.ref = device_clip;
         s.invalidate();
     });
 }
 
-int vnlbgpu_render_frame(vnlbgpu_session* session, int n, float* const* planes, const ptrdiff_t* strides) {
+int vnlbgpu_required_source_range(vnlbgpu_session* session, int n, int* first, int* last) {
     return guarded([&]() {
+        if (!session || !first || !last) vnlbgpu::fail("VNLB CUDA: null argument");
         Session& s = session->impl;
-        std::lock_guard guard(s.lock);
         if (n < 0 || n >= s.frames) vnlbgpu::fail("VNLB CUDA: frame index out of range");
-        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
-        s.require_sources();
-        s.fork();
-        s.render_to_device(n, s.d_out_frame.ptr);
-        s.join();
-        copy_planes_out(s.d_out_frame.ptr, planes, strides, s.width, s.height, s.channels, s.stream);
-        s.check_status();
+        s.required_range(n, *first, *last);
     });
 }
+
+namespace {
+
+// The per-frame render shared by vnlbgpu_render_frame and
+// vnlbgpu_render_frame_window: queue under the lock on the worker's stream,
+// wait with the lock released, copy out.
+void render_one(Session& s, int n, int first, int count, const float* const* clip_planes,
+                const ptrdiff_t* clip_strides, const float* const* ref_planes, const ptrdiff_t* ref_strides,
+                float* const* planes, const ptrdiff_t* strides) {
+    if (!planes || !strides) vnlbgpu::fail("VNLB CUDA: null argument");
+    vnlbgpu::WorkerLease lease(s);
+    vnlbgpu::FrameClaim claim(s);
+    std::unique_lock lk(s.lock);
+    if (n < 0 || n >= s.frames) vnlbgpu::fail("VNLB CUDA: frame index out of range");
+    vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+    if (count > 0) {
+        if (!clip_planes || !clip_strides || (s.stage == 1 && (!ref_planes || !ref_strides)))
+            vnlbgpu::fail("VNLB CUDA: null argument");
+        if (first < 0 || first + count > s.frames) vnlbgpu::fail("VNLB CUDA: source frame range outside the clip");
+        if (count > s.ring)
+            vnlbgpu::fail("VNLB CUDA: " + std::to_string(count) + " source frames exceed the " +
+                          std::to_string(s.ring) + " frame slots of the session");
+        for (int i = 0; i < count * s.channels; ++i)
+            if (clip_strides[i] < static_cast<ptrdiff_t>(s.width * sizeof(float)) ||
+                (s.stage == 1 && ref_strides[i] < static_cast<ptrdiff_t>(s.width * sizeof(float))))
+                vnlbgpu::fail("VNLB CUDA: unsupported frame stride");
+        for (int i = 0; i < count; ++i) {
+            const size_t k = static_cast<size_t>(i) * s.channels;
+            claim.given.push_back({VNLBGPU_SOURCE_CLIP, first + i, clip_planes + k, clip_strides + k});
+            if (s.stage == 1) claim.given.push_back({VNLBGPU_SOURCE_REF, first + i, ref_planes + k, ref_strides + k});
+        }
+    }
+    lease.w = &s.acquire_worker(lk);
+    Session::Worker& w = *lease.w;
+    if (count > 0) {
+        claim.take(lk);
+        claim.copy(lk, w);
+    }
+    s.require_sources();
+    while (s.frames_pending(n)) s.changed.wait(lk);
+    s.render_to_device(n, w.out.ptr, w.stream);
+    vnlbgpu::check(cudaMemcpyAsync(w.host_out, w.out.ptr, s.frame_values() * sizeof(float), cudaMemcpyDeviceToHost,
+                                   w.stream),
+                   "cudaMemcpyAsync(frame download)");
+    vnlbgpu::check(cudaMemcpyAsync(w.host_status, s.d_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, w.stream),
+                   "cudaMemcpyAsync(status)");
+    vnlbgpu::check(cudaEventRecord(w.done, w.stream), "cudaEventRecord(frame done)");
+    claim.release_locked();
+    lk.unlock();
+    vnlbgpu::check(cudaEventSynchronize(w.done), "cudaEventSynchronize(frame done)");
+    const size_t plane = s.plane();
+    for (int c = 0; c < s.channels; ++c) {
+        const float* src = w.host_out + static_cast<size_t>(c) * plane;
+        char* dst = reinterpret_cast<char*>(planes[c]);
+        if (strides[c] == static_cast<ptrdiff_t>(s.width * sizeof(float))) {
+            std::memcpy(dst, src, plane * sizeof(float));
+        } else {
+            for (int y = 0; y < s.height; ++y)
+                std::memcpy(dst + static_cast<size_t>(y) * strides[c], src + static_cast<size_t>(y) * s.width,
+                            static_cast<size_t>(s.width) * sizeof(float));
+        }
+    }
+    if (*w.host_status != 0) {
+        lk.lock();
+        s.check_status();  // resets the status word and raises its message
+    }
+}
+
+}  // namespace
+
+int vnlbgpu_render_frame(vnlbgpu_session* session, int n, float* const* planes, const ptrdiff_t* strides) {
+    return guarded([&]() {
+        if (!session) vnlbgpu::fail("VNLB CUDA: null argument");
+        for (int c = 0; planes && strides && c < session->impl.channels; ++c)
+            if (strides[c] < static_cast<ptrdiff_t>(session->impl.width * sizeof(float)))
+                vnlbgpu::fail("VNLB CUDA: unsupported frame stride");
+        render_one(session->impl, n, 0, 0, nullptr, nullptr, nullptr, nullptr, planes, strides);
+    });
+}
+
+int vnlbgpu_render_frame_window(vnlbgpu_session* session, int n, int first, int count,
+                                const float* const* clip_planes, const ptrdiff_t* clip_strides,
+                                const float* const* ref_planes, const ptrdiff_t* ref_strides, float* const* planes,
+                                const ptrdiff_t* strides) {
+    return guarded([&]() {
+        if (!session) vnlbgpu::fail("VNLB CUDA: null argument");
+        for (int c = 0; planes && strides && c < session->impl.channels; ++c)
+            if (strides[c] < static_cast<ptrdiff_t>(session->impl.width * sizeof(float)))
+                vnlbgpu::fail("VNLB CUDA: unsupported frame stride");
+        render_one(session->impl, n, first, count, clip_planes, clip_strides, ref_planes, ref_strides, planes,
+                   strides);
+    });
+}
+
+namespace {
+
+// Whole-clip renders read every frame: wait while another call still copies
+// one, and raise if one is missing.
+void require_all_frames(Session& s, std::unique_lock<std::mutex>& lk) {
+    for (;;) {
+        bool pending = false;
+        for (int n = 0; n < s.frames; ++n) pending |= s.frames_pending(n);
+        if (!pending) return;
+        s.changed.wait(lk);
+    }
+}
+
+}  // namespace
 
 int vnlbgpu_render_clip_device(vnlbgpu_session* session, float* device_out) {
     return guarded([&]() {
         Session& s = session->impl;
-        std::lock_guard guard(s.lock);
+        std::unique_lock lk(s.lock);
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
         s.require_sources();
+        require_all_frames(s, lk);
         s.fork();
         for (int n = 0; n < s.frames; ++n) s.render_to_device(n, device_out + static_cast<size_t>(n) * s.frame_values());
         s.join();
@@ -1256,11 +1811,12 @@ int vnlbgpu_render_clip_device(vnlbgpu_session* session, float* device_out) {
 int vnlbgpu_render_clip_host(vnlbgpu_session* session, float* out) {
     return guarded([&]() {
         Session& s = session->impl;
-        std::lock_guard guard(s.lock);
+        std::unique_lock lk(s.lock);
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.require_sources();
+        require_all_frames(s, lk);
         if (!s.d_pack.ptr || s.d_pack.count < s.frame_values() * s.frames)
             s.d_pack.allocate(s.frame_values() * s.frames, "cudaMalloc(clip output)");
-        s.require_sources();
         // Pinned output: each frame goes down on the download stream as soon
         // as it is normalised.  Pageable output: a copy into pageable memory
         // holds the calling thread, so everything is enqueued first and the
@@ -1309,23 +1865,23 @@ int vnlbgpu_synchronize(vnlbgpu_session* session) {
 int vnlbgpu_render_stack(vnlbgpu_session* session, int n, float* const* planes, const ptrdiff_t* strides) {
     return guarded([&]() {
         Session& s = session->impl;
-        std::lock_guard guard(s.lock);
+        std::unique_lock lk(s.lock);
         if (n < 0 || n >= s.frames) vnlbgpu::fail("VNLB CUDA: frame index out of range");
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
         s.require_sources();
         const size_t packed = static_cast<size_t>(s.channels) * s.slots * 2 * s.plane();
-        if (!s.d_pack.ptr || s.d_pack.count < packed) s.d_pack.allocate(std::max(packed, s.frame_values() * s.frames), "cudaMalloc(stack pack)");
+        if (!s.d_pack.ptr || s.d_pack.count < packed) s.d_pack.allocate(packed, "cudaMalloc(stack pack)");
         if (n > s.frames - s.Pt) {
             vnlbgpu::check(cudaMemsetAsync(s.d_pack.ptr, 0, packed * sizeof(float), s.stream), "cudaMemsetAsync(stack)");
         } else {
+            while (s.frames_pending(n, true)) s.changed.wait(lk);
             s.fork();
             Session::CachedStack* c = s.stack_for(n);
             vnlbgpu::check(cudaStreamWaitEvent(s.stream, c->ready, 0), "cudaStreamWaitEvent(stack ready)");
             vnlbgpu::check(vnlbgpu::launch_pack_stack(c->data.ptr, s.width, s.height, s.channels, s.slots, s.d_pack.ptr,
                                                       s.stream),
                            "pack kernel launch");
-            vnlbgpu::check(cudaEventRecord(c->released, s.stream), "cudaEventRecord(stack release)");
-            c->pending_release = true;
+            c->reads.push_back(s.record_read(s.stream));
             s.join();
         }
         const int rows = s.slots * 2 * s.height;
@@ -1459,6 +2015,56 @@ int vnlbgpu_set_mvtools_frame(vnlbgpu_session* session, int direction, int frame
     });
 }
 
+int vnlbgpu_shard_plan(int frames, int world, int rank, int basic_search_bwd, int basic_search_fwd,
+                       int basic_patch_time, int final_search_bwd, int final_search_fwd, int final_patch_time,
+                       int out[2], int basic[2], int source[2]) {
+    return guarded([&]() {
+        if (!out || !basic || !source) vnlbgpu::fail("VNLB CUDA: null argument");
+        if (frames <= 0 || world <= 0 || rank < 0 || rank >= world)
+            vnlbgpu::fail("VNLB CUDA: shard plan needs frames > 0 and 0 <= rank < world");
+        if (basic_patch_time <= 0 || final_patch_time <= 0 || basic_patch_time > frames || final_patch_time > frames ||
+            basic_search_bwd < 0 || basic_search_fwd < 0 || final_search_bwd < 0 || final_search_fwd < 0)
+            vnlbgpu::fail("VNLB CUDA: patch_time must fit inside the clip and the search radii must be non-negative");
+        // required_source_range of one stage (cuda_plugin.cpp:809-858)
+        auto required = [frames](int sb, int sf, int pt, int n, int& lo, int& hi) {
+            const int valid = frames - pt + 1;
+            lo = hi = n;
+            const int a0 = std::max(0, n - (sf + pt - 1));
+            const int a1 = std::min(valid - 1, n + sb);
+            for (int a = a0; a <= a1; ++a) {
+                int low, high;
+                vnlbgpu::temporal_range(frames, pt, sb, sf, a, low, high);
+                lo = std::min(lo, low);
+                hi = std::max(hi, high + pt - 1);
+            }
+        };
+        const long long o0 = static_cast<long long>(rank) * frames / world;
+        const long long o1 = static_cast<long long>(rank + 1) * frames / world - 1;
+        out[0] = out[1] = basic[0] = basic[1] = source[0] = source[1] = -1;
+        if (o1 < o0) return;
+        out[0] = static_cast<int>(o0);
+        out[1] = static_cast<int>(o1);
+        int b0 = out[0], b1 = out[1];
+        for (int n = out[0]; n <= out[1]; ++n) {
+            int lo, hi;
+            required(final_search_bwd, final_search_fwd, final_patch_time, n, lo, hi);
+            b0 = std::min(b0, lo);
+            b1 = std::max(b1, hi);
+        }
+        basic[0] = b0;
+        basic[1] = b1;
+        int s0 = b0, s1 = b1;
+        for (int m = b0; m <= b1; ++m) {
+            int lo, hi;
+            required(basic_search_bwd, basic_search_fwd, basic_patch_time, m, lo, hi);
+            s0 = std::min(s0, lo);
+            s1 = std::max(s1, hi);
+        }
+        source[0] = s0;
+        source[1] = s1;
+    });
+}
+
 int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats) {
     return guarded([&]() {
         if (!session || !stats) vnlbgpu::fail("VNLB CUDA: null argument");
@@ -1472,6 +2078,8 @@ int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats) {
         s.stats.active_groups = static_cast<long long>(totals[0]);
         s.stats.rows = static_cast<long long>(totals[1]);
         s.stats.pipeline_lanes = s.lane_count;
+        s.stats.source_slots = s.ring;
+        s.stats.source_uploads = s.stats_uploads;
         *stats = s.stats;
     });
 }
@@ -1504,6 +2112,18 @@ int vnlbgpu_diag_kernel_timing(vnlbgpu_session* session, int enable, double* ms,
             s.kernel_count[i] = 0;
         }
         s.timing = enable != 0;
+    });
+}
+
+int vnlbgpu_diag_set_lanes(vnlbgpu_session* session, int lanes) {
+    return guarded([&]() {
+        if (!session) vnlbgpu::fail("VNLB CUDA: null argument");
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.drain();
+        s.lane_count = lanes <= 0 ? s.lanes_allocated : std::min(lanes, s.lanes_allocated);
+        s.next_lane = 0;
     });
 }
 

@@ -29,9 +29,15 @@ struct Strip {
     int region_h;
 };
 
+// Source frames on the device: frame f of a source lives in slot f % ring of
+// a store of ring + patch_time - 1 frame slots [slot][channels][H][W], whose
+// last patch_time - 1 slots repeat the first ones, so that the patch_time
+// consecutive frames of a patch are consecutive slots.  ring = frames for a
+// whole resident clip.
 struct MatchLaunch {
-    const float* video;   // search source [frames][channels][H][W]
+    const float* video;   // search source, frame slots as above
     int width, height, channels, frames;
+    int ring;             // frame slots of the source store (f -> f % ring)
     int search_channels;  // channels compared (1 = first plane only)
     int P, Pt, search_window;
     int K, soft_cap, max_rows;
@@ -148,8 +154,9 @@ cudaError_t launch_paste(const PasteLaunch& L, cudaStream_t stream);
 cudaError_t launch_anchor_map(const int2* anchors, int count, int width, int* map, cudaStream_t stream);
 
 struct FilterLaunch {
-    const float* noisy;     // [frames][C][H][W]
-    const float* basic;     // Final only
+    const float* noisy;     // frame slots [slot][C][H][W] (MatchLaunch)
+    const float* basic;     // Final only, the same slots
+    int ring;               // frame slots of both stores (f -> f % ring)
     int width, height, channels;
     int stage;
     int P, Pt, patch_dim, dim;
@@ -186,6 +193,12 @@ constexpr int kGroupSkip = 2;  // rank not covered: reported through the status 
 // Three launches: prepare (equality, flat flag, means, Gram), batched Jacobi,
 // and apply (basis, coefficients, weights, reconstruction).
 cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t stream);
+
+// The most dynamic shared memory one CTA of the three filter kernels asks for
+// at this shape (dim, rank, nmax, model rows, stage), and the most a CTA may
+// have; a shape above the limit cannot be filtered.
+size_t filter_shared_bytes(const FilterLaunch& L);
+size_t filter_shared_limit();
 
 struct TileLaunch {
     int width, height, channels;

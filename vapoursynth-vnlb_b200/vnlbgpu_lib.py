@@ -43,7 +43,8 @@ class Params(ctypes.Structure):
 
 class Stats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_longlong) for name in
-                ("anchor_frames", "groups", "active_groups", "rows", "kernel_launches", "pipeline_lanes")]
+                ("anchor_frames", "groups", "active_groups", "rows", "kernel_launches", "pipeline_lanes",
+                 "source_slots", "source_uploads")]
 
 
 class MVToolsAnalysis(ctypes.Structure):
@@ -64,13 +65,14 @@ class DiagRow(ctypes.Structure):
 
 EXPORTS = [
     "vnlbgpu_last_error", "vnlbgpu_create", "vnlbgpu_destroy", "vnlbgpu_set_frame",
-    "vnlbgpu_set_clip_host", "vnlbgpu_set_clip_device", "vnlbgpu_render_frame",
+    "vnlbgpu_set_clip_host", "vnlbgpu_set_clip_device", "vnlbgpu_required_source_range",
+    "vnlbgpu_render_frame", "vnlbgpu_render_frame_window",
     "vnlbgpu_render_clip_host", "vnlbgpu_render_clip_device", "vnlbgpu_synchronize",
     "vnlbgpu_render_stack", "vnlbgpu_aggregate", "vnlbgpu_aggregate_frame_noalloc", "vnlbgpu_get_stats",
     "vnlbgpu_stream",
-    "vnlbgpu_set_stream", "vnlbgpu_diag_anchor", "vnlbgpu_diag_kernel_timing",
+    "vnlbgpu_set_stream", "vnlbgpu_diag_anchor", "vnlbgpu_diag_kernel_timing", "vnlbgpu_diag_set_lanes",
     "vnlbgpu_parse_mvtools_analysis", "vnlbgpu_parse_mvtools_vectors", "vnlbgpu_set_mvtools_analysis",
-    "vnlbgpu_set_mvtools_frame",
+    "vnlbgpu_set_mvtools_frame", "vnlbgpu_shard_plan",
 ]
 KERNEL_CLASSES = ("match", "paste", "filter", "tiles", "normalize")
 
@@ -98,6 +100,13 @@ def load() -> ctypes.CDLL:
             lib.vnlbgpu_render_frame.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                                  ctypes.POINTER(ctypes.c_ssize_t)]
             lib.vnlbgpu_render_stack.argtypes = lib.vnlbgpu_render_frame.argtypes
+            lib.vnlbgpu_required_source_range.argtypes = [ctypes.c_void_p, ctypes.c_int,
+                                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+            lib.vnlbgpu_render_frame_window.argtypes = [
+                ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ssize_t),
+                ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ssize_t),
+                ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ssize_t)]
             lib.vnlbgpu_render_clip_host.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.vnlbgpu_render_clip_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.vnlbgpu_synchronize.argtypes = [ctypes.c_void_p]
@@ -115,6 +124,7 @@ def load() -> ctypes.CDLL:
             lib.vnlbgpu_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.vnlbgpu_diag_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                        ctypes.c_void_p]
+            lib.vnlbgpu_diag_set_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
             lib.vnlbgpu_parse_mvtools_analysis.argtypes = [ctypes.c_char_p, ctypes.c_size_t,
                                                            ctypes.POINTER(MVToolsAnalysis)]
             lib.vnlbgpu_parse_mvtools_vectors.argtypes = [
@@ -124,6 +134,7 @@ def load() -> ctypes.CDLL:
                                                          ctypes.c_size_t]
             lib.vnlbgpu_set_mvtools_frame.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
                                                       ctypes.c_size_t, ctypes.c_int]
+            lib.vnlbgpu_shard_plan.argtypes = [ctypes.c_int] * 9 + [ctypes.POINTER(ctypes.c_int)] * 3
             _lib = lib
     return _lib
 
@@ -154,6 +165,17 @@ def parse_mvtools_vectors(data: bytes, analysis: MVToolsAnalysis):
     _check(load().vnlbgpu_parse_mvtools_vectors(bytes(data), len(data), ctypes.byref(analysis), ctypes.byref(valid),
                                                 xy.ctypes.data, cap, ctypes.byref(count)))
     return bool(valid.value), xy[:count.value]
+
+
+def shard_plan(frames: int, world: int, rank: int, basic: tuple[int, int, int], final: tuple[int, int, int]):
+    """vnlbgpu_shard_plan: rank's block of Final output frames, the Basic
+    frames it reads and the source frames both stages read, each an inclusive
+    (first, last) range or None.  basic / final are (search_bwd, search_fwd,
+    patch_time) of the two stages.  Host only."""
+    out, bas, src = (ctypes.c_int * 2)(), (ctypes.c_int * 2)(), (ctypes.c_int * 2)()
+    _check(load().vnlbgpu_shard_plan(frames, world, rank, *basic, *final, out, bas, src))
+    pick = lambda r: None if r[0] < 0 else (r[0], r[1])
+    return {"out": pick(out), "basic": pick(bas), "source": pick(src)}
 
 
 class Session:
@@ -230,6 +252,38 @@ class Session:
         _check(self.lib.vnlbgpu_render_frame(self.handle, n, ptrs, strides))
         return out
 
+    def set_frame(self, source: int, frame: int, planes):
+        """vnlbgpu_set_frame: one frame from per-plane 2-D arrays (any row
+        stride); a frame already on the device is not copied again."""
+        ptrs, strides = self._planes(list(planes))
+        _check(self.lib.vnlbgpu_set_frame(self.handle, source, frame, ptrs, strides))
+
+    def required_source_range(self, n: int) -> tuple[int, int]:
+        first, last = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.vnlbgpu_required_source_range(self.handle, n, ctypes.byref(first), ctypes.byref(last)))
+        return first.value, last.value
+
+    def render_frame_window(self, n: int, clip_frames, ref_frames=None, first: int | None = None,
+                            out: np.ndarray | None = None) -> np.ndarray:
+        """vnlbgpu_render_frame_window: output frame n, giving the source
+        frames first .. first + len(clip_frames) - 1 as sequences of per-plane
+        2-D arrays (VapourSynth frames: one array per plane, any row stride).
+        `first` defaults to the start of the required source range."""
+        frames, channels, height, width = self.shape
+        if first is None:
+            first = self.required_source_range(n)[0]
+        count = len(clip_frames)
+        clip_planes = [p for f in clip_frames for p in f]
+        cp, cs = self._planes(clip_planes)
+        rp = rs = None
+        if ref_frames is not None:
+            rp, rs = self._planes([p for f in ref_frames for p in f])
+        if out is None:
+            out = np.empty((channels, height, width), np.float32)
+        op, os_ = self._planes([out[c] for c in range(channels)])
+        _check(self.lib.vnlbgpu_render_frame_window(self.handle, n, first, count, cp, cs, rp, rs, op, os_))
+        return out
+
     def render_stack(self, n: int) -> np.ndarray:
         frames, channels, height, width = self.shape
         slots = self.params.search_bwd + self.params.search_fwd + self.params.patch_time
@@ -255,6 +309,10 @@ class Session:
         n = np.zeros(len(KERNEL_CLASSES), np.int64)
         _check(self.lib.vnlbgpu_diag_kernel_timing(self.handle, 1 if enable else 0, ms.ctypes.data, n.ctypes.data))
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(KERNEL_CLASSES)}
+
+    def set_lanes(self, lanes: int):
+        """vnlbgpu_diag_set_lanes: use at most `lanes` pipeline lanes (0: all)."""
+        _check(self.lib.vnlbgpu_diag_set_lanes(self.handle, lanes))
 
     def diag_anchor(self, anchor: int):
         """Runs one anchor frame and returns (grid, active) read-backs."""
