@@ -20,17 +20,21 @@ estimator dimension 294, about 230k groups per anchor frame), plain form only
 (the chosen matchers need 8x8 patches and at most 32 retained rows), without
 the CPU sample.
 
-Under torchrun every rank (one GPU each) denoises its own clip (weak scaling,
-no collective on the data path); rank 0 prints one JSON line.  `value` is
-measured with the clip already resident in HBM; `e2e` goes through the C ABI
-with pinned host buffers, the plugin's copies inside the timed region (clip
-up for Basic and for Final -- Final's copy issued first, it does not depend on
-Basic -- Basic frames down, Basic frames up for Final, Final frames down).
-`config.e2e_frame_path` is the same metric through the per-frame plugin path
-(vnlbgpu_render_frame_window from eight frame threads per stage, pageable
-host frames, a long clip through bounded source stores).  The roofline is
-taken from one more step with one pipeline lane per session, so that each
-timed launch runs alone.  `--impl reference` times the reference CPU implementation
+Under torchrun every rank (one GPU each) denoises its own clip for `value`
+(weak scaling, no collective on the data path); rank 0 prints one JSON line.
+`value` is measured with the clip already resident in HBM, Basic into Final
+chained on the device (vnlbgpu_render_chain_device: a Final anchor frame
+starts once the Basic frames of its window are out).  `e2e` is the same
+metric through the plugin's per-frame call, vnlbgpu_render_frame_window (the
+vnlbcu getFrame), from eight frame threads per stage with pageable host
+frames, over a long clip through bounded source stores: every frame's copies
+up and down are inside the timed region.  Under torchrun that clip is split
+between the ranks by vnlbgpu_shard_plan (blocks of output frames with their
+halos, no exchange).  `config.e2e_whole_clip` is the whole-clip host path
+(pinned buffers: clip up for Basic and for Final, Basic frames down and up
+again, Final frames down).  The roofline is taken from one more step with one
+pipeline lane per session, so that each timed launch runs alone.  `--impl
+reference` times the reference CPU implementation
 (oracle/_ref, the reference's own sources; the C restatement if that build is
 absent) on a bounded sample of the same workload on the host cores.
 """
@@ -275,6 +279,14 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
         sb.render_clip_device(d_basic.data_ptr())
         sf.render_clip_device(d_final.data_ptr())
 
+    def chain_step():
+        # Basic into Final on the device, the stages overlapped frame by frame
+        # (a Final anchor frame starts once its window's Basic frames are out)
+        sb.set_clip_device(lib.SOURCE_CLIP, d_noisy.data_ptr())
+        sf.set_clip_device(lib.SOURCE_CLIP, d_noisy.data_ptr())
+        sf.set_clip_device(lib.SOURCE_REF, d_basic.data_ptr())
+        lib.render_chain_device(sb, sf, d_basic.data_ptr(), d_final.data_ptr())
+
     for _ in range(args.warmup):
         step()
     sb.synchronize()
@@ -290,12 +302,11 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
     ranks.barrier()
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        start.record(stream)
-        for _ in range(args.steps):
-            step()
-        end.record(stream)
-        torch.cuda.synchronize()
+    start.record(stream)
+    for _ in range(args.steps):
+        step()
+    end.record(stream)
+    torch.cuda.synchronize()
     sb.synchronize()
     sf.synchronize()
     elapsed_ms = start.elapsed_time(end)
@@ -332,6 +343,18 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
     e2e_value = whole_job_rate(ranks.world, FRAMES, e2e_steps, ranks.max(e0.elapsed_time(e1)))
     same = bool(torch.equal(h_final, d_final.cpu()))
 
+    # the chained render (vnlbgpu_render_chain_device), device-resident
+    chain_step()
+    torch.cuda.synchronize()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record(stream)
+    for _ in range(args.steps):
+        chain_step()
+    c1.record(stream)
+    torch.cuda.synchronize()
+    chain_value = whole_job_rate(ranks.world, FRAMES, args.steps, ranks.max(c0.elapsed_time(c1)))
+    chain_same = bool(torch.equal(d_final.cpu(), torch.from_numpy(final_out)))
+
     # One more device-resident step with one pipeline lane per session: the
     # anchor frames' kernels then run one after another, so each launch's
     # event-timed duration is that of the kernel alone (the roofline's
@@ -340,6 +363,7 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
         s.set_lanes(1)
     step()
     torch.cuda.synchronize()
+    stats1 = [sb.stats(), sf.stats()]
     sb.kernel_timing(True)
     sf.kernel_timing(True)
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -356,10 +380,13 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
     sf.close()
     kernels = {k: (kb[k][0] + kf[k][0], kb[k][1] + kf[k][1]) for k in kb}
     serial = {"kernels": {k: (kb1[k][0] + kf1[k][0], kb1[k][1] + kf1[k][1]) for k in kb1},
-              "ms_per_step": s0.elapsed_time(s1), "stats": serial_stats}
+              "basic": kb1, "final": kf1, "ms_per_step": s0.elapsed_time(s1), "stats": serial_stats,
+              "basic_stats": {k: stats2[0][k] - stats1[0][k] for k in stats0[0]},
+              "final_stats": {k: stats2[1][k] - stats1[1][k] for k in stats0[0]}}
     return {"form": form, "value": value, "max_ms": max_ms, "e2e": e2e_value, "same": same, "psnr": psnr,
-            "kernels": kernels, "stats": delta, "lanes": lanes, "clocks": clocks.summary(), "bp": bp,
-            "serial": serial, "outputs": (basic_out, final_out)}
+            "kernels": kernels, "stats": delta, "lanes": lanes, "bp": bp,
+            "serial": serial, "chain": {"value": chain_value, "output_matches_sequential": chain_same},
+            "outputs": (basic_out, final_out)}
 
 
 def measure_frame_path(form, args, ranks, noisy, local, threads=8):
@@ -502,11 +529,12 @@ def measure_frame_path(form, args, ranks, noisy, local, threads=8):
 # the Basic and Final launches; the filter class sums prepare, Jacobi and
 # apply.  None where no capture of the current kernels exists.
 TRAFFIC_PER_LAUNCH = {
-    ("cpu", "match/plain"): 59.3e6,
-    ("cpu", "filter"): 504.5e6,
+    ("cpu", "match/plain"): 57.4e6,       # match_kernel<8,0,0>: Basic 31.6 MB, Final 83.2 MB
+    ("cpu", "match/chosen_tc"): 337.1e6,  # tc_distance + tc_select: Basic 281.3 MB, Final 392.8 MB
+    ("cpu", "filter"): 494.6e6,           # prepare + jacobi + apply: Basic 403.7 MB, Final 585.5 MB
 }
-TRAFFIC_SOURCE = ("ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none "
-                  "python bench.py --profile-case --form plain")
+TRAFFIC_SOURCE = ("ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum "
+                  "--clock-control none python bench.py --profile-case --form chosen_tc (and --form plain)")
 
 
 def roofline_of(r, steps, which=None):
@@ -584,6 +612,68 @@ def measured_peak(key: str, fallback: float) -> float:
         return fallback
 
 
+def reference_cuda_stages(head):
+    """The reference's own CUDA stage kernels (src/cuda: block matcher with
+    CUB sorts, group filter with cuBLAS and cuSOLVER, scatter aggregation),
+    built for sm_100a by baseline/Makefile, timed by the reference's own
+    stage benchmarks (tools/benchmark_cuda_*.cpp) at this workload's per
+    anchor frame shapes, beside our kernels' one-lane per-launch times of the
+    same run.  Their frames are 640x360 synthetic ones (the benchmarks' own);
+    what carries over is the work per group: every grid anchor matched over
+    19x19x3 candidates (K 8, buffer 32, patch 8), and every active group
+    filtered (B 8, D 192, S the measured mean rows, rank 8) and scattered."""
+    tools = ROOT / "baseline" / "_ref"
+    if not (tools / "bench_block_match").exists():
+        return {"unavailable": "baseline/_ref not built (make -C baseline needs the reference sources)"}
+    serial = head["serial"]
+    out = {"source": "reference src/cuda built for sm_100a (baseline/Makefile), timed by its "
+                     "tools/benchmark_cuda_{block_match,group_filter,aggregation}.cpp; ours: one-lane event "
+                     "times of this run, per launch (one anchor frame of one stage)"}
+
+    def run(args_):
+        try:
+            r = subprocess.run([str(a) for a in args_], capture_output=True, text=True, timeout=300)
+        except (OSError, subprocess.TimeoutExpired) as e:
+            return None, str(e)
+        if r.returncode != 0:
+            return None, (r.stderr or r.stdout).strip()[-300:]
+        for line in r.stdout.splitlines():
+            if line.startswith("average batch:") or line.startswith("average clear+scatter:"):
+                return float(line.split(":")[1].split()[0]), None
+        return None, "no timing line"
+
+    for stage, name in ((serial["basic_stats"], "basic"), (serial["final_stats"], "final")):
+        frames = max(1, stage["anchor_frames"])
+        groups = int(round(stage["groups"] / frames))
+        active = int(round(stage["active_groups"] / frames))
+        rows = stage["rows"] / max(1, stage["active_groups"])
+        ours = serial[name]
+        entry = {"grid_groups": groups, "active_groups": active, "mean_rows": rows}
+        ms, err = run([tools / "bench_block_match", 8, groups, 20, name, "topk", 1, "contiguous", "--patch", 8,
+                       "--channels", 3, "--window", 19, "--search-bwd", 1, "--search-fwd", 1, "--retained", 32])
+        entry["match"] = {"reference_ms": ms, "ours_ms": ours["match"][0] / max(1, ours["match"][1])}
+        if err:
+            entry["match"]["error"] = err
+        # the filter benchmark runs the reference's Basic-stage filter
+        ms, err = run([tools / "bench_group_filter", 8, 192, min(32, max(8, int(round(rows)))), active, 20, 8])
+        entry["filter"] = {"reference_ms": ms, "ours_ms": ours["filter"][0] / max(1, ours["filter"][1])}
+        if err:
+            entry["filter"]["error"] = err
+        ms, err = run([tools / "bench_aggregation", min(32, max(8, int(round(rows)))), 32, active, 20, 1, "k",
+                       "spread"])
+        entry["aggregate"] = {"reference_ms": ms, "ours_ms": (ours["tiles"][0] + ours["normalize"][0]) /
+                              max(1, ours["tiles"][1]),
+                              "ours_kernels": "stack tiles + normalise"}
+        if err:
+            entry["aggregate"]["error"] = err
+        for k in ("match", "filter", "aggregate"):
+            e = entry[k]
+            if e.get("reference_ms") and e.get("ours_ms"):
+                e["speedup"] = e["reference_ms"] / e["ours_ms"]
+        out[name] = entry
+    return out
+
+
 def run_ours(args):
     import torch
 
@@ -602,11 +692,17 @@ def run_ours(args):
     forms = ["plain", "chosen", "chosen_tc"] if args.form == "all" else [args.form]
     if PARAMS == "vnlbcu":
         forms = ["plain"]
-    results = {f: measure_form(f, args, ranks, stream, noisy, clean, d_noisy, local) for f in forms}
-    head = results[forms[-1]]
-    frame_path = None
-    if not args.no_frame_path:
-        frame_path = measure_frame_path(head["form"], args, ranks, noisy, local)
+    # clocks sampled over every timed measurement below (the GPU is busy from
+    # the first warm-up step to the last frame of the per-frame run)
+    with ClockSampler(local) as clocks:
+        results = {f: measure_form(f, args, ranks, stream, noisy, clean, d_noisy, local) for f in forms}
+        head = results[forms[-1]]
+        frame_path = None
+        if not args.no_frame_path:
+            frame_path = measure_frame_path(head["form"], args, ranks, noisy, local)
+    reference_cuda = None
+    if rank == 0 and not args.no_reference_cuda and PARAMS == "cpu":
+        reference_cuda = reference_cuda_stages(head)
     per_kernel = {}
     total_kernel_ms = sum(v[0] for v in head["kernels"].values())
     for k, v in head["kernels"].items():
@@ -648,18 +744,29 @@ def run_ours(args):
                                    "match_ms_per_step": other["kernels"]["match"][0] / args.steps}
         if head["form"] != "plain" and not roofline["kernel"].startswith("match"):
             config["match_roofline"] = roofline_of(head, args.steps, which="match")
+        e2e_whole = {"value": head["e2e"], "unit": UNIT, "h2d_bytes_per_step": 3 * clip_bytes,
+                     "d2h_bytes_per_step": 2 * clip_bytes,
+                     "api": "vnlbgpu_set_clip_host + vnlbgpu_render_clip_host per stage (whole clip, pinned host "
+                            "buffers), CUDA events on the sessions' stream"}
+        config["chain"] = dict(head["chain"], api="vnlbgpu_render_chain_device (Basic into Final, stages "
+                                                      "overlapped on the device), device-resident")
+        if reference_cuda is not None:
+            config["reference_cuda"] = reference_cuda
         if frame_path is not None:
-            config["e2e_frame_path"] = dict(
-                frame_path, unit=UNIT, h2d_bytes_per_step=3 * clip_bytes, d2h_bytes_per_step=2 * clip_bytes,
-                api="vnlbgpu_render_frame_window per output frame (the plugin's getFrame), pageable host frames, "
-                    "frame threads per stage = num_streams; wall time, synchronised")
+            e2e = dict(value=frame_path["value"], unit=UNIT, h2d_bytes_per_step=3 * clip_bytes,
+                       d2h_bytes_per_step=2 * clip_bytes,
+                       api="vnlbgpu_render_frame_window per output frame (the plugin's getFrame), pageable host "
+                           "frames, eight frame threads per stage; wall time, synchronised, max over ranks")
+            config["e2e_frame_path"] = frame_path
+            config["e2e_whole_clip"] = e2e_whole
+        else:
+            e2e = e2e_whole
         line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": head["max_ms"] / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32" if head["form"] == "chosen_tc" else "f32",
                 "data": "synthetic", "config": config, "roofline": roofline, "cpu_baseline": cpu_baseline,
-                "e2e": {"value": head["e2e"], "unit": UNIT, "h2d_bytes_per_step": 3 * clip_bytes,
-                        "d2h_bytes_per_step": 2 * clip_bytes},
-                "gpu_launches": head["stats"]["kernel_launches"], "clocks": head["clocks"]}
+                "e2e": e2e,
+                "gpu_launches": head["stats"]["kernel_launches"], "clocks": clocks.summary()}
         print(json.dumps(line), flush=True)
     ranks.close()
     return 0
@@ -706,6 +813,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip timing the reference's own CUDA stage kernels (baseline/_ref, if built)")
     ap.add_argument("--no-frame-path", action="store_true",
                     help="skip the end-to-end run through the per-frame path (vnlbgpu_render_frame_window)")
     ap.add_argument("--form", choices=("all", "plain", "chosen", "chosen_tc"), default="all",

@@ -99,10 +99,20 @@ typedef struct vnlbgpu_params {
  * accumulation in tensor memory) and also needs a search window of at most 64
  * columns by 32 rows.  Both apply to 8x8 patches with a buffer of at most 32
  * patches (group_size * cap_factor) and group_size <= 32; other
- * configurations run PLAIN. */
+ * configurations run PLAIN.  With either chosen matcher the group filter runs
+ * in mixed precision too: the dual Gram on TF32 tensor cores with FP32
+ * accumulation, the Jacobi rotation angles in FP64. */
 #define VNLBGPU_FORM_PLAIN 0
 #define VNLBGPU_FORM_CHOSEN 1
 #define VNLBGPU_FORM_CHOSEN_TC 2
+/* LEARNED: learned block-match proposals (vnlbgpu_set_learned).  An MLP
+ * scores every offset of each anchor's search window from coarse features
+ * of its neighbourhood; exact SSD runs on the best-scored offsets (and the
+ * anchor itself) only, and the plain selection rule picks the rows among
+ * them.  In every tile of anchors the full search runs for one anchor as the
+ * judge; where the learned rows' recall of its K nearest is below the
+ * threshold, the whole tile is searched in full instead. */
+#define VNLBGPU_FORM_LEARNED 3
 
 typedef struct vnlbgpu_session vnlbgpu_session;
 
@@ -117,6 +127,8 @@ typedef struct vnlbgpu_stats {
                                   device memory at create time) */
     long long source_slots;    /* frames each source store holds on the device */
     long long source_uploads;  /* source frames copied to the device */
+    long long learned_tiles;   /* learned form: tiles checked against the full search */
+    long long learned_fallback_tiles; /* ... and searched in full after the check */
 } vnlbgpu_stats;
 
 const char* vnlbgpu_last_error(void);
@@ -186,6 +198,19 @@ int vnlbgpu_render_clip_host(vnlbgpu_session* session, float* out);
 int vnlbgpu_render_clip_device(vnlbgpu_session* session, float* device_out);
 int vnlbgpu_synchronize(vnlbgpu_session* session);
 
+/* vnlbcu.Basic into vnlbcu.Final over a whole clip on the device, the two
+ * stages overlapped: Basic frame n is normalised on the Basic session's
+ * stream, and the Final session's anchor frames start as soon as the Basic
+ * frames of their windows are out, instead of after the whole Basic clip.
+ * The Final session's ref must be basic_out (vnlbgpu_set_clip_device); every
+ * source frame must be on the device.  Enqueues and returns; the Basic
+ * session's stream ends after all of the chain's work (vnlbgpu_synchronize on
+ * either session waits and reports device-side errors).  The reference runs
+ * the two filters as separate VapourSynth nodes; this is their frame-level
+ * dependency, scheduled on the device. */
+int vnlbgpu_render_chain_device(vnlbgpu_session* basic_session, vnlbgpu_session* final_session, float* basic_out,
+                                float* final_out);
+
 /* vnlb.Basic / vnlb.Final: the contribution stack of anchor frame n in the
  * plugin's frame layout (per plane, slots*2*H rows: numerators then weights,
  * weights repeated in every plane). */
@@ -239,6 +264,49 @@ int vnlbgpu_shard_plan(int frames, int world, int rank, int basic_search_bwd, in
                        int out[2], int basic[2], int source[2]);
 
 int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats);
+
+/* Learned block-match proposals (no reference counterpart): a multilayer
+ * perceptron trained and run by this library's own CUDA kernels.
+ *
+ * The network maps `inputs` features through `layers` hidden ReLU layers of
+ * `hidden` units to `outputs` logits.  Weights are FP32 for the optimiser and
+ * BF16 for the products, which accumulate in FP32.  Training minimises the
+ * softmax cross-entropy against up to tk target classes per row (class ids,
+ * -1 = none, each weighted equally) with Adam.  x, targets, logits and
+ * shortlist buffers are device pointers; weights and gradients are host
+ * arrays laid out layer by layer as [W_l (fan_out x fan_in)][b_l]. */
+typedef struct vnlbgpu_mlp vnlbgpu_mlp;
+int vnlbgpu_mlp_create(int inputs, int hidden, int layers, int outputs, int max_batch, unsigned seed, int device_id,
+                       vnlbgpu_mlp** out);
+void vnlbgpu_mlp_destroy(vnlbgpu_mlp* mlp);
+long long vnlbgpu_mlp_parameters(const vnlbgpu_mlp* mlp);
+int vnlbgpu_mlp_get_weights(vnlbgpu_mlp* mlp, float* host);
+int vnlbgpu_mlp_set_weights(vnlbgpu_mlp* mlp, const float* host);
+/* gradients of the mean loss over the batch (no update) */
+int vnlbgpu_mlp_gradients(vnlbgpu_mlp* mlp, const float* x, const int* targets, int batch, int tk, float* host_grads,
+                          float* mean_loss);
+int vnlbgpu_mlp_train_step(vnlbgpu_mlp* mlp, const float* x, const int* targets, int batch, int tk, float lr,
+                           float* mean_loss);
+int vnlbgpu_mlp_logits(vnlbgpu_mlp* mlp, const float* x, int batch, float* logits);
+/* the k best-scored classes of each row, [batch][k] */
+int vnlbgpu_mlp_shortlist(vnlbgpu_mlp* mlp, const float* x, int batch, int k, int* out);
+
+/* Attaches a network to a session of form VNLBGPU_FORM_LEARNED (not owned;
+ * it must outlive the session's renders).  Its inputs must be
+ * (search_bwd + search_fwd + 1) * (1 for Basic, planes for Final) * 9 and its
+ * outputs (search_bwd + search_fwd + 1) * search_window^2; shortlist offsets
+ * (1..128) per anchor, the recall threshold of the per-tile check (0: the
+ * learned rows always stand; above 1: every tile is searched in full), and
+ * the tile edge in pixels (64 in this build). */
+int vnlbgpu_set_learned(vnlbgpu_session* session, vnlbgpu_mlp* mlp, int shortlist, float recall_threshold,
+                        int tile);
+
+/* Training pairs of anchor frame `anchor`: for each grid anchor (raster
+ * order) its features ([count][inputs], the learned form's) and the classes
+ * of its k nearest rows under the full exact search ([count][k], -1 past the
+ * retained rows), into host arrays of `capacity` anchors.  Any form. */
+int vnlbgpu_learned_pairs(vnlbgpu_session* session, int anchor, float* features, int* targets, int capacity, int k,
+                          int* count, int* inputs);
 
 /* The CUDA stream the session enqueues on (a cudaStream_t), for callers that
  * time or order device work around it. */

@@ -40,6 +40,17 @@ int vnlbgpu_diag_anchor(vnlbgpu_session* session, int anchor, int* grid_xy, int*
  * Timing brackets each launch with CUDA events on the session's stream. */
 int vnlbgpu_diag_kernel_timing(vnlbgpu_session* session, int enable, double* ms, long long* launches);
 
+/* Runs anchor frame `anchor` and copies the filtered rows of its processed
+ * groups, [*rows][*row_dim] floats in the order of vnlbgpu_diag_anchor's
+ * active rows, up to `capacity` rows (*rows receives the true count). */
+int vnlbgpu_diag_filtered(vnlbgpu_session* session, int anchor, float* out, int capacity, int* rows, int* row_dim);
+
+/* Test switch of the tensor-core matcher's bounded waits: with on != 0 its
+ * MMA warp issues no MMA, so every wait for MMA completion runs out after
+ * its iteration limit, the kernel returns with nothing in flight, and the
+ * render raises "timed out".  0 restores normal matching. */
+int vnlbgpu_diag_stall_tensor_waits(vnlbgpu_session* session, int on);
+
 /* Limits the pipeline lanes the session uses to min(lanes, the lanes it
  * allocated) after waiting for its queued work; lanes <= 0 restores them all.
  * With one lane the anchor frames' kernels run one after another, so the

@@ -68,22 +68,28 @@ def test_chosen_selects_the_plain_rows(stage, form, agree):
     plain = rows_of(stage, "plain", noisy, ref)
     chosen = rows_of(stage, form, noisy, ref)
     assert np.array_equal(plain["xy"], chosen["xy"])
-    same = 0
+    same = ordered = 0
     groups = len(plain["counts"])
+    place = lambda r: (int(r["x"]), int(r["y"]), int(r["frame"]))
     for gi in range(groups):
         a = plain["grid_rows"][gi][: plain["counts"][gi]]
         b = chosen["grid_rows"][gi][: chosen["counts"][gi]]
-        key = lambda r: {(int(x["x"]), int(x["y"]), int(x["frame"])): x["distance"] for x in r}
-        ka, kb = key(a), key(b)
-        if set(ka) == set(kb):
-            same += 1
+        ka = {place(x): x["distance"] for x in a}
+        kb = {place(x): x["distance"] for x in b}
         for pos in set(ka) & set(kb):  # exact re-rank: the plain form's distance bits
             assert np.float32(ka[pos]).view(np.uint32) == np.float32(kb[pos]).view(np.uint32)
-        # the K nearest are the plain form's first rows, in order
-        k = min(8, len(a), len(b))
-        assert [tuple(r[["x", "y", "frame"]]) for r in a[:k]] == [tuple(r[["x", "y", "frame"]]) for r in b[:k]] \
-            or same < groups
+        if set(ka) != set(kb):
+            continue
+        same += 1
+        # the same rows: both forms put the K nearest first, in ascending
+        # distance (partial_sort's sorted front); with no tie among them the
+        # order is unique and must be the same
+        k = min(8, len(a))
+        if len(set(np.float32(a["distance"][:k]).view(np.uint32).tolist())) == k:
+            assert [place(r) for r in a[:k]] == [place(r) for r in b[:k]], gi
+            ordered += 1
     assert same / groups >= agree, (same, groups)
+    assert ordered >= 0.5 * same, (ordered, same)  # the order check ran on most of the agreeing groups
 
 
 @pytest.mark.parametrize("form", ["chosen", "chosen_tc"])
@@ -94,3 +100,23 @@ def test_chosen_needs_8x8_patches(form):
     plain = vnlbcu.Basic(noisy, sigma=20.0, **kw)
     chosen = vnlbcu.Basic(noisy, sigma=20.0, form=form, **kw)
     assert np.array_equal(plain, chosen)
+
+
+def test_tensor_core_waits_run_out_and_report():
+    """The tensor-core matcher's MMA-completion waits are bounded: with its
+    MMA warp told to issue nothing (a test switch; no MMA is in flight), every
+    wait runs out, the kernel returns, and the render raises; the session then
+    renders normally again and equals a fresh session's output."""
+    _, noisy = synth.make_clip(96, 64, 4, 3, 20.0, seed=85)
+    params = vnlbcu.parse_parameters(lib.STAGE_BASIC, noisy, 20.0, dict(CPU_DEFAULTS, form="chosen_tc", **BASIC))
+    frames, planes, h, w = noisy.shape
+    s = lib.Session(params, w, h, frames, planes)
+    s.set_clip(lib.SOURCE_CLIP, noisy)
+    s.stall_tensor_waits(True)
+    with pytest.raises(lib.VNLBError, match="timed out waiting for its MMAs"):
+        s.render_clip()
+    s.stall_tensor_waits(False)
+    again = s.render_clip()
+    s.close()
+    fresh = vnlbcu.Basic(noisy, sigma=20.0, form="chosen_tc", **CPU_DEFAULTS, **BASIC)
+    assert np.array_equal(again, fresh)

@@ -75,6 +75,9 @@ def test_golden_reference_outputs(golden):
 
 CASES = [
     ("gray_defaults", 64, 48, 4, 1, 20.0, {}),
+    # a row pitch that is not a multiple of 16 bytes: the matcher stages its
+    # regions with plain loads instead of tensor-memory-accelerator tiles
+    ("yuv_odd_width", 66, 50, 4, 3, 20.0, {}),
     ("yuv_defaults", 96, 80, 5, 3, 20.0, {}),
     ("yuv_cuda_like", 96, 72, 4, 3, 20.0, dict(block_size=7, patch_time=2, bm_range=6, group_size=16, rank=15,
                                                block_step=3)),
@@ -257,3 +260,51 @@ def test_full_size_anchor_frames_bit_exact():
             assert np.array_equal(bits(s.render_stack(a)), bits(want[a])), (stage, a)
     again = session_for(lib.STAGE_BASIC, bp, noisy).render_clip()
     assert np.array_equal(bits(again), bits(basic))  # deterministic
+
+
+@pytest.mark.parametrize("kw", [dict(block_size=8, block_step=8, group_size=8, bm_range=9, radius=1, patch_time=1,
+                                     rank=8),
+                                dict(block_size=7, block_step=3, group_size=16, bm_range=6, search_bwd=2,
+                                     search_fwd=1, patch_time=2, rank=15)],
+                         ids=["cpu_defaults", "patch_time2_asymmetric"])
+def test_chain_render_matches_oracle(kw):
+    """Basic into Final with the two stages overlapped on the device
+    (vnlbgpu_render_chain_device) equals the oracle's chain bit for bit, the
+    sessions sharing one caller stream as the bench runs them."""
+    import torch
+
+    _, noisy = synth.make_clip(72, 56, 9, 3, 20.0, seed=77)
+    bp = O.cpu_params(O.BASIC, 20.0, **kw)
+    fp = O.cpu_params(O.FINAL, 20.0, **kw)
+    ob, of = O.Oracle("port").chain(noisy, bp, fp)
+    d_noisy = torch.from_numpy(noisy).cuda()
+    d_basic = torch.empty_like(d_noisy)
+    d_final = torch.empty_like(d_noisy)
+    sessions = []
+    for stage, p in ((lib.STAGE_BASIC, bp), (lib.STAGE_FINAL, fp)):
+        d = {f: getattr(p, f) for f in p.__dataclass_fields__}
+        params = lib.Params(stage=stage, device_id=0, num_streams=1, chunk_size=768,
+                            **{k: (float(v) if isinstance(v, (float, np.floating)) else int(v)) for k, v in d.items()})
+        sessions.append(lib.Session(params, 72, 56, 9, 3))
+    sb, sf = sessions
+    stream = torch.cuda.Stream()
+    for s in sessions:
+        s.set_stream(stream.cuda_stream)
+    sb.set_clip_device(lib.SOURCE_CLIP, d_noisy.data_ptr())
+    sf.set_clip_device(lib.SOURCE_CLIP, d_noisy.data_ptr())
+    sf.set_clip_device(lib.SOURCE_REF, d_basic.data_ptr())
+    for _ in range(2):  # the second pass reuses the cached stacks' slots
+        d_basic.fill_(float("nan"))
+        d_final.fill_(float("nan"))
+        torch.cuda.synchronize()
+        sb.set_clip_device(lib.SOURCE_CLIP, d_noisy.data_ptr())  # drops the cached stacks
+        sf.set_clip_device(lib.SOURCE_CLIP, d_noisy.data_ptr())
+        sf.set_clip_device(lib.SOURCE_REF, d_basic.data_ptr())
+        lib.render_chain_device(sb, sf, d_basic.data_ptr(), d_final.data_ptr())
+        sb.synchronize()
+        sf.synchronize()
+        stream.synchronize()
+        assert np.array_equal(bits(d_basic.cpu().numpy()), bits(ob))
+        assert np.array_equal(bits(d_final.cpu().numpy()), bits(of))
+    with pytest.raises(lib.VNLBError, match="ref must be the chain's Basic output"):
+        lib.render_chain_device(sb, sf, d_final.data_ptr(), d_basic.data_ptr())

@@ -92,6 +92,54 @@ __device__ __forceinline__ size_t row_base(const FilterLaunch& L, const MatchRow
 
 __device__ __forceinline__ int bmax_of(const FilterLaunch& L) { return min(L.model_cap, L.max_rows); }
 
+// One m16n8k8 TF32 tensor-core MMA with FP32 accumulation (row-major A,
+// column-major B): d += a * b.
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// Dual Gram X X^T / B of up to 16 centred rows (row stride ldx, D a multiple
+// of 8) on the tensor cores, one warp: A = the rows (16 x 8 per step), B =
+// their transpose in tiles of 8 columns; rows and columns past B are zero.
+// Lane (g, q) = (lane / 4, lane % 4) holds A rows g, g + 8 at columns q, q + 4
+// and the accumulators of rows g, g + 8 at columns 2q, 2q + 1.
+__device__ __forceinline__ void gram_tf32(const float* X, int ldx, int B, int D, float scale, float* gram,
+                                          int lane) {
+    const int g = lane >> 2, q = lane & 3;
+    for (int n0 = 0; n0 < B; n0 += 8) {
+        float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        for (int k0 = 0; k0 < D; k0 += 8) {
+            uint32_t a[4], b[2];
+            a[0] = g < B ? to_tf32(X[g * ldx + k0 + q]) : 0u;
+            a[1] = g + 8 < B ? to_tf32(X[(g + 8) * ldx + k0 + q]) : 0u;
+            a[2] = g < B ? to_tf32(X[g * ldx + k0 + q + 4]) : 0u;
+            a[3] = g + 8 < B ? to_tf32(X[(g + 8) * ldx + k0 + q + 4]) : 0u;
+            const int n = n0 + g;  // B's column n is row n of X
+            b[0] = n < B ? to_tf32(X[n * ldx + k0 + q]) : 0u;
+            b[1] = n < B ? to_tf32(X[n * ldx + k0 + q + 4]) : 0u;
+            mma_tf32(acc, a, b);
+        }
+        const int c0 = n0 + 2 * q;
+        const int rows[2] = {g, g + 8};
+        for (int h = 0; h < 2; ++h) {
+            const int r = rows[h];
+            if (r >= B) continue;
+            if (c0 < B) gram[r * B + c0] = acc[2 * h] * scale;
+            if (c0 + 1 < B) gram[r * B + c0 + 1] = acc[2 * h + 1] * scale;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // prepare: W warps per group.  W = 1 runs four groups per CTA, one per warp;
 // W = 4 gives a CTA to one group, for model rows too large for four copies in
@@ -284,7 +332,10 @@ __global__ void __launch_bounds__(32 * kPrepareWarps) prepare_kernel(FilterLaunc
         if (L.rank > 0) {
             const float scale = __fdiv_rn(1.0f, static_cast<float>(B));
             float* gram = L.gram + static_cast<size_t>(v) * L.nmax * L.nmax;
-            if (D >= 64 && B < D) {
+            if (D >= 64 && B < D && L.mixed && W == 1 && B <= 16 && D % 8 == 0) {
+                // chosen forms: TF32 tensor-core Gram, FP32 accumulation
+                gram_tf32(X, ldx, B, D, scale, gram, lane);
+            } else if (D >= 64 && B < D) {
                 // dual Gram (compute_gram_centered): octet k takes pair e0 + k;
                 // lane j of the octet runs the pinned chain j (octet_dot8)
                 const int pairs = B * (B + 1) / 2;
@@ -395,13 +446,26 @@ __global__ void __launch_bounds__(256) jacobi_kernel(FilterLaunch L, int seg, in
                         __syncwarp();
                         if (rot) {
                             // jacobi_rotate (linalg.cpp:152-196)
-                            const float tau = __fdiv_rn(__fsub_rn(aqq, app), __fmul_rn(2.0f, apq));
-                            const float tau_abs = fabsf(tau);
-                            const float t_abs =
-                                __fdiv_rn(1.0f, __fadd_rn(tau_abs, __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(tau, tau)))));
-                            const float t = tau < 0.0f ? -t_abs : t_abs;
-                            const float c = __fdiv_rn(1.0f, __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(t, t))));
-                            const float s = __fmul_rn(t, c);
+                            float c, s;
+                            if (L.mixed) {
+                                // chosen forms: the rotation angle in FP64, so that near-degenerate
+                                // pairs (aqq - app tiny against apq) keep their angle
+                                const double tau = (static_cast<double>(aqq) - static_cast<double>(app)) /
+                                                   (2.0 * static_cast<double>(apq));
+                                const double t_abs = 1.0 / (fabs(tau) + sqrt(1.0 + tau * tau));
+                                const double t = tau < 0.0 ? -t_abs : t_abs;
+                                const double cd = 1.0 / sqrt(1.0 + t * t);
+                                c = static_cast<float>(cd);
+                                s = static_cast<float>(t * cd);
+                            } else {
+                                const float tau = __fdiv_rn(__fsub_rn(aqq, app), __fmul_rn(2.0f, apq));
+                                const float tau_abs = fabsf(tau);
+                                const float t_abs = __fdiv_rn(
+                                    1.0f, __fadd_rn(tau_abs, __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(tau, tau)))));
+                                const float t = tau < 0.0f ? -t_abs : t_abs;
+                                c = __fdiv_rn(1.0f, __fsqrt_rn(__fadd_rn(1.0f, __fmul_rn(t, t))));
+                                s = __fmul_rn(t, c);
+                            }
                             for (int r = r0; r < B; r += seg) {
                                 if (r != p && r != q) {
                                     const float arp = m[r * ld + p];
@@ -994,10 +1058,12 @@ __global__ void __launch_bounds__(kApplyThreads, 3) apply_kernel(FilterLaunch L)
 constexpr int kWarpApplyWarps = 4;
 
 struct WarpApplyLayout {
-    int basis, u, v, dual, scal, scores, bases, per_warp;
+    int basis, u, v, dual, scal, scores, recon, rw, bases, per_warp;
 };
 
-__host__ __device__ inline WarpApplyLayout warp_apply_layout(int D, int max_rows) {
+// scatter: also the rows' scaled projections [max_rows][8] and weights
+// [max_rows], kept for the second pass that adds the rows into the stack
+__host__ __device__ inline WarpApplyLayout warp_apply_layout(int D, int max_rows, bool scatter = false) {
     WarpApplyLayout w{};
     int off = 0;
     w.basis = off;  off += 8 * D;
@@ -1006,6 +1072,8 @@ __host__ __device__ inline WarpApplyLayout warp_apply_layout(int D, int max_rows
     w.dual = off;   off += 64;
     w.scal = off;   off += 5 * 8;
     w.scores = off; off += max_rows;
+    w.recon = off;  off += scatter ? 8 * max_rows : 0;
+    w.rw = off;     off += scatter ? max_rows : 0;
     off = (off + 1) & ~1;
     w.bases = off;  off += 2 * max_rows;
     off = (off + 3) & ~3;
@@ -1037,7 +1105,37 @@ __device__ __forceinline__ float octet_reduce(float v) {
 #define VNLB_APPLY_MIN_BLOCKS 4
 #endif
 
-template <int D>
+// Chosen forms: a lane's columns of one filtered row added into the anchor
+// frame's stack, weight cw times the window at each pixel; the weight plane
+// gets the same once per pixel (the columns of plane 0).  Slots outside the
+// window are dropped, as the stack tiles drop them.
+template <int kCols>
+__device__ __forceinline__ void scatter_row(const FilterLaunch& L, const MatchRow& m, const float (&o)[kCols],
+                                            float cw, int lane) {
+    const size_t plane = static_cast<size_t>(L.height) * L.width;
+    const int C = L.channels;
+    const int P = L.P;
+    const size_t base = static_cast<size_t>(m.y) * L.width + m.x;
+    const int slot0 = m.frame + L.search_bwd - L.anchor_frame;
+#pragma unroll
+    for (int jj = 0; jj < kCols; ++jj) {
+        // column (plane c, layer t, py, px)
+        const int col = lane + 32 * jj;
+        const int c = col / L.patch_dim;
+        const int pos = col - c * L.patch_dim;
+        const int t = pos / (P * P);
+        const int rem = pos - t * P * P;
+        const int py = rem / P;
+        const int slot = slot0 + t;
+        if (slot < 0 || slot >= L.slots) continue;
+        const float w = L.windowed ? cw * __ldg(L.window + rem) : cw;
+        const size_t at = base + static_cast<size_t>(py) * L.width + (rem - py * P);
+        atomicAdd(L.scatter + (static_cast<size_t>(slot) * (C + 1) + c) * plane + at, w * o[jj]);
+        if (c == 0) atomicAdd(L.scatter + (static_cast<size_t>(slot) * (C + 1) + C) * plane + at, w);
+    }
+}
+
+template <int D, bool kScatter>
 __global__ void __launch_bounds__(32 * kWarpApplyWarps, VNLB_APPLY_MIN_BLOCKS) apply_warp_kernel(FilterLaunch L) {
     static_assert(D % 32 == 0, "columns are owned in blocks of 32");
     constexpr int kCols = D / 32;
@@ -1047,7 +1145,7 @@ __global__ void __launch_bounds__(32 * kWarpApplyWarps, VNLB_APPLY_MIN_BLOCKS) a
     const int warp = threadIdx.x >> 5;
     const int j8 = lane & 7;
     const int oct = lane >> 3;
-    const WarpApplyLayout lay = warp_apply_layout(D, L.max_rows);
+    const WarpApplyLayout lay = warp_apply_layout(D, L.max_rows, kScatter);
     int* coloff = reinterpret_cast<int*>(sm);
     float* wr = sm + D + warp * lay.per_warp;
     float2* basis2 = reinterpret_cast<float2*>(wr + lay.basis);
@@ -1085,7 +1183,25 @@ __global__ void __launch_bounds__(32 * kWarpApplyWarps, VNLB_APPLY_MIN_BLOCKS) a
 
     for (int mi = blockIdx.x * kWarpApplyWarps + warp; mi < active_count * models;
          mi += gridDim.x * kWarpApplyWarps) {
-        if (L.flags[mi] != 0) continue;  // equal groups are done, skipped ones reported
+        if (L.flags[mi] != 0) {  // equal groups are done, skipped ones reported
+            if constexpr (kScatter) {
+                if (L.flags[mi] == kGroupDone) {
+                    // the pass-through rows prepare wrote, with their weights
+                    const int g0 = L.active[mi];
+                    const int S0 = L.row_counts[g0];
+                    const int q0 = L.row_offset[mi];
+                    const MatchRow* rows0 = L.rows + static_cast<size_t>(g0) * L.max_rows;
+                    for (int i = 0; i < S0; ++i) {
+                        float o[kCols];
+#pragma unroll
+                        for (int jj = 0; jj < kCols; ++jj)
+                            o[jj] = L.filtered[static_cast<size_t>(q0 + i) * L.row_dim + lane + 32 * jj];
+                        scatter_row(L, rows0[i], o, L.weights[q0 + i], lane);
+                    }
+                }
+            }
+            continue;
+        }
         const int a = mi / models;
         const int mc = mi - a * models;
         const int g = L.active[a];
@@ -1301,6 +1417,11 @@ __global__ void __launch_bounds__(32 * kWarpApplyWarps, VNLB_APPLY_MIN_BLOCKS) a
             }
             // reconstruction (project_bayes_estimate), components in order
             const float scaled = lane < R ? __fmul_rn(coef[lane], rk) : 0.0f;
+            if constexpr (kScatter) {
+                // kept for the pass after the weights
+                if (lane < 8) wr[lay.recon + i * 8 + lane] = scaled;
+                __syncwarp();
+            } else {
             float o[kCols];
 #pragma unroll
             for (int jj = 0; jj < kCols; ++jj) o[jj] = 0.0f;
@@ -1317,6 +1438,7 @@ __global__ void __launch_bounds__(32 * kWarpApplyWarps, VNLB_APPLY_MIN_BLOCKS) a
 #pragma unroll
             for (int jj = 0; jj < kCols; ++jj) out[lane + 32 * jj] = __fadd_rn(o[jj], cc[jj]);
             __syncwarp();
+            }
         }
         // aggregation weights (accumulate_aggregation_model + finalize)
         for (int i = lane; i < S; i += 32) {
@@ -1341,8 +1463,32 @@ __global__ void __launch_bounds__(32 * kWarpApplyWarps, VNLB_APPLY_MIN_BLOCKS) a
                 w = cr_expf(lw);
             }
             L.weights[r0 + i] = w;
+            if constexpr (kScatter) wr[lay.rw + i] = w;
         }
         __syncwarp();
+        if constexpr (kScatter) {
+            // each row rebuilt from its scaled projections and added into the
+            // stack with its weight
+            for (int i = 0; i < S; ++i) {
+                const float* sc = wr + lay.recon + i * 8;
+                float o[kCols];
+#pragma unroll
+                for (int jj = 0; jj < kCols; ++jj) o[jj] = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    if (c >= R) break;
+                    if (coef[c] == 0.0f) continue;
+                    const float scv = sc[c];
+#pragma unroll
+                    for (int jj = 0; jj < kCols; ++jj)
+                        o[jj] = __fmaf_rn(scv, basis_f[((c & 3) * D + lane + 32 * jj) * 2 + (c >> 2)], o[jj]);
+                }
+#pragma unroll
+                for (int jj = 0; jj < kCols; ++jj) o[jj] = __fadd_rn(o[jj], cc[jj]);
+                scatter_row(L, rows[i], o, wr[lay.rw + i], lane);
+            }
+            __syncwarp();
+        }
     }
 }
 
@@ -1396,13 +1542,14 @@ JacobiShape jacobi_shape(int N) {
 
 template <int D>
 cudaError_t launch_apply_warp(const FilterLaunch& L, int max_groups, cudaStream_t stream) {
-    const WarpApplyLayout lay = warp_apply_layout(D, L.max_rows);
+    const bool scatter = L.scatter != nullptr;
+    const WarpApplyLayout lay = warp_apply_layout(D, L.max_rows, scatter);
     const size_t smem = (static_cast<size_t>(D) + static_cast<size_t>(kWarpApplyWarps) * lay.per_warp) * sizeof(float);
-    cudaError_t err = cudaFuncSetAttribute(apply_warp_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           static_cast<int>(smem));
+    auto kernel = scatter ? apply_warp_kernel<D, true> : apply_warp_kernel<D, false>;
+    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (err != cudaSuccess) return err;
     const int ctas = std::max(1, std::min((max_groups + kWarpApplyWarps - 1) / kWarpApplyWarps, 148 * 8));
-    apply_warp_kernel<D><<<ctas, 32 * kWarpApplyWarps, smem, stream>>>(L);
+    kernel<<<ctas, 32 * kWarpApplyWarps, smem, stream>>>(L);
     return cudaGetLastError();
 }
 
@@ -1427,6 +1574,13 @@ size_t filter_shared_bytes(const FilterLaunch& L) {
 }
 
 size_t filter_shared_limit() { return kFilterSharedLimit; }
+
+bool filter_can_scatter(const FilterLaunch& L) {
+    const int D = L.dim;
+    const int Bmax = std::min(L.model_cap, L.max_rows);
+    return L.models == 1 && L.rank <= 8 && Bmax <= 8 && L.nmax == Bmax &&
+           (D == 64 || D == 128 || D == 192 || D == 256);
+}
 
 cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t stream) {
     if (max_groups_in <= 0) return cudaSuccess;
@@ -1475,7 +1629,9 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
 #ifndef VNLB_APPLY_WARP
 #define VNLB_APPLY_WARP 1  // the warp-per-group apply for its shapes; a build parameter for comparisons
 #endif
-    if (VNLB_APPLY_WARP && R <= 8 && Bmax <= 8 && L.nmax == Bmax && (D == 64 || D == 128 || D == 192 || D == 256)) {
+    const bool warp_shape = R <= 8 && Bmax <= 8 && L.nmax == Bmax && (D == 64 || D == 128 || D == 192 || D == 256);
+    if (L.scatter && !(warp_shape && L.models == 1)) return cudaErrorInvalidValue;  // see filter_can_scatter
+    if ((VNLB_APPLY_WARP || L.scatter) && warp_shape) {
         cudaError_t err = D == 64    ? launch_apply_warp<64>(L, max_groups, stream)
                           : D == 128 ? launch_apply_warp<128>(L, max_groups, stream)
                           : D == 192 ? launch_apply_warp<192>(L, max_groups, stream)

@@ -243,16 +243,59 @@ __device__ __forceinline__ float exact_distance8(const float* planes, int plane_
     return d;
 }
 
+// Staging with the tensor memory accelerator: one thread arms an mbarrier
+// with the byte count of the frame's planes and issues one 2-D tile load per
+// plane (box = region_stride x region_rows, x a multiple of 4 floats, no
+// multicast); every thread then waits on the barrier's phase.
+constexpr int kTmaSpinLimit = 1 << 24;  // barrier polls before a staging wait gives up
+
+__device__ __forceinline__ void stage_bar_init(uint32_t bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void stage_bar_expect(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool stage_bar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
 template <int P, bool kApprox, bool kFlow>  // kFlow: search centres from L.centers
-__global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
-    extern __shared__ __align__(16) float smem[];
+__global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L, const __grid_constant__ CUtensorMap tmap) {
+    extern __shared__ __align__(128) float smem[];
+    __shared__ __align__(8) unsigned long long stage_bar;
+    __shared__ int stage_failed;
+    if (L.tile_fail && !L.tile_fail[L.strip_tile[blockIdx.x]]) return;  // the learned rows stand
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const Strip strip = L.strips[blockIdx.x];
     const int Pd = L.P;
     const int Cs = L.search_channels;
     const int planes_n = Cs * L.Pt;
-    const int plane_values = L.region_rows * L.region_stride;
+    const int plane_values = L.plane_floats;
+    const bool tma = !kFlow && L.tma != 0;
+    const uint32_t bar = static_cast<uint32_t>(__cvta_generic_to_shared(&stage_bar));
+    uint32_t stage_phase = 0;
+    if (tma && threadIdx.x == 0) {
+        stage_bar_init(bar);
+        stage_failed = 0;
+    }
 
     float* planes = smem;
     // chosen form: per-frame norm table of every patch origin in the region,
@@ -349,16 +392,49 @@ __global__ void __launch_bounds__(256, 3) match_kernel(MatchLaunch L) {
         // Stage the strip's region of every plane (channel, t) of frame k.
         const int rows = rh;
         const int cols = rw;
-        for (int q = 0; q < planes_n; ++q) {
-            const int c = q / L.Pt;
-            const int t = q % L.Pt;
-            const float* src = L.video + ((static_cast<size_t>(frame % L.ring + t) * L.channels + c) * L.height +
-                                          ry0) * static_cast<size_t>(L.width) + rx0;
-            float* dst = planes + q * plane_values;
-            for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
-                const int r = i / cols;
-                const int cx = i - r * cols;
-                dst[r * L.region_stride + cx] = __ldg(src + static_cast<size_t>(r) * L.width + cx);
+        if (tma) {
+            // whole boxes (region_stride x region_rows) from row (slot, c, ry0)
+            // of the store; rows and columns past the region are never read
+            if (threadIdx.x == 0) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier reads of these planes
+                stage_bar_expect(bar, static_cast<uint32_t>(planes_n) * L.region_rows * L.region_stride * 4u);
+                for (int q = 0; q < planes_n; ++q) {
+                    const int c = q / L.Pt;
+                    const int t = q % L.Pt;
+                    const int y = (((frame % L.ring) + t) * L.channels + c) * L.height + ry0;
+                    tma_load_tile(static_cast<uint32_t>(__cvta_generic_to_shared(planes + q * plane_values)), &tmap,
+                                  rx0, y, bar);
+                }
+            }
+            int spins = 0;
+            while (!stage_bar_try_wait(bar, stage_phase))
+                if (++spins >= kTmaSpinLimit) break;
+            stage_phase ^= 1u;
+            if (spins >= kTmaSpinLimit) stage_failed = 1;
+            __syncthreads();
+            if (stage_failed) {
+                // the load never completed: report it, and give it a bounded
+                // second chance to land before the block's shared memory goes
+                if (threadIdx.x == 0) {
+                    atomicCAS(L.status, 0, kStatusTmaTimeout);
+                    for (int i = 0; i < kTmaSpinLimit && !stage_bar_try_wait(bar, stage_phase ^ 1u); ++i) {
+                    }
+                }
+                __syncthreads();
+                return;
+            }
+        } else {
+            for (int q = 0; q < planes_n; ++q) {
+                const int c = q / L.Pt;
+                const int t = q % L.Pt;
+                const float* src = L.video + ((static_cast<size_t>(frame % L.ring + t) * L.channels + c) * L.height +
+                                              ry0) * static_cast<size_t>(L.width) + rx0;
+                float* dst = planes + q * plane_values;
+                for (int i = threadIdx.x; i < rows * cols; i += blockDim.x) {
+                    const int r = i / cols;
+                    const int cx = i - r * cols;
+                    dst[r * L.region_stride + cx] = __ldg(src + static_cast<size_t>(r) * L.width + cx);
+                }
             }
         }
         __syncthreads();
@@ -790,7 +866,7 @@ cudaError_t launch_centers(const CentersLaunch& L, cudaStream_t stream) {
 }
 
 size_t match_shared_bytes(const MatchLaunch& L, int warps) {
-    const size_t plane = static_cast<size_t>(L.region_rows) * L.region_stride;
+    const size_t plane = static_cast<size_t>(L.plane_floats);
     const size_t planes = static_cast<size_t>(L.search_channels) * L.Pt * plane + (L.approx ? 2 * plane : 0);
     return (planes + static_cast<size_t>(warps) * L.warp_floats) * sizeof(float);
 }
@@ -800,15 +876,45 @@ int match_warp_floats(int window_cells, int planes_n, int P, int buffer_cap) {
     return (f + 3) & ~3;
 }
 
-cudaError_t launch_match(const MatchLaunch& L, int strips, int warps, cudaStream_t stream) {
+bool encode_store_map(CUtensorMap* map, const float* base, int width, long long rows, int box_w, int box_h) {
+    const uintptr_t addr = reinterpret_cast<uintptr_t>(base);
+    if (!base || addr % 16 != 0 || (static_cast<size_t>(width) * sizeof(float)) % 16 != 0 || box_w <= 0 ||
+        box_w > 256 || box_h <= 0 || box_h > 256 || (box_w * sizeof(float)) % 16 != 0 || rows <= 0)
+        return false;
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Encode encode = [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult found{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &found) != cudaSuccess ||
+            found != cudaDriverEntryPointSuccess)
+            fn = nullptr;
+        return reinterpret_cast<Encode>(fn);
+    }();
+    if (!encode) return false;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(width), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(width) * sizeof(float)};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(box_w), static_cast<cuuint32_t>(box_h)};
+    const cuuint32_t elem[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, elem,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cudaError_t launch_match(const MatchLaunch& L, int strips, int warps, const CUtensorMap* tmap, cudaStream_t stream) {
     if (strips <= 0) return cudaSuccess;
+    if (L.tma && (!tmap || L.centers || L.region_stride % 4 != 0 || L.plane_floats % 32 != 0))
+        return cudaErrorInvalidValue;
     const size_t smem = match_shared_bytes(L, warps);
     const dim3 block(32 * warps);
+    CUtensorMap map{};
+    if (tmap) map = *tmap;
     cudaError_t err = cudaSuccess;
     auto launch = [&](auto kernel) {
         err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (err != cudaSuccess) return;
-        kernel<<<strips, block, smem, stream>>>(L);
+        kernel<<<strips, block, smem, stream>>>(L, map);
         err = cudaGetLastError();
     };
     if (L.centers) {  // flow-guided search: windows around per-frame search centres

@@ -248,12 +248,17 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    // completion of every MMA this CTA issued, committed once before the
+    // tensor memory is released
+    __shared__ __align__(8) unsigned long long drain_bar;
+    const uint32_t drain = smem_addr(reinterpret_cast<unsigned char*>(&drain_bar));
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
             mbar_init(full_bar(bars, s), 1);
             mbar_init(tfull_bar(bars, s), 1);
             mbar_init(free_bar(bars, s), kConsumerWarps);
         }
+        mbar_init(drain, 1);
     }
     tc_fence_before();
     __syncthreads();
@@ -414,6 +419,11 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
             for (int k = 0; k < T; ++k, ++i) {
                 const int b = i & 1;
                 wait(full_bar(bars, b), (i >> 1) & 1);
+                // after a wait ran out no further MMA is issued (the whole
+                // warp agrees); L.stall_mma, a test switch, issues none at
+                // all so that the consumers' waits run out
+                timed_out = __any_sync(0xffffffffu, timed_out);
+                if (timed_out || L.stall_mma) continue;
                 tc_fence_after();
                 {
                     const unsigned char* st = smem + b * lay.stage_bytes;
@@ -486,11 +496,18 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
             }
         }
     }
-    // release the tensor memory (every MMA completed and was read back)
+    // release the tensor memory once every MMA issued has completed: a
+    // commit of all of them to the drain barrier, waited for with a bound,
+    // also after a timeout left MMAs unread
     tc_fence_before();
     __syncthreads();
     if (warp == kMmaWarp) {
         tc_fence_after();
+        tc_commit(drain, lane == 0 ? 1u : 0u);
+        int polls = 0;
+        while (!mbar_try_wait(drain, 0) && ++polls < kSpinLimit) {
+        }
+        if (polls >= kSpinLimit) atomicCAS(L.status, 0, kStatusTensorTimeout);
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kPipeTmemCols)
                      : "memory");
     }

@@ -23,6 +23,7 @@
 
 #include "../../include/vnlbgpu.h"
 #include "../../include/vnlbgpu_diag.h"
+#include "learned.h"
 #include "mvtools.h"
 #include "vnlb_kernels.h"
 
@@ -103,6 +104,14 @@ struct Grid {
     // the same for the flow-guided search, built for flow_reach (x, y)
     DeviceArray<int2> d_flow_grid_rows, d_flow_anchors;
     int2 flow_reach = make_int2(-1, -1);
+    // learned form: strips that do not cross a tile, each strip's tile, and
+    // per tile the anchor the full search checks (its first), as a one-anchor
+    // strip over a compact anchor list
+    std::vector<Strip> tile_strips;
+    DeviceArray<Strip> d_tile_strips, d_check_strips;
+    DeviceArray<int> d_strip_tile, d_check_anchor;
+    DeviceArray<int2> d_check_anchors;
+    int tiles = 0;
 };
 
 }  // namespace
@@ -138,6 +147,20 @@ struct Session {
     cudaStream_t own_stream = nullptr;  // created by the session
     vnlbgpu_stats stats{};
     long long stats_uploads = 0;  // source frames copied to the device
+    bool allow_scatter = true;    // off while a diagnostic reads the filtered rows back
+    bool force_plain_match = false;  // the learned form's training pairs: the full search
+    bool stall_mma = false;          // test switch: the tensor-core matcher issues no MMA
+    // learned form (VNLBGPU_FORM_LEARNED): the attached network, shortlist
+    // size, recall threshold of the per-tile check, tile edge; the network
+    // sees slots_max scheduled frames of search_channels planes
+    bool learned = false;
+    vnlbgpu_mlp* mlp = nullptr;
+    MlpDevice mlp_net{};
+    int shortlist_len = 64, learned_tile = 64, slots_max = 1, learned_inputs = 0, learned_outputs = 0;
+    int cells_w = 0, cells_h = 0, max_tiles = 0;
+    float recall_threshold = 0.9f;
+    static constexpr int kLearnedChunk = 4096;  // anchors per network pass
+    static constexpr float kFeatureScale = 10.0f;
 
     // optional per-kernel timing: (category, start, stop) event triples
     bool timing = false;
@@ -358,6 +381,10 @@ struct Session {
         DeviceArray<FrameCounters> counters;
         DeviceArray<float> filtered, weights, gmeans, gram, eig, dual, logw;
         DeviceArray<float> approx;  // tensor-core form: approximate distances [G][approx_stride]
+        // learned form
+        DeviceArray<float> features, cells, mlp_acts, mlp_logits;
+        DeviceArray<int> shortlist, check_counts, check_vcounts, check_victims, tile_fail;
+        DeviceArray<MatchRow> check_rows;
     };
 #ifndef VNLB_MAX_LANES
 #define VNLB_MAX_LANES 8  // a build parameter for comparisons
@@ -460,6 +487,7 @@ struct Session {
     // Waits for everything the session queued on any of its streams.
     void drain() {
         if (stream) cudaStreamSynchronize(stream);
+        if (own_stream && own_stream != stream) cudaStreamSynchronize(own_stream);
         for (Lane& l : lanes)
             if (l.stream) cudaStreamSynchronize(l.stream);
         for (auto& w : workers)
@@ -480,6 +508,33 @@ struct Session {
             check(cudaEventRecord(ev_lane[i], lanes[i].stream), "cudaEventRecord(join)");
             check(cudaStreamWaitEvent(stream, ev_lane[i], 0), "cudaStreamWaitEvent(join)");
         }
+    }
+
+    // Shared floats per staged plane of the plain matcher: whole 128-byte
+    // units, so that every plane starts where a tensor-memory-accelerator
+    // tile load may write.
+    static int plane_floats_of(int rows, int stride) { return (rows * stride + 31) & ~31; }
+
+    // The plain matcher stages its search regions with tile loads from a
+    // tensor map over the search store (rows of `width` floats: every plane
+    // of every slot), when the row pitch allows (width a multiple of 4).
+#ifndef VNLB_MATCH_TMA
+#define VNLB_MATCH_TMA 1  // a build parameter for comparisons
+#endif
+    CUtensorMap search_map{};
+    const float* search_map_base = nullptr;
+    long long search_map_rows = 0;
+    const CUtensorMap* search_tensor_map(const float* base) {
+        if (!VNLB_MATCH_TMA) return nullptr;
+        const int src = stage == 1 ? VNLBGPU_SOURCE_REF : VNLBGPU_SOURCE_CLIP;
+        const long long slots = store[src].borrowed ? frames : ring + (ring < frames ? Pt - 1 : 0);
+        const long long rows = slots * channels * static_cast<long long>(height);
+        if (base == search_map_base && rows == search_map_rows) return &search_map;
+        search_map_base = nullptr;
+        if (!encode_store_map(&search_map, base, width, rows, region_stride, region_rows)) return nullptr;
+        search_map_base = base;
+        search_map_rows = rows;
+        return &search_map;
     }
 
     size_t plane() const { return static_cast<size_t>(width) * height; }
@@ -521,8 +576,9 @@ struct Session {
         require(p.device_id >= 0, "device_id must be non-negative");
         require(p.num_streams >= 1 && p.num_streams <= 32, "num_streams must be in the range 1..32");
         require(p.chunk_size > 0, "chunk_size must be positive");
-        require(p.form == VNLBGPU_FORM_PLAIN || p.form == VNLBGPU_FORM_CHOSEN || p.form == VNLBGPU_FORM_CHOSEN_TC,
-                "form must be plain (0), chosen (1) or chosen_tc (2)");
+        require(p.form == VNLBGPU_FORM_PLAIN || p.form == VNLBGPU_FORM_CHOSEN || p.form == VNLBGPU_FORM_CHOSEN_TC ||
+                    p.form == VNLBGPU_FORM_LEARNED,
+                "form must be plain (0), chosen (1), chosen_tc (2) or learned (3)");
     }
 
     void configure(const vnlbgpu_params& p, int w, int h, int n, int c) {
@@ -615,6 +671,7 @@ struct Session {
             probe.Pt = Pt;
             probe.region_rows = region_rows;
             probe.region_stride = region_stride;
+            probe.plane_floats = plane_floats_of(region_rows, region_stride);
             probe.approx = approx ? 1 : 0;
             probe.warp_floats = match_warp_floats(cw0 * ch0, search_channels * Pt, P, buffer_cap);
             if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
@@ -632,6 +689,7 @@ struct Session {
             probe.Pt = Pt;
             probe.region_rows = flow_region_rows;
             probe.region_stride = flow_region_stride;
+            probe.plane_floats = plane_floats_of(flow_region_rows, flow_region_stride);
             probe.warp_floats = match_warp_floats(cw0 * ch0, search_channels * Pt, P, buffer_cap);
             if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
         }
@@ -710,8 +768,31 @@ struct Session {
             l.row_info.allocate(R, "cudaMalloc(row info)");
             l.row_group.allocate(R, "cudaMalloc(row groups)");
         }
-        d_totals.allocate(2, "cudaMalloc(totals)");
-        check(cudaMemset(d_totals.ptr, 0, 2 * sizeof(unsigned long long)), "cudaMemset(totals)");
+        // learned form: network shape and per-lane buffers (the network's own
+        // activations follow once one is attached)
+        learned = p.form == VNLBGPU_FORM_LEARNED;
+        slots_max = p.search_bwd + p.search_fwd + 1;
+        learned_inputs = slots_max * search_channels * 9;
+        learned_outputs = slots_max * p.search_window * p.search_window;
+        cells_w = (width + kFeatureCell - 1) / kFeatureCell;
+        cells_h = (height + kFeatureCell - 1) / kFeatureCell;
+        if (learned) {
+            max_tiles = ((width + learned_tile - 1) / learned_tile) * ((height + learned_tile - 1) / learned_tile);
+            for (int li = 0; li < lane_count; ++li) {
+                Lane& l = lanes[li];
+                l.features.allocate(G * learned_inputs, "cudaMalloc(learned features)");
+                l.cells.allocate(static_cast<size_t>(slots_max) * search_channels * cells_w * cells_h,
+                                 "cudaMalloc(learned cells)");
+                l.shortlist.allocate(G * kShortlistMax, "cudaMalloc(learned shortlist)");
+                l.check_rows.allocate(static_cast<size_t>(max_tiles) * max_rows, "cudaMalloc(check rows)");
+                l.check_counts.allocate(max_tiles, "cudaMalloc(check counts)");
+                l.check_vcounts.allocate(max_tiles, "cudaMalloc(check victims)");
+                l.check_victims.allocate(static_cast<size_t>(max_tiles) * victim_stride, "cudaMalloc(check victims)");
+                l.tile_fail.allocate(max_tiles, "cudaMalloc(tile flags)");
+            }
+        }
+        d_totals.allocate(4, "cudaMalloc(totals)");
+        check(cudaMemset(d_totals.ptr, 0, 4 * sizeof(unsigned long long)), "cudaMemset(totals)");
         d_status.allocate(1, "cudaMalloc(status)");
         check(cudaMemset(d_status.ptr, 0, sizeof(int)), "cudaMemset(status)");
         check(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "cudaEventCreate");
@@ -910,6 +991,92 @@ struct Session {
         Grid& ref_grid = *grid;
         grids.emplace(key, std::move(grid));
         return ref_grid;
+    }
+
+    // Learned form: the grid's tiles (learned_tile pixels by anchor
+    // position), strips that stay inside one tile, and each tile's checked
+    // anchor (its first) as a one-anchor strip over a compact anchor list.
+    void ensure_tiles(Grid& grid) {
+        if (grid.tiles > 0 && grid.d_tile_strips.ptr) return;
+        const auto& a = grid.anchors;
+        const int tx_n = (width + learned_tile - 1) / learned_tile;
+        auto tile_of = [&](int2 p) { return (p.y / learned_tile) * tx_n + p.x / learned_tile; };
+        std::vector<int> compact(static_cast<size_t>(max_tiles), -1);
+        std::vector<int> check_anchor;
+        for (size_t i = 0; i < a.size(); ++i) {
+            int& c = compact[static_cast<size_t>(tile_of(a[i]))];
+            if (c < 0) {
+                c = static_cast<int>(check_anchor.size());
+                check_anchor.push_back(static_cast<int>(i));
+            }
+        }
+        std::vector<Strip> strips;
+        std::vector<int> strip_tile;
+        size_t i = 0;
+        while (i < a.size()) {
+            Strip st{};
+            st.first = static_cast<int>(i);
+            st.y = a[i].y;
+            int yl, yh;
+            spatial_range(st.y, height, P, params.search_window, yl, yh);
+            st.region_y = yl;
+            st.region_h = yh - yl + 1 + P - 1;
+            const int tile = tile_of(a[i]);
+            int x0 = INT_MAX, x1 = INT_MIN, count = 0;
+            while (i < a.size() && a[i].y == st.y && count < warps && tile_of(a[i]) == tile) {
+                int xl, xh;
+                spatial_range(a[i].x, width, P, params.search_window, xl, xh);
+                const int nx0 = std::min(x0, xl & ~3), nx1 = std::max(x1, xh + P - 1);
+                if (count > 0 && nx1 - nx0 + 1 > region_w_max) break;
+                x0 = nx0;
+                x1 = nx1;
+                ++count;
+                ++i;
+            }
+            st.count = count;
+            st.region_x = x0;
+            st.region_w = x1 - x0 + 1;
+            strips.push_back(st);
+            strip_tile.push_back(compact[static_cast<size_t>(tile)]);
+        }
+        std::vector<Strip> checks;
+        std::vector<int2> check_xy;
+        for (size_t t = 0; t < check_anchor.size(); ++t) {
+            const int2 p = a[static_cast<size_t>(check_anchor[t])];
+            Strip st{};
+            st.first = static_cast<int>(t);
+            st.count = 1;
+            st.y = p.y;
+            int lo, hi;
+            spatial_range(p.y, height, P, params.search_window, lo, hi);
+            st.region_y = lo;
+            st.region_h = hi - lo + 1 + P - 1;
+            spatial_range(p.x, width, P, params.search_window, lo, hi);
+            st.region_x = lo & ~3;
+            st.region_w = hi + P - 1 - st.region_x + 1;
+            checks.push_back(st);
+            check_xy.push_back(p);
+        }
+        grid.tiles = static_cast<int>(check_anchor.size());
+        grid.tile_strips = strips;
+        grid.d_tile_strips.allocate(strips.size(), "cudaMalloc(tile strips)");
+        grid.d_strip_tile.allocate(strip_tile.size(), "cudaMalloc(strip tiles)");
+        grid.d_check_strips.allocate(checks.size(), "cudaMalloc(check strips)");
+        grid.d_check_anchor.allocate(check_anchor.size(), "cudaMalloc(check anchors)");
+        grid.d_check_anchors.allocate(check_xy.size(), "cudaMalloc(check anchors)");
+        check(cudaMemcpy(grid.d_tile_strips.ptr, strips.data(), strips.size() * sizeof(Strip), cudaMemcpyHostToDevice),
+              "cudaMemcpy(tile strips)");
+        check(cudaMemcpy(grid.d_strip_tile.ptr, strip_tile.data(), strip_tile.size() * sizeof(int),
+                         cudaMemcpyHostToDevice),
+              "cudaMemcpy(strip tiles)");
+        check(cudaMemcpy(grid.d_check_strips.ptr, checks.data(), checks.size() * sizeof(Strip), cudaMemcpyHostToDevice),
+              "cudaMemcpy(check strips)");
+        check(cudaMemcpy(grid.d_check_anchor.ptr, check_anchor.data(), check_anchor.size() * sizeof(int),
+                         cudaMemcpyHostToDevice),
+              "cudaMemcpy(check anchors)");
+        check(cudaMemcpy(grid.d_check_anchors.ptr, check_xy.data(), check_xy.size() * sizeof(int2),
+                         cudaMemcpyHostToDevice),
+              "cudaMemcpy(check anchors)");
     }
 
     void require_sources() {
@@ -1136,6 +1303,7 @@ struct Session {
         m.anchor_map = grid.d_map.ptr;
         m.region_rows = region_rows;
         m.region_stride = region_stride;
+        m.plane_floats = plane_floats_of(region_rows, region_stride);
         const int cw = std::min(params.search_window, width - P + 1);
         const int chh = std::min(params.search_window, height - P + 1);
         m.window_cells = cw * chh;
@@ -1172,8 +1340,88 @@ struct Session {
             m.approx = 0;
             m.region_rows = flow_region_rows;
             m.region_stride = flow_region_stride;
+            m.plane_floats = plane_floats_of(flow_region_rows, flow_region_stride);
             m.region_w_max = flow_region_w_max;
-            check(launch_match(m, static_cast<int>(grid.strips.size()), warps, ls), "match kernel launch");
+            check(launch_match(m, static_cast<int>(grid.strips.size()), warps, nullptr, ls), "match kernel launch");
+        } else if (learned && !force_plain_match) {
+            if (!mlp) fail("VNLB CUDA: the learned form needs a network (vnlbgpu_set_learned)");
+            ensure_tiles(grid);
+            LearnedLaunch ll{};
+            ll.video = search;
+            ll.ring = ring;
+            ll.width = width;
+            ll.height = height;
+            ll.channels = channels;
+            ll.search_channels = search_channels;
+            ll.P = P;
+            ll.Pt = Pt;
+            ll.search_window = params.search_window;
+            for (int i = 0; i < schedule_len; ++i) ll.schedule[i] = schedule[i];
+            ll.schedule_len = schedule_len;
+            ll.slots_max = slots_max;
+            ll.anchor_frame = anchor;
+            ll.anchors = grid.d_anchors.ptr;
+            ll.anchor_count = G;
+            ll.anchor_map = grid.d_map.ptr;
+            ll.cells = lane.cells.ptr;
+            ll.cells_w = cells_w;
+            ll.cells_h = cells_h;
+            ll.features = lane.features.ptr;
+            ll.inputs = learned_inputs;
+            ll.feature_scale = kFeatureScale;
+            ll.shortlist = lane.shortlist.ptr;
+            ll.shortlist_len = shortlist_len;
+            ll.K = K;
+            ll.soft_cap = soft_cap;
+            ll.max_rows = max_rows;
+            ll.tau = params.tau;
+            ll.rows = lane.rows.ptr;
+            ll.row_counts = lane.row_counts.ptr;
+            ll.victims = lane.victims.ptr;
+            ll.victim_counts = lane.victim_counts.ptr;
+            ll.victim_stride = victim_stride;
+            ll.tiles = grid.tiles;
+            ll.check_anchor = grid.d_check_anchor.ptr;
+            ll.check_rows = lane.check_rows.ptr;
+            ll.check_counts = lane.check_counts.ptr;
+            ll.recall_threshold = recall_threshold;
+            ll.tile_fail = lane.tile_fail.ptr;
+            ll.totals = d_totals.ptr + 2;
+            // features, the network's shortlist in chunks, the shortlist matcher
+            check(launch_learned_features(ll, ls), "learned features launch");
+            float* acts[kMlpMaxLayers];
+            for (int l = 0; l < mlp_net.layers; ++l)
+                acts[l] = lane.mlp_acts.ptr + static_cast<size_t>(l) * kLearnedChunk * mlp_net.hidden;
+            for (int g0 = 0; g0 < G; g0 += kLearnedChunk) {
+                const int n = std::min(kLearnedChunk, G - g0);
+                check(mlp_forward(mlp_net, lane.features.ptr + static_cast<size_t>(g0) * learned_inputs, n, acts,
+                                  lane.mlp_logits.ptr, ls),
+                      "learned network launch");
+                check(logits_topk(lane.mlp_logits.ptr, n, learned_outputs, shortlist_len,
+                                  lane.shortlist.ptr + static_cast<size_t>(g0) * shortlist_len, ls),
+                      "shortlist launch");
+            }
+            check(launch_learned_match(ll, ls), "learned match launch");
+            // the judge: the full search for each tile's checked anchor
+            const CUtensorMap* map = search_tensor_map(search);
+            MatchLaunch mc = m;
+            mc.tma = map ? 1 : 0;
+            mc.anchors = grid.d_check_anchors.ptr;
+            mc.strips = grid.d_check_strips.ptr;
+            mc.rows = lane.check_rows.ptr;
+            mc.row_counts = lane.check_counts.ptr;
+            mc.victims = lane.check_victims.ptr;
+            mc.victim_counts = lane.check_vcounts.ptr;
+            check(launch_match(mc, grid.tiles, warps, map, ls), "check match launch");
+            check(launch_learned_recall(ll, ls), "recall launch");
+            // the full search for the tiles that failed it
+            MatchLaunch mf = m;
+            mf.tma = map ? 1 : 0;
+            mf.strips = grid.d_tile_strips.ptr;
+            mf.strip_tile = grid.d_strip_tile.ptr;
+            mf.tile_fail = lane.tile_fail.ptr;
+            check(launch_match(mf, static_cast<int>(grid.tile_strips.size()), warps, map, ls), "fallback match launch");
+            stats.kernel_launches += 6 + 2 * ((G + kLearnedChunk - 1) / kLearnedChunk) * (mlp_net.layers + 1);
         } else if (chosen) {
             m.strips = grid.d_strips_chosen.ptr;
             m.tiles_x = chosen_tiles_x;
@@ -1182,9 +1430,12 @@ struct Session {
             m.anchor_count = static_cast<int>(grid.anchors.size());
             m.strip_count = static_cast<int>(grid.strips_chosen.size());
             m.window_rows = chosen_wy;
+            m.stall_mma = stall_mma ? 1 : 0;
             check(launch_match_chosen(m, static_cast<int>(grid.strips_chosen.size()), ls), "match kernel launch");
         } else {
-            check(launch_match(m, static_cast<int>(grid.strips.size()), warps, ls), "match kernel launch");
+            const CUtensorMap* map = search_tensor_map(search);
+            m.tma = map ? 1 : 0;
+            check(launch_match(m, static_cast<int>(grid.strips.size()), warps, map, ls), "match kernel launch");
         }
         end_timed(kTimedMatch, t0, ls);
 
@@ -1210,6 +1461,9 @@ struct Session {
         fl.noisy = clip;
         fl.basic = ref;
         fl.ring = ring;
+        // the chosen forms' filter (TF32 Gram, FP64 angles) goes with their
+        // matchers; configurations that run the plain matcher stay exact
+        fl.mixed = (approx || chosen) && !flow_on() ? 1 : 0;
         fl.width = width;
         fl.height = height;
         fl.channels = channels;
@@ -1243,6 +1497,18 @@ struct Session {
         fl.eig = lane.eig.ptr;
         fl.dual = lane.dual.ptr;
         fl.flags = lane.gflags.ptr;
+        // chosen forms on the warp-per-group shapes: apply adds its rows
+        // straight into the cleared stack, and no stack tiles run
+        const bool scatter = fl.mixed && allow_scatter && filter_can_scatter(fl);
+        if (scatter) {
+            check(cudaMemsetAsync(stack, 0, stack_values() * sizeof(float), ls), "cudaMemsetAsync(stack)");
+            fl.scatter = stack;
+            fl.window = d_window.ptr;
+            fl.windowed = params.weight_gamma != 0.0f ? 1 : 0;
+            fl.slots = slots;
+            fl.search_bwd = params.search_bwd;
+            fl.anchor_frame = anchor;
+        }
         t0 = begin_timed(ls);
         check(launch_filter(fl, G, ls), "filter kernel launch");
         end_timed(kTimedFilter, t0, ls);
@@ -1282,13 +1548,15 @@ struct Session {
             tl.tile_grid_rows = grid.d_flow_grid_rows.ptr;
             tl.tile_anchors = grid.d_flow_anchors.ptr;
         }
-        t0 = begin_timed(ls);
-        check(launch_tiles(tl, ls), "tile kernel launch");
-        end_timed(kTimedTiles, t0, ls);
+        if (!scatter) {
+            t0 = begin_timed(ls);
+            check(launch_tiles(tl, ls), "tile kernel launch");
+            end_timed(kTimedTiles, t0, ls);
+        }
         read_frames(ls, low, high + Pt - 1);
         stats.anchor_frames += 1;
         stats.groups += G;
-        stats.kernel_launches += params.rank > 0 ? 6 : 5;
+        stats.kernel_launches += (params.rank > 0 ? 6 : 5) - (scatter ? 1 : 0);
     }
 
     // The stack of `anchor`, computed on the next lane when not cached.  The
@@ -1409,6 +1677,8 @@ struct Session {
             if (status == kStatusRankNotCovered) fail("VNLB CUDA: group_size must cover the effective VNLB rank");
             if (status == kStatusTensorTimeout)
                 fail("VNLB CUDA: the tensor-core matcher timed out waiting for its MMAs");
+            if (status == kStatusTmaTimeout)
+                fail("VNLB CUDA: the matcher timed out waiting for a tensor-memory-accelerator load");
             fail("VNLB CUDA: device status " + std::to_string(status));
         }
     }
@@ -1853,6 +2123,68 @@ int vnlbgpu_render_clip_host(vnlbgpu_session* session, float* out) {
     });
 }
 
+int vnlbgpu_render_chain_device(vnlbgpu_session* basic_session, vnlbgpu_session* final_session, float* basic_out,
+                                float* final_out) {
+    return guarded([&]() {
+        if (!basic_session || !final_session || !basic_out || !final_out) vnlbgpu::fail("VNLB CUDA: null argument");
+        Session& b = basic_session->impl;
+        Session& f = final_session->impl;
+        if (&b == &f || b.stage != 0 || f.stage != 1)
+            vnlbgpu::fail("VNLB CUDA: a chain takes a Basic session and a Final session");
+        if (b.width != f.width || b.height != f.height || b.frames != f.frames || b.channels != f.channels ||
+            b.device != f.device)
+            vnlbgpu::fail("VNLB CUDA: the Basic and Final sessions of a chain must share clip geometry and device");
+        std::scoped_lock locks(b.lock, f.lock);
+        if (!f.store[1].borrowed || f.ref != basic_out)
+            vnlbgpu::fail("VNLB CUDA: the Final session's ref must be the chain's Basic output "
+                          "(vnlbgpu_set_clip_device with that buffer)");
+        vnlbgpu::check(cudaSetDevice(b.device), "cudaSetDevice");
+        b.require_sources();
+        f.require_sources();
+        for (int n = 0; n < b.frames; ++n)
+            if (b.frames_pending(n) || f.frames_pending(n))
+                vnlbgpu::fail("VNLB CUDA: a chain render needs every source frame on the device, with no copy in flight");
+        // Basic on its stream; Final's normalisations on a stream of its own
+        // (its session stream, or its own stream when the two share one), so
+        // that Final frames do not hold up later Basic frames; the caller's
+        // Basic stream waits for everything at the end.
+        cudaStream_t fs = f.stream == b.stream ? f.own_stream : f.stream;
+        b.fork(b.stream);
+        f.fork(b.stream);
+        vnlbgpu::check(cudaEventRecord(f.ev_fork, b.stream), "cudaEventRecord(chain fork)");
+        vnlbgpu::check(cudaStreamWaitEvent(fs, f.ev_fork, 0), "cudaStreamWaitEvent(chain fork)");
+        const size_t fv = b.frame_values();
+        int next_final = 0;
+        for (int n = 0; n < b.frames; ++n) {
+            b.render_to_device(n, basic_out + fv * n, b.stream);
+            int lo, hi;
+            if (next_final < f.frames) f.required_range(next_final, lo, hi);
+            if (next_final < f.frames && (hi <= n || n == b.frames - 1)) {
+                // Basic frames 0..n are normalised once this point of the
+                // Basic stream is reached (in frame order): Final's lanes may
+                // read them after it
+                auto ready = b.record_read(b.stream);
+                for (int i = 0; i < f.lane_count; ++i)
+                    vnlbgpu::check(cudaStreamWaitEvent(f.lanes[i].stream, ready.get(), 0),
+                                   "cudaStreamWaitEvent(chain Basic frames)");
+                while (next_final < f.frames) {
+                    f.required_range(next_final, lo, hi);
+                    if (hi > n) break;
+                    f.render_to_device(next_final, final_out + fv * next_final, fs);
+                    ++next_final;
+                }
+            }
+        }
+        b.join();
+        for (int i = 0; i < f.lane_count; ++i) {
+            vnlbgpu::check(cudaEventRecord(f.ev_lane[i], f.lanes[i].stream), "cudaEventRecord(chain join)");
+            vnlbgpu::check(cudaStreamWaitEvent(fs, f.ev_lane[i], 0), "cudaStreamWaitEvent(chain join)");
+        }
+        vnlbgpu::check(cudaEventRecord(f.ev_main, fs), "cudaEventRecord(chain end)");
+        vnlbgpu::check(cudaStreamWaitEvent(b.stream, f.ev_main, 0), "cudaStreamWaitEvent(chain end)");
+    });
+}
+
 int vnlbgpu_synchronize(vnlbgpu_session* session) {
     return guarded([&]() {
         Session& s = session->impl;
@@ -2065,18 +2397,155 @@ int vnlbgpu_shard_plan(int frames, int world, int rank, int basic_search_bwd, in
     });
 }
 
+int vnlbgpu_set_learned(vnlbgpu_session* session, vnlbgpu_mlp* mlp, int shortlist, float recall_threshold,
+                        int tile) {
+    return guarded([&]() {
+        if (!session || !mlp) vnlbgpu::fail("VNLB CUDA: null argument");
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        if (!s.learned) vnlbgpu::fail("VNLB CUDA: the session's form is not learned (3)");
+        if (shortlist < 1 || shortlist > vnlbgpu::kShortlistMax)
+            vnlbgpu::fail("VNLB CUDA: the shortlist must hold 1.." + std::to_string(vnlbgpu::kShortlistMax) +
+                          " offsets");
+        if (!(recall_threshold >= 0.0f) || !std::isfinite(recall_threshold))
+            vnlbgpu::fail("VNLB CUDA: the recall threshold must be finite and non-negative");
+        if (tile != s.learned_tile) vnlbgpu::fail("VNLB CUDA: the tile edge of this build is " +
+                                                  std::to_string(s.learned_tile) + " pixels");
+        const vnlbgpu::MlpDevice net = vnlbgpu::mlp_device(mlp);
+        if (net.inputs != s.learned_inputs || net.outputs != s.learned_outputs)
+            vnlbgpu::fail("VNLB CUDA: the network must have " + std::to_string(s.learned_inputs) + " inputs and " +
+                          std::to_string(s.learned_outputs) + " outputs for this session");
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.drain();
+        for (int li = 0; li < s.lanes_allocated; ++li) {
+            Session::Lane& l = s.lanes[li];
+            l.mlp_acts.allocate(static_cast<size_t>(net.layers) * Session::kLearnedChunk * net.hidden,
+                                "cudaMalloc(network activations)");
+            l.mlp_logits.allocate(static_cast<size_t>(Session::kLearnedChunk) * net.outputs,
+                                  "cudaMalloc(network logits)");
+        }
+        s.mlp = mlp;
+        s.mlp_net = net;
+        s.shortlist_len = shortlist;
+        s.recall_threshold = recall_threshold;
+        s.invalidate();
+    });
+}
+
+int vnlbgpu_learned_pairs(vnlbgpu_session* session, int anchor, float* features, int* targets, int capacity, int k,
+                          int* count, int* inputs) {
+    return guarded([&]() {
+        if (!session || !count || !inputs || k <= 0) vnlbgpu::fail("VNLB CUDA: null argument");
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.require_sources();
+        if (anchor < 0 || anchor > s.frames - s.Pt) vnlbgpu::fail("VNLB CUDA: anchor frame out of range");
+        vnlbgpu::DeviceArray<float> stack, cells, feats;
+        stack.allocate(s.stack_values(), "cudaMalloc(diag stack)");
+        vnlbgpu::Grid& grid = s.grid_for(anchor);
+        const int G = static_cast<int>(grid.anchors.size());
+        *count = G;
+        *inputs = s.learned_inputs;
+        // the full exact search (and the rest of the anchor frame) on lane 0
+        s.fork();
+        Session::Lane& lane = s.lanes[0];
+        s.force_plain_match = true;
+        s.allow_scatter = false;
+        try {
+            s.compute_anchor(anchor, stack.ptr, lane);
+        } catch (...) {
+            s.force_plain_match = false;
+            s.allow_scatter = true;
+            throw;
+        }
+        s.force_plain_match = false;
+        s.allow_scatter = true;
+        // features of the same anchors
+        int low, high;
+        vnlbgpu::temporal_range(s.frames, s.Pt, s.params.search_bwd, s.params.search_fwd, anchor, low, high);
+        vnlbgpu::LearnedLaunch ll{};
+        ll.video = s.stage == 1 ? s.ref : s.clip;
+        ll.ring = s.ring;
+        ll.width = s.width;
+        ll.height = s.height;
+        ll.channels = s.channels;
+        ll.search_channels = s.search_channels;
+        ll.P = s.P;
+        ll.Pt = s.Pt;
+        ll.search_window = s.params.search_window;
+        int schedule[vnlbgpu::kMaxContributors];
+        int len = 0;
+        schedule[len++] = anchor;
+        for (int f = anchor + 1; f <= high; ++f) schedule[len++] = f;
+        for (int f = anchor - 1; f >= low; --f) schedule[len++] = f;
+        for (int i = 0; i < len; ++i) ll.schedule[i] = schedule[i];
+        ll.schedule_len = len;
+        ll.slots_max = s.slots_max;
+        ll.anchor_frame = anchor;
+        ll.anchors = grid.d_anchors.ptr;
+        ll.anchor_count = G;
+        cells.allocate(static_cast<size_t>(s.slots_max) * s.search_channels * s.cells_w * s.cells_h, "cudaMalloc");
+        feats.allocate(static_cast<size_t>(G) * s.learned_inputs, "cudaMalloc(features)");
+        ll.cells = cells.ptr;
+        ll.cells_w = s.cells_w;
+        ll.cells_h = s.cells_h;
+        ll.features = feats.ptr;
+        ll.inputs = s.learned_inputs;
+        ll.feature_scale = Session::kFeatureScale;
+        vnlbgpu::check(vnlbgpu::launch_learned_features(ll, lane.stream), "learned features launch");
+        s.join();
+        s.check_status();
+        const int n = std::min(G, capacity);
+        if (features && n > 0)
+            vnlbgpu::check(cudaMemcpy(features, feats.ptr, static_cast<size_t>(n) * s.learned_inputs * sizeof(float),
+                                      cudaMemcpyDeviceToHost),
+                           "copy");
+        if (targets && n > 0) {
+            std::vector<int> counts(G);
+            std::vector<vnlbgpu::MatchRow> rows(static_cast<size_t>(G) * s.max_rows);
+            vnlbgpu::check(cudaMemcpy(counts.data(), lane.row_counts.ptr, G * sizeof(int), cudaMemcpyDeviceToHost),
+                           "copy");
+            vnlbgpu::check(cudaMemcpy(rows.data(), lane.rows.ptr, rows.size() * sizeof(vnlbgpu::MatchRow),
+                                      cudaMemcpyDeviceToHost),
+                           "copy");
+            const int W = s.params.search_window;
+            for (int g = 0; g < n; ++g) {
+                const int2 a = grid.anchors[static_cast<size_t>(g)];
+                int xl, xh, yl, yh;
+                vnlbgpu::spatial_range(a.x, s.width, s.P, W, xl, xh);
+                vnlbgpu::spatial_range(a.y, s.height, s.P, W, yl, yh);
+                for (int j = 0; j < k; ++j) {
+                    int cls = -1;
+                    if (j < counts[g]) {
+                        const vnlbgpu::MatchRow m = rows[static_cast<size_t>(g) * s.max_rows + j];
+                        int kk = 0;
+                        while (kk < len && schedule[kk] != m.frame) ++kk;
+                        if (kk < len) cls = (kk * W + (m.y - yl)) * W + (m.x - xl);
+                    }
+                    targets[static_cast<size_t>(g) * k + j] = cls;
+                }
+            }
+        }
+        s.invalidate();
+    });
+}
+
 int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats) {
     return guarded([&]() {
         if (!session || !stats) vnlbgpu::fail("VNLB CUDA: null argument");
         Session& s = session->impl;
         std::lock_guard guard(s.lock);
         vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
-        unsigned long long totals[2] = {0, 0};
+        unsigned long long totals[4] = {0, 0, 0, 0};
+        s.drain();
         vnlbgpu::check(cudaMemcpyAsync(totals, s.d_totals.ptr, sizeof(totals), cudaMemcpyDeviceToHost, s.stream),
                        "cudaMemcpyAsync(totals)");
         vnlbgpu::check(cudaStreamSynchronize(s.stream), "cudaStreamSynchronize");
         s.stats.active_groups = static_cast<long long>(totals[0]);
         s.stats.rows = static_cast<long long>(totals[1]);
+        s.stats.learned_tiles = static_cast<long long>(totals[2]);
+        s.stats.learned_fallback_tiles = static_cast<long long>(totals[3]);
         s.stats.pipeline_lanes = s.lane_count;
         s.stats.source_slots = s.ring;
         s.stats.source_uploads = s.stats_uploads;
@@ -2115,6 +2584,16 @@ int vnlbgpu_diag_kernel_timing(vnlbgpu_session* session, int enable, double* ms,
     });
 }
 
+int vnlbgpu_diag_stall_tensor_waits(vnlbgpu_session* session, int on) {
+    return guarded([&]() {
+        if (!session) vnlbgpu::fail("VNLB CUDA: null argument");
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        s.stall_mma = on != 0;
+        s.invalidate();
+    });
+}
+
 int vnlbgpu_diag_set_lanes(vnlbgpu_session* session, int lanes) {
     return guarded([&]() {
         if (!session) vnlbgpu::fail("VNLB CUDA: null argument");
@@ -2124,6 +2603,41 @@ int vnlbgpu_diag_set_lanes(vnlbgpu_session* session, int lanes) {
         s.drain();
         s.lane_count = lanes <= 0 ? s.lanes_allocated : std::min(lanes, s.lanes_allocated);
         s.next_lane = 0;
+    });
+}
+
+int vnlbgpu_diag_filtered(vnlbgpu_session* session, int anchor, float* out, int capacity, int* rows, int* row_dim) {
+    return guarded([&]() {
+        if (!session || !rows || !row_dim) vnlbgpu::fail("VNLB CUDA: null argument");
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.require_sources();
+        if (anchor < 0 || anchor > s.frames - s.Pt) vnlbgpu::fail("VNLB CUDA: anchor frame out of range");
+        vnlbgpu::DeviceArray<float> stack;
+        stack.allocate(s.stack_values(), "cudaMalloc(diag stack)");
+        s.fork();
+        Session::Lane& lane = s.lanes[0];
+        s.allow_scatter = false;  // the rows are written out, for the read-back
+        try {
+            s.compute_anchor(anchor, stack.ptr, lane);
+        } catch (...) {
+            s.allow_scatter = true;
+            throw;
+        }
+        s.allow_scatter = true;
+        s.join();
+        s.check_status();
+        vnlbgpu::FrameCounters c{};
+        vnlbgpu::check(cudaMemcpy(&c, lane.counters.ptr, sizeof(c), cudaMemcpyDeviceToHost), "copy");
+        *rows = c.rows;
+        *row_dim = s.row_dim;
+        const int n = std::min(c.rows, capacity);
+        if (out && n > 0)
+            vnlbgpu::check(cudaMemcpy(out, lane.filtered.ptr, static_cast<size_t>(n) * s.row_dim * sizeof(float),
+                                      cudaMemcpyDeviceToHost),
+                           "copy");
+        s.invalidate();
     });
 }
 

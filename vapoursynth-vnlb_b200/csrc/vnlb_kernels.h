@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cstddef>
+#include <cuda.h>  // CUtensorMap (the type only; the encoder is fetched at run time)
 #include <cuda_runtime.h>
 
 #include "vnlb_common.cuh"
@@ -50,6 +51,10 @@ struct MatchLaunch {
     const int* anchor_map;  // [H][W] anchor index or -1
     int region_rows;      // shared rows per plane (incl. padding)
     int region_stride;    // shared row stride in floats
+    int plane_floats;     // shared floats per plane (region_rows * region_stride, or rounded up to 32
+                          // floats when the planes are loaded by the tensor memory accelerator)
+    int tma;              // stage each frame's planes with cp.async.bulk.tensor (the tensor map
+                          // covers the source store as rows of width `width`)
     int region_w_max;     // widest region a pass may stage (flow-guided search)
     int window_cells;     // max Wx*Wy
     int buffer_cap;       // match buffer capacity per warp
@@ -68,6 +73,13 @@ struct MatchLaunch {
     int approx_stride;    // >= schedule_len * window_cells
     int anchor_count;     // grid anchors of this anchor frame
     int strip_count;      // strips of the launch (tensor-core form)
+    // learned form's fallback: strip s belongs to tile strip_tile[s] and runs
+    // only when tile_fail of that tile is set (null: every strip runs)
+    const int* strip_tile;
+    const int* tile_fail;
+    // tensor-core matcher, for tests of its bounded waits: the MMA warp issues
+    // no MMA, so the waits for their completion run out (no MMA in flight)
+    int stall_mma;
     // outputs
     MatchRow* rows;       // [G][max_rows]
     int* row_counts;      // [G]
@@ -117,7 +129,14 @@ cudaError_t launch_centers(const CentersLaunch& L, cudaStream_t stream);
 
 size_t match_shared_bytes(const MatchLaunch& L, int warps);
 int match_warp_floats(int window_cells, int planes_n, int P, int buffer_cap);
-cudaError_t launch_match(const MatchLaunch& L, int strips, int warps, cudaStream_t stream);
+// tmap: the search source store as a 2-D float tensor (width x rows of every
+// plane of every slot), box (region_stride, region_rows); used when L.tma.
+cudaError_t launch_match(const MatchLaunch& L, int strips, int warps, const CUtensorMap* tmap,
+                         cudaStream_t stream);
+// Encodes the tensor map of a source store for the plain matcher's staging:
+// rows of `width` floats, `rows` of them, box (box_w, box_h).  False when the
+// layout cannot be loaded by TMA (row pitch or base not 16-byte aligned).
+bool encode_store_map(CUtensorMap* map, const float* base, int width, long long rows, int box_w, int box_h);
 
 // Device-side counters of one anchor frame.
 struct FrameCounters {
@@ -130,6 +149,7 @@ struct FrameCounters {
 constexpr int kStatusRankNotCovered = 1;  // fewer model rows than the rank
 constexpr int kStatusPasteCapacity = 2;   // too many anchors for the paste kernel
 constexpr int kStatusTensorTimeout = 3;   // an MMA completion wait ran out (tensor-core matcher)
+constexpr int kStatusTmaTimeout = 4;      // a tensor-memory-accelerator load wait ran out (plain matcher)
 
 struct PasteLaunch {
     int groups;
@@ -165,6 +185,14 @@ struct FilterLaunch {
     int models;             // models per group: 1, or the planes of an uncoupled clip
     int nmax;               // largest eigen problem: model rows, or dim where a covariance model occurs
     int row_dim;            // filtered row width: patch_dim * planes (dim when coupled)
+    int mixed;              // chosen forms: dual Gram on TF32 tensor cores (FP32 accumulation) and
+                            // FP64 Jacobi rotation angles; 0 = the CPU core's FP32 arithmetic
+    // chosen forms, warp-per-group shapes: the apply kernel adds each filtered
+    // row straight into the anchor frame's stack (atomics, any order) instead
+    // of writing it out for the stack tiles; null = write the rows
+    float* scatter;         // [slots][C+1][H][W], cleared before the launch
+    const float* window;    // [P*P] aggregation window
+    int windowed, slots, search_bwd, anchor_frame;
     StageConfig cfg;
     const MatchRow* rows;   // [G][max_rows]
     const int* row_counts;
@@ -199,6 +227,9 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups, cudaStream_t st
 // have; a shape above the limit cannot be filtered.
 size_t filter_shared_bytes(const FilterLaunch& L);
 size_t filter_shared_limit();
+// The shapes whose apply kernel can add rows straight into the stack
+// (FilterLaunch::scatter): warp-per-group, one model per group.
+bool filter_can_scatter(const FilterLaunch& L);
 
 struct TileLaunch {
     int width, height, channels;

@@ -128,9 +128,10 @@ def parse_parameters(stage: int, clip: np.ndarray, sigma, args: dict) -> lib.Par
     # distances on BF16 tensor cores (tcgen05, FP32 accumulation)
     p["form"] = lib.FORM_PLAIN
     if "form" in given:
-        forms = {"plain": lib.FORM_PLAIN, "chosen": lib.FORM_CHOSEN, "chosen_tc": lib.FORM_CHOSEN_TC}
+        forms = {"plain": lib.FORM_PLAIN, "chosen": lib.FORM_CHOSEN, "chosen_tc": lib.FORM_CHOSEN_TC,
+                 "learned": lib.FORM_LEARNED}
         if g("form") not in forms:
-            _err('form must be "plain", "chosen" or "chosen_tc"')
+            _err('form must be "plain", "chosen", "chosen_tc" or "learned"')
         p["form"] = forms[g("form")]
     # default group/rank clamps (cuda_plugin.cpp:482-534)
     default_group = "group_size" not in given

@@ -17,7 +17,7 @@ import numpy as np
 LIB_PATH = Path(os.environ.get("VNLBGPU_LIBRARY") or Path(__file__).resolve().parent / "lib" / "libvnlbgpu.so")
 
 STAGE_BASIC, STAGE_FINAL = 0, 1
-FORM_PLAIN, FORM_CHOSEN, FORM_CHOSEN_TC = 0, 1, 2
+FORM_PLAIN, FORM_CHOSEN, FORM_CHOSEN_TC, FORM_LEARNED = 0, 1, 2, 3
 SOURCE_CLIP, SOURCE_REF = 0, 1
 
 
@@ -44,7 +44,7 @@ class Params(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_longlong) for name in
                 ("anchor_frames", "groups", "active_groups", "rows", "kernel_launches", "pipeline_lanes",
-                 "source_slots", "source_uploads")]
+                 "source_slots", "source_uploads", "learned_tiles", "learned_fallback_tiles")]
 
 
 class MVToolsAnalysis(ctypes.Structure):
@@ -67,12 +67,16 @@ EXPORTS = [
     "vnlbgpu_last_error", "vnlbgpu_create", "vnlbgpu_destroy", "vnlbgpu_set_frame",
     "vnlbgpu_set_clip_host", "vnlbgpu_set_clip_device", "vnlbgpu_required_source_range",
     "vnlbgpu_render_frame", "vnlbgpu_render_frame_window",
-    "vnlbgpu_render_clip_host", "vnlbgpu_render_clip_device", "vnlbgpu_synchronize",
+    "vnlbgpu_render_clip_host", "vnlbgpu_render_clip_device", "vnlbgpu_render_chain_device", "vnlbgpu_synchronize",
     "vnlbgpu_render_stack", "vnlbgpu_aggregate", "vnlbgpu_aggregate_frame_noalloc", "vnlbgpu_get_stats",
     "vnlbgpu_stream",
     "vnlbgpu_set_stream", "vnlbgpu_diag_anchor", "vnlbgpu_diag_kernel_timing", "vnlbgpu_diag_set_lanes",
+    "vnlbgpu_diag_filtered", "vnlbgpu_diag_stall_tensor_waits",
     "vnlbgpu_parse_mvtools_analysis", "vnlbgpu_parse_mvtools_vectors", "vnlbgpu_set_mvtools_analysis",
-    "vnlbgpu_set_mvtools_frame", "vnlbgpu_shard_plan",
+    "vnlbgpu_set_mvtools_frame", "vnlbgpu_shard_plan", "vnlbgpu_mlp_create", "vnlbgpu_mlp_destroy",
+    "vnlbgpu_mlp_parameters", "vnlbgpu_mlp_get_weights", "vnlbgpu_mlp_set_weights", "vnlbgpu_mlp_gradients",
+    "vnlbgpu_mlp_train_step", "vnlbgpu_mlp_logits", "vnlbgpu_mlp_shortlist", "vnlbgpu_set_learned",
+    "vnlbgpu_learned_pairs",
 ]
 KERNEL_CLASSES = ("match", "paste", "filter", "tiles", "normalize")
 
@@ -109,6 +113,7 @@ def load() -> ctypes.CDLL:
                 ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_ssize_t)]
             lib.vnlbgpu_render_clip_host.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
             lib.vnlbgpu_render_clip_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.vnlbgpu_render_chain_device.argtypes = [ctypes.c_void_p] * 4
             lib.vnlbgpu_synchronize.argtypes = [ctypes.c_void_p]
             lib.vnlbgpu_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(Stats)]
             lib.vnlbgpu_stream.argtypes = [ctypes.c_void_p]
@@ -125,6 +130,9 @@ def load() -> ctypes.CDLL:
             lib.vnlbgpu_diag_kernel_timing.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
                                                        ctypes.c_void_p]
             lib.vnlbgpu_diag_set_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            lib.vnlbgpu_diag_stall_tensor_waits.argtypes = [ctypes.c_void_p, ctypes.c_int]
+            lib.vnlbgpu_diag_filtered.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                                  ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
             lib.vnlbgpu_parse_mvtools_analysis.argtypes = [ctypes.c_char_p, ctypes.c_size_t,
                                                            ctypes.POINTER(MVToolsAnalysis)]
             lib.vnlbgpu_parse_mvtools_vectors.argtypes = [
@@ -135,6 +143,26 @@ def load() -> ctypes.CDLL:
             lib.vnlbgpu_set_mvtools_frame.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
                                                       ctypes.c_size_t, ctypes.c_int]
             lib.vnlbgpu_shard_plan.argtypes = [ctypes.c_int] * 9 + [ctypes.POINTER(ctypes.c_int)] * 3
+            lib.vnlbgpu_mlp_create.argtypes = [ctypes.c_int] * 5 + [ctypes.c_uint, ctypes.c_int,
+                                                                   ctypes.POINTER(ctypes.c_void_p)]
+            lib.vnlbgpu_mlp_destroy.argtypes = [ctypes.c_void_p]
+            lib.vnlbgpu_mlp_destroy.restype = None
+            lib.vnlbgpu_mlp_parameters.argtypes = [ctypes.c_void_p]
+            lib.vnlbgpu_mlp_parameters.restype = ctypes.c_longlong
+            lib.vnlbgpu_mlp_get_weights.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.vnlbgpu_mlp_set_weights.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+            lib.vnlbgpu_mlp_gradients.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                  ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]
+            lib.vnlbgpu_mlp_train_step.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                                   ctypes.c_int, ctypes.c_float, ctypes.POINTER(ctypes.c_float)]
+            lib.vnlbgpu_mlp_logits.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+            lib.vnlbgpu_mlp_shortlist.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                  ctypes.c_void_p]
+            lib.vnlbgpu_set_learned.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_float,
+                                                ctypes.c_int]
+            lib.vnlbgpu_learned_pairs.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                  ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                  ctypes.POINTER(ctypes.c_int)]
             _lib = lib
     return _lib
 
@@ -165,6 +193,74 @@ def parse_mvtools_vectors(data: bytes, analysis: MVToolsAnalysis):
     _check(load().vnlbgpu_parse_mvtools_vectors(bytes(data), len(data), ctypes.byref(analysis), ctypes.byref(valid),
                                                 xy.ctypes.data, cap, ctypes.byref(count)))
     return bool(valid.value), xy[:count.value]
+
+
+class MLP:
+    """vnlbgpu_mlp: the learned proposals' network, trained and run by the
+    library's CUDA kernels.  x / targets / outputs are device pointers (e.g.
+    torch CUDA tensors' data_ptr()); weights and gradients are flat host
+    arrays, layer by layer [W_l (fan_out x fan_in)][b_l]."""
+
+    def __init__(self, inputs: int, hidden: int, layers: int, outputs: int, max_batch: int = 4096, seed: int = 0,
+                 device_id: int = 0):
+        self.lib = load()
+        self.shape = (inputs, hidden, layers, outputs)
+        handle = ctypes.c_void_p()
+        _check(self.lib.vnlbgpu_mlp_create(inputs, hidden, layers, outputs, max_batch, seed, device_id,
+                                           ctypes.byref(handle)))
+        self.handle = handle
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.vnlbgpu_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def parameters(self) -> int:
+        return int(self.lib.vnlbgpu_mlp_parameters(self.handle))
+
+    def get_weights(self) -> np.ndarray:
+        out = np.empty(self.parameters(), np.float32)
+        _check(self.lib.vnlbgpu_mlp_get_weights(self.handle, out.ctypes.data))
+        return out
+
+    def set_weights(self, flat: np.ndarray):
+        flat = _f32(flat)
+        if flat.size != self.parameters():
+            raise VNLBError("VNLB CUDA: weight count does not match the network")
+        _check(self.lib.vnlbgpu_mlp_set_weights(self.handle, flat.ctypes.data))
+
+    def gradients(self, x_ptr: int, targets_ptr: int, batch: int, tk: int):
+        grads = np.empty(self.parameters(), np.float32)
+        loss = ctypes.c_float()
+        _check(self.lib.vnlbgpu_mlp_gradients(self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(targets_ptr), batch,
+                                              tk, grads.ctypes.data, ctypes.byref(loss)))
+        return grads, loss.value
+
+    def train_step(self, x_ptr: int, targets_ptr: int, batch: int, tk: int, lr: float) -> float:
+        loss = ctypes.c_float()
+        _check(self.lib.vnlbgpu_mlp_train_step(self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(targets_ptr),
+                                               batch, tk, lr, ctypes.byref(loss)))
+        return loss.value
+
+    def logits(self, x_ptr: int, batch: int, out_ptr: int):
+        _check(self.lib.vnlbgpu_mlp_logits(self.handle, ctypes.c_void_p(x_ptr), batch, ctypes.c_void_p(out_ptr)))
+
+    def shortlist(self, x_ptr: int, batch: int, k: int, out_ptr: int):
+        _check(self.lib.vnlbgpu_mlp_shortlist(self.handle, ctypes.c_void_p(x_ptr), batch, k,
+                                              ctypes.c_void_p(out_ptr)))
+
+
+def render_chain_device(basic: "Session", final: "Session", basic_out_ptr: int, final_out_ptr: int):
+    """vnlbgpu_render_chain_device: Basic into Final over the whole clip on
+    the device, the stages overlapped; final's ref must be basic_out_ptr."""
+    _check(load().vnlbgpu_render_chain_device(basic.handle, final.handle, ctypes.c_void_p(basic_out_ptr),
+                                              ctypes.c_void_p(final_out_ptr)))
 
 
 def shard_plan(frames: int, world: int, rank: int, basic: tuple[int, int, int], final: tuple[int, int, int]):
@@ -310,9 +406,40 @@ class Session:
         _check(self.lib.vnlbgpu_diag_kernel_timing(self.handle, 1 if enable else 0, ms.ctypes.data, n.ctypes.data))
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(KERNEL_CLASSES)}
 
+    def set_learned(self, mlp: MLP, shortlist: int = 64, recall_threshold: float = 0.9, tile: int = 64):
+        """vnlbgpu_set_learned: the network of a learned-form session."""
+        self._keep["mlp"] = mlp
+        _check(self.lib.vnlbgpu_set_learned(self.handle, mlp.handle, shortlist, recall_threshold, tile))
+
+    def learned_pairs(self, anchor: int, k: int = 8):
+        """vnlbgpu_learned_pairs: (features [G][inputs], target classes [G][k])
+        of anchor frame `anchor`'s grid anchors under the full search."""
+        count, inputs = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.vnlbgpu_learned_pairs(self.handle, anchor, None, None, 0, k, ctypes.byref(count),
+                                              ctypes.byref(inputs)))
+        feats = np.zeros((max(1, count.value), inputs.value), np.float32)
+        targets = np.full((max(1, count.value), k), -1, np.int32)
+        _check(self.lib.vnlbgpu_learned_pairs(self.handle, anchor, feats.ctypes.data, targets.ctypes.data, count.value,
+                                              k, ctypes.byref(count), ctypes.byref(inputs)))
+        return feats[:count.value], targets[:count.value]
+
+    def stall_tensor_waits(self, on: bool):
+        """vnlbgpu_diag_stall_tensor_waits: the tensor-core matcher's test switch."""
+        _check(self.lib.vnlbgpu_diag_stall_tensor_waits(self.handle, 1 if on else 0))
+
     def set_lanes(self, lanes: int):
         """vnlbgpu_diag_set_lanes: use at most `lanes` pipeline lanes (0: all)."""
         _check(self.lib.vnlbgpu_diag_set_lanes(self.handle, lanes))
+
+    def diag_filtered(self, anchor: int) -> np.ndarray:
+        """The filtered rows [rows][row_dim] of anchor frame `anchor`'s
+        processed groups, in the order of diag_anchor's active rows."""
+        rows, dim = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.vnlbgpu_diag_filtered(self.handle, anchor, None, 0, ctypes.byref(rows), ctypes.byref(dim)))
+        out = np.zeros((max(1, rows.value), dim.value), np.float32)
+        _check(self.lib.vnlbgpu_diag_filtered(self.handle, anchor, out.ctypes.data, rows.value, ctypes.byref(rows),
+                                              ctypes.byref(dim)))
+        return out[:rows.value]
 
     def diag_anchor(self, anchor: int):
         """Runs one anchor frame and returns (grid, active) read-backs."""
