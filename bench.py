@@ -287,6 +287,9 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
         sf.set_clip_device(lib.SOURCE_REF, d_basic.data_ptr())
         lib.render_chain_device(sb, sf, d_basic.data_ptr(), d_final.data_ptr())
 
+    step()  # Basic output for Final's ref, then the tile-shape autotuner on anchor frame 1 of each stage
+    torch.cuda.synchronize()
+    tuning = {"basic": sb.autotune(1), "final": sf.autotune(1)}
     for _ in range(args.warmup):
         step()
     sb.synchronize()
@@ -386,6 +389,7 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
     return {"form": form, "value": value, "max_ms": max_ms, "e2e": e2e_value, "same": same, "psnr": psnr,
             "kernels": kernels, "stats": delta, "lanes": lanes, "bp": bp,
             "serial": serial, "chain": {"value": chain_value, "output_matches_sequential": chain_same},
+            "tuning": tuning,
             "outputs": (basic_out, final_out)}
 
 
@@ -612,6 +616,75 @@ def measured_peak(key: str, fallback: float) -> float:
         return fallback
 
 
+# The other configurations of the workload list, measured beside the
+# headline (device-resident, Basic then Final, plain form: their groups keep
+# up to 64 rows, beyond the chosen matchers' 32): frames/s with the same
+# clock, PSNR against the clean clip.
+EXTRA_WORKLOADS = {
+    "configs0_gray_256x256x8_sigma10": dict(
+        width=256, height=256, frames=8, planes=1, sigma=10.0, steps=20, warmup=3,
+        basic=dict(CPU_DEFAULTS), final=dict(CPU_DEFAULTS, tau=400.0, variance_threshold=1.7)),
+    "configs2_gray_1080p_32f_sigma25_tau400": dict(
+        width=1920, height=1080, frames=32, planes=1, sigma=25.0, steps=2, warmup=1,
+        basic=dict(block_size=8, block_step=4, group_size=16, bm_range=9, radius=2, patch_time=2, rank=16,
+                   cap_factor=4.0, tau=400.0),
+        final=dict(block_size=8, block_step=4, group_size=16, bm_range=9, radius=2, patch_time=2, rank=16,
+                   cap_factor=4.0, tau=400.0, variance_threshold=1.7)),
+}
+
+
+def measure_workload(spec, args, ranks, stream, local):
+    """Device-resident Basic + Final frames/s of one workload (plain form)."""
+    import torch
+    import vnlbcu
+    import vnlbgpu_lib as lib
+
+    w, h, n, planes, sigma = spec["width"], spec["height"], spec["frames"], spec["planes"], spec["sigma"]
+    clean, noisy = synth.make_clip(w, h, n, planes, sigma, seed=ranks.rank)
+    shape = np.empty((n, planes, h, w), np.float32)
+    bp = vnlbcu.parse_parameters(lib.STAGE_BASIC, shape, sigma, dict(spec["basic"]))
+    fp = vnlbcu.parse_parameters(lib.STAGE_FINAL, shape, sigma, dict(spec["final"]))
+    bp.device_id = fp.device_id = local
+    d_noisy = torch.from_numpy(noisy).cuda()
+    d_basic, d_final = torch.empty_like(d_noisy), torch.empty_like(d_noisy)
+    sb, sf = lib.Session(bp, w, h, n, planes), lib.Session(fp, w, h, n, planes)
+    for s in (sb, sf):
+        s.set_stream(stream.cuda_stream)
+
+    def step():
+        sb.set_clip_device(lib.SOURCE_CLIP, d_noisy.data_ptr())
+        sf.set_clip_device(lib.SOURCE_CLIP, d_noisy.data_ptr())
+        sf.set_clip_device(lib.SOURCE_REF, d_basic.data_ptr())
+        sb.render_clip_device(d_basic.data_ptr())
+        sf.render_clip_device(d_final.data_ptr())
+
+    for _ in range(spec["warmup"]):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ranks.barrier()
+    e0.record(stream)
+    for _ in range(spec["steps"]):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sb.synchronize()
+    sf.synchronize()
+    ms = ranks.max(e0.elapsed_time(e1))
+    out = d_final.cpu().numpy()
+    basic = d_basic.cpu().numpy()
+    st = [sb.stats(), sf.stats()]
+    sb.close()
+    sf.close()
+    return {"value": whole_job_rate(ranks.world, n, spec["steps"], ms), "unit": UNIT,
+            "ms_per_step": ms / spec["steps"], "steps": spec["steps"], "warmup": spec["warmup"],
+            "form": "plain", "params": {"basic": spec["basic"], "final": spec["final"]},
+            "psnr_db": {"noisy": synth.psnr(noisy, clean), "basic": synth.psnr(basic, clean),
+                        "final": synth.psnr(out, clean)},
+            "rows_per_active_group": {"basic": st[0]["rows"] / max(1, st[0]["active_groups"]),
+                                      "final": st[1]["rows"] / max(1, st[1]["active_groups"])}}
+
+
 def reference_cuda_stages(head):
     """The reference's own CUDA stage kernels (src/cuda: block matcher with
     CUB sorts, group filter with cuBLAS and cuSOLVER, scatter aggregation),
@@ -703,6 +776,10 @@ def run_ours(args):
     reference_cuda = None
     if rank == 0 and not args.no_reference_cuda and PARAMS == "cpu":
         reference_cuda = reference_cuda_stages(head)
+    workloads = {}
+    if not args.no_workloads and PARAMS == "cpu":
+        for name, spec in EXTRA_WORKLOADS.items():
+            workloads[name] = measure_workload(spec, args, ranks, stream, local)
     per_kernel = {}
     total_kernel_ms = sum(v[0] for v in head["kernels"].values())
     for k, v in head["kernels"].items():
@@ -750,6 +827,9 @@ def run_ours(args):
                             "buffers), CUDA events on the sessions' stream"}
         config["chain"] = dict(head["chain"], api="vnlbgpu_render_chain_device (Basic into Final, stages "
                                                       "overlapped on the device), device-resident")
+        config["autotune"] = head["tuning"]
+        if workloads:
+            config["workloads"] = workloads
         if reference_cuda is not None:
             config["reference_cuda"] = reference_cuda
         if frame_path is not None:
@@ -769,6 +849,91 @@ def run_ours(args):
                 "gpu_launches": head["stats"]["kernel_launches"], "clocks": clocks.summary()}
         print(json.dumps(line), flush=True)
     ranks.close()
+    return 0
+
+
+def run_learned(args):
+    """Learned block-match proposals at a 33 x 33 x 5 window (bm_range 16,
+    radius 2), 1920x1080 YUV444PS, sigma 20, the CPU defaults otherwise: one
+    network per stage, trained by the library's kernels on the full search's
+    top-8 offsets of independently seeded clips (every grid anchor of
+    `--learned-train-frames` anchor frames per clip, two clips), then the
+    clip rendered (device-resident, Basic then Final, 16 frames) by the full
+    search and by the learned form at recall thresholds 0.9 (the per-tile
+    check decides) and 0 (the learned rows always stand).  Prints one JSON
+    line: frames/s, PSNR, held-out recall, share of tiles kept."""
+    import torch
+    import learned as LR
+    import vnlbgpu_lib as lib
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    kw = dict(CPU_DEFAULTS, bm_range=16, radius=2)
+    stage_kw = {lib.STAGE_BASIC: dict(kw, variance_threshold=1.1, weight_alpha=0.75, weight_beta=0.35,
+                                      weight_gamma=1.0),
+                lib.STAGE_FINAL: dict(kw, tau=400.0, variance_threshold=1.7, flat_areas=1, weight_alpha=1.0,
+                                      weight_beta=0.5, weight_gamma=1.0)}
+    frames_train = args.learned_train_frames
+    clips = LR.synthetic_clips(WIDTH, HEIGHT, frames_train, PLANES, SIGMA, seeds=(1001, 1002))
+    refs = [LR.session(lib.STAGE_BASIC, c, SIGMA, stage_kw[lib.STAGE_BASIC]).render_clip() for c in clips]
+    clean, noisy = synth.make_clip(WIDTH, HEIGHT, FRAMES, PLANES, SIGMA, seed=0)
+    nets, train_info = {}, {}
+    for stage in (lib.STAGE_BASIC, lib.STAGE_FINAL):
+        feats, targets = LR.training_pairs(stage, clips, SIGMA, stage_kw[stage],
+                                           refs if stage == lib.STAGE_FINAL else None)
+        inputs, outputs = LR.network_shape(stage, PLANES, stage_kw[stage], noisy, SIGMA)
+        net = lib.MLP(inputs, 128, 3, outputs, max_batch=4096, seed=7 + stage)
+        t0 = time.perf_counter()
+        losses = LR.train(net, feats, targets, steps=args.learned_steps, batch=4096, lr=1e-3)
+        torch.cuda.synchronize()
+        train_s = time.perf_counter() - t0
+        nets[stage] = net
+        train_info[stage] = {"pairs": int(feats.shape[0]), "steps": args.learned_steps, "batch": 4096,
+                             "seconds": train_s, "loss_first": float(np.mean(losses[:10])),
+                             "loss_last": float(np.mean(losses[-10:]))}
+
+    def render(form, threshold=None):
+        sb = LR.session(lib.STAGE_BASIC, noisy, SIGMA, stage_kw[lib.STAGE_BASIC], form=form)
+        if form == "learned":
+            sb.set_learned(nets[lib.STAGE_BASIC], 64, threshold, 64)
+        basic = sb.render_clip()  # warm-up: grids, buffers
+        sf = LR.session(lib.STAGE_FINAL, noisy, SIGMA, stage_kw[lib.STAGE_FINAL], ref=basic, form=form)
+        if form == "learned":
+            sf.set_learned(nets[lib.STAGE_FINAL], 64, threshold, 64)
+        sf.render_clip()
+        st0 = [sb.stats(), sf.stats()]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            sb.set_clip(lib.SOURCE_CLIP, noisy)
+            basic = sb.render_clip()
+            sf.set_clip(lib.SOURCE_CLIP, noisy)
+            sf.set_clip(lib.SOURCE_REF, basic)
+            final = sf.render_clip()
+        seconds = (time.perf_counter() - t0) / args.steps
+        st = [sb.stats(), sf.stats()]
+        tiles = sum(st[i]["learned_tiles"] - st0[i]["learned_tiles"] for i in range(2))
+        fell = sum(st[i]["learned_fallback_tiles"] - st0[i]["learned_fallback_tiles"] for i in range(2))
+        sb.close()
+        sf.close()
+        return {"value": FRAMES / seconds, "ms_per_step": seconds * 1e3,
+                "psnr_db": {"basic": synth.psnr(basic, clean), "final": synth.psnr(final, clean)},
+                "tiles_checked": tiles, "tiles_kept": tiles - fell}
+
+    hold = {}
+    for stage in (lib.STAGE_BASIC, lib.STAGE_FINAL):
+        ref = None
+        if stage == lib.STAGE_FINAL:
+            ref = LR.session(lib.STAGE_BASIC, noisy, SIGMA, stage_kw[lib.STAGE_BASIC]).render_clip()
+        f, t = LR.training_pairs(stage, [noisy], SIGMA, stage_kw[stage], [ref] if ref is not None else None)
+        hold[stage] = LR.recall(nets[stage], f, t, 64)
+    out = {"metric": "learned block-match proposals, 1080p YUV444PS Basic+Final frames/s at bm_range 16, radius 2",
+           "unit": UNIT, "steps": args.steps, "timing": "host wall time around whole-clip host renders",
+           "full_search": render("plain"), "learned_threshold_0.9": render("learned", 0.9),
+           "learned_threshold_0": render("learned", 0.0),
+           "held_out_recall_at_64": {"basic": hold[lib.STAGE_BASIC], "final": hold[lib.STAGE_FINAL]},
+           "training": {"basic": train_info[lib.STAGE_BASIC], "final": train_info[lib.STAGE_FINAL]}}
+    print(json.dumps(out), flush=True)
     return 0
 
 
@@ -815,6 +980,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA stage kernels (baseline/_ref, if built)")
+    ap.add_argument("--no-workloads", action="store_true",
+                    help="skip the other workload configurations measured beside the headline")
     ap.add_argument("--no-frame-path", action="store_true",
                     help="skip the end-to-end run through the per-frame path (vnlbgpu_render_frame_window)")
     ap.add_argument("--form", choices=("all", "plain", "chosen", "chosen_tc"), default="all",
@@ -825,6 +992,11 @@ def main():
                     help="run only a small case (one anchor frame per stage) for ncu captures")
     ap.add_argument("--profile-size", default=None, metavar="WxH",
                     help="frame size of the profile case (default: the workload's 1920x1080)")
+    ap.add_argument("--learned", action="store_true",
+                    help="measure the learned block-match proposals at bm_range 16, radius 2 instead")
+    ap.add_argument("--learned-train-frames", type=int, default=6,
+                    help="frames per training clip (two clips) for --learned")
+    ap.add_argument("--learned-steps", type=int, default=600, help="Adam steps per network for --learned")
     ap.add_argument("--params", choices=("cpu", "vnlbcu"), default="cpu",
                     help="parameter set: the CPU core's defaults (the headline) or vnlbcu's own defaults")
     args = ap.parse_args()
@@ -832,6 +1004,8 @@ def main():
     PARAMS = args.params
     if args.profile_case:
         return run_profile_case(args)
+    if args.learned:
+        return run_learned(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -110,7 +110,7 @@ typedef struct vnlbgpu_params {
  * of its neighbourhood; exact SSD runs on the best-scored offsets (and the
  * anchor itself) only, and the plain selection rule picks the rows among
  * them.  In every tile of anchors the full search runs for one anchor as the
- * judge; where the learned rows' recall of its K nearest is below the
+ * check; where the learned rows' recall of its K nearest is below the
  * threshold, the whole tile is searched in full instead. */
 #define VNLBGPU_FORM_LEARNED 3
 

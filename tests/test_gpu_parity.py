@@ -308,3 +308,18 @@ def test_chain_render_matches_oracle(kw):
         assert np.array_equal(bits(d_final.cpu().numpy()), bits(of))
     with pytest.raises(lib.VNLBError, match="ref must be the chain's Basic output"):
         lib.render_chain_device(sb, sf, d_final.data_ptr(), d_basic.data_ptr())
+
+
+def test_autotuned_session_stays_bit_exact():
+    """The autotuner times strip widths and apply kernels and keeps the
+    fastest; every candidate computes the same bits, so the tuned session
+    still equals the oracle."""
+    _, noisy = synth.make_clip(160, 96, 4, 3, 20.0, seed=78)
+    bp = O.cpu_params(O.BASIC, 20.0)
+    ob = O.Oracle("port").chain(noisy, bp, O.cpu_params(O.FINAL, 20.0))[0]
+    s = session_for(lib.STAGE_BASIC, bp, noisy)
+    choice = s.autotune(1)
+    assert choice["match_warps"] in (2, 4, 8)
+    assert len(choice["timings"]) >= 2, choice
+    out = s.render_clip()
+    assert np.array_equal(bits(out), bits(ob))

@@ -5,7 +5,7 @@ The parity tests pin bit-exactness against the reference sources built with a
 correctly rounded libm (oracle/libm_pin.c), so that every platform computes
 the same bits.  The reference as users build it calls the stock glibc expf /
 logf / log1pf / powf, whose last bits can differ.  The bar there is the one
-the north star states for the plain form: at most 1e-4 max abs and 0.01 dB of
+stated for the plain form against the reference CPU path: at most 1e-4 max abs and 0.01 dB of
 PSNR against the clean clip.  The second test runs the bench's workload
 (1920x1080 YUV444PS, 16 frames, sigma 20, the CPU core's default parameters)
 through Basic and Final on the GPU and compares every output frame with the
@@ -22,7 +22,7 @@ import vnlbcu
 
 pytestmark = pytest.mark.gpu
 
-MAX_ABS = 1e-4   # north-star tolerance of the plain form against the reference CPU path
+MAX_ABS = 1e-4   # the plain form's tolerance against the reference CPU path
 MAX_DB = 0.01
 
 CPU_DEFAULTS = dict(block_size=8, block_step=8, group_size=8, bm_range=9, radius=1, patch_time=1, rank=8,

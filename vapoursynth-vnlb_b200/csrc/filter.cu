@@ -1631,7 +1631,7 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
 #endif
     const bool warp_shape = R <= 8 && Bmax <= 8 && L.nmax == Bmax && (D == 64 || D == 128 || D == 192 || D == 256);
     if (L.scatter && !(warp_shape && L.models == 1)) return cudaErrorInvalidValue;  // see filter_can_scatter
-    if ((VNLB_APPLY_WARP || L.scatter) && warp_shape) {
+    if ((VNLB_APPLY_WARP || L.scatter) && warp_shape && (!L.apply_general || L.scatter)) {
         cudaError_t err = D == 64    ? launch_apply_warp<64>(L, max_groups, stream)
                           : D == 128 ? launch_apply_warp<128>(L, max_groups, stream)
                           : D == 192 ? launch_apply_warp<192>(L, max_groups, stream)

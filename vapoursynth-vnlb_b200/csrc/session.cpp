@@ -510,6 +510,50 @@ struct Session {
         }
     }
 
+    // The plain matcher's strips: `w` anchors (warps) per CTA, whose search
+    // regions fit a reservation of region_w_max columns; false when the
+    // staged planes and the warps' scratch exceed the shared memory.
+    int max_warps = 8;  // the widest strip that fits
+    bool match_width_fits(int w) {
+        const int cw0 = std::min(params.search_window, width - P + 1);
+        const int ch0 = std::min(params.search_window, height - P + 1);
+        region_w_max = ((w - 1) * step + cw0 + P - 1 + 3 + 3) & ~3;
+        // stride = 4 (mod 8): the 4 candidate rows of one lane task start 16
+        // banks apart, which keeps neighbouring lane tasks off each other's banks
+        region_stride = region_w_max;
+        while (region_stride % 8 != 4) ++region_stride;
+        MatchLaunch probe{};
+        probe.search_channels = search_channels;
+        probe.Pt = Pt;
+        probe.region_rows = region_rows;
+        probe.region_stride = region_stride;
+        probe.plane_floats = plane_floats_of(region_rows, region_stride);
+        probe.approx = approx ? 1 : 0;
+        probe.warp_floats = match_warp_floats(cw0 * ch0, search_channels * Pt, P, buffer_cap);
+        return match_shared_bytes(probe, w) <= 200 * 1024;
+    }
+    // flow-guided search: the strips' reservation widened by up to 16 columns
+    // and 8 rows while the shared memory allows
+    void set_flow_region() {
+        const int cw0 = std::min(params.search_window, width - P + 1);
+        const int ch0 = std::min(params.search_window, height - P + 1);
+        for (int slack = 16; slack >= 0; slack -= 4) {
+            flow_region_w_max = region_w_max + slack;
+            flow_region_rows = region_rows + slack / 2;
+            flow_region_stride = flow_region_w_max;
+            while (flow_region_stride % 8 != 4) ++flow_region_stride;
+            MatchLaunch probe{};
+            probe.search_channels = search_channels;
+            probe.Pt = Pt;
+            probe.region_rows = flow_region_rows;
+            probe.region_stride = flow_region_stride;
+            probe.plane_floats = plane_floats_of(flow_region_rows, flow_region_stride);
+            probe.warp_floats = match_warp_floats(cw0 * ch0, search_channels * Pt, P, buffer_cap);
+            if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
+        }
+    }
+    bool apply_general = false;  // autotuned: the row-tiled apply where the warp-per-group one also fits
+
     // Shared floats per staged plane of the plain matcher: whole 128-byte
     // units, so that every plane starts where a tensor-memory-accelerator
     // tile load may write.
@@ -524,16 +568,19 @@ struct Session {
     CUtensorMap search_map{};
     const float* search_map_base = nullptr;
     long long search_map_rows = 0;
+    int search_map_stride = 0;
     const CUtensorMap* search_tensor_map(const float* base) {
         if (!VNLB_MATCH_TMA) return nullptr;
         const int src = stage == 1 ? VNLBGPU_SOURCE_REF : VNLBGPU_SOURCE_CLIP;
         const long long slots = store[src].borrowed ? frames : ring + (ring < frames ? Pt - 1 : 0);
         const long long rows = slots * channels * static_cast<long long>(height);
-        if (base == search_map_base && rows == search_map_rows) return &search_map;
+        if (base == search_map_base && rows == search_map_rows && region_stride == search_map_stride)
+            return &search_map;
         search_map_base = nullptr;
         if (!encode_store_map(&search_map, base, width, rows, region_stride, region_rows)) return nullptr;
         search_map_base = base;
         search_map_rows = rows;
+        search_map_stride = region_stride;
         return &search_map;
     }
 
@@ -660,39 +707,11 @@ struct Session {
         // approximate distances need 8x8 patches and the register replay
         // (buffer and K front within a warp)
         approx = p.form == VNLBGPU_FORM_CHOSEN && P == kLanes && cap_eff <= 32 && K <= 32;
-        for (warps = 8; warps >= 1; warps /= 2) {
-            region_w_max = ((warps - 1) * step + cw0 + P - 1 + 3 + 3) & ~3;
-            // stride = 4 (mod 8): the 4 candidate rows of one lane task start 16
-            // banks apart, which keeps neighbouring lane tasks off each other's banks
-            region_stride = region_w_max;
-            while (region_stride % 8 != 4) ++region_stride;
-            MatchLaunch probe{};
-            probe.search_channels = search_channels;
-            probe.Pt = Pt;
-            probe.region_rows = region_rows;
-            probe.region_stride = region_stride;
-            probe.plane_floats = plane_floats_of(region_rows, region_stride);
-            probe.approx = approx ? 1 : 0;
-            probe.warp_floats = match_warp_floats(cw0 * ch0, search_channels * Pt, P, buffer_cap);
-            if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
-        }
+        for (warps = 8; warps >= 1; warps /= 2)
+            if (match_width_fits(warps)) break;
         if (warps < 1) fail("VNLB CUDA: the search region of one anchor does not fit in shared memory");
-        // flow-guided search: the strips' reservation widened by up to 16
-        // columns and 8 rows while the shared memory allows
-        for (int slack = 16; slack >= 0; slack -= 4) {
-            flow_region_w_max = region_w_max + slack;
-            flow_region_rows = region_rows + slack / 2;
-            flow_region_stride = flow_region_w_max;
-            while (flow_region_stride % 8 != 4) ++flow_region_stride;
-            MatchLaunch probe{};
-            probe.search_channels = search_channels;
-            probe.Pt = Pt;
-            probe.region_rows = flow_region_rows;
-            probe.region_stride = flow_region_stride;
-            probe.plane_floats = plane_floats_of(flow_region_rows, flow_region_stride);
-            probe.warp_floats = match_warp_floats(cw0 * ch0, search_channels * Pt, P, buffer_cap);
-            if (match_shared_bytes(probe, warps) <= 200 * 1024) break;
-        }
+        max_warps = warps;
+        set_flow_region();
         // tensor-core matcher: strips of up to kChosenAnchors anchors whose
         // windows lie within kChosenCols candidate columns
         if (p.form == VNLBGPU_FORM_CHOSEN_TC && chosen_match_supported(P, search_channels * Pt, cw0, ch0)) {
@@ -1402,7 +1421,7 @@ struct Session {
                       "shortlist launch");
             }
             check(launch_learned_match(ll, ls), "learned match launch");
-            // the judge: the full search for each tile's checked anchor
+            // the check: the full search for each tile's checked anchor
             const CUtensorMap* map = search_tensor_map(search);
             MatchLaunch mc = m;
             mc.tma = map ? 1 : 0;
@@ -1464,6 +1483,7 @@ struct Session {
         // the chosen forms' filter (TF32 Gram, FP64 angles) goes with their
         // matchers; configurations that run the plain matcher stay exact
         fl.mixed = (approx || chosen) && !flow_on() ? 1 : 0;
+        fl.apply_general = apply_general ? 1 : 0;
         fl.width = width;
         fl.height = height;
         fl.channels = channels;
@@ -1664,6 +1684,78 @@ struct Session {
             check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
             w.staged.push_back(e);
             w.staged_used.push_back(false);
+        }
+    }
+
+    // Device time of one timed kernel class for anchor frame `anchor` on lane
+    // 0: one untimed pass (grids, caches), then the least of three timed ones.
+    double time_class(int anchor, int category) {
+        DeviceArray<float> stack;
+        stack.allocate(stack_values(), "cudaMalloc(tuning stack)");
+        fork();
+        compute_anchor(anchor, stack.ptr, lanes[0]);
+        join();
+        check_status();
+        const bool was = timing;
+        collect_timing();
+        timing = true;
+        double best = 1e30;
+        for (int rep = 0; rep < 3; ++rep) {
+            const double before = kernel_ms[category];
+            fork();
+            compute_anchor(anchor, stack.ptr, lanes[0]);
+            join();
+            collect_timing();
+            best = std::min(best, kernel_ms[category] - before);
+        }
+        check_status();
+        timing = was;
+        invalidate();
+        return best;
+    }
+
+    // The autotuner: the plain matcher's strip width (anchors per CTA) and
+    // the apply kernel (warp per group or row tiles, where both fit) by
+    // measured time on one anchor frame.  Every choice computes the same
+    // bits; only the speed differs.
+    void autotune(int anchor, std::vector<std::pair<std::string, double>>& log) {
+        const bool plain_matcher = !chosen && !flow_on();
+        if (plain_matcher) {
+            int best_w = warps;
+            double best_t = 1e30;
+            for (int w = max_warps; w >= 2; w /= 2) {
+                if (!match_width_fits(w)) continue;
+                warps = w;
+                set_flow_region();
+                grids.clear();
+                const double t = time_class(anchor, kTimedMatch);
+                log.emplace_back("match strip " + std::to_string(w), t);
+                if (t < best_t) {
+                    best_t = t;
+                    best_w = w;
+                }
+            }
+            warps = best_w;
+            match_width_fits(warps);
+            set_flow_region();
+            grids.clear();
+        }
+        FilterLaunch probe{};
+        probe.dim = dim;
+        probe.rank = params.rank;
+        probe.nmax = nmax;
+        probe.model_cap = model_cap;
+        probe.max_rows = max_rows;
+        probe.models = models;
+        const bool scatter = (approx || chosen) && filter_can_scatter(probe);
+        if (!scatter && filter_can_scatter(probe)) {  // both apply kernels fit this shape
+            double t[2];
+            for (int g = 0; g < 2; ++g) {
+                apply_general = g == 1;
+                t[g] = time_class(anchor, kTimedFilter);
+                log.emplace_back(g ? "apply row tiles" : "apply warp per group", t[g]);
+            }
+            apply_general = t[1] < t[0];
         }
     }
 
@@ -2581,6 +2673,32 @@ int vnlbgpu_diag_kernel_timing(vnlbgpu_session* session, int enable, double* ms,
             s.kernel_count[i] = 0;
         }
         s.timing = enable != 0;
+    });
+}
+
+int vnlbgpu_autotune(vnlbgpu_session* session, int anchor, int* match_warps, int* apply_rows, char* log,
+                     size_t log_size) {
+    return guarded([&]() {
+        if (!session) vnlbgpu::fail("VNLB CUDA: null argument");
+        Session& s = session->impl;
+        std::lock_guard guard(s.lock);
+        vnlbgpu::check(cudaSetDevice(s.device), "cudaSetDevice");
+        s.require_sources();
+        if (anchor < 0 || anchor > s.frames - s.Pt) vnlbgpu::fail("VNLB CUDA: anchor frame out of range");
+        if (s.learned) vnlbgpu::fail("VNLB CUDA: the learned form is not autotuned");
+        s.drain();
+        std::vector<std::pair<std::string, double>> entries;
+        s.autotune(anchor, entries);
+        if (match_warps) *match_warps = s.warps;
+        if (apply_rows) *apply_rows = s.apply_general ? 1 : 0;
+        if (log && log_size > 0) {
+            std::ostringstream o;
+            for (const auto& e : entries) o << e.first << ": " << e.second << " ms\n";
+            const std::string text = o.str();
+            const size_t n = std::min(log_size - 1, text.size());
+            std::memcpy(log, text.data(), n);
+            log[n] = '\0';
+        }
     });
 }
 

@@ -190,6 +190,7 @@ struct FilterLaunch {
     // chosen forms, warp-per-group shapes: the apply kernel adds each filtered
     // row straight into the anchor frame's stack (atomics, any order) instead
     // of writing it out for the stack tiles; null = write the rows
+    int apply_general;      // the row-tiled apply even where the warp-per-group one fits (autotuner)
     float* scatter;         // [slots][C+1][H][W], cleared before the launch
     const float* window;    // [P*P] aggregation window
     int windowed, slots, search_bwd, anchor_frame;

@@ -8,7 +8,7 @@ offset of the search window (class = scheduled frame, window row, window
 column).  Its targets are the offsets of the K nearest rows of the full exact
 search on synthetic clips (vnlbgpu_learned_pairs), so the plain matcher
 teaches it.  A session of form "learned" then runs exact SSD on the top
-`shortlist` offsets only, with the full search as the judge and fallback per
+`shortlist` offsets only, with the full search as the check and fallback per
 tile.
 
 Device buffers come from torch (plumbing only); every computation is the

@@ -76,7 +76,7 @@ EXPORTS = [
     "vnlbgpu_set_mvtools_frame", "vnlbgpu_shard_plan", "vnlbgpu_mlp_create", "vnlbgpu_mlp_destroy",
     "vnlbgpu_mlp_parameters", "vnlbgpu_mlp_get_weights", "vnlbgpu_mlp_set_weights", "vnlbgpu_mlp_gradients",
     "vnlbgpu_mlp_train_step", "vnlbgpu_mlp_logits", "vnlbgpu_mlp_shortlist", "vnlbgpu_set_learned",
-    "vnlbgpu_learned_pairs",
+    "vnlbgpu_learned_pairs", "vnlbgpu_autotune",
 ]
 KERNEL_CLASSES = ("match", "paste", "filter", "tiles", "normalize")
 
@@ -143,6 +143,8 @@ def load() -> ctypes.CDLL:
             lib.vnlbgpu_set_mvtools_frame.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
                                                       ctypes.c_size_t, ctypes.c_int]
             lib.vnlbgpu_shard_plan.argtypes = [ctypes.c_int] * 9 + [ctypes.POINTER(ctypes.c_int)] * 3
+            lib.vnlbgpu_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_size_t]
             lib.vnlbgpu_mlp_create.argtypes = [ctypes.c_int] * 5 + [ctypes.c_uint, ctypes.c_int,
                                                                    ctypes.POINTER(ctypes.c_void_p)]
             lib.vnlbgpu_mlp_destroy.argtypes = [ctypes.c_void_p]
@@ -426,6 +428,15 @@ class Session:
     def stall_tensor_waits(self, on: bool):
         """vnlbgpu_diag_stall_tensor_waits: the tensor-core matcher's test switch."""
         _check(self.lib.vnlbgpu_diag_stall_tensor_waits(self.handle, 1 if on else 0))
+
+    def autotune(self, anchor: int = 1) -> dict:
+        """vnlbgpu_autotune: the fastest bit-identical strip width and apply
+        kernel on anchor frame `anchor`."""
+        w, rows = ctypes.c_int(), ctypes.c_int()
+        buf = ctypes.create_string_buffer(1024)
+        _check(self.lib.vnlbgpu_autotune(self.handle, anchor, ctypes.byref(w), ctypes.byref(rows), buf, 1024))
+        return {"match_warps": w.value, "apply_rows": bool(rows.value),
+                "timings": [line for line in buf.value.decode().splitlines() if line]}
 
     def set_lanes(self, lanes: int):
         """vnlbgpu_diag_set_lanes: use at most `lanes` pipeline lanes (0: all)."""
