@@ -16,9 +16,9 @@ CPU core.
 
 `--params vnlbcu` runs the same clip with vnlbcu's own defaults instead (block
 7, automatic step 3, group 16, bm_range 13, radius 1, patch_time 2, rank 15:
-estimator dimension 294, about 230k groups per anchor frame), plain form only
-(the chosen matchers need 8x8 patches and at most 32 retained rows), without
-the CPU sample.
+estimator dimension 294, about 230k groups per anchor frame), in the plain
+form and the tensor-core form (the FP32 chosen form needs 8x8 patches),
+without the CPU sample.
 
 Under torchrun every rank (one GPU each) denoises its own clip for `value`
 (weak scaling, no collective on the data path); rank 0 prints one JSON line.
@@ -617,15 +617,14 @@ def measured_peak(key: str, fallback: float) -> float:
 
 
 # The other configurations of the workload list, measured beside the
-# headline (device-resident, Basic then Final, plain form: their groups keep
-# up to 64 rows, beyond the chosen matchers' 32): frames/s with the same
-# clock, PSNR against the clean clip.
+# headline (device-resident, Basic then Final, in each listed form): frames/s
+# with the same clock, PSNR against the clean clip.
 EXTRA_WORKLOADS = {
     "configs0_gray_256x256x8_sigma10": dict(
-        width=256, height=256, frames=8, planes=1, sigma=10.0, steps=20, warmup=3,
+        forms=["plain"], width=256, height=256, frames=8, planes=1, sigma=10.0, steps=20, warmup=3,
         basic=dict(CPU_DEFAULTS), final=dict(CPU_DEFAULTS, tau=400.0, variance_threshold=1.7)),
     "configs2_gray_1080p_32f_sigma25_tau400": dict(
-        width=1920, height=1080, frames=32, planes=1, sigma=25.0, steps=2, warmup=1,
+        forms=["plain", "chosen_tc"], width=1920, height=1080, frames=32, planes=1, sigma=25.0, steps=2, warmup=1,
         basic=dict(block_size=8, block_step=4, group_size=16, bm_range=9, radius=2, patch_time=2, rank=16,
                    cap_factor=4.0, tau=400.0),
         final=dict(block_size=8, block_step=4, group_size=16, bm_range=9, radius=2, patch_time=2, rank=16,
@@ -633,8 +632,150 @@ EXTRA_WORKLOADS = {
 }
 
 
-def measure_workload(spec, args, ranks, stream, local):
-    """Device-resident Basic + Final frames/s of one workload (plain form)."""
+# the mixed stream: 4 GrayS 1280x720 + 2 YUV444PS 1920x1080 + 1 GrayS
+# 3840x2160, 24 frames each, sigma cycling 5 / 15 / 30, tau 200, cap 4,
+# patch_time 2, rank by noise level (24 at sigma 5, 16 at 15, 8 at 30)
+MIXED_STREAM = dict(
+    clips=[(1280, 720, 1, 5.0), (1280, 720, 1, 15.0), (1280, 720, 1, 30.0), (1280, 720, 1, 5.0),
+           (1920, 1080, 3, 15.0), (1920, 1080, 3, 30.0), (3840, 2160, 1, 15.0)],
+    frames=24, steps=2, warmup=3, rank={5.0: 24, 15.0: 16, 30.0: 8},
+    stage=dict(block_size=8, block_step=8, group_size=8, bm_range=9, radius=1, patch_time=2, cap_factor=4.0,
+               tau=200.0))
+
+
+def measure_mixed_stream(form, args, ranks, local):
+    """Frames/s of the mixed stream in one form: every clip has its own Basic
+    and Final sessions on its own CUDA stream, driven by its own host thread,
+    all clips in flight at once; the step is the whole batch of clips, timed
+    with events from one start event that every clip stream waits on to an
+    end event that waits on every clip stream.  Chosen forms are autotuned
+    per session before the timed steps."""
+    import threading
+
+    import torch
+    import vnlbcu
+    import vnlbgpu_lib as lib
+
+    spec = MIXED_STREAM
+    n = spec["frames"]
+    clips = []
+    for i, (w, h, c, sigma) in enumerate(spec["clips"]):
+        clean, noisy = synth.make_clip(w, h, n, c, sigma, seed=100 * ranks.rank + i)
+        shape = np.empty((n, c, h, w), np.float32)
+        kw = dict(spec["stage"], rank=spec["rank"][sigma], form=form)
+        bp = vnlbcu.parse_parameters(lib.STAGE_BASIC, shape, sigma, dict(kw))
+        fp = vnlbcu.parse_parameters(lib.STAGE_FINAL, shape, sigma, dict(kw, variance_threshold=None))
+        bp.device_id = fp.device_id = local
+        st = torch.cuda.Stream()
+        d_noisy = torch.from_numpy(noisy).cuda()
+        clip = dict(size=f"{w}x{h}x{c}", sigma=sigma, clean=clean, noisy=noisy, stream=st, d_noisy=d_noisy,
+                    d_basic=torch.empty_like(d_noisy), d_final=torch.empty_like(d_noisy),
+                    sb=lib.Session(bp, w, h, n, c), sf=lib.Session(fp, w, h, n, c), done=torch.cuda.Event())
+        for s in (clip["sb"], clip["sf"]):
+            s.set_stream(st.cuda_stream)
+        clips.append(clip)
+
+    def run(clip, start):
+        if start is not None:
+            clip["stream"].wait_event(start)
+        sb, sf = clip["sb"], clip["sf"]
+        sb.set_clip_device(lib.SOURCE_CLIP, clip["d_noisy"].data_ptr())
+        sf.set_clip_device(lib.SOURCE_CLIP, clip["d_noisy"].data_ptr())
+        sf.set_clip_device(lib.SOURCE_REF, clip["d_basic"].data_ptr())
+        sb.render_clip_device(clip["d_basic"].data_ptr())
+        sf.render_clip_device(clip["d_final"].data_ptr())
+        clip["done"].record(clip["stream"])
+
+    def step(start=None):
+        errors = []
+
+        def body(clip):
+            try:
+                run(clip, start)
+            except Exception as e:  # re-raised on the calling thread
+                errors.append(e)
+        threads = [threading.Thread(target=body, args=(c,)) for c in clips]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
+
+    step()
+    torch.cuda.synchronize()
+    tuning = []
+    if form != "plain":
+        for c in clips:
+            tuning.append({"clip": c["size"], "basic": c["sb"].autotune(1)["match_warps"],
+                           "final": c["sf"].autotune(1)["match_warps"]})
+    for _ in range(spec["warmup"]):
+        step()
+    torch.cuda.synchronize()
+    main = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ranks.barrier()
+    torch.cuda.synchronize()
+    e0.record(main)
+    for _ in range(spec["steps"]):
+        step(e0)
+    for c in clips:
+        main.wait_event(c["done"])
+    e1.record(main)
+    torch.cuda.synchronize()
+    ms = ranks.max(e0.elapsed_time(e1))
+    per_clip = []
+    for c in clips:
+        c["sb"].synchronize()
+        c["sf"].synchronize()
+        out = c["d_final"].cpu().numpy()
+        per_clip.append({"clip": c["size"], "sigma": c["sigma"], "psnr_noisy_db": synth.psnr(c["noisy"], c["clean"]),
+                         "psnr_final_db": synth.psnr(out, c["clean"]), "final": out})
+        c["sb"].close()
+        c["sf"].close()
+    total = n * len(clips)
+    return {"value": whole_job_rate(ranks.world, total, spec["steps"], ms), "unit": UNIT,
+            "ms_per_step": ms / spec["steps"], "frames_per_step": total, "form": form, "clips": per_clip,
+            "autotune": tuning}
+
+
+def mixed_stream_line(args, ranks, local):
+    """The mixed stream in the plain form and in the chosen_tc form, with each
+    clip's PSNR change between the two (the chosen form's bar is 0.05 dB)."""
+    plain = measure_mixed_stream("plain", args, ranks, local)
+    tc = measure_mixed_stream("chosen_tc", args, ranks, local)
+    clips = []
+    for a, b in zip(plain["clips"], tc["clips"]):
+        clips.append({"clip": a["clip"], "sigma": a["sigma"], "psnr_noisy_db": a["psnr_noisy_db"],
+                      "psnr_plain_db": a["psnr_final_db"], "psnr_chosen_tc_db": b["psnr_final_db"],
+                      "max_abs_vs_plain": float(np.max(np.abs(a["final"] - b["final"])))})
+    return {"frames_per_step": plain["frames_per_step"], "steps": MIXED_STREAM["steps"],
+            "warmup": MIXED_STREAM["warmup"], "plain": {"value": plain["value"], "ms_per_step": plain["ms_per_step"]},
+            "chosen_tc": {"value": tc["value"], "ms_per_step": tc["ms_per_step"], "autotune": tc["autotune"]},
+            "speedup_chosen_tc_vs_plain": tc["value"] / plain["value"],
+            "max_psnr_loss_db": max(c["psnr_plain_db"] - c["psnr_chosen_tc_db"] for c in clips), "clips": clips,
+            "params": dict(MIXED_STREAM["stage"], rank=MIXED_STREAM["rank"]), "unit": UNIT,
+            "pipeline": "one host thread and one CUDA stream per clip, all clips in flight; not graph-captured"}
+
+
+def workload_line(spec, args, ranks, stream, local):
+    """One workload in each of its forms; with a chosen form beside the plain
+    one, its speed-up and PSNR change against the plain form."""
+    runs = {f: measure_workload(spec, args, ranks, stream, local, f) for f in spec["forms"]}
+    out = dict(runs["plain"])
+    for f, r in runs.items():
+        if f == "plain":
+            continue
+        out[f + "_form"] = dict(r, speedup_vs_plain=r["value"] / out["value"],
+                                psnr_loss_vs_plain_db=out["psnr_db"]["final"] - r["psnr_db"]["final"],
+                                max_abs_vs_plain=float(np.max(np.abs(r.pop("final_out") - out["final_out"]))))
+    out.pop("final_out")
+    return out
+
+
+def measure_workload(spec, args, ranks, stream, local, form="plain"):
+    """Device-resident Basic + Final frames/s of one workload in one form
+    (a chosen form autotuned per session first)."""
     import torch
     import vnlbcu
     import vnlbgpu_lib as lib
@@ -642,8 +783,8 @@ def measure_workload(spec, args, ranks, stream, local):
     w, h, n, planes, sigma = spec["width"], spec["height"], spec["frames"], spec["planes"], spec["sigma"]
     clean, noisy = synth.make_clip(w, h, n, planes, sigma, seed=ranks.rank)
     shape = np.empty((n, planes, h, w), np.float32)
-    bp = vnlbcu.parse_parameters(lib.STAGE_BASIC, shape, sigma, dict(spec["basic"]))
-    fp = vnlbcu.parse_parameters(lib.STAGE_FINAL, shape, sigma, dict(spec["final"]))
+    bp = vnlbcu.parse_parameters(lib.STAGE_BASIC, shape, sigma, dict(spec["basic"], form=form))
+    fp = vnlbcu.parse_parameters(lib.STAGE_FINAL, shape, sigma, dict(spec["final"], form=form))
     bp.device_id = fp.device_id = local
     d_noisy = torch.from_numpy(noisy).cuda()
     d_basic, d_final = torch.empty_like(d_noisy), torch.empty_like(d_noisy)
@@ -658,6 +799,11 @@ def measure_workload(spec, args, ranks, stream, local):
         sb.render_clip_device(d_basic.data_ptr())
         sf.render_clip_device(d_final.data_ptr())
 
+    tuning = None
+    if form != "plain":
+        step()
+        torch.cuda.synchronize()
+        tuning = {"basic": sb.autotune(1)["match_warps"], "final": sf.autotune(1)["match_warps"]}
     for _ in range(spec["warmup"]):
         step()
     torch.cuda.synchronize()
@@ -678,7 +824,8 @@ def measure_workload(spec, args, ranks, stream, local):
     sf.close()
     return {"value": whole_job_rate(ranks.world, n, spec["steps"], ms), "unit": UNIT,
             "ms_per_step": ms / spec["steps"], "steps": spec["steps"], "warmup": spec["warmup"],
-            "form": "plain", "params": {"basic": spec["basic"], "final": spec["final"]},
+            "form": form, "autotune": tuning, "final_out": out,
+            "params": {"basic": spec["basic"], "final": spec["final"]},
             "psnr_db": {"noisy": synth.psnr(noisy, clean), "basic": synth.psnr(basic, clean),
                         "final": synth.psnr(out, clean)},
             "rows_per_active_group": {"basic": st[0]["rows"] / max(1, st[0]["active_groups"]),
@@ -764,7 +911,7 @@ def run_ours(args):
     torch.cuda.set_stream(stream)
     forms = ["plain", "chosen", "chosen_tc"] if args.form == "all" else [args.form]
     if PARAMS == "vnlbcu":
-        forms = ["plain"]
+        forms = [f for f in forms if f != "chosen"]
     # clocks sampled over every timed measurement below (the GPU is busy from
     # the first warm-up step to the last frame of the per-frame run)
     with ClockSampler(local) as clocks:
@@ -779,7 +926,8 @@ def run_ours(args):
     workloads = {}
     if not args.no_workloads and PARAMS == "cpu":
         for name, spec in EXTRA_WORKLOADS.items():
-            workloads[name] = measure_workload(spec, args, ranks, stream, local)
+            workloads[name] = workload_line(spec, args, ranks, stream, local)
+        workloads["configs4_mixed_stream"] = mixed_stream_line(args, ranks, local)
     per_kernel = {}
     total_kernel_ms = sum(v[0] for v in head["kernels"].values())
     for k, v in head["kernels"].items():
@@ -994,8 +1142,9 @@ def main():
                     help="frame size of the profile case (default: the workload's 1920x1080)")
     ap.add_argument("--learned", action="store_true",
                     help="measure the learned block-match proposals at bm_range 16, radius 2 instead")
-    ap.add_argument("--learned-train-frames", type=int, default=6,
-                    help="frames per training clip (two clips) for --learned")
+    ap.add_argument("--learned-train-frames", type=int, default=30,
+                    help="frames per training clip (two clips) for --learned; 30 gives about 2e6 (anchor, "
+                         "top-8) pairs at 1080p")
     ap.add_argument("--learned-steps", type=int, default=600, help="Adam steps per network for --learned")
     ap.add_argument("--params", choices=("cpu", "vnlbcu"), default="cpu",
                     help="parameter set: the CPU core's defaults (the headline) or vnlbcu's own defaults")

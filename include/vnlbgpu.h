@@ -96,10 +96,13 @@ typedef struct vnlbgpu_params {
  * FP32 distance of every retained candidate and selects on the exact values:
  * within a PSNR tolerance of PLAIN rather than bit-identical.  CHOSEN_TC does
  * the same with the dot products on BF16 tensor cores (tcgen05, FP32
- * accumulation in tensor memory) and also needs a search window of at most 64
- * columns by 32 rows.  Both apply to 8x8 patches with a buffer of at most 32
- * patches (group_size * cap_factor) and group_size <= 32; other
- * configurations run PLAIN.  With either chosen matcher the group filter runs
+ * accumulation in tensor memory).  CHOSEN applies to 8x8 patches with a
+ * buffer of at most 32 patches (group_size * cap_factor) and group_size <= 32.
+ * CHOSEN_TC applies to 7x7 and 8x8 patches compared over at most 6 planes
+ * (search channels x patch_time), a search window of at most 64 columns by
+ * 32 rows, a buffer of at most 64 patches and group_size <= 32: vnlbcu's own
+ * defaults included.  Other configurations run PLAIN.  With either chosen
+ * matcher the group filter runs
  * in mixed precision too: the dual Gram on TF32 tensor cores with FP32
  * accumulation, the Jacobi rotation angles in FP64. */
 #define VNLBGPU_FORM_PLAIN 0

@@ -45,8 +45,10 @@ def test_chosen_psnr_within_tolerance_of_plain(form, planes, shape, seed):
         assert np.isfinite(chosen).all()
 
 
-def rows_of(stage, form, noisy, ref=None, anchor=2):
-    kw = dict(CPU_DEFAULTS, form=form, **(FINAL if stage == lib.STAGE_FINAL else BASIC))
+def rows_of(stage, form, noisy, ref=None, anchor=2, base=CPU_DEFAULTS):
+    kw = dict(base, form=form)
+    if base is CPU_DEFAULTS:
+        kw.update(FINAL if stage == lib.STAGE_FINAL else BASIC)
     params = vnlbcu.parse_parameters(stage, noisy, 20.0, kw)
     frames, planes, h, w = noisy.shape
     s = lib.Session(params, w, h, frames, planes)
@@ -92,14 +94,79 @@ def test_chosen_selects_the_plain_rows(stage, form, agree):
     assert ordered >= 0.5 * same, (ordered, same)  # the order check ran on most of the agreeing groups
 
 
-@pytest.mark.parametrize("form", ["chosen", "chosen_tc"])
-def test_chosen_needs_8x8_patches(form):
-    """Other patch sizes keep the plain matcher: the output is the plain one."""
+@pytest.mark.parametrize("form,block", [("chosen", 7), ("chosen_tc", 6), ("chosen_tc", 10)])
+def test_unsupported_patch_sizes_keep_the_plain_matcher(form, block):
+    """The FP32 chosen form takes 8 x 8 patches, the tensor-core form 7 x 7
+    and 8 x 8; other sizes keep the plain matcher: the output is the plain
+    one."""
     _, noisy = synth.make_clip(64, 48, 4, 1, 20.0, seed=84)
-    kw = dict(block_size=7, block_step=4, group_size=8, bm_range=5, rank=8)
+    kw = dict(block_size=block, block_step=4, group_size=8, bm_range=5, rank=8)
     plain = vnlbcu.Basic(noisy, sigma=20.0, **kw)
     chosen = vnlbcu.Basic(noisy, sigma=20.0, form=form, **kw)
     assert np.array_equal(plain, chosen)
+
+
+def sorted_rows(rows):
+    d = rows["distance"]
+    return bool(np.all(d[1:] >= d[:-1]))
+
+
+@pytest.mark.parametrize("stage,tau", [(lib.STAGE_BASIC, None), (lib.STAGE_FINAL, None), (lib.STAGE_FINAL, 1e6)],
+                         ids=["basic", "final", "final_tau1e6"])
+def test_tensor_core_matcher_on_vnlbcu_defaults(stage, tau):
+    """vnlbcu's own defaults on a YUV444 clip: 7 x 7 patches, patch_time 2 (six
+    planes: two shared-memory stages of planes per frame, accumulated in
+    tensor memory), step 3, group 16 with cap factor 4 (buffers of 64, two
+    slots per lane).  The retained rows agree with the plain form's, with the
+    plain form's exact distance bits; every group's rows come out sorted by
+    distance (the chosen forms' step 4).  With tau raised to 1e6 every
+    candidate passes the threshold, so every group keeps a full buffer of 64
+    rows: the buffer's second register per lane and the replacement of its
+    worst entry carry the selection, and the plain form's heap replay leaves
+    rows past the K-th unsorted where the tensor-core path sorts them, which
+    shows that path ran."""
+    _, noisy = synth.make_clip(128, 96, 5, 3, 20.0, seed=86)
+    ref = vnlbcu.Basic(noisy, sigma=20.0) if stage == lib.STAGE_FINAL else None
+    base = {} if tau is None else {"tau": tau}
+    plain = rows_of(stage, "plain", noisy, ref, base=base)
+    tc = rows_of(stage, "chosen_tc", noisy, ref, base=base)
+    assert plain["max_rows"] == 64
+    assert np.array_equal(plain["xy"], tc["xy"])
+    place = lambda r: (int(r["x"]), int(r["y"]), int(r["frame"]))
+    groups = len(plain["counts"])
+    same = unsorted_plain = shared = total = 0
+    for gi in range(groups):
+        a = plain["grid_rows"][gi][: plain["counts"][gi]]
+        b = tc["grid_rows"][gi][: tc["counts"][gi]]
+        assert sorted_rows(b), gi
+        unsorted_plain += not sorted_rows(a)
+        ka = {place(x): x["distance"] for x in a}
+        kb = {place(x): x["distance"] for x in b}
+        for pos in set(ka) & set(kb):
+            assert np.float32(ka[pos]).view(np.uint32) == np.float32(kb[pos]).view(np.uint32)
+        same += set(ka) == set(kb)
+        shared += len(set(ka) & set(kb))
+        total += len(ka)
+    if tau is None:
+        assert same / groups >= 0.9, (same, groups)
+    else:
+        assert np.all(plain["counts"] == 64) and np.all(tc["counts"] == 64)
+        assert unsorted_plain > 0
+        # the boundary of 64 of 2187 candidates moves under BF16 distances
+        assert shared / total >= 0.97, (shared, total)
+
+
+def test_tensor_core_psnr_on_vnlbcu_defaults():
+    """Basic then Final with vnlbcu's defaults: the tensor-core form within
+    0.05 dB of the plain form's PSNR."""
+    clean, noisy = synth.make_clip(160, 128, 6, 3, 20.0, seed=87)
+    pb = vnlbcu.Basic(noisy, sigma=20.0)
+    pf = vnlbcu.Final(noisy, ref=pb, sigma=20.0)
+    tb = vnlbcu.Basic(noisy, sigma=20.0, form="chosen_tc")
+    tf = vnlbcu.Final(noisy, ref=tb, sigma=20.0, form="chosen_tc")
+    for plain, tc in ((pb, tb), (pf, tf)):
+        assert np.isfinite(tc).all()
+        assert synth.psnr(plain, clean) - synth.psnr(tc, clean) <= 0.05
 
 
 def test_tensor_core_waits_run_out_and_report():

@@ -30,8 +30,12 @@
 // selection kernel runs steps 2-4 with one warp per anchor at full occupancy.
 //
 // Distance kernel.  One CTA takes a strip of up to 8 consecutive anchors of
-// one grid row whose search windows lie within 64 consecutive candidate
-// columns.  Per scheduled frame:
+// each of one or two consecutive grid rows (anchor slots 0-7 and 8-15),
+// whose search windows lie within 64 consecutive candidate columns and span
+// at most 32 rows.  Pairing two grid rows fills the MMA's 16 anchor columns
+// (a strip of one row fills about 6 at step 8), so each staged region row
+// serves twice the anchors.  Per scheduled frame, and per group of up to
+// three planes of it:
 //
 //   a. The strip's search region is read from global memory once and written
 //      to shared memory as BF16 core matrices of the tcgen05 no-swizzle
@@ -46,21 +50,33 @@
 //      builds one region row: each lane loads 3 samples, the 8-sample rows of
 //      candidate columns lane and lane + 32 come from the other lanes by
 //      shuffles, and the 64 block rows go out as consecutive 16-byte stores
-//      (no bank conflicts).  The same pass sums the squares of the 8-sample
-//      row segments (candidate norms).
+//      (no bank conflicts).  The same pass sums the squares of the P-sample
+//      row segments (candidate norms).  7 x 7 patches use the same 8 x 8
+//      blocks: the reference operand's eighth column and eighth row are zero,
+//      so the eighth sample of every block row adds nothing.
 //   b. One thread issues, per pair of candidate rows p, the M = 128 x N = 16 x
-//      K = 16 MMAs over the patch rows and planes into tensor-memory columns
-//      16 p .. 16 p + 15 (column n = anchor n; reference rows of missing
-//      anchors are zero) and commits them to an mbarrier.
-//   c. The 8 warps read the accumulators back (tcgen05.ld; warp w reads TMEM
-//      lanes 32 (w % 4) .. + 31, i.e. candidate row 2p + (w % 4) / 2, columns
-//      32 (w % 2) .. + 31) and store each anchor's window distances.
+//      K = 16 MMAs over the patch rows and the group's planes into
+//      tensor-memory columns 16 p .. 16 p + 15 (column n = anchor slot n;
+//      reference rows of empty slots are zero), accumulating over the
+//      plane groups of the frame, and commits them to mbarriers: one that
+//      frees the group's shared-memory stage, and after the last group one
+//      that hands the accumulators to the readers.
+//   c. The 4 reader warps read the accumulators back (tcgen05.ld; warp w
+//      reads TMEM lanes 32 (w % 4) .. + 31, i.e. candidate row
+//      2p + (w % 4) / 2, columns 32 (w % 2) .. + 31) and store each anchor's
+//      window distances (rows relative to that anchor's own window).
 //
-// Tensor memory: each CTA allocates kChosenTmemCols columns and holds at most
-// two CTAs per SM (launch bounds and shared memory), so allocations never
-// wait on each other.  The MMA completion wait is bounded: when it runs out
-// the kernel records kStatusTensorTimeout in the session status word, which
-// the host turns into an error, and carries on without spinning further.
+// A frame of more planes than one shared-memory stage holds (vnlbcu's
+// defaults: 3 channels x patch_time 2 = 6 planes of a 27-row window) takes
+// several stages, so shared-memory stages and tensor-memory halves turn over
+// separately: a stage is free once its MMAs completed, a tensor-memory half
+// once its readers are done.
+//
+// Tensor memory: each CTA allocates 2 x kChosenTmemCols columns and holds
+// one CTA per SM (launch bounds and shared memory), so allocations never
+// wait on each other.  Every mbarrier wait is bounded: when one runs out the
+// kernel records kStatusTensorTimeout in the session status word, which the
+// host turns into an error, and carries on without spinning further.
 #include <cuda_bf16.h>
 
 #include <cstdint>
@@ -71,7 +87,7 @@ namespace vnlbgpu {
 namespace {
 
 constexpr int kTcThreads = 32 * kChosenWarps;
-constexpr int kPatch = 8;  // the tensor-core matcher is built for 8 x 8 patches
+constexpr int kBlock = 8;  // core-matrix side: patch rows and columns are padded to 8
 constexpr int kTcN = 16;   // MMA N: anchor slots per strip (kChosenAnchors used)
 // Instruction descriptor of tcgen05.mma kind::f16: FP32 accumulator (bits
 // 4-5 = 1), BF16 A and B (bits 7-9, 10-12 = 1), both K-major (bits 15, 16 =
@@ -84,44 +100,74 @@ constexpr int kProducerWarps = 8;
 constexpr int kConsumerWarps = 4;  // warps 8-11: tensor-memory lane quarters 0-3
 constexpr int kMmaWarp = kProducerWarps + kConsumerWarps;
 constexpr int kPipeThreads = 32 * (kMmaWarp + 1);
-constexpr int kStages = 2;
+constexpr int kStages = 2;  // shared-memory stages, and tensor-memory halves
 constexpr int kPipeTmemCols = kStages * kChosenTmemCols;
+constexpr int kMaxPlaneGroup = 3;
 // shared memory of at least this size keeps a second distance CTA (and its
 // tensor-memory allocation) off the SM
 constexpr int kMinSharedBytes = 116 * 1024;
+constexpr int kSharedLimit = 227 * 1024;
 
-// Per-stage window metadata (producers -> consumers).
+// Per-item window metadata and reference norms (producers -> readers), one
+// per tensor-memory half.  Anchor slot n is anchor n % 8 of grid row n / 8
+// of the strip.
 struct StageMeta {
-    int first, count, k, pad;
-    int win_lo[kChosenAnchors];  // window columns relative to the strip origin
-    int win_wx[kChosenAnchors];
-    float na[kChosenAnchors];    // reference norms
+    int k;        // scheduled frame
+    int rows;     // window rows the strip's anchors span
+    int off1;     // first window row of the second grid row's anchors
+    int h[2];     // window rows of each grid row's anchors
+    int pad[3];
+    int win_lo[kTcN];  // window columns relative to the strip origin
+    int win_wx[kTcN];  // 0: no anchor in the slot
+    int gi[kTcN];      // anchor index
+    float na[kTcN];    // reference norms
 };
 
+// The rows of a strip's windows: yl of the first grid row's anchors, and the
+// rows spanned from there to the last row of the second grid row's.
+__device__ __forceinline__ void strip_rows(const MatchLaunch& L, const TcStrip& st, int& yl0, int& yh0, int& yl1,
+                                           int& yh1) {
+    spatial_range(st.y[0], L.height, L.P, L.search_window, yl0, yh0);
+    yl1 = yl0;
+    yh1 = yh0;
+    if (st.count[1] > 0) spatial_range(st.y[1], L.height, L.P, L.search_window, yl1, yh1);
+}
+
 // Shared-memory layout of the distance kernel in bytes (128-byte aligned
-// parts): two stages of [BF16 blocks | reference block | norms | metadata],
-// then the producers' row sums, the mbarriers and the tensor-memory address.
+// parts): two stages of [BF16 blocks | reference blocks] for `group` planes,
+// then per tensor-memory half the candidate norms and the metadata, the
+// producers' row sums, the mbarriers and the tensor-memory address.
 struct PipeLayout {
-    int hank, bop, nb, meta, stage_bytes, rowsq, bars, tmem, bytes;
+    int hank, bop, stage_bytes, nb, meta, rowsq, bars, tmem, bytes;
 };
 
 __host__ __device__ inline int align128(int v) { return (v + 127) & ~127; }
 
-__host__ __device__ inline PipeLayout pipe_layout(int planes_n, int pairs) {
-    const int R = 2 * pairs + kPatch - 1;  // region rows
+__host__ __device__ inline int region_rows(int pairs) { return 2 * pairs + kBlock - 1; }
+
+__host__ __device__ inline PipeLayout pipe_layout(int group, int pairs) {
+    const int R = region_rows(pairs);
     PipeLayout l{};
     int off = 0;
-    l.hank = off;  off = align128(off + planes_n * R * 8 * 128);       // [q][r][b] 8x8 BF16 blocks
-    l.bop = off;   off = align128(off + planes_n * kPatch * 2 * 128);   // [q][py][n/8] 8x8 BF16 blocks
-    l.nb = off;    off = align128(off + 2 * pairs * kChosenCols * 4);   // candidate norms
-    l.meta = off;  off = align128(off + static_cast<int>(sizeof(StageMeta)));
+    l.hank = off;  off = align128(off + group * R * 8 * 128);           // [q][r][b] 8x8 BF16 blocks
+    l.bop = off;   off = align128(off + group * kBlock * 2 * 128);      // [q][py][n/8] 8x8 BF16 blocks
     l.stage_bytes = off;
     off = kStages * l.stage_bytes;
+    l.nb = off;    off = align128(off + kStages * 2 * pairs * kChosenCols * 4);  // candidate norms per half
+    l.meta = off;  off = align128(off + kStages * static_cast<int>(sizeof(StageMeta)));
     l.rowsq = off; off = align128(off + R * kChosenCols * 4);           // row sums of squares
-    l.bars = off;  off += 3 * kStages * 8;
+    l.bars = off;  off += 5 * kStages * 8;
     l.tmem = off;  off += 8;
     l.bytes = align128(off);
     return l;
+}
+
+// planes per shared-memory stage: the most (up to three) whose two stages
+// fit in shared memory
+inline int plane_group(int planes_n, int pairs) {
+    for (int g = planes_n < kMaxPlaneGroup ? planes_n : kMaxPlaneGroup; g > 1; --g)
+        if (pipe_layout(g, pairs).bytes <= kSharedLimit) return g;
+    return 1;
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -188,9 +234,15 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
+// stage s filled (producers -> issuer); stage s consumed by its MMAs (MMA
+// completion -> producers); half h accumulated (MMA completion -> readers);
+// half h read (readers -> issuer, producers); half h's norms and metadata
+// written (producers -> readers)
 __device__ __forceinline__ uint32_t full_bar(uint32_t bars, int s) { return bars + 8 * s; }
-__device__ __forceinline__ uint32_t tfull_bar(uint32_t bars, int s) { return bars + 8 * (kStages + s); }
-__device__ __forceinline__ uint32_t free_bar(uint32_t bars, int s) { return bars + 8 * (2 * kStages + s); }
+__device__ __forceinline__ uint32_t sfree_bar(uint32_t bars, int s) { return bars + 8 * (kStages + s); }
+__device__ __forceinline__ uint32_t tfull_bar(uint32_t bars, int h) { return bars + 8 * (2 * kStages + h); }
+__device__ __forceinline__ uint32_t tfree_bar(uint32_t bars, int h) { return bars + 8 * (3 * kStages + h); }
+__device__ __forceinline__ uint32_t mfull_bar(uint32_t bars, int h) { return bars + 8 * (4 * kStages + h); }
 
 // named barrier of the producer warps
 __device__ __forceinline__ void producer_sync() {
@@ -217,30 +269,37 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 }
 
 // Persistent, warp-specialised distance kernel.  Each CTA walks the items
-// (strip, scheduled frame) of strips blockIdx.x, blockIdx.x + gridDim.x, ...
-// through two shared-memory stages and two halves of its tensor memory:
-//   warps 0-7   producers: build stage i % 2 (BF16 blocks, reference block,
-//               norms, window metadata), then arrive on full[i % 2];
-//   warp 12     issuer: waits full, issues the item's MMAs into tensor-memory
-//               columns 256 (i % 2) .., commits them to tfull[i % 2];
-//   warps 8-11  consumers (TMEM lane quarters 0-3): wait tfull, read the
-//               accumulators back, store the distances, arrive on free[i % 2],
-//               which the producers wait for before refilling the stage.
-template <int PLANES>  // planes compared: search channels x patch_time
+// (strip, scheduled frame) of strips blockIdx.x, blockIdx.x + gridDim.x, ...;
+// item i takes tensor-memory half i % 2 and fills shared-memory stages with
+// its plane groups, fill j in stage j % 2:
+//   warps 0-7   producers: per plane group fill a stage (BF16 blocks and
+//               reference blocks) and arrive on full; after the last group
+//               write the half's norms and metadata and arrive on mfull;
+//   warp 12     issuer: per plane group wait full, issue the MMAs into the
+//               item's tensor-memory half, commit them to sfree (the
+//               producers' wait before refilling the stage); after the last
+//               group commit to tfull;
+//   warps 8-11  readers (TMEM lane quarters 0-3): wait mfull and tfull, read
+//               the accumulators back, store the distances, arrive on tfree,
+//               which the issuer and the producers wait for before reusing
+//               the half.
+template <int P, int G>  // patch size (7 or 8), planes per shared-memory stage
 __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunch L) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    constexpr int P = kPatch;
     const int Wy = L.window_rows;
     const int pairs = (Wy + 1) >> 1;
-    const int R = 2 * pairs + P - 1;
-    const PipeLayout lay = pipe_layout(PLANES, pairs);
+    const int R = region_rows(pairs);
+    const PipeLayout lay = pipe_layout(G, pairs);
     const uint32_t bars = smem_addr(smem + lay.bars);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + lay.tmem);
     float* rowsq = reinterpret_cast<float*>(smem + lay.rowsq);
     const size_t plane_values = static_cast<size_t>(L.height) * L.width;
     const int T = L.schedule_len;
+    const int planes_n = L.search_channels * L.Pt;
+    const int groups = (planes_n + G - 1) / G;
+    const int nb_floats = 2 * pairs * kChosenCols;
 
     if (warp == kMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
@@ -255,8 +314,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
             mbar_init(full_bar(bars, s), 1);
+            mbar_init(sfree_bar(bars, s), 1);
             mbar_init(tfull_bar(bars, s), 1);
-            mbar_init(free_bar(bars, s), kConsumerWarps);
+            mbar_init(tfree_bar(bars, s), kConsumerWarps);
+            mbar_init(mfull_bar(bars, s), 1);
         }
         mbar_init(drain, 1);
     }
@@ -278,170 +339,213 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
     };
 
     if (warp < kProducerWarps) {
-        int i = 0;
+        int i = 0, j = 0;
+        const float* anchor_frame =
+            L.video + static_cast<size_t>(L.schedule[0] % L.ring) * L.channels * plane_values;
         for (int si = blockIdx.x; si < L.strip_count; si += gridDim.x) {
-            const Strip strip = L.strips[si];
-            int yl, yh;
-            spatial_range(strip.y, L.height, P, L.search_window, yl, yh);
+            const TcStrip strip = L.tc_strips[si];
+            int yl, yh0, yl1, yh1;
+            strip_rows(L, strip, yl, yh0, yl1, yh1);
+            const int wy = yh1 - yl + 1;
+            const int Rs = region_rows((wy + 1) >> 1);  // region rows this strip uses
+            const int nb_used = 2 * ((wy + 1) >> 1) * kChosenCols;
             const int rx0 = strip.region_x;
-            const int count = strip.count;
+            // the anchors whose reference rows this warp stages: slot warp
+            // (first grid row) and slot warp + 8 (second grid row)
+            int2 anc[2];
+            bool has[2];
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                has[half] = warp < strip.count[half];
+                anc[half] = has[half] ? L.anchors[strip.first[half] + warp] : make_int2(0, 0);
+            }
             for (int k = 0; k < T; ++k, ++i) {
-                const int b = i & 1;
+                const int h = i & 1;
                 const int frame = L.schedule[k];
-                // global loads that need no stage: the reference samples of
-                // anchor `warp` (pairs of columns) and the first region row
-                const int n = warp;
-                float refv[PLANES][2];
-                {
-                    int2 a = make_int2(0, 0);
-                    if (n < count) a = L.anchors[strip.first + n];
-                    const float* anchor_frame =
-                        L.video + static_cast<size_t>(L.schedule[0] % L.ring) * L.channels * plane_values;
-#pragma unroll
-                    for (int j = 0; j < PLANES; ++j) {
-                        const int e = 2 * (lane + 32 * j);
-                        const int q = e >> 6, py = (e >> 3) & 7, px = e & 7;
-                        const int c = q / L.Pt, tt = q % L.Pt;
-                        const float* src = anchor_frame + (static_cast<size_t>(tt) * L.channels + c) * plane_values +
-                                           static_cast<size_t>(a.y + py) * L.width + a.x + px;
-                        refv[j][0] = n < count ? __ldg(src) : 0.0f;
-                        refv[j][1] = n < count ? __ldg(src + 1) : 0.0f;
+                // the half's norms and metadata are rewritten below: its
+                // readers must be done with item i - 2
+                wait(tfree_bar(bars, h), ((i >> 1) & 1) ^ 1);
+                StageMeta* meta = reinterpret_cast<StageMeta*>(smem + lay.meta) + h;
+                float* nb = reinterpret_cast<float*>(smem + lay.nb) + h * nb_floats;
+                if (threadIdx.x < kTcN) {
+                    const int m = threadIdx.x, row = m >> 3, idx = m & 7;
+                    int xl = 0, xh = -1, gi = 0;
+                    if (idx < strip.count[row]) {
+                        gi = strip.first[row] + idx;
+                        spatial_range(L.anchors[gi].x, L.width, P, L.search_window, xl, xh);
                     }
-                }
-                float cur[PLANES][3], nxt[PLANES][3];
-                auto load_row = [&](int r, float (&s)[PLANES][3]) {
-                    const int gy = yl + r;
-                    const bool row_in = gy < L.height;
-                    const int x0 = rx0 + lane;
-#pragma unroll
-                    for (int q = 0; q < PLANES; ++q) {
-                        const int c = q / L.Pt, tt = q % L.Pt;
-                        const float* src = L.video + (static_cast<size_t>(frame % L.ring + tt) * L.channels + c) * plane_values +
-                                           static_cast<size_t>(row_in ? gy : 0) * L.width;
-                        s[q][0] = row_in && x0 < L.width ? __ldg(src + x0) : 0.0f;
-                        s[q][1] = row_in && x0 + 32 < L.width ? __ldg(src + x0 + 32) : 0.0f;
-                        s[q][2] = row_in && lane < P - 1 && x0 + 64 < L.width ? __ldg(src + x0 + 64) : 0.0f;
-                    }
-                };
-                if (warp < R) load_row(warp, cur);
-                wait(free_bar(bars, b), ((i >> 1) & 1) ^ 1);
-                unsigned char* st = smem + b * lay.stage_bytes;
-                unsigned char* hank = st + lay.hank;
-                uint32_t* b32 = reinterpret_cast<uint32_t*>(st + lay.bop);
-                float* nb = reinterpret_cast<float*>(st + lay.nb);
-                StageMeta* meta = reinterpret_cast<StageMeta*>(st + lay.meta);
-                if (threadIdx.x < kChosenAnchors) {
-                    const int m = threadIdx.x;
-                    int xl = 0, xh = -1;
-                    if (m < count) spatial_range(L.anchors[strip.first + m].x, L.width, P, L.search_window, xl, xh);
                     meta->win_lo[m] = xl - rx0;
                     meta->win_wx[m] = xh - xl + 1;
+                    meta->gi[m] = gi;
                 }
                 if (threadIdx.x == 0) {
-                    meta->first = strip.first;
-                    meta->count = count;
                     meta->k = k;
+                    meta->rows = wy;
+                    meta->off1 = yl1 - yl;
+                    meta->h[0] = yh0 - yl + 1;
+                    meta->h[1] = yh1 - yl1 + 1;
                 }
-                {
-                    // B operand and reference norm: warp n takes anchor n (row
-                    // n of block (q * 8 + py, 0)) and zeroes row n of block
-                    // (q * 8 + py, 1); absent anchors are zero
-                    float acc = 0.0f;
+                float na[2] = {0.0f, 0.0f};
+                for (int g = 0; g < groups; ++g, ++j) {
+                    const int b = j & 1;
+                    const int q0 = g * G;
+                    float cur[G][3], nxt[G][3];
+                    auto load_row = [&](int r, float (&v)[G][3]) {
+                        const int gy = yl + r;
+                        const bool row_in = gy < L.height;
+                        const int x0 = rx0 + lane;
 #pragma unroll
-                    for (int j = 0; j < PLANES; ++j) {
-                        const int e = 2 * (lane + 32 * j);
-                        const int qpy = e >> 3, px = e & 7;
-                        acc = fmaf(refv[j][0], refv[j][0], acc);
-                        acc = fmaf(refv[j][1], refv[j][1], acc);
-                        b32[(((qpy * 2) * 8 + n) * 8 + px) >> 1] = pack_bf16(refv[j][0], refv[j][1]);
-                        b32[(((qpy * 2 + 1) * 8 + n) * 8 + px) >> 1] = 0u;
-                    }
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                    if (lane == 0) meta->na[n] = acc;
-                }
-                // BF16 blocks and row sums of squares, one region row per warp:
-                // lane l holds samples l, l + 32 and l + 64 (l < 7) of the row;
-                // block row c (= 8 b + i) is samples c .. c + 7, for c = l and
-                // c = l + 32.  The next row's samples are loaded ahead.
-                for (int r = warp; r < R; r += kProducerWarps) {
-                    if (r + kProducerWarps < R) load_row(r + kProducerWarps, nxt);
-                    float sq0 = 0.0f, sq1 = 0.0f;
-#pragma unroll
-                    for (int q = 0; q < PLANES; ++q) {
-                        float av[8], bv[8];
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            // source lane m = (lane + j) % 32 serves lane m - j
-                            // (no wrap: wants its sample m) when m >= j, else
-                            // lane m - j + 32 (wrap: wants its sample m + 64)
-                            const int from = (lane + j) & 31;
-                            const float f1 = __shfl_sync(0xffffffffu, cur[q][1], from);
-                            const float f02 = __shfl_sync(0xffffffffu, lane >= j ? cur[q][0] : cur[q][2], from);
-                            const bool wrap = lane + j >= 32;
-                            av[j] = wrap ? f1 : f02;  // sample lane + j
-                            bv[j] = wrap ? f02 : f1;  // sample lane + 32 + j
+                        for (int ql = 0; ql < G; ++ql) {
+                            const int q = q0 + ql;
+                            const bool in = row_in && q < planes_n;
+                            const int c = q / L.Pt, tt = q % L.Pt;
+                            const float* src =
+                                L.video + (static_cast<size_t>(frame % L.ring + tt) * L.channels + c) * plane_values +
+                                static_cast<size_t>(row_in ? gy : 0) * L.width;
+                            v[ql][0] = in && x0 < L.width ? __ldg(src + x0) : 0.0f;
+                            v[ql][1] = in && x0 + 32 < L.width ? __ldg(src + x0 + 32) : 0.0f;
+                            v[ql][2] = in && lane < kBlock - 1 && x0 + 64 < L.width ? __ldg(src + x0 + 64) : 0.0f;
                         }
-                        uint4* dst = reinterpret_cast<uint4*>(hank + (q * R + r) * 1024);
-                        dst[lane] = make_uint4(pack_bf16(av[0], av[1]), pack_bf16(av[2], av[3]),
-                                               pack_bf16(av[4], av[5]), pack_bf16(av[6], av[7]));
-                        dst[lane + 32] = make_uint4(pack_bf16(bv[0], bv[1]), pack_bf16(bv[2], bv[3]),
-                                                    pack_bf16(bv[4], bv[5]), pack_bf16(bv[6], bv[7]));
+                    };
+                    if (warp < Rs) load_row(warp, cur);
+                    // the stage's MMAs of fill j - 2 have completed
+                    wait(sfree_bar(bars, b), ((j >> 1) & 1) ^ 1);
+                    unsigned char* st = smem + b * lay.stage_bytes;
+                    unsigned char* hank = st + lay.hank;
+                    uint32_t* b32 = reinterpret_cast<uint32_t*>(st + lay.bop);
 #pragma unroll
-                        for (int j = 0; j < 8; ++j) {
-                            sq0 = fmaf(av[j], av[j], sq0);
-                            sq1 = fmaf(bv[j], bv[j], sq1);
+                    for (int half = 0; half < 2; ++half) {
+                        // B operand: the warp writes the rows of anchor slot
+                        // warp + 8 half (row `warp` of block (q * 8 + py,
+                        // half)), in pairs of columns; absent anchors, planes
+                        // past the last, and a 7 x 7 patch's eighth row and
+                        // column are zero
+#pragma unroll
+                        for (int jj = 0; jj < G; ++jj) {
+                            const int e = 2 * (lane + 32 * jj);
+                            const int ql = e >> 6, py = (e >> 3) & 7, px = e & 7;
+                            const int q = q0 + ql;
+                            float r0 = 0.0f, r1 = 0.0f;
+                            if (has[half] && q < planes_n && py < P && px < P) {
+                                const int c = q / L.Pt, tt = q % L.Pt;
+                                const float* src = anchor_frame +
+                                                   (static_cast<size_t>(tt) * L.channels + c) * plane_values +
+                                                   static_cast<size_t>(anc[half].y + py) * L.width + anc[half].x + px;
+                                r0 = __ldg(src);
+                                if (px + 1 < P) r1 = __ldg(src + 1);
+                            }
+                            na[half] = fmaf(r0, r0, na[half]);
+                            na[half] = fmaf(r1, r1, na[half]);
+                            b32[((((e >> 3) * 2 + half) * 8 + warp) * 8 + px) >> 1] = pack_bf16(r0, r1);
                         }
                     }
-                    rowsq[r * kChosenCols + lane] = sq0;
-                    rowsq[r * kChosenCols + lane + 32] = sq1;
+                    // BF16 blocks and row sums of squares, one region row per
+                    // warp: lane l holds samples l, l + 32 and l + 64 (l < 7)
+                    // of the row; block row c (= 8 b + i) is samples c .. c + 7,
+                    // for c = l and c = l + 32.  The next row's samples are
+                    // loaded ahead.  The row sums add up over plane groups.
+                    for (int r = warp; r < Rs; r += kProducerWarps) {
+                        if (r + kProducerWarps < Rs) load_row(r + kProducerWarps, nxt);
+                        float sq0 = 0.0f, sq1 = 0.0f;
 #pragma unroll
-                    for (int q = 0; q < PLANES; ++q)
+                        for (int ql = 0; ql < G; ++ql) {
+                            float av[8], bv[8];
 #pragma unroll
-                        for (int e = 0; e < 3; ++e) cur[q][e] = nxt[q][e];
+                            for (int jj = 0; jj < 8; ++jj) {
+                                // source lane m = (lane + jj) % 32 serves lane
+                                // m - jj (no wrap: wants its sample m) when
+                                // m >= jj, else lane m - jj + 32 (wrap: wants
+                                // its sample m + 64)
+                                const int from = (lane + jj) & 31;
+                                const float f1 = __shfl_sync(0xffffffffu, cur[ql][1], from);
+                                const float f02 = __shfl_sync(0xffffffffu, lane >= jj ? cur[ql][0] : cur[ql][2], from);
+                                const bool wrap = lane + jj >= 32;
+                                av[jj] = wrap ? f1 : f02;  // sample lane + jj
+                                bv[jj] = wrap ? f02 : f1;  // sample lane + 32 + jj
+                            }
+                            uint4* dst = reinterpret_cast<uint4*>(hank + (ql * R + r) * 1024);
+                            dst[lane] = make_uint4(pack_bf16(av[0], av[1]), pack_bf16(av[2], av[3]),
+                                                   pack_bf16(av[4], av[5]), pack_bf16(av[6], av[7]));
+                            dst[lane + 32] = make_uint4(pack_bf16(bv[0], bv[1]), pack_bf16(bv[2], bv[3]),
+                                                        pack_bf16(bv[4], bv[5]), pack_bf16(bv[6], bv[7]));
+#pragma unroll
+                            for (int jj = 0; jj < P; ++jj) {
+                                sq0 = fmaf(av[jj], av[jj], sq0);
+                                sq1 = fmaf(bv[jj], bv[jj], sq1);
+                            }
+                        }
+                        if (g == 0) {
+                            rowsq[r * kChosenCols + lane] = sq0;
+                            rowsq[r * kChosenCols + lane + 32] = sq1;
+                        } else {
+                            rowsq[r * kChosenCols + lane] += sq0;
+                            rowsq[r * kChosenCols + lane + 32] += sq1;
+                        }
+#pragma unroll
+                        for (int ql = 0; ql < G; ++ql)
+#pragma unroll
+                            for (int e = 0; e < 3; ++e) cur[ql][e] = nxt[ql][e];
+                    }
+                    fence_async_shared();
+                    producer_sync();  // stage complete (and, after the last group, the row sums)
+                    if (threadIdx.x == 0) mbar_arrive(full_bar(bars, b));
                 }
-                producer_sync();  // row sums complete
-                for (int it = threadIdx.x; it < 2 * pairs * kChosenCols; it += kProducerWarps * 32) {
+                // reference norms and candidate norms of the half
+#pragma unroll
+                for (int half = 0; half < 2; ++half) {
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) na[half] += __shfl_xor_sync(0xffffffffu, na[half], o);
+                    if (lane == 0) meta->na[warp + 8 * half] = na[half];
+                }
+                for (int it = threadIdx.x; it < nb_used; it += kProducerWarps * 32) {
                     const int y = it / kChosenCols, c = it - y * kChosenCols;
                     float acc = 0.0f;
 #pragma unroll
                     for (int r = 0; r < P; ++r) acc += rowsq[(y + r) * kChosenCols + c];
                     nb[it] = acc;
                 }
-                fence_async_shared();
-                producer_sync();  // stage complete; the row sums free for the next item
-                if (threadIdx.x == 0) mbar_arrive(full_bar(bars, b));
+                producer_sync();  // norms complete; the row sums free for the next item
+                if (threadIdx.x == 0) mbar_arrive(mfull_bar(bars, h));
             }
         }
     } else if (warp == kMmaWarp) {
-        int i = 0;
+        int i = 0, j = 0;
+        const uint32_t leader = lane == 0 ? 1u : 0u;
         for (int si = blockIdx.x; si < L.strip_count; si += gridDim.x) {
+            const TcStrip strip = L.tc_strips[si];
+            int yl, yh0, yl1, yh1;
+            strip_rows(L, strip, yl, yh0, yl1, yh1);
+            const int pairs_s = (yh1 - yl + 2) >> 1;  // row pairs this strip uses
             for (int k = 0; k < T; ++k, ++i) {
-                const int b = i & 1;
-                wait(full_bar(bars, b), (i >> 1) & 1);
-                // after a wait ran out no further MMA is issued (the whole
-                // warp agrees); L.stall_mma, a test switch, issues none at
-                // all so that the consumers' waits run out
-                timed_out = __any_sync(0xffffffffu, timed_out);
-                if (timed_out || L.stall_mma) continue;
-                tc_fence_after();
-                {
+                const int h = i & 1;
+                const uint32_t td = tmem + static_cast<uint32_t>(h * kChosenTmemCols);
+                wait(tfree_bar(bars, h), ((i >> 1) & 1) ^ 1);
+                for (int g = 0; g < groups; ++g, ++j) {
+                    const int b = j & 1;
+                    wait(full_bar(bars, b), (j >> 1) & 1);
+                    // after a wait ran out no further MMA is issued (the whole
+                    // warp agrees); L.stall_mma, a test switch, issues none at
+                    // all so that the other roles' waits run out
+                    timed_out = __any_sync(0xffffffffu, timed_out);
+                    if (timed_out || L.stall_mma) continue;
+                    tc_fence_after();
                     const unsigned char* st = smem + b * lay.stage_bytes;
                     const uint32_t ha = smem_addr(st + lay.hank), ba = smem_addr(st + lay.bop);
-                    const uint32_t td = tmem + static_cast<uint32_t>(b * kChosenTmemCols);
-                    const uint32_t leader = lane == 0 ? 1u : 0u;
-                    for (int p = 0; p < pairs; ++p) {
+                    const int gq = planes_n - g * G < G ? planes_n - g * G : G;  // planes of this group
+                    for (int p = 0; p < pairs_s; ++p) {
 #pragma unroll
-                        for (int s = 0; s < PLANES * 4; ++s) {
-                            const int q = s >> 2, py = 2 * (s & 3);
-                            const uint64_t ad = tc_desc(ha + (q * R + 2 * p + py) * 1024, 1024, 128);
-                            const uint64_t bd = tc_desc(ba + (q * P + py) * 256, 256, 128);
-                            tc_mma(td + p * kTcN, ad, bd, s > 0 ? 1u : 0u, leader);
+                        for (int s = 0; s < G * 4; ++s) {
+                            const int ql = s >> 2, py = 2 * (s & 3);
+                            if (ql >= gq) break;
+                            const uint64_t ad = tc_desc(ha + (ql * R + 2 * p + py) * 1024, 1024, 128);
+                            const uint64_t bd = tc_desc(ba + (ql * kBlock + py) * 256, 256, 128);
+                            tc_mma(td + p * kTcN, ad, bd, (g > 0 || s > 0) ? 1u : 0u, leader);
                         }
                     }
-                    tc_commit(tfull_bar(bars, b), leader);
+                    tc_commit(sfree_bar(bars, b), leader);
+                    if (g == groups - 1) tc_commit(tfull_bar(bars, h), leader);
+                    __syncwarp();
                 }
-                __syncwarp();
             }
         }
     } else if (warp < kProducerWarps + kConsumerWarps) {
@@ -451,48 +555,50 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
         int i = 0;
         for (int si = blockIdx.x; si < L.strip_count; si += gridDim.x) {
             for (int k = 0; k < T; ++k, ++i) {
-                const int b = i & 1;
+                const int h = i & 1;
                 const uint32_t parity = (i >> 1) & 1;
-                wait(full_bar(bars, b), parity);  // the stage's metadata (producers' writes)
-                wait(tfull_bar(bars, b), parity);
+                wait(mfull_bar(bars, h), parity);  // the half's norms and metadata (producers' writes)
+                wait(tfull_bar(bars, h), parity);
                 tc_fence_after();
-                const unsigned char* st = smem + b * lay.stage_bytes;
-                const float* nb = reinterpret_cast<const float*>(st + lay.nb);
-                const StageMeta* meta = reinterpret_cast<const StageMeta*>(st + lay.meta);
-                const int count = meta->count;
-                // per anchor: this lane's window column (or -1), row stride,
-                // reference norm and output base
-                int rel[kChosenAnchors], wx[kChosenAnchors];
-                float na[kChosenAnchors];
-                float* out[kChosenAnchors];
+                const float* nb = reinterpret_cast<const float*>(smem + lay.nb) + h * nb_floats;
+                const StageMeta* meta = reinterpret_cast<const StageMeta*>(smem + lay.meta) + h;
+                const int wy = meta->rows, off1 = meta->off1, h0 = meta->h[0], h1 = meta->h[1];
+                const size_t kofs = static_cast<size_t>(meta->k) * L.window_cells;
+                // per anchor slot: this lane's window column (or -1) and the
+                // reference norm; the row stride and the anchor index are
+                // read from the metadata at the stores
+                int rel[kTcN];
+                float na[kTcN];
 #pragma unroll
-                for (int n = 0; n < kChosenAnchors; ++n) {
+                for (int n = 0; n < kTcN; ++n) {
                     const int r0 = x - meta->win_lo[n];
-                    wx[n] = meta->win_wx[n];
-                    rel[n] = n < count && r0 >= 0 && r0 < wx[n] ? r0 : -1;
+                    rel[n] = r0 >= 0 && r0 < meta->win_wx[n] ? r0 : -1;
                     na[n] = meta->na[n];
-                    out[n] = L.approx_dist + static_cast<size_t>(meta->first + n) * L.approx_stride +
-                             static_cast<size_t>(meta->k) * L.window_cells;
                 }
                 const uint32_t ta = tmem + (static_cast<uint32_t>(32 * quarter) << 16) +
-                                    static_cast<uint32_t>(b * kChosenTmemCols);
-                for (int p0 = 0; p0 < pairs; p0 += 2) {
+                                    static_cast<uint32_t>(h * kChosenTmemCols);
+                const int pairs_s = (wy + 1) >> 1;
+                for (int p0 = 0; p0 < pairs_s; p0 += 2) {
                     uint32_t v[32];
                     tmem_load32(ta + static_cast<uint32_t>(p0 * kTcN), v);
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int cy = 2 * (p0 + h) + dy;
-                        if (cy >= Wy) continue;
+                    for (int hh = 0; hh < 2; ++hh) {
+                        const int cy = 2 * (p0 + hh) + dy;
+                        if (cy >= wy) continue;
                         const float bn = nb[cy * kChosenCols + x];
 #pragma unroll
-                        for (int n = 0; n < kChosenAnchors; ++n)
-                            if (rel[n] >= 0)
-                                out[n][cy * wx[n] + rel[n]] = fmaxf(na[n] + bn - 2.0f * __uint_as_float(v[16 * h + n]), 0.0f);
+                        for (int n = 0; n < kTcN; ++n) {
+                            const int row = n < 8 ? cy : cy - off1;
+                            if (rel[n] < 0 || row < 0 || row >= (n < 8 ? h0 : h1)) continue;
+                            float* o = L.approx_dist + static_cast<size_t>(meta->gi[n]) * L.approx_stride + kofs +
+                                       row * meta->win_wx[n] + rel[n];
+                            *o = fmaxf(na[n] + bn - 2.0f * __uint_as_float(v[16 * hh + n]), 0.0f);
+                        }
                     }
                 }
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(free_bar(bars, b));
+                if (lane == 0) mbar_arrive(tfree_bar(bars, h));
             }
         }
     }
@@ -513,14 +619,55 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
     }
 }
 
-// Steps 2-4 for one anchor per warp, from the approximate distances.
-template <int PLANES>
+// Exact FP32 distance of candidate (frame, row y, column col) to the anchor,
+// in the plain form's arithmetic order: planes (channel, t), patch rows, the
+// row SSD of row_ssd (packed pairs for 8 samples).
+template <int P>
+__device__ __forceinline__ float exact_distance(const MatchLaunch& L, const float* anchor_frame, int2 anchor,
+                                                int frame, int y, int col, int planes_n, size_t plane_values) {
+    float d = 0.0f;
+#pragma unroll 1
+    for (int q = 0; q < planes_n; ++q) {
+        const int c = q / L.Pt, t = q % L.Pt;
+        const float* rp = anchor_frame + (static_cast<size_t>(t) * L.channels + c) * plane_values +
+                          static_cast<size_t>(anchor.y) * L.width + anchor.x;
+        const float* cp = L.video + (static_cast<size_t>(frame % L.ring + t) * L.channels + c) * plane_values +
+                          static_cast<size_t>(y) * L.width + col;
+        // the candidate's samples first (all loads in flight), the reference
+        // rows (one address for the whole warp) as they are used
+        float cv[P][P];
+#pragma unroll
+        for (int r = 0; r < P; ++r)
+#pragma unroll
+            for (int ii = 0; ii < P; ++ii) cv[r][ii] = __ldg(cp + static_cast<size_t>(r) * L.width + ii);
+#pragma unroll
+        for (int r = 0; r < P; ++r) {
+            const float* rr = rp + static_cast<size_t>(r) * L.width;
+            if constexpr (P == kLanes) {
+                float2 a2[4], b2[4];
+#pragma unroll
+                for (int ii = 0; ii < 4; ++ii) {
+                    a2[ii] = make_float2(__ldg(rr + 2 * ii), __ldg(rr + 2 * ii + 1));
+                    b2[ii] = make_float2(cv[r][2 * ii], cv[r][2 * ii + 1]);
+                }
+                d = row_ssd8_x2(d, a2, b2);
+            } else {
+                d = row_ssd<P>(d, [&](int ii) { return __ldg(rr + ii); }, [&](int ii) { return cv[r][ii]; });
+            }
+        }
+    }
+    return d;
+}
+
+// Steps 2-4 for one anchor per warp, from the approximate distances.  The
+// capped buffer's slot s lives in lane s % 32, register s / 32 (CW registers:
+// buffers of up to 32 CW entries).
+template <int P, int CW>
 __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
-    __shared__ float sorted_d[kChosenWarps][32];
-    __shared__ int sorted_i[kChosenWarps][32];
+    __shared__ float sorted_d[kChosenWarps][32 * CW];
+    __shared__ int sorted_i[kChosenWarps][32 * CW];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    constexpr int P = kPatch;
     const int gi = blockIdx.x * kChosenWarps + warp;
     if (gi >= L.anchor_count) return;  // no block-wide synchronisation below
     const int2 anchor = L.anchors[gi];
@@ -530,6 +677,7 @@ __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
     const int Wx = xh - xl + 1;
     const int cells = Wx * (yh - yl + 1);
     const size_t plane_values = static_cast<size_t>(L.height) * L.width;
+    const int planes_n = L.search_channels * L.Pt;
     const float* approx = L.approx_dist + static_cast<size_t>(gi) * L.approx_stride;
     const float* anchor_frame = L.video + static_cast<size_t>(L.schedule[0] % L.ring) * L.channels * plane_values;
 
@@ -545,14 +693,40 @@ __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
     s.worst = kInf;
     s.top_count = 0;
     s.top_front = kInf;
-    unsigned reg_d = 0u, reg_top = 0u;  // bits of non-negative distances
-    int reg_id = 0;
-    float reg_exact = 0.0f;
+    unsigned reg_d[CW], reg_top = 0u;  // bits of non-negative distances
+    int reg_id[CW];
+    float reg_exact[CW];
+#pragma unroll
+    for (int w = 0; w < CW; ++w) {
+        reg_d[w] = 0u;
+        reg_id[w] = 0;
+        reg_exact[w] = 0.0f;
+    }
+    // the buffer's largest distance and its lowest slot
+    auto find_worst = [&]() {
+        unsigned m = reg_d[0];
+#pragma unroll
+        for (int w = 1; w < CW; ++w) m = m > reg_d[w] ? m : reg_d[w];
+        const unsigned wmax = __reduce_max_sync(0xffffffffu, m);
+        s.worst = __uint_as_float(wmax);
+#pragma unroll
+        for (int w = CW - 1; w >= 0; --w) {
+            const unsigned hit = __ballot_sync(0xffffffffu, reg_d[w] == wmax);
+            if (hit) s.worst_idx = 32 * w + __ffs(hit) - 1;
+        }
+    };
+    auto put = [&](int slot, float d, int id) {
+#pragma unroll
+        for (int w = 0; w < CW; ++w)
+            if (slot >> 5 == w && lane == (slot & 31)) {
+                reg_d[w] = __float_as_uint(d);
+                reg_id[w] = id;
+            }
+    };
 
     for (int k = 0; k < L.schedule_len; ++k) {
         // the CPU's sequential selection over frame k (raster order) on the
-        // approximate distances: the K-smallest front and the capped buffer,
-        // buffer slot i in lane i (the plain matcher's register replay)
+        // approximate distances: the K-smallest front and the capped buffer
         const float* dk = approx + k * L.window_cells;
         float next = lane < cells ? __ldg(dk + lane) : kInf;
         for (int base = 0; base < cells; base += 32) {
@@ -571,24 +745,12 @@ __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
                 if (!(d <= limit)) continue;
                 const int id = (k << 20) | (base + src_lane);
                 if (s.count < s.cap) {
-                    if (lane == s.count) {
-                        reg_d = __float_as_uint(d);
-                        reg_id = id;
-                    }
+                    put(s.count, d, id);
                     s.count++;
-                    if (s.count == s.cap) {
-                        const unsigned w = __reduce_max_sync(0xffffffffu, reg_d);
-                        s.worst_idx = __ffs(__ballot_sync(0xffffffffu, reg_d == w)) - 1;
-                        s.worst = __uint_as_float(w);
-                    }
+                    if (s.count == s.cap) find_worst();
                 } else if (d < s.worst) {
-                    if (lane == s.worst_idx) {
-                        reg_d = __float_as_uint(d);
-                        reg_id = id;
-                    }
-                    const unsigned w = __reduce_max_sync(0xffffffffu, reg_d);
-                    s.worst_idx = __ffs(__ballot_sync(0xffffffffu, reg_d == w)) - 1;
-                    s.worst = __uint_as_float(w);
+                    put(s.worst_idx, d, id);
+                    find_worst();
                 }
                 if (s.top_count < K) {
                     if (lane == s.top_count) reg_top = __float_as_uint(d);
@@ -603,41 +765,16 @@ __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
             }
         }
     }
-    // exact FP32 distance of every entry left in the buffer (slot i in lane
-    // i), in the plain form's arithmetic order: once, after the last frame
-    if (lane < s.count) {
-        const int i = reg_id & 0xfffff;
-        const int cy = i / Wx;
-        const int col = xl + (i - cy * Wx);
-        const int frame = L.schedule[reg_id >> 20];
-        float d = 0.0f;
-#pragma unroll 1
-        for (int q = 0; q < PLANES; ++q) {
-            const int c = q / L.Pt, t = q % L.Pt;
-            const float* rp = anchor_frame + (static_cast<size_t>(t) * L.channels + c) * plane_values +
-                              static_cast<size_t>(anchor.y) * L.width + anchor.x;
-            const float* cp = L.video + (static_cast<size_t>(frame % L.ring + t) * L.channels + c) * plane_values +
-                              static_cast<size_t>(yl + cy) * L.width + col;
-            // the candidate's samples first (all loads in flight), the
-            // reference rows (one address for the whole warp) as they are used
-            float cv[P][P];
+    // exact FP32 distance of every entry left in the buffer, in the plain
+    // form's arithmetic order: once, after the last frame
 #pragma unroll
-            for (int r = 0; r < P; ++r)
-#pragma unroll
-                for (int ii = 0; ii < P; ++ii) cv[r][ii] = __ldg(cp + static_cast<size_t>(r) * L.width + ii);
-#pragma unroll
-            for (int r = 0; r < P; ++r) {
-                const float* rr = rp + static_cast<size_t>(r) * L.width;
-                float2 a2[4], b2[4];
-#pragma unroll
-                for (int ii = 0; ii < 4; ++ii) {
-                    a2[ii] = make_float2(__ldg(rr + 2 * ii), __ldg(rr + 2 * ii + 1));
-                    b2[ii] = make_float2(cv[r][2 * ii], cv[r][2 * ii + 1]);
-                }
-                d = row_ssd8_x2(d, a2, b2);
-            }
+    for (int w = 0; w < CW; ++w) {
+        if (32 * w + lane < s.count) {
+            const int i = reg_id[w] & 0xfffff;
+            const int cy = i / Wx;
+            reg_exact[w] = exact_distance<P>(L, anchor_frame, anchor, L.schedule[reg_id[w] >> 20], yl + cy,
+                                             xl + (i - cy * Wx), planes_n, plane_values);
         }
-        reg_exact = d;
     }
 
     // select_similar_patches on the exact distances of the buffer: the K
@@ -655,20 +792,37 @@ __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
         }
         S = 1;
     } else {
-        int rank = 0;
-        for (int j = 0; j < n; ++j) {
-            const float dj = __shfl_sync(0xffffffffu, reg_exact, j);
-            const int ij = __shfl_sync(0xffffffffu, reg_id, j);
-            rank += (dj < reg_exact || (dj == reg_exact && ij < reg_id)) ? 1 : 0;
+        int rank[CW];
+#pragma unroll
+        for (int w = 0; w < CW; ++w) rank[w] = 0;
+        for (int jj = 0; jj < n; ++jj) {
+            float dsrc = reg_exact[0];
+            int isrc = reg_id[0];
+#pragma unroll
+            for (int w = 1; w < CW; ++w)
+                if (jj >> 5 == w) {
+                    dsrc = reg_exact[w];
+                    isrc = reg_id[w];
+                }
+            const float dj = __shfl_sync(0xffffffffu, dsrc, jj & 31);
+            const int ij = __shfl_sync(0xffffffffu, isrc, jj & 31);
+#pragma unroll
+            for (int w = 0; w < CW; ++w)
+                rank[w] += (dj < reg_exact[w] || (dj == reg_exact[w] && ij < reg_id[w])) ? 1 : 0;
         }
-        if (lane < n) {
-            sd[rank] = reg_exact;
-            si[rank] = reg_id;
-        }
+#pragma unroll
+        for (int w = 0; w < CW; ++w)
+            if (32 * w + lane < n) {
+                sd[rank[w]] = reg_exact[w];
+                si[rank[w]] = reg_id[w];
+            }
         __syncwarp();
         const int selected = min(K, n);
         const float threshold = std_max(L.tau, sd[selected - 1]);
-        const int within = __popc(__ballot_sync(0xffffffffu, lane < n && sd[lane] <= threshold));
+        int within = 0;
+#pragma unroll
+        for (int w = 0; w < CW; ++w)
+            within += __popc(__ballot_sync(0xffffffffu, 32 * w + lane < n && sd[32 * w + lane] <= threshold));
         S = min(within, min(L.soft_cap, n));
     }
     __syncwarp();
@@ -733,27 +887,38 @@ __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
 }  // namespace
 
 bool chosen_match_supported(int P, int planes_n, int window_w, int window_h) {
-    return P == kPatch && planes_n >= 1 && planes_n <= 3 && window_w <= kChosenCols && window_h <= kChosenMaxRows;
+    return (P == 7 || P == 8) && planes_n >= 1 && planes_n <= kChosenMaxPlanes && window_w <= kChosenCols &&
+           window_h <= kChosenMaxRows;
 }
 
 size_t chosen_match_shared_bytes(const MatchLaunch& L) {
     const int planes_n = L.search_channels * L.Pt;
-    const PipeLayout lay = pipe_layout(planes_n, (L.window_rows + 1) / 2);
+    const int pairs = (L.window_rows + 1) / 2;
+    const PipeLayout lay = pipe_layout(plane_group(planes_n, pairs), pairs);
     return static_cast<size_t>(lay.bytes > kMinSharedBytes ? lay.bytes : kMinSharedBytes);
 }
 
 cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t stream) {
     if (strips <= 0) return cudaSuccess;
     const int planes_n = L.search_channels * L.Pt;
-    if (L.P != kPatch || planes_n < 1 || planes_n > 3 || L.window_rows > kChosenMaxRows || !L.status ||
-        !L.approx_dist || L.approx_stride < L.schedule_len * L.window_cells || L.strip_count != strips)
+    // entries the buffer can hold at once: the cap, or every candidate of
+    // the window when there are fewer
+    const long long candidates = static_cast<long long>(L.window_cells) * L.schedule_len;
+    const int cap = L.soft_cap < candidates ? L.soft_cap : static_cast<int>(candidates);
+    if (!chosen_match_supported(L.P, planes_n, kChosenCols, L.window_rows) || !L.status || !L.approx_dist ||
+        !L.tc_strips ||
+        L.approx_stride < L.schedule_len * L.window_cells || L.strip_count != strips || L.K > 32 ||
+        cap > kChosenMaxBuffer || L.max_rows < cap)
         return cudaErrorInvalidValue;
     int device = 0, sms = 0;
     cudaError_t err = cudaGetDevice(&device);
     if (err != cudaSuccess) return err;
     err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (err != cudaSuccess) return err;
+    const int pairs = (L.window_rows + 1) / 2;
+    const int group = plane_group(planes_n, pairs);
     const size_t smem = chosen_match_shared_bytes(L);
+    if (smem > static_cast<size_t>(kSharedLimit)) return cudaErrorInvalidValue;
     // a quarter of the SMs stays free for the other pipeline lane's kernels
     // (measured: +1.5% frames/s at 1080p over a grid of every SM)
     const int persistent = sms - sms / 4;
@@ -768,10 +933,27 @@ cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t s
         select<<<select_blocks, kTcThreads, 0, stream>>>(L);
         err = cudaGetLastError();
     };
-    switch (planes_n) {
-        case 1: launch(tc_distance_kernel<1>, tc_select_kernel<1>); break;
-        case 2: launch(tc_distance_kernel<2>, tc_select_kernel<2>); break;
-        default: launch(tc_distance_kernel<3>, tc_select_kernel<3>); break;
+    auto with_select = [&](auto distance) {
+        if (L.P == 8) {
+            if (cap <= 32) launch(distance, tc_select_kernel<8, 1>);
+            else launch(distance, tc_select_kernel<8, 2>);
+        } else {
+            if (cap <= 32) launch(distance, tc_select_kernel<7, 1>);
+            else launch(distance, tc_select_kernel<7, 2>);
+        }
+    };
+    if (L.P == 8) {
+        switch (group) {
+            case 1: with_select(tc_distance_kernel<8, 1>); break;
+            case 2: with_select(tc_distance_kernel<8, 2>); break;
+            default: with_select(tc_distance_kernel<8, 3>); break;
+        }
+    } else {
+        switch (group) {
+            case 1: with_select(tc_distance_kernel<7, 1>); break;
+            case 2: with_select(tc_distance_kernel<7, 2>); break;
+            default: with_select(tc_distance_kernel<7, 3>); break;
+        }
     }
     return err;
 }

@@ -93,10 +93,10 @@ void temporal_range(int source_frames, int patch_time, int bwd, int fwd, int anc
 struct Grid {
     std::vector<int2> anchors;
     std::vector<Strip> strips;
-    std::vector<Strip> strips_chosen;  // up to kChosenAnchors anchors per strip (chosen matcher)
+    std::vector<TcStrip> strips_chosen;  // tensor-core matcher strips (one or two grid rows)
     DeviceArray<int2> d_anchors;
     DeviceArray<Strip> d_strips;
-    DeviceArray<Strip> d_strips_chosen;
+    DeviceArray<TcStrip> d_strips_chosen;
     DeviceArray<int> d_map;  // [H][W] anchor index or -1
     // stack-tile reach tables (TileLaunch)
     DeviceArray<int2> d_tile_grid_rows;  // [tiles_y]
@@ -722,10 +722,15 @@ struct Session {
             probe.window_rows = chosen_wy = ch0;
             probe.tiles_x = chosen_tiles_x = kChosenCols / 8;
             probe.window_cells = cw0 * ch0;
-            // the register replay: the buffer and the K front fit in a warp;
-            // each anchor's distance array doubles as its 32 + 32 sorted rows
-            chosen = cap_eff <= 32 && K <= 32 && 64 <= cw0 * ch0 &&
+            // the register replay: the K front fits in a warp, the buffer in
+            // two registers per lane
+            chosen = cap_eff <= kChosenMaxBuffer && K <= 32 && 64 <= cw0 * ch0 &&
                      chosen_match_shared_bytes(probe) <= 227 * 1024;
+            // strips of two grid rows: their windows span up to the window
+            // plus the grid step (consecutive grid rows are at most a step
+            // apart); pairs whose span is larger stay single rows
+            probe.window_rows = std::min(kChosenMaxRows, ch0 + std::max(1, step));
+            if (chosen && chosen_match_shared_bytes(probe) <= 227 * 1024) chosen_wy = probe.window_rows;
             approx_stride = sched_max * cw0 * ch0;
         }
 
@@ -964,30 +969,62 @@ struct Session {
             grid->strips.push_back(s);
         }
         if (chosen) {
-            size_t k = 0;
-            while (k < a.size()) {
-                Strip st{};
-                st.first = static_cast<int>(k);
-                st.y = a[k].y;
-                int x0 = INT_MAX, x1 = INT_MIN, count = 0;
-                while (k < a.size() && a[k].y == st.y && count < kChosenAnchors) {
-                    int xl, xh;
-                    spatial_range(a[k].x, width, P, params.search_window, xl, xh);
-                    const int nx0 = std::min(x0, xl), nx1 = std::max(x1, xh);
-                    if (count > 0 && nx1 - nx0 + 1 > 8 * chosen_tiles_x) break;
-                    x0 = nx0;
-                    x1 = nx1;
-                    ++count;
-                    ++k;
+            // the grid's rows [begin, end) in the anchor list
+            std::vector<std::pair<size_t, size_t>> rows;
+            for (size_t k = 0; k < a.size();) {
+                size_t e = k;
+                while (e < a.size() && a[e].y == a[k].y) ++e;
+                rows.emplace_back(k, e);
+                k = e;
+            }
+            auto window_x = [&](size_t k, int& xl, int& xh) {
+                spatial_range(a[k].x, width, P, params.search_window, xl, xh);
+            };
+            for (size_t r = 0; r < rows.size();) {
+                // pair row r with row r + 1 when their windows span at most
+                // chosen_wy rows
+                bool pair = false;
+                if (r + 1 < rows.size()) {
+                    int yl0, yh0, yl1, yh1;
+                    spatial_range(a[rows[r].first].y, height, P, params.search_window, yl0, yh0);
+                    spatial_range(a[rows[r + 1].first].y, height, P, params.search_window, yl1, yh1);
+                    pair = yh1 - yl0 + 1 <= chosen_wy;
                 }
-                st.count = count;
-                st.region_x = x0;  // first candidate column
-                st.region_w = x1 - x0 + 1;
-                grid->strips_chosen.push_back(st);
+                size_t k[2] = {rows[r].first, pair ? rows[r + 1].first : 0};
+                const size_t end[2] = {rows[r].second, pair ? rows[r + 1].second : 0};
+                while (k[0] < end[0] || k[1] < end[1]) {
+                    TcStrip st{};
+                    for (int h = 0; h < 2; ++h) {
+                        st.first[h] = static_cast<int>(k[h]);
+                        st.y[h] = k[h] < end[h] ? a[k[h]].y : a[rows[r].first].y;
+                    }
+                    int x0 = INT_MAX, x1 = INT_MIN;
+                    // take the anchors of both rows in x order while their
+                    // windows fit in kChosenCols columns
+                    for (;;) {
+                        int h = -1;
+                        for (int c = 0; c < 2; ++c)
+                            if (k[c] < end[c] && st.count[c] < kChosenAnchors && (h < 0 || a[k[c]].x < a[k[h]].x))
+                                h = c;
+                        if (h < 0) break;
+                        int xl, xh;
+                        window_x(k[h], xl, xh);
+                        const int nx0 = std::min(x0, xl), nx1 = std::max(x1, xh);
+                        if (st.count[0] + st.count[1] > 0 && nx1 - nx0 + 1 > kChosenCols) break;
+                        x0 = nx0;
+                        x1 = nx1;
+                        ++st.count[h];
+                        ++k[h];
+                    }
+                    if (st.count[1] == 0) st.y[1] = st.y[0];
+                    st.region_x = x0;  // first candidate column
+                    grid->strips_chosen.push_back(st);
+                }
+                r += pair ? 2 : 1;
             }
             grid->d_strips_chosen.allocate(grid->strips_chosen.size(), "cudaMalloc(strips)");
             check(cudaMemcpy(grid->d_strips_chosen.ptr, grid->strips_chosen.data(),
-                             grid->strips_chosen.size() * sizeof(Strip), cudaMemcpyHostToDevice),
+                             grid->strips_chosen.size() * sizeof(TcStrip), cudaMemcpyHostToDevice),
                   "cudaMemcpy(strips)");
         }
         grid->d_anchors.allocate(a.size(), "cudaMalloc(anchors)");
@@ -1442,7 +1479,7 @@ struct Session {
             check(launch_match(mf, static_cast<int>(grid.tile_strips.size()), warps, map, ls), "fallback match launch");
             stats.kernel_launches += 6 + 2 * ((G + kLearnedChunk - 1) / kLearnedChunk) * (mlp_net.layers + 1);
         } else if (chosen) {
-            m.strips = grid.d_strips_chosen.ptr;
+            m.tc_strips = grid.d_strips_chosen.ptr;
             m.tiles_x = chosen_tiles_x;
             m.approx_dist = lane.approx.ptr;
             m.approx_stride = approx_stride;

@@ -30,6 +30,17 @@ struct Strip {
     int region_h;
 };
 
+// A strip of the tensor-core matcher: up to kChosenAnchors consecutive
+// anchors of each of one or two consecutive grid rows, all of whose search
+// windows lie within kChosenCols candidate columns from region_x.
+struct TcStrip {
+    int first[2];  // index of each row's first anchor in the anchor list
+    int count[2];  // anchors of each row (the second row's may be 0)
+    int y[2];      // the rows' anchor y
+    int region_x;  // first candidate column
+    int pad;
+};
+
 // Source frames on the device: frame f of a source lives in slot f % ring of
 // a store of ring + patch_time - 1 frame slots [slot][channels][H][W], whose
 // last patch_time - 1 slots repeat the first ones, so that the patch_time
@@ -48,6 +59,7 @@ struct MatchLaunch {
     int schedule_len;
     const int2* anchors;  // grid anchors in raster order
     const Strip* strips;
+    const TcStrip* tc_strips;  // tensor-core matcher strips
     const int* anchor_map;  // [H][W] anchor index or -1
     int region_rows;      // shared rows per plane (incl. padding)
     int region_stride;    // shared row stride in floats
@@ -88,17 +100,23 @@ struct MatchLaunch {
     int victim_stride;
 };
 
-// Chosen form on tensor cores (match_chosen.cu): a CTA of kChosenWarps warps
-// matches up to kChosenAnchors consecutive anchors of one grid row whose
-// search windows lie within kChosenCols consecutive candidate columns.  One
-// tcgen05 MMA (M = 128, N = 16, K = 16) covers two candidate rows of those
-// columns against every anchor of the strip, so the window may have at most
-// 2 * 16 rows (16 row pairs of 16 accumulator columns fill kChosenTmemCols).
+// Chosen form on tensor cores (match_chosen.cu): a CTA matches a strip of up
+// to kChosenAnchors consecutive anchors of each of one or two consecutive
+// grid rows whose search windows lie within kChosenCols consecutive
+// candidate columns.  One tcgen05 MMA (M = 128, N = 16, K = 16) covers two
+// candidate rows of those columns against the strip's 16 anchor slots, so
+// the strip's windows may span at most 2 * 16 rows (16 row pairs of 16
+// accumulator columns fill kChosenTmemCols).
+// Patches are 7 x 7 or 8 x 8, compared over up to kChosenMaxPlanes planes
+// (search channels x patch_time), and the capped buffer holds up to
+// kChosenMaxBuffer entries.
 constexpr int kChosenAnchors = 8;
 constexpr int kChosenWarps = 8;
 constexpr int kChosenCols = 64;
 constexpr int kChosenMaxRows = 32;
 constexpr int kChosenTmemCols = 256;
+constexpr int kChosenMaxPlanes = 6;
+constexpr int kChosenMaxBuffer = 64;
 
 bool chosen_match_supported(int P, int planes_n, int window_w, int window_h);
 size_t chosen_match_shared_bytes(const MatchLaunch& L);
