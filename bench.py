@@ -634,13 +634,13 @@ EXTRA_WORKLOADS = {
 
 # the mixed stream: 4 GrayS 1280x720 + 2 YUV444PS 1920x1080 + 1 GrayS
 # 3840x2160, 24 frames each, sigma cycling 5 / 15 / 30, tau 200, cap 4,
-# patch_time 2, rank by noise level (24 at sigma 5, 16 at 15, 8 at 30)
+# patch_time 2, rank by noise level (24 at sigma 5, 16 at 15, 8 at 30) with a
+# group of the same size (the rank is at most the group)
 MIXED_STREAM = dict(
     clips=[(1280, 720, 1, 5.0), (1280, 720, 1, 15.0), (1280, 720, 1, 30.0), (1280, 720, 1, 5.0),
            (1920, 1080, 3, 15.0), (1920, 1080, 3, 30.0), (3840, 2160, 1, 15.0)],
     frames=24, steps=2, warmup=3, rank={5.0: 24, 15.0: 16, 30.0: 8},
-    stage=dict(block_size=8, block_step=8, group_size=8, bm_range=9, radius=1, patch_time=2, cap_factor=4.0,
-               tau=200.0))
+    stage=dict(block_size=8, block_step=8, bm_range=9, radius=1, patch_time=2, cap_factor=4.0, tau=200.0))
 
 
 def measure_mixed_stream(form, args, ranks, local):
@@ -662,7 +662,7 @@ def measure_mixed_stream(form, args, ranks, local):
     for i, (w, h, c, sigma) in enumerate(spec["clips"]):
         clean, noisy = synth.make_clip(w, h, n, c, sigma, seed=100 * ranks.rank + i)
         shape = np.empty((n, c, h, w), np.float32)
-        kw = dict(spec["stage"], rank=spec["rank"][sigma], form=form)
+        kw = dict(spec["stage"], rank=spec["rank"][sigma], group_size=spec["rank"][sigma], form=form)
         bp = vnlbcu.parse_parameters(lib.STAGE_BASIC, shape, sigma, dict(kw))
         fp = vnlbcu.parse_parameters(lib.STAGE_FINAL, shape, sigma, dict(kw, variance_threshold=None))
         bp.device_id = fp.device_id = local
@@ -754,7 +754,7 @@ def mixed_stream_line(args, ranks, local):
             "chosen_tc": {"value": tc["value"], "ms_per_step": tc["ms_per_step"], "autotune": tc["autotune"]},
             "speedup_chosen_tc_vs_plain": tc["value"] / plain["value"],
             "max_psnr_loss_db": max(c["psnr_plain_db"] - c["psnr_chosen_tc_db"] for c in clips), "clips": clips,
-            "params": dict(MIXED_STREAM["stage"], rank=MIXED_STREAM["rank"]), "unit": UNIT,
+            "params": dict(MIXED_STREAM["stage"], rank=MIXED_STREAM["rank"], group_size="= rank"), "unit": UNIT,
             "pipeline": "one host thread and one CUDA stream per clip, all clips in flight; not graph-captured"}
 
 

@@ -100,7 +100,7 @@ typedef struct vnlbgpu_params {
  * buffer of at most 32 patches (group_size * cap_factor) and group_size <= 32.
  * CHOSEN_TC applies to 7x7 and 8x8 patches compared over at most 6 planes
  * (search channels x patch_time), a search window of at most 64 columns by
- * 32 rows, a buffer of at most 64 patches and group_size <= 32: vnlbcu's own
+ * 32 rows, a buffer of at most 96 patches and group_size <= 32: vnlbcu's own
  * defaults included.  Other configurations run PLAIN.  With either chosen
  * matcher the group filter runs
  * in mixed precision too: the dual Gram on TF32 tensor cores with FP32

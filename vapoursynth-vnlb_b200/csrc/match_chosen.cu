@@ -103,6 +103,8 @@ constexpr int kPipeThreads = 32 * (kMmaWarp + 1);
 constexpr int kStages = 2;  // shared-memory stages, and tensor-memory halves
 constexpr int kPipeTmemCols = kStages * kChosenTmemCols;
 constexpr int kMaxPlaneGroup = 3;
+// region rows per producer warp and plane group (at most 2 * 16 + 7 rows)
+constexpr int kRowsPerWarp = (2 * kChosenMaxRows / 2 + kBlock - 1 + kProducerWarps - 1) / kProducerWarps;
 // shared memory of at least this size keeps a second distance CTA (and its
 // tensor-memory allocation) off the SM
 constexpr int kMinSharedBytes = 116 * 1024;
@@ -284,7 +286,9 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 //               which the issuer and the producers wait for before reusing
 //               the half.
 template <int P, int G>  // patch size (7 or 8), planes per shared-memory stage
-__global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunch L) {
+// 152 registers: 13 warps x 32 x 152 = 63,232 of the SM's 65,536 (one CTA
+// per SM); the producers hold their rows of a plane group in registers.
+__global__ void __maxnreg__(152) tc_distance_kernel(MatchLaunch L) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -389,7 +393,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                 for (int g = 0; g < groups; ++g, ++j) {
                     const int b = j & 1;
                     const int q0 = g * G;
-                    float cur[G][3], nxt[G][3];
+                    // this warp's region rows r = warp + 8 rr of the group,
+                    // all loaded before the stage wait (one global latency
+                    // per group, overlapping the stage's previous MMAs)
+                    float rowv[kRowsPerWarp][G][3];
                     auto load_row = [&](int r, float (&v)[G][3]) {
                         const int gy = yl + r;
                         const bool row_in = gy < L.height;
@@ -407,7 +414,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                             v[ql][2] = in && lane < kBlock - 1 && x0 + 64 < L.width ? __ldg(src + x0 + 64) : 0.0f;
                         }
                     };
-                    if (warp < Rs) load_row(warp, cur);
+#pragma unroll
+                    for (int rr = 0; rr < kRowsPerWarp; ++rr)
+                        if (warp + kProducerWarps * rr < Rs) load_row(warp + kProducerWarps * rr, rowv[rr]);
                     // the stage's MMAs of fill j - 2 have completed
                     wait(sfree_bar(bars, b), ((j >> 1) & 1) ^ 1);
                     unsigned char* st = smem + b * lay.stage_bytes;
@@ -442,10 +451,13 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                     // BF16 blocks and row sums of squares, one region row per
                     // warp: lane l holds samples l, l + 32 and l + 64 (l < 7)
                     // of the row; block row c (= 8 b + i) is samples c .. c + 7,
-                    // for c = l and c = l + 32.  The next row's samples are
-                    // loaded ahead.  The row sums add up over plane groups.
-                    for (int r = warp; r < Rs; r += kProducerWarps) {
-                        if (r + kProducerWarps < Rs) load_row(r + kProducerWarps, nxt);
+                    // for c = l and c = l + 32.  The row sums add up over plane
+                    // groups.
+#pragma unroll
+                    for (int rr = 0; rr < kRowsPerWarp; ++rr) {
+                        const int r = warp + kProducerWarps * rr;
+                        if (r >= Rs) break;
+                        float (&cur)[G][3] = rowv[rr];
                         float sq0 = 0.0f, sq1 = 0.0f;
 #pragma unroll
                         for (int ql = 0; ql < G; ++ql) {
@@ -481,10 +493,6 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                             rowsq[r * kChosenCols + lane] += sq0;
                             rowsq[r * kChosenCols + lane + 32] += sq1;
                         }
-#pragma unroll
-                        for (int ql = 0; ql < G; ++ql)
-#pragma unroll
-                            for (int e = 0; e < 3; ++e) cur[ql][e] = nxt[ql][e];
                     }
                     fence_async_shared();
                     producer_sync();  // stage complete (and, after the last group, the row sums)
@@ -559,20 +567,33 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                 const uint32_t parity = (i >> 1) & 1;
                 wait(mfull_bar(bars, h), parity);  // the half's norms and metadata (producers' writes)
                 wait(tfull_bar(bars, h), parity);
+                // after a wait ran out the metadata may not be written yet:
+                // the warp reads and stores nothing more (the status word
+                // already reports the failure)
+                timed_out = __any_sync(0xffffffffu, timed_out);
+                if (timed_out) {
+                    if (lane == 0) mbar_arrive(tfree_bar(bars, h));
+                    continue;
+                }
                 tc_fence_after();
                 const float* nb = reinterpret_cast<const float*>(smem + lay.nb) + h * nb_floats;
                 const StageMeta* meta = reinterpret_cast<const StageMeta*>(smem + lay.meta) + h;
                 const int wy = meta->rows, off1 = meta->off1, h0 = meta->h[0], h1 = meta->h[1];
-                const size_t kofs = static_cast<size_t>(meta->k) * L.window_cells;
-                // per anchor slot: this lane's window column (or -1) and the
-                // reference norm; the row stride and the anchor index are
-                // read from the metadata at the stores
-                int rel[kTcN];
+                const unsigned kofs = static_cast<unsigned>(meta->k) * static_cast<unsigned>(L.window_cells);
+                // per anchor slot: this lane's window column and the row
+                // stride packed (rel | wx << 8; -1: the column is outside the
+                // window), the offset of the anchor's frame-k distances
+                // (32-bit: the launch checks the buffer's size), and the
+                // reference norm
+                int relwx[kTcN];
+                unsigned base[kTcN];
                 float na[kTcN];
 #pragma unroll
                 for (int n = 0; n < kTcN; ++n) {
                     const int r0 = x - meta->win_lo[n];
-                    rel[n] = r0 >= 0 && r0 < meta->win_wx[n] ? r0 : -1;
+                    const int wxn = meta->win_wx[n];
+                    relwx[n] = r0 >= 0 && r0 < wxn ? r0 | (wxn << 8) : -1;
+                    base[n] = static_cast<unsigned>(meta->gi[n]) * static_cast<unsigned>(L.approx_stride) + kofs;
                     na[n] = meta->na[n];
                 }
                 const uint32_t ta = tmem + (static_cast<uint32_t>(32 * quarter) << 16) +
@@ -589,10 +610,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
 #pragma unroll
                         for (int n = 0; n < kTcN; ++n) {
                             const int row = n < 8 ? cy : cy - off1;
-                            if (rel[n] < 0 || row < 0 || row >= (n < 8 ? h0 : h1)) continue;
-                            float* o = L.approx_dist + static_cast<size_t>(meta->gi[n]) * L.approx_stride + kofs +
-                                       row * meta->win_wx[n] + rel[n];
-                            *o = fmaxf(na[n] + bn - 2.0f * __uint_as_float(v[16 * hh + n]), 0.0f);
+                            const unsigned rows_n = static_cast<unsigned>(n < 8 ? h0 : h1);
+                            if (relwx[n] < 0 || static_cast<unsigned>(row) >= rows_n) continue;
+                            const unsigned o = base[n] + static_cast<unsigned>(row * (relwx[n] >> 8) + (relwx[n] & 0xff));
+                            L.approx_dist[o] = fmaxf(na[n] + bn - 2.0f * __uint_as_float(v[16 * hh + n]), 0.0f);
                         }
                     }
                 }
@@ -908,6 +929,8 @@ cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t s
     if (!chosen_match_supported(L.P, planes_n, kChosenCols, L.window_rows) || !L.status || !L.approx_dist ||
         !L.tc_strips ||
         L.approx_stride < L.schedule_len * L.window_cells || L.strip_count != strips || L.K > 32 ||
+        static_cast<unsigned long long>(L.anchor_count) * static_cast<unsigned long long>(L.approx_stride) >
+            0xffffffffull ||
         cap > kChosenMaxBuffer || L.max_rows < cap)
         return cudaErrorInvalidValue;
     int device = 0, sms = 0;
@@ -936,10 +959,12 @@ cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t s
     auto with_select = [&](auto distance) {
         if (L.P == 8) {
             if (cap <= 32) launch(distance, tc_select_kernel<8, 1>);
-            else launch(distance, tc_select_kernel<8, 2>);
+            else if (cap <= 64) launch(distance, tc_select_kernel<8, 2>);
+            else launch(distance, tc_select_kernel<8, 3>);
         } else {
             if (cap <= 32) launch(distance, tc_select_kernel<7, 1>);
-            else launch(distance, tc_select_kernel<7, 2>);
+            else if (cap <= 64) launch(distance, tc_select_kernel<7, 2>);
+            else launch(distance, tc_select_kernel<7, 3>);
         }
     };
     if (L.P == 8) {

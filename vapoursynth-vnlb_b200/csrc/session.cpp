@@ -723,7 +723,7 @@ struct Session {
             probe.tiles_x = chosen_tiles_x = kChosenCols / 8;
             probe.window_cells = cw0 * ch0;
             // the register replay: the K front fits in a warp, the buffer in
-            // two registers per lane
+            // up to three registers per lane
             chosen = cap_eff <= kChosenMaxBuffer && K <= 32 && 64 <= cw0 * ch0 &&
                      chosen_match_shared_bytes(probe) <= 227 * 1024;
             // strips of two grid rows: their windows span up to the window
@@ -1630,6 +1630,9 @@ struct Session {
         next_lane = (next_lane + 1) % lane_count;
         Lane& lane = lanes[li];
         wait_reads(lane.stream, victim->reads);  // its previous contents may still be read
+        // and still be written: a stack computed on another lane and evicted
+        // before anything read it (its reads then ordered nothing)
+        check(cudaStreamWaitEvent(lane.stream, victim->ready, 0), "cudaStreamWaitEvent(stack written)");
         victim->anchor = -1;                     // until the work below is queued
         compute_anchor(anchor, victim->data.ptr, lane);
         check(cudaEventRecord(victim->ready, lane.stream), "cudaEventRecord(stack ready)");
@@ -1803,6 +1806,9 @@ struct Session {
         check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
         if (status != 0) {
             check(cudaMemsetAsync(d_status.ptr, 0, sizeof(int), stream), "cudaMemsetAsync(status)");
+            // any stack computed since the last check may hold the failed
+            // kernel's output: none is reused
+            invalidate();
             if (status == kStatusRankNotCovered) fail("VNLB CUDA: group_size must cover the effective VNLB rank");
             if (status == kStatusTensorTimeout)
                 fail("VNLB CUDA: the tensor-core matcher timed out waiting for its MMAs");
@@ -1818,6 +1824,10 @@ void Session::queue_copy(int source, int f, const float* host_frame, cudaStream_
     const int j = f % ring;
     FrameSlot& sl = st.slots[static_cast<size_t>(j)];
     wait_reads(on, sl.reads);  // the previous frame's readers
+    // and the previous frame's copy, which may be queued on another stream
+    // and not have been read at all (a window frame that no queued work
+    // needed): two copies into one slot must not overlap
+    check(cudaStreamWaitEvent(on, sl.ready, 0), "cudaStreamWaitEvent(slot written)");
     const size_t bytes = frame_values() * sizeof(float);
     float* dst = st.own.ptr + static_cast<size_t>(j) * frame_values();
     check(cudaMemcpyAsync(dst, host_frame, bytes, cudaMemcpyHostToDevice, on), "cudaMemcpyAsync(frame upload)");

@@ -116,7 +116,7 @@ constexpr int kChosenCols = 64;
 constexpr int kChosenMaxRows = 32;
 constexpr int kChosenTmemCols = 256;
 constexpr int kChosenMaxPlanes = 6;
-constexpr int kChosenMaxBuffer = 64;
+constexpr int kChosenMaxBuffer = 96;
 
 bool chosen_match_supported(int P, int planes_n, int window_w, int window_h);
 size_t chosen_match_shared_bytes(const MatchLaunch& L);
