@@ -33,6 +33,20 @@ def unpack(flat: np.ndarray, inputs: int, hidden: int, layers: int, outputs: int
     return ws, bs
 
 
+def forward_logits(flat, shape, x, bf16_last_input=False):
+    """Logits in float64 with the BF16-rounded weights; bf16_last_input
+    also rounds the output layer's input activations to BF16, as the
+    tensor-core inference does (learned.cu, tc_logits_kernel)."""
+    inputs, hidden, layers, outputs = shape
+    ws, bs = unpack(flat, *shape)
+    a = np.asarray(x, np.float64)
+    for l in range(layers):
+        a = np.maximum(a @ bf16(ws[l].astype(np.float32)).T + bs[l], 0.0)
+    if bf16_last_input:
+        a = bf16(a.astype(np.float32))
+    return a @ bf16(ws[layers].astype(np.float32)).T + bs[layers]
+
+
 def loss_and_gradients(flat, shape, x, targets, round_weights=True):
     """(mean loss, flat gradients) in float64."""
     inputs, hidden, layers, outputs = shape

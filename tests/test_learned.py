@@ -43,6 +43,36 @@ def test_gradients_match_the_fp64_oracle():
     assert err <= 2e-2
 
 
+def test_tensor_core_output_layer_and_radix_shortlist():
+    """The shortlist path (vnlbgpu_mlp_shortlist, as the learned form runs
+    it): the output layer on the tensor cores (tcgen05, BF16 activations and
+    weights, FP32 accumulation) at the configs' shape (5445 offsets, hidden
+    128), a batch that is no multiple of the 128-row tile and outputs that
+    are no multiple of the 256-column tile, then the top 64 by radix select.
+    Against the FP64 oracle of the same arithmetic (activations rounded to
+    BF16 before the output layer) the shortlists share at least 98% of their
+    ids (the hidden layers' FP32 sums can move an activation across a BF16
+    rounding boundary, which reorders near-ties at the 64th place)."""
+    import torch
+
+    shape = (45, 128, 3, 5445)
+    net = lib.MLP(*shape, max_batch=512, seed=11)
+    rng = np.random.default_rng(12)
+    x = rng.normal(0.0, 1.0, (300, shape[0])).astype(np.float32)
+    dx = torch.from_numpy(x).cuda()
+    out = torch.empty((300, 64), dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    net.shortlist(dx.data_ptr(), 300, 64, out.data_ptr())
+    got = out.cpu().numpy()
+    z = M.forward_logits(net.get_weights(), shape, x, bf16_last_input=True)
+    want = np.argsort(-z, axis=1, kind="stable")[:, :64]
+    assert got.min() >= 0 and got.max() < shape[3]
+    assert all(len(set(r.tolist())) == 64 for r in got)  # 64 distinct ids per row
+    overlap = np.mean([len(set(g.tolist()) & set(w.tolist())) / 64.0 for g, w in zip(got, want)])
+    print(f"shortlist overlap with the FP64 oracle {overlap:.4f}")
+    assert overlap >= 0.98
+
+
 def test_training_lowers_the_loss():
     rng = np.random.default_rng(4)
     n, inputs, outputs = 4096, 20, 50

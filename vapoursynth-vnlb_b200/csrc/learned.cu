@@ -12,8 +12,10 @@
 //
 // Kernels (all hand-written): a tiled GEMM C = op(A) op(B) (+ bias, ReLU) with
 // FP32 or BF16 operands, the softmax loss and its gradient, the ReLU
-// gradient, column sums (bias gradients), Adam, and a per-row top-k of the
-// logits for the shortlist.
+// gradient, column sums (bias gradients), Adam; for inference the output
+// layer on the 5th-generation tensor cores (tcgen05.mma, BF16 operands in
+// shared memory, FP32 accumulators in tensor memory) and a per-row top-k of
+// the logits by radix select for the shortlist.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -199,47 +201,273 @@ __global__ void to_bf16_kernel(const float* w, __nv_bfloat16* w16, size_t n) {
 }
 
 // The `k` largest logits of each row, as class ids (ties by the lower id):
-// one block per row finds the k-th largest value by bisection on its
-// order-preserving bits, then the ids above it and, in id order, enough of
-// those equal to it.
-__global__ void topk_kernel(const float* logits, int classes, int k, int* out) {
-    __shared__ int s_count;
-    __shared__ int s_pos;
-    const int row = blockIdx.x;
-    const float* z = logits + static_cast<size_t>(row) * classes;
-    auto key = [](float f) {
-        const unsigned u = __float_as_uint(f);
-        return (u & 0x80000000u) ? ~u : (u | 0x80000000u);  // larger float -> larger key
-    };
-    unsigned lo = 0u, hi = 0xffffffffu;  // the k-th largest key lies in [lo, hi]
-    while (lo < hi) {
-        const unsigned mid = static_cast<unsigned>((static_cast<unsigned long long>(lo) + hi + 1ull) / 2ull);
-        if (threadIdx.x == 0) s_count = 0;
+// one block per row loads the row's order-preserving keys into shared
+// memory, finds the k-th largest key by a radix select (four passes of 8
+// bits from the top, per-warp histograms), then writes the ids above it and,
+// in id order, enough of those equal to it.
+constexpr int kTopkThreads = 256;
+constexpr int kTopkWarps = kTopkThreads / 32;
+
+__device__ __forceinline__ unsigned order_key(float f) {
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);  // larger float -> larger key
+}
+
+__global__ void __launch_bounds__(kTopkThreads) topk_kernel(const float* logits, int classes, int k, int* out) {
+    extern __shared__ unsigned keys[];  // [classes]
+    __shared__ int hist[kTopkWarps][256];
+    __shared__ int suffix[257];
+    __shared__ int s_pos, s_digit, s_above;
+    __shared__ int warp_ties[kTopkWarps];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const float* z = logits + static_cast<size_t>(blockIdx.x) * classes;
+    for (int i = tid; i < classes; i += kTopkThreads) keys[i] = order_key(z[i]);
+    unsigned prefix = 0u, mask = 0u;
+    int need = k;  // keys still to take among those matching the prefix
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int i = lane; i < 256; i += 32) hist[warp][i] = 0;
         __syncthreads();
-        int c = 0;
-        for (int i = threadIdx.x; i < classes; i += blockDim.x) c += key(z[i]) >= mid;
-        atomicAdd(&s_count, c);
+        for (int base = 0; base < classes; base += kTopkThreads) {
+            // lanes with the same digit add once, by their lowest lane
+            const int i = base + tid;
+            const unsigned key = i < classes ? keys[i] : 0u;
+            const bool in = i < classes && (key & mask) == prefix;
+            const unsigned digit = (key >> shift) & 0xffu;
+            const unsigned peers = __match_any_sync(0xffffffffu, in ? digit : 256u + lane);
+            if (in && lane == __ffs(peers) - 1) atomicAdd(&hist[warp][digit], __popc(peers));
+        }
         __syncthreads();
-        const int count = s_count;
+        // suffix[d] = keys (matching the prefix) whose digit is >= d
+        if (tid < 256) {
+            int c = 0;
+            for (int w = 0; w < kTopkWarps; ++w) c += hist[w][tid];
+            suffix[tid] = c;
+        }
+        if (tid == 0) suffix[256] = 0;
         __syncthreads();
-        if (count >= k) lo = mid; else hi = mid - 1u;
+        if (warp == 0) {
+            // suffix sums over the 256 digits, 8 per lane from the top
+            int part[8], run = 0;
+#pragma unroll
+            for (int j = 7; j >= 0; --j) {
+                run += suffix[lane * 8 + j];
+                part[j] = run;
+            }
+            int incl = run;  // this lane's block and every block of higher digits
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_down_sync(0xffffffffu, incl, o);
+                if (lane + o < 32) incl += v;
+            }
+            const int after = incl - run;  // the blocks of higher digits
+            // the lanes above contribute `after`; write the suffix sums
+#pragma unroll
+            for (int j = 0; j < 8; ++j) suffix[lane * 8 + j] = part[j] + after;
+        }
+        __syncthreads();
+        // the digit: the largest d with suffix[d] >= need (suffix[0], the
+        // keys matching the prefix, is at least need: k <= classes)
+        if (tid < 256 && suffix[tid] >= need && suffix[tid + 1] < need) {
+            s_digit = tid;
+            s_above = suffix[tid + 1];
+        }
+        __syncthreads();
+        const int d = s_digit;
+        need -= s_above;
+        prefix |= static_cast<unsigned>(d) << shift;
+        mask |= 0xffu << shift;
+        __syncthreads();
     }
-    const unsigned kth = lo;
-    if (threadIdx.x == 0) s_pos = 0;
+    const unsigned kth = prefix;  // `need` ids equal to it complete the k
+    if (tid == 0) s_pos = 0;
     __syncthreads();
-    int* o = out + static_cast<size_t>(row) * k;
-    for (int i = threadIdx.x; i < classes; i += blockDim.x)
-        if (key(z[i]) > kth) o[atomicAdd(&s_pos, 1)] = i;
+    int* o = out + static_cast<size_t>(blockIdx.x) * k;
+    for (int i = tid; i < classes; i += kTopkThreads)
+        if (keys[i] > kth) o[atomicAdd(&s_pos, 1)] = i;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int p = s_pos;
-        for (int i = 0; i < classes && p < k; ++i)
-            if (key(z[i]) == kth) o[p++] = i;
-        for (; p < k; ++p) o[p] = -1;
+    const int above = s_pos;
+    // the ties, in id order: chunks of 256 ids, ordered positions by ballots
+    int taken = 0;
+    for (int base = 0; base < classes && taken < need; base += kTopkThreads) {
+        const int i = base + tid;
+        const bool tie = i < classes && keys[i] == kth;
+        const unsigned b = __ballot_sync(0xffffffffu, tie);
+        if (lane == 0) warp_ties[warp] = __popc(b);
+        __syncthreads();
+        int before = taken;
+        for (int w = 0; w < warp; ++w) before += warp_ties[w];
+        const int pos = before + __popc(b & ((1u << lane) - 1u));
+        if (tie && pos < need) o[above + pos] = i;
+        int total = 0;
+        for (int w = 0; w < kTopkWarps; ++w) total += warp_ties[w];
+        taken += total;
+        __syncthreads();
     }
+    for (int p = above + need + tid; p < k; p += kTopkThreads) o[p] = -1;  // fewer classes than k
 }
 
 int grid_for(size_t n) { return static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 16)); }
+
+// The output layer for inference on the 5th-generation tensor cores: logits
+// [M][N] = bf16(act)[M][K] * W16[N][K]^T + bias, FP32 accumulation in tensor
+// memory.  One CTA of 4 warps takes 128 rows x 256 outputs: the rows'
+// activations, rounded to BF16, and the 256 weight rows go to shared memory
+// as no-swizzle K-major core matrices (8 rows x 16 bytes; core matrix (kc,
+// g) of an operand with R rows at ((kc * R / 8) + g) * 128 bytes), one
+// thread issues the K / 16 MMAs (M = 128, N = 256, K = 16) and commits them
+// to an mbarrier, and each warp reads its 32 accumulator lanes back 32
+// columns at a time, adds the bias and writes its rows through a shared
+// transpose so that every store is a coalesced 128-byte row segment.
+constexpr int kTcM = 128, kTcNOut = 256, kTcThreadsL = 128, kTcMaxK = 128;
+constexpr int kTcSpin = 1 << 22;  // mbarrier polls before the wait gives up
+constexpr uint32_t kLogitsIdesc = (1u << 4) | (1u << 7) | (1u << 10) |
+                                  (static_cast<uint32_t>(kTcNOut >> 3) << 17) | (static_cast<uint32_t>(kTcM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ uint64_t kmajor_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+           (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ bool bar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__global__ void __launch_bounds__(kTcThreadsL) tc_logits_kernel(int M, int N, int K, const float* act,
+                                                                 const __nv_bfloat16* w16, const float* bias,
+                                                                 float* logits, int* status) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long done_bar;
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcNOut;
+    unsigned char* a_s = smem;                                   // [K / 8][16][8 rows][16 B]
+    unsigned char* b_s = smem + static_cast<size_t>(kTcM) * K * 2;  // [K / 8][32][8 rows][16 B]
+    const uint32_t bar = smem_u32(&done_bar);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(kTcNOut)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // A: row m0 + tid, 8 activations per core-matrix row, rounded to BF16
+    {
+        const int r = tid, m = m0 + r;
+        for (int kc = 0; kc < K / 8; ++kc) {
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (m < M) {
+                const float4* src = reinterpret_cast<const float4*>(act + static_cast<size_t>(m) * K + 8 * kc);
+                const float4 lo = src[0], hi = src[1];
+                __nv_bfloat162 p0 = __floats2bfloat162_rn(lo.x, lo.y), p1 = __floats2bfloat162_rn(lo.z, lo.w);
+                __nv_bfloat162 p2 = __floats2bfloat162_rn(hi.x, hi.y), p3 = __floats2bfloat162_rn(hi.z, hi.w);
+                v = make_uint4(*reinterpret_cast<uint32_t*>(&p0), *reinterpret_cast<uint32_t*>(&p1),
+                               *reinterpret_cast<uint32_t*>(&p2), *reinterpret_cast<uint32_t*>(&p3));
+            }
+            *reinterpret_cast<uint4*>(a_s + ((kc * (kTcM / 8) + (r >> 3)) * 128 + (r & 7) * 16)) = v;
+        }
+    }
+    // B: weight rows n0 + tid and n0 + tid + 128
+    for (int h = 0; h < 2; ++h) {
+        const int r = tid + kTcThreadsL * h, n = n0 + r;
+        for (int kc = 0; kc < K / 8; ++kc) {
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (n < N) v = *reinterpret_cast<const uint4*>(w16 + static_cast<size_t>(n) * K + 8 * kc);
+            *reinterpret_cast<uint4*>(b_s + ((kc * (kTcNOut / 8) + (r >> 3)) * 128 + (r & 7) * 16)) = v;
+        }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    if (warp == 0) {
+        const uint32_t leader = lane == 0 ? 1u : 0u;
+        const uint32_t a0 = smem_u32(a_s), b0 = smem_u32(b_s);
+        for (int s = 0; s < K / 16; ++s) {
+            const uint64_t ad = kmajor_desc(a0 + 2 * s * (kTcM / 8) * 128, (kTcM / 8) * 128, 128);
+            const uint64_t bd = kmajor_desc(b0 + 2 * s * (kTcNOut / 8) * 128, (kTcNOut / 8) * 128, 128);
+            asm volatile(
+                "{\n\t.reg .pred p, e;\n\tsetp.ne.b32 p, %4, 0;\n\tsetp.ne.b32 e, %5, 0;\n\t"
+                "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                "l"(ad), "l"(bd), "r"(kLogitsIdesc), "r"(s > 0 ? 1u : 0u), "r"(leader)
+                : "memory");
+        }
+        asm volatile(
+            "{\n\t.reg .pred e;\n\tsetp.ne.b32 e, %1, 0;\n\t"
+            "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}\n" ::"r"(bar),
+            "r"(leader)
+            : "memory");
+        __syncwarp();
+    }
+    // the accumulators are complete once the commit arrives (bounded wait)
+    int polls = 0;
+    bool ok = true;
+    while (!bar_try_wait(bar, 0)) {
+        if (++polls >= kTcSpin) {
+            ok = false;
+            break;
+        }
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+        if (lane == 0 && status) atomicCAS(status, 0, kStatusLogitsTimeout);
+    } else {
+        // epilogue: 32 columns at a time through a [128][33] transpose in the
+        // (now free) operand memory; warp w owns rows 32 w .. 32 w + 31
+        float* tile = reinterpret_cast<float*>(smem) + warp * 32 * 33;
+        for (int c0 = 0; c0 < kTcNOut; c0 += 32) {
+            if (n0 + c0 >= N) break;  // uniform
+            uint32_t v[32];
+            const uint32_t ta = tmem + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>(c0);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                "[%32];\n\ttcgen05.wait::ld.sync.aligned;"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(ta)
+                : "memory");
+#pragma unroll
+            for (int c = 0; c < 32; ++c) tile[lane * 33 + c] = __uint_as_float(v[c]);
+            __syncwarp();
+            const int n = n0 + c0 + lane;
+            const float bn = n < N && bias ? bias[n] : 0.0f;
+            for (int r = 0; r < 32; ++r) {
+                const int m = m0 + 32 * warp + r;
+                if (m < M && n < N) logits[static_cast<size_t>(m) * N + n] = tile[r * 33 + lane] + bn;
+            }
+            __syncwarp();
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        // after a wait that ran out, a bounded second wait for the MMAs
+        // before the tensor memory goes
+        if (!ok) {
+            for (int i = 0; i < kTcSpin && !bar_try_wait(bar, 0); ++i) {
+            }
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcNOut) : "memory");
+    }
+}
 
 }  // namespace
 
@@ -256,6 +484,29 @@ cudaError_t mlp_forward(const MlpDevice& net, const float* x, int batch, float* 
     }
     return gemm<false, true>(batch, net.outputs, width, in, width, net.w16[net.layers], width, logits, net.outputs,
                              net.b[net.layers], false, 1.0f, false, stream);
+}
+
+cudaError_t mlp_infer(const MlpDevice& net, const float* x, int batch, float* const* acts, float* logits,
+                      int* status, cudaStream_t stream) {
+    const int K = net.layers > 0 ? net.hidden : net.inputs;
+    if (K % 16 != 0 || K > kTcMaxK || batch <= 0)
+        return mlp_forward(net, x, batch, acts, logits, stream);  // the CUDA-core GEMM for other widths
+    const float* in = x;
+    int width = net.inputs;
+    for (int l = 0; l < net.layers; ++l) {
+        cudaError_t e = gemm<false, true>(batch, net.hidden, width, in, width, net.w16[l], width, acts[l], net.hidden,
+                                          net.b[l], true, 1.0f, false, stream);
+        if (e != cudaSuccess) return e;
+        in = acts[l];
+        width = net.hidden;
+    }
+    const int smem = (kTcM + kTcNOut) * K * 2;
+    cudaError_t e = cudaFuncSetAttribute(tc_logits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid((net.outputs + kTcNOut - 1) / kTcNOut, (batch + kTcM - 1) / kTcM);
+    tc_logits_kernel<<<grid, kTcThreadsL, smem, stream>>>(batch, net.outputs, K, in, net.w16[net.layers],
+                                                         net.b[net.layers], logits, status);
+    return cudaGetLastError();
 }
 
 cudaError_t mlp_backward(const MlpDevice& net, const float* x, int batch, float* const* acts, float* dlogits,
@@ -313,7 +564,13 @@ cudaError_t weights_to_bf16(const float* w, __nv_bfloat16* w16, size_t n, cudaSt
 
 cudaError_t logits_topk(const float* logits, int rows, int classes, int k, int* out, cudaStream_t stream) {
     if (rows <= 0) return cudaSuccess;
-    topk_kernel<<<rows, 256, 0, stream>>>(logits, classes, k, out);
+    if (k <= 0 || k > classes) return cudaErrorInvalidValue;
+    const size_t smem = static_cast<size_t>(classes) * sizeof(unsigned);
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return e;
+    topk_kernel<<<rows, kTopkThreads, smem, stream>>>(logits, classes, k, out);
     return cudaGetLastError();
 }
 

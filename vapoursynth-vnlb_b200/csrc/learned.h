@@ -38,6 +38,15 @@ cudaError_t mlp_adam(const MlpDevice& net, float* const* gw, float* const* gb, f
 
 cudaError_t weights_to_bf16(const float* w, __nv_bfloat16* w16, size_t n, cudaStream_t stream);
 
+// Inference for the shortlist: the hidden layers as mlp_forward, the output
+// layer on the tensor cores (activations rounded to BF16, BF16 weights, FP32
+// accumulation in tensor memory) when the last hidden width is a multiple of
+// 16 up to 128, else as mlp_forward.  A tensor-core wait that runs out sets
+// *status (when given) to kStatusLogitsTimeout.
+constexpr int kStatusLogitsTimeout = 5;
+cudaError_t mlp_infer(const MlpDevice& net, const float* x, int batch, float* const* acts, float* logits, int* status,
+                      cudaStream_t stream);
+
 // out[row][k]: the ids of the k largest logits of each row (ties: lower id).
 cudaError_t logits_topk(const float* logits, int rows, int classes, int k, int* out, cudaStream_t stream);
 

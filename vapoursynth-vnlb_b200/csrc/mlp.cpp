@@ -52,6 +52,7 @@ struct vnlbgpu_mlp {
     float* dacts[vnlbgpu::kMlpMaxLayers] = {};
     float* logits = nullptr;
     float* loss = nullptr;
+    int* status = nullptr;  // the inference kernels' status word
 
     int fan_in(int l) const { return l == 0 ? inputs : hidden; }
     int fan_out(int l) const { return l == layers ? outputs : hidden; }
@@ -75,6 +76,7 @@ struct vnlbgpu_mlp {
         }
         if (logits) cudaFree(logits);
         if (loss) cudaFree(loss);
+        if (status) cudaFree(status);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -169,6 +171,8 @@ int vnlbgpu_mlp_create(int inputs, int hidden, int layers, int outputs, int max_
             m->dacts[l] = vnlbgpu::device_alloc<float>(static_cast<size_t>(max_batch) * hidden, "cudaMalloc(MLP)");
         }
         m->logits = vnlbgpu::device_alloc<float>(static_cast<size_t>(max_batch) * outputs, "cudaMalloc(MLP logits)");
+        m->status = vnlbgpu::device_alloc<int>(1, "cudaMalloc(MLP status)");
+        vnlbgpu::check(cudaMemset(m->status, 0, sizeof(int)), "cudaMemset(MLP status)");
         m->loss = vnlbgpu::device_alloc<float>(static_cast<size_t>(max_batch), "cudaMalloc(MLP loss)");
         vnlbgpu::check(cudaStreamSynchronize(m->stream), "cudaStreamSynchronize(MLP)");
         *out = m.release();
@@ -276,14 +280,21 @@ int vnlbgpu_mlp_shortlist(vnlbgpu_mlp* mlp, const float* x, int batch, int k, in
         if (k <= 0 || k > mlp->outputs) throw std::invalid_argument("VNLB CUDA: shortlist size out of range");
         for (int b0 = 0; b0 < batch; b0 += mlp->max_batch) {
             const int n = std::min(mlp->max_batch, batch - b0);
-            vnlbgpu::check(vnlbgpu::mlp_forward(mlp->net, x + static_cast<size_t>(b0) * mlp->inputs, n, mlp->acts,
-                                                mlp->logits, mlp->stream),
-                           "MLP forward");
+            vnlbgpu::check(vnlbgpu::mlp_infer(mlp->net, x + static_cast<size_t>(b0) * mlp->inputs, n, mlp->acts,
+                                              mlp->logits, mlp->status, mlp->stream),
+                           "MLP inference");
             vnlbgpu::check(vnlbgpu::logits_topk(mlp->logits, n, mlp->outputs, k, out + static_cast<size_t>(b0) * k,
                                                 mlp->stream),
                            "shortlist");
         }
+        int st = 0;
+        vnlbgpu::check(cudaMemcpyAsync(&st, mlp->status, sizeof(int), cudaMemcpyDeviceToHost, mlp->stream),
+                       "cudaMemcpyAsync(status)");
         vnlbgpu::check(cudaStreamSynchronize(mlp->stream), "cudaStreamSynchronize(MLP)");
+        if (st != 0) {
+            vnlbgpu::check(cudaMemset(mlp->status, 0, sizeof(int)), "cudaMemset(status)");
+            throw std::runtime_error("VNLB CUDA: the network's tensor-core output layer timed out waiting for its MMAs");
+        }
     });
 }
 

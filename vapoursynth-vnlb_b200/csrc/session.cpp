@@ -1450,8 +1450,8 @@ struct Session {
                 acts[l] = lane.mlp_acts.ptr + static_cast<size_t>(l) * kLearnedChunk * mlp_net.hidden;
             for (int g0 = 0; g0 < G; g0 += kLearnedChunk) {
                 const int n = std::min(kLearnedChunk, G - g0);
-                check(mlp_forward(mlp_net, lane.features.ptr + static_cast<size_t>(g0) * learned_inputs, n, acts,
-                                  lane.mlp_logits.ptr, ls),
+                check(mlp_infer(mlp_net, lane.features.ptr + static_cast<size_t>(g0) * learned_inputs, n, acts,
+                                lane.mlp_logits.ptr, d_status.ptr, ls),
                       "learned network launch");
                 check(logits_topk(lane.mlp_logits.ptr, n, learned_outputs, shortlist_len,
                                   lane.shortlist.ptr + static_cast<size_t>(g0) * shortlist_len, ls),
@@ -1814,6 +1814,8 @@ struct Session {
                 fail("VNLB CUDA: the tensor-core matcher timed out waiting for its MMAs");
             if (status == kStatusTmaTimeout)
                 fail("VNLB CUDA: the matcher timed out waiting for a tensor-memory-accelerator load");
+            if (status == kStatusLogitsTimeout)
+                fail("VNLB CUDA: the network's tensor-core output layer timed out waiting for its MMAs");
             fail("VNLB CUDA: device status " + std::to_string(status));
         }
     }
