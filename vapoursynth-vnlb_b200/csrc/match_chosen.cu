@@ -286,9 +286,9 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
 //               which the issuer and the producers wait for before reusing
 //               the half.
 template <int P, int G>  // patch size (7 or 8), planes per shared-memory stage
-// 152 registers: 13 warps x 32 x 152 = 63,232 of the SM's 65,536 (one CTA
-// per SM); the producers hold their rows of a plane group in registers.
-__global__ void __maxnreg__(152) tc_distance_kernel(MatchLaunch L) {
+// 128 registers per thread: the 13 warps spread over the SM's four
+// 16,384-register partitions 4-3-3-3, and 4 warps x 32 x 128 fill one.
+__global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunch L) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -393,10 +393,12 @@ __global__ void __maxnreg__(152) tc_distance_kernel(MatchLaunch L) {
                 for (int g = 0; g < groups; ++g, ++j) {
                     const int b = j & 1;
                     const int q0 = g * G;
-                    // this warp's region rows r = warp + 8 rr of the group,
-                    // all loaded before the stage wait (one global latency
-                    // per group, overlapping the stage's previous MMAs)
-                    float rowv[kRowsPerWarp][G][3];
+                    // this warp's region rows r = warp + 8 rr of the group:
+                    // the first kPre loaded before the stage wait (their
+                    // latency overlaps the stage's previous MMAs), each later
+                    // one as soon as a register slot is free
+                    constexpr int kPre = G == 1 ? kRowsPerWarp : (G == 2 ? 4 : 3);
+                    float rowv[kPre][G][3];
                     auto load_row = [&](int r, float (&v)[G][3]) {
                         const int gy = yl + r;
                         const bool row_in = gy < L.height;
@@ -415,7 +417,7 @@ __global__ void __maxnreg__(152) tc_distance_kernel(MatchLaunch L) {
                         }
                     };
 #pragma unroll
-                    for (int rr = 0; rr < kRowsPerWarp; ++rr)
+                    for (int rr = 0; rr < kPre; ++rr)
                         if (warp + kProducerWarps * rr < Rs) load_row(warp + kProducerWarps * rr, rowv[rr]);
                     // the stage's MMAs of fill j - 2 have completed
                     wait(sfree_bar(bars, b), ((j >> 1) & 1) ^ 1);
@@ -457,7 +459,7 @@ __global__ void __maxnreg__(152) tc_distance_kernel(MatchLaunch L) {
                     for (int rr = 0; rr < kRowsPerWarp; ++rr) {
                         const int r = warp + kProducerWarps * rr;
                         if (r >= Rs) break;
-                        float (&cur)[G][3] = rowv[rr];
+                        float (&cur)[G][3] = rowv[rr % kPre];
                         float sq0 = 0.0f, sq1 = 0.0f;
 #pragma unroll
                         for (int ql = 0; ql < G; ++ql) {
@@ -486,6 +488,9 @@ __global__ void __maxnreg__(152) tc_distance_kernel(MatchLaunch L) {
                                 sq1 = fmaf(bv[jj], bv[jj], sq1);
                             }
                         }
+                        // the slot is read: the row kPre rows further takes it
+                        if (rr + kPre < kRowsPerWarp && r + kProducerWarps * kPre < Rs)
+                            load_row(r + kProducerWarps * kPre, rowv[rr % kPre]);
                         if (g == 0) {
                             rowsq[r * kChosenCols + lane] = sq0;
                             rowsq[r * kChosenCols + lane + 32] = sq1;
