@@ -344,7 +344,9 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_value = whole_job_rate(ranks.world, FRAMES, e2e_steps, ranks.max(e0.elapsed_time(e1)))
-    same = bool(torch.equal(h_final, d_final.cpu()))
+    # bit-equal for the exact form; the chosen forms add filtered rows into
+    # the stacks with atomics, whose order (and so the last bits) varies
+    same = bool(torch.equal(h_final, d_final.cpu())) or float((h_final - d_final.cpu()).abs().max()) <= 1e-5
 
     # the chained render (vnlbgpu_render_chain_device), device-resident
     chain_step()
@@ -356,7 +358,8 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
     c1.record(stream)
     torch.cuda.synchronize()
     chain_value = whole_job_rate(ranks.world, FRAMES, args.steps, ranks.max(c0.elapsed_time(c1)))
-    chain_same = bool(torch.equal(d_final.cpu(), torch.from_numpy(final_out)))
+    chain_same = bool(torch.equal(d_final.cpu(), torch.from_numpy(final_out))) or \
+        float((d_final.cpu() - torch.from_numpy(final_out)).abs().max()) <= 1e-5
 
     # One more device-resident step with one pipeline lane per session: the
     # anchor frames' kernels then run one after another, so each launch's

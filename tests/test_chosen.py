@@ -175,7 +175,9 @@ def test_tensor_core_waits_run_out_and_report():
     """The tensor-core matcher's MMA-completion waits are bounded: with its
     MMA warp told to issue nothing (a test switch; no MMA is in flight), every
     wait runs out, the kernel returns, and the render raises; the session then
-    renders normally again and equals a fresh session's output."""
+    renders normally again and equals a fresh session's output (up to the
+    order of the atomic additions of filtered rows into the stacks, which the
+    chosen forms use: 1e-5 max abs)."""
     _, noisy = synth.make_clip(96, 64, 4, 3, 20.0, seed=85)
     params = vnlbcu.parse_parameters(lib.STAGE_BASIC, noisy, 20.0, dict(CPU_DEFAULTS, form="chosen_tc", **BASIC))
     frames, planes, h, w = noisy.shape
@@ -188,4 +190,4 @@ def test_tensor_core_waits_run_out_and_report():
     again = s.render_clip()
     s.close()
     fresh = vnlbcu.Basic(noisy, sigma=20.0, form="chosen_tc", **CPU_DEFAULTS, **BASIC)
-    assert np.array_equal(again, fresh)
+    assert float(np.max(np.abs(again - fresh))) <= 1e-5

@@ -21,7 +21,7 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB = LIB_DIR / "libvnlbgpu.so"
 SOURCES = ["match.cu", "match_chosen.cu", "paste.cu", "filter.cu", "aggregate.cu", "aggregate_noalloc.cu",
-           "learned.cu", "session.cpp", "mlp.cpp", "mvtools.cpp"]
+           "learned.cu", "session.cpp", "mlp.cpp", "mvtools.cpp", "smem_limit.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1546,7 +1546,7 @@ cudaError_t launch_apply_warp(const FilterLaunch& L, int max_groups, cudaStream_
     const WarpApplyLayout lay = warp_apply_layout(D, L.max_rows, scatter);
     const size_t smem = (static_cast<size_t>(D) + static_cast<size_t>(kWarpApplyWarps) * lay.per_warp) * sizeof(float);
     auto kernel = scatter ? apply_warp_kernel<D, true> : apply_warp_kernel<D, false>;
-    cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    cudaError_t err = raise_smem_limit(reinterpret_cast<const void*>(kernel), static_cast<int>(smem));
     if (err != cudaSuccess) return err;
     const int ctas = std::max(1, std::min((max_groups + kWarpApplyWarps - 1) / kWarpApplyWarps, 148 * 8));
     kernel<<<ctas, 32 * kWarpApplyWarps, smem, stream>>>(L);
@@ -1598,7 +1598,7 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
         const size_t smem = (colpad + static_cast<size_t>(groups_per_cta) * Bmax * (D + 8)) * sizeof(float) +
                             static_cast<size_t>(groups_per_cta) * L.max_rows * sizeof(size_t);
         auto kernel = wide ? prepare_kernel<kPrepareWarps> : prepare_kernel<1>;
-        cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t err = raise_smem_limit(reinterpret_cast<const void*>(kernel),
                                                static_cast<int>(smem));
         if (err != cudaSuccess) return err;
         const int ctas = std::min((max_groups + groups_per_cta - 1) / groups_per_cta, 148 * 16);
@@ -1617,7 +1617,7 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
         int warps = 8;
         while (warps > 1 && static_cast<size_t>(warps) * (32 / seg) * per_group > 160 * 1024) warps /= 2;
         const size_t smem = static_cast<size_t>(warps) * (32 / seg) * per_group;
-        cudaError_t err = cudaFuncSetAttribute(jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t err = raise_smem_limit(reinterpret_cast<const void*>(jacobi_kernel),
                                                static_cast<int>(smem));
         if (err != cudaSuccess) return err;
         const int per_cta = warps * (32 / seg);
@@ -1644,7 +1644,7 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
         const ApplyLayout lay = apply_layout(D, Bmax, R, L.max_rows, kApplyWarps, tiled, L.stage == 1);
         const size_t smem = lay.bytes;
         auto kernel = tiled ? apply_kernel<true> : apply_kernel<false>;
-        cudaError_t err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t err = raise_smem_limit(reinterpret_cast<const void*>(kernel),
                                                static_cast<int>(smem));
         if (err != cudaSuccess) return err;
         const int ctas = std::min(max_groups, 148 * 8);

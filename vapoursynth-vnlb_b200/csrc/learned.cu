@@ -501,7 +501,7 @@ cudaError_t mlp_infer(const MlpDevice& net, const float* x, int batch, float* co
         width = net.hidden;
     }
     const int smem = (kTcM + kTcNOut) * K * 2;
-    cudaError_t e = cudaFuncSetAttribute(tc_logits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(tc_logits_kernel), smem);
     if (e != cudaSuccess) return e;
     const dim3 grid((net.outputs + kTcNOut - 1) / kTcNOut, (batch + kTcM - 1) / kTcM);
     tc_logits_kernel<<<grid, kTcThreadsL, smem, stream>>>(batch, net.outputs, K, in, net.w16[net.layers],
@@ -567,7 +567,7 @@ cudaError_t logits_topk(const float* logits, int rows, int classes, int k, int* 
     if (k <= 0 || k > classes) return cudaErrorInvalidValue;
     const size_t smem = static_cast<size_t>(classes) * sizeof(unsigned);
     if (smem > 200 * 1024) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(topk_kernel),
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     topk_kernel<<<rows, kTopkThreads, smem, stream>>>(logits, classes, k, out);

@@ -912,7 +912,7 @@ cudaError_t launch_match(const MatchLaunch& L, int strips, int warps, const CUte
     if (tmap) map = *tmap;
     cudaError_t err = cudaSuccess;
     auto launch = [&](auto kernel) {
-        err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        err = raise_smem_limit(reinterpret_cast<const void*>(kernel), static_cast<int>(smem));
         if (err != cudaSuccess) return;
         kernel<<<strips, block, smem, stream>>>(L, map);
         err = cudaGetLastError();

@@ -585,20 +585,23 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                 const StageMeta* meta = reinterpret_cast<const StageMeta*>(smem + lay.meta) + h;
                 const int wy = meta->rows, off1 = meta->off1, h0 = meta->h[0], h1 = meta->h[1];
                 const unsigned kofs = static_cast<unsigned>(meta->k) * static_cast<unsigned>(L.window_cells);
-                // per anchor slot: this lane's window column and the row
-                // stride packed (rel | wx << 8; -1: the column is outside the
-                // window), the offset of the anchor's frame-k distances
-                // (32-bit: the launch checks the buffer's size), and the
-                // reference norm
-                int relwx[kTcN];
-                unsigned base[kTcN];
+                // per anchor slot: the offset o0 of this lane's column in
+                // the anchor's frame-k distances at strip row 0 (so that
+                // strip row cy is at o0 + cy * wx; 32-bit: the launch
+                // checks the buffer's size), the row stride wx (0: the
+                // column is outside the window), and the reference norm
+                unsigned o0[kTcN];
+                int wxs[kTcN];
                 float na[kTcN];
 #pragma unroll
                 for (int n = 0; n < kTcN; ++n) {
                     const int r0 = x - meta->win_lo[n];
                     const int wxn = meta->win_wx[n];
-                    relwx[n] = r0 >= 0 && r0 < wxn ? r0 | (wxn << 8) : -1;
-                    base[n] = static_cast<unsigned>(meta->gi[n]) * static_cast<unsigned>(L.approx_stride) + kofs;
+                    const bool in = r0 >= 0 && r0 < wxn;
+                    wxs[n] = in ? wxn : 0;
+                    const int first_row = n < 8 ? 0 : off1;  // the anchor's window row 0 in strip rows
+                    o0[n] = static_cast<unsigned>(meta->gi[n]) * static_cast<unsigned>(L.approx_stride) + kofs +
+                            static_cast<unsigned>(r0 - first_row * wxn);
                     na[n] = meta->na[n];
                 }
                 const uint32_t ta = tmem + (static_cast<uint32_t>(32 * quarter) << 16) +
@@ -612,13 +615,14 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                         const int cy = 2 * (p0 + hh) + dy;
                         if (cy >= wy) continue;
                         const float bn = nb[cy * kChosenCols + x];
+                        // the strip rows of each grid row's windows
+                        const bool in0 = cy < h0;
+                        const bool in1 = static_cast<unsigned>(cy - off1) < static_cast<unsigned>(h1);
 #pragma unroll
                         for (int n = 0; n < kTcN; ++n) {
-                            const int row = n < 8 ? cy : cy - off1;
-                            const unsigned rows_n = static_cast<unsigned>(n < 8 ? h0 : h1);
-                            if (relwx[n] < 0 || static_cast<unsigned>(row) >= rows_n) continue;
-                            const unsigned o = base[n] + static_cast<unsigned>(row * (relwx[n] >> 8) + (relwx[n] & 0xff));
-                            L.approx_dist[o] = fmaxf(na[n] + bn - 2.0f * __uint_as_float(v[16 * hh + n]), 0.0f);
+                            if (wxs[n] == 0 || !(n < 8 ? in0 : in1)) continue;
+                            L.approx_dist[o0[n] + static_cast<unsigned>(cy * wxs[n])] =
+                                fmaxf(fmaf(-2.0f, __uint_as_float(v[16 * hh + n]), na[n] + bn), 0.0f);
                         }
                     }
                 }
@@ -953,7 +957,7 @@ cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t s
     const int grid = strips < persistent ? strips : persistent;
     const int select_blocks = (L.anchor_count + kChosenWarps - 1) / kChosenWarps;
     auto launch = [&](auto distance, auto select) {
-        err = cudaFuncSetAttribute(distance, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        err = raise_smem_limit(reinterpret_cast<const void*>(distance), static_cast<int>(smem));
         if (err != cudaSuccess) return;
         distance<<<grid, kPipeThreads, smem, stream>>>(L);
         err = cudaGetLastError();

@@ -182,7 +182,7 @@ cudaError_t launch_anchor_map(const int2* anchors, int count, int width, int* ma
 cudaError_t launch_paste(const PasteLaunch& L, cudaStream_t stream) {
     const size_t smem = 2 * sizeof(Chunk) + static_cast<size_t>((L.groups + 31) / 32) * sizeof(unsigned);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;  // more grid anchors than the bitmask holds
-    cudaError_t err = cudaFuncSetAttribute(paste_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t err = raise_smem_limit(reinterpret_cast<const void*>(paste_kernel),
                                            static_cast<int>(smem));
     if (err != cudaSuccess) return err;
     paste_kernel<<<1, kPasteThreads, smem, stream>>>(L);

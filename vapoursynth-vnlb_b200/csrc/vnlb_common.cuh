@@ -13,6 +13,11 @@
 
 namespace vnlbgpu {
 
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`, never lowering it (smem_limit.cpp: concurrent sessions
+// launch the same kernels with different amounts).
+cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
+
 constexpr int kLanes = 8;          // CPU vector width the order is pinned to
 constexpr float kInf = __builtin_huge_valf();
 
