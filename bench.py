@@ -536,9 +536,11 @@ def measure_frame_path(form, args, ranks, noisy, local, threads=8):
 # the Basic and Final launches; the filter class sums prepare, Jacobi and
 # apply.  None where no capture of the current kernels exists.
 TRAFFIC_PER_LAUNCH = {
-    ("cpu", "match/plain"): 57.4e6,       # match_kernel<8,0,0>: Basic 31.6 MB, Final 83.2 MB
-    ("cpu", "match/chosen_tc"): 337.1e6,  # tc_distance + tc_select: Basic 281.3 MB, Final 392.8 MB
-    ("cpu", "filter"): 494.6e6,           # prepare + jacobi + apply: Basic 403.7 MB, Final 585.5 MB
+    ("cpu", "match/plain"): 57.4e6,        # match_kernel<8,0,0>: Basic 31.8 MB, Final 83.0 MB
+    ("cpu", "match/chosen_tc"): 336.0e6,   # tc_distance + tc_select: Basic 281.5 MB, Final 390.4 MB
+    ("cpu", "filter/plain"): 492.8e6,      # prepare + jacobi + apply: Basic 402.0 MB, Final 583.6 MB
+    ("cpu", "filter/chosen"): 514.0e6,     # the same, apply adding rows into the stacks: 423.0 / 604.9 MB
+    ("cpu", "filter/chosen_tc"): 514.0e6,
 }
 TRAFFIC_SOURCE = ("ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum "
                   "--clock-control none python bench.py --profile-case --form chosen_tc (and --form plain)")
@@ -566,7 +568,7 @@ def roofline_of(r, steps, which=None):
               "timing": "CUDA events around each launch in a step with one pipeline lane per session (kernels "
                         "serialised), mean over the launches of the step",
               "serial_step_ms": serial["ms_per_step"]}
-    traffic = TRAFFIC_PER_LAUNCH.get((PARAMS, dominant if dominant == "filter" else "match/" + r["form"]))
+    traffic = TRAFFIC_PER_LAUNCH.get((PARAMS, dominant + "/" + r["form"]))
     if traffic is not None:
         common.update(traffic=traffic, traffic_unit="DRAM bytes per launch (ncu, one capture of the profile case)",
                       traffic_source=TRAFFIC_SOURCE)
@@ -884,9 +886,12 @@ def reference_cuda_stages(head):
             entry["filter"]["error"] = err
         ms, err = run([tools / "bench_aggregation", min(32, max(8, int(round(rows)))), 32, active, 20, 1, "k",
                        "spread"])
-        entry["aggregate"] = {"reference_ms": ms, "ours_ms": (ours["tiles"][0] + ours["normalize"][0]) /
-                              max(1, ours["tiles"][1]),
-                              "ours_kernels": "stack tiles + normalise"}
+        tiles_ms = ours["tiles"][0] / ours["tiles"][1] if ours["tiles"][1] else 0.0
+        entry["aggregate"] = {"reference_ms": ms,
+                              "ours_ms": tiles_ms + ours["normalize"][0] / max(1, ours["normalize"][1]),
+                              "ours_kernels": "stack tiles + normalise" if ours["tiles"][1] else
+                              "normalise (the chosen form adds the rows into the stacks inside the filter's apply "
+                              "kernel, timed with the filter)"}
         if err:
             entry["aggregate"]["error"] = err
         for k in ("match", "filter", "aggregate"):

@@ -202,9 +202,10 @@ __global__ void to_bf16_kernel(const float* w, __nv_bfloat16* w16, size_t n) {
 
 // The `k` largest logits of each row, as class ids (ties by the lower id):
 // one block per row loads the row's order-preserving keys into shared
-// memory, finds the k-th largest key by a radix select (four passes of 8
-// bits from the top, per-warp histograms), then writes the ids above it and,
-// in id order, enough of those equal to it.
+// memory and bisects on the key bits for the k-th largest, counting the keys
+// at or above the midpoint with a block reduction; it stops early when
+// exactly k keys are at or above it (continuous logits: after about 15 of
+// the 32 steps), else it resolves the ties at the k-th key in id order.
 constexpr int kTopkThreads = 256;
 constexpr int kTopkWarps = kTopkThreads / 32;
 
@@ -215,95 +216,71 @@ __device__ __forceinline__ unsigned order_key(float f) {
 
 __global__ void __launch_bounds__(kTopkThreads) topk_kernel(const float* logits, int classes, int k, int* out) {
     extern __shared__ unsigned keys[];  // [classes]
-    __shared__ int hist[kTopkWarps][256];
-    __shared__ int suffix[257];
-    __shared__ int s_pos, s_digit, s_above;
-    __shared__ int warp_ties[kTopkWarps];
+    __shared__ int warp_count[2][kTopkWarps];
+    __shared__ int s_pos;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const float* z = logits + static_cast<size_t>(blockIdx.x) * classes;
     for (int i = tid; i < classes; i += kTopkThreads) keys[i] = order_key(z[i]);
-    unsigned prefix = 0u, mask = 0u;
-    int need = k;  // keys still to take among those matching the prefix
-    for (int shift = 24; shift >= 0; shift -= 8) {
-        for (int i = lane; i < 256; i += 32) hist[warp][i] = 0;
+    __syncthreads();
+    // keys >= mid, summed over the block (double-buffered partial sums: one
+    // barrier per step)
+    int parity = 0;
+    auto count_at_least = [&](unsigned mid) {
+        int c = 0;
+        for (int i = tid; i < classes; i += kTopkThreads) c += keys[i] >= mid;
+        c = __reduce_add_sync(0xffffffffu, c);
+        if (lane == 0) warp_count[parity][warp] = c;
         __syncthreads();
-        for (int base = 0; base < classes; base += kTopkThreads) {
-            // lanes with the same digit add once, by their lowest lane
-            const int i = base + tid;
-            const unsigned key = i < classes ? keys[i] : 0u;
-            const bool in = i < classes && (key & mask) == prefix;
-            const unsigned digit = (key >> shift) & 0xffu;
-            const unsigned peers = __match_any_sync(0xffffffffu, in ? digit : 256u + lane);
-            if (in && lane == __ffs(peers) - 1) atomicAdd(&hist[warp][digit], __popc(peers));
-        }
-        __syncthreads();
-        // suffix[d] = keys (matching the prefix) whose digit is >= d
-        if (tid < 256) {
-            int c = 0;
-            for (int w = 0; w < kTopkWarps; ++w) c += hist[w][tid];
-            suffix[tid] = c;
-        }
-        if (tid == 0) suffix[256] = 0;
-        __syncthreads();
-        if (warp == 0) {
-            // suffix sums over the 256 digits, 8 per lane from the top
-            int part[8], run = 0;
+        int total = 0;
 #pragma unroll
-            for (int j = 7; j >= 0; --j) {
-                run += suffix[lane * 8 + j];
-                part[j] = run;
-            }
-            int incl = run;  // this lane's block and every block of higher digits
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_down_sync(0xffffffffu, incl, o);
-                if (lane + o < 32) incl += v;
-            }
-            const int after = incl - run;  // the blocks of higher digits
-            // the lanes above contribute `after`; write the suffix sums
-#pragma unroll
-            for (int j = 0; j < 8; ++j) suffix[lane * 8 + j] = part[j] + after;
+        for (int w = 0; w < kTopkWarps; ++w) total += warp_count[parity][w];
+        parity ^= 1;
+        return total;
+    };
+    unsigned lo = 0u, hi = 0xffffffffu;  // the k-th largest key lies in [lo, hi]
+    bool exact = false;                  // exactly k keys are >= lo
+    while (lo < hi) {
+        const unsigned mid = static_cast<unsigned>((static_cast<unsigned long long>(lo) + hi + 1ull) / 2ull);
+        const int count = count_at_least(mid);
+        if (count == k) {
+            lo = mid;
+            exact = true;
+            break;
         }
-        __syncthreads();
-        // the digit: the largest d with suffix[d] >= need (suffix[0], the
-        // keys matching the prefix, is at least need: k <= classes)
-        if (tid < 256 && suffix[tid] >= need && suffix[tid + 1] < need) {
-            s_digit = tid;
-            s_above = suffix[tid + 1];
-        }
-        __syncthreads();
-        const int d = s_digit;
-        need -= s_above;
-        prefix |= static_cast<unsigned>(d) << shift;
-        mask |= 0xffu << shift;
-        __syncthreads();
+        if (count > k) lo = mid; else hi = mid - 1u;
     }
-    const unsigned kth = prefix;  // `need` ids equal to it complete the k
     if (tid == 0) s_pos = 0;
     __syncthreads();
     int* o = out + static_cast<size_t>(blockIdx.x) * k;
+    if (exact) {
+        for (int i = tid; i < classes; i += kTopkThreads)
+            if (keys[i] >= lo) o[atomicAdd(&s_pos, 1)] = i;
+        return;
+    }
+    const unsigned kth = lo;
     for (int i = tid; i < classes; i += kTopkThreads)
         if (keys[i] > kth) o[atomicAdd(&s_pos, 1)] = i;
     __syncthreads();
     const int above = s_pos;
+    const int need = k - above;
     // the ties, in id order: chunks of 256 ids, ordered positions by ballots
     int taken = 0;
     for (int base = 0; base < classes && taken < need; base += kTopkThreads) {
         const int i = base + tid;
         const bool tie = i < classes && keys[i] == kth;
         const unsigned b = __ballot_sync(0xffffffffu, tie);
-        if (lane == 0) warp_ties[warp] = __popc(b);
+        if (lane == 0) warp_count[0][warp] = __popc(b);
         __syncthreads();
-        int before = taken;
-        for (int w = 0; w < warp; ++w) before += warp_ties[w];
+        int before = taken, total = 0;
+        for (int w = 0; w < kTopkWarps; ++w) {
+            if (w < warp) before += warp_count[0][w];
+            total += warp_count[0][w];
+        }
         const int pos = before + __popc(b & ((1u << lane) - 1u));
         if (tie && pos < need) o[above + pos] = i;
-        int total = 0;
-        for (int w = 0; w < kTopkWarps; ++w) total += warp_ties[w];
         taken += total;
         __syncthreads();
     }
-    for (int p = above + need + tid; p < k; p += kTopkThreads) o[p] = -1;  // fewer classes than k
 }
 
 int grid_for(size_t n) { return static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 16)); }

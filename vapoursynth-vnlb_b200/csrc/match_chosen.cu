@@ -314,6 +314,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
     // completion of every MMA this CTA issued, committed once before the
     // tensor memory is released
     __shared__ __align__(8) unsigned long long drain_bar;
+    __shared__ float plane_offset[kChosenMaxPlanes];  // the current strip's offset per plane (producers)
     const uint32_t drain = smem_addr(reinterpret_cast<unsigned char*>(&drain_bar));
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -363,6 +364,28 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                 has[half] = warp < strip.count[half];
                 anc[half] = has[half] ? L.anchors[strip.first[half] + warp] : make_int2(0, 0);
             }
+            // The strip's offset of each plane: the mean of its first
+            // anchor's reference patch.  Candidates and references are
+            // staged minus it (a distance does not change), so the BF16
+            // roundings scale with the samples' spread around the local level
+            // rather than with the level itself: at low noise the
+            // approximate distances are small differences of large norms.
+            producer_sync();  // the previous strip's groups are staged
+            if (warp == 0) {
+                const int first = strip.count[0] > 0 ? strip.first[0] : strip.first[1];
+                const int2 a0 = L.anchors[first];
+                for (int q = 0; q < planes_n; ++q) {
+                    const int c = q / L.Pt, tt = q % L.Pt;
+                    const float* src = anchor_frame + (static_cast<size_t>(tt) * L.channels + c) * plane_values +
+                                       static_cast<size_t>(a0.y) * L.width + a0.x;
+                    float sum = 0.0f;
+                    for (int e = lane; e < P * P; e += 32) sum += __ldg(src + static_cast<size_t>(e / P) * L.width + e % P);
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+                    if (lane == 0) plane_offset[q] = sum / static_cast<float>(P * P);
+                }
+            }
+            producer_sync();
             for (int k = 0; k < T; ++k, ++i) {
                 const int h = i & 1;
                 const int frame = L.schedule[k];
@@ -411,9 +434,12 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                             const float* src =
                                 L.video + (static_cast<size_t>(frame % L.ring + tt) * L.channels + c) * plane_values +
                                 static_cast<size_t>(row_in ? gy : 0) * L.width;
-                            v[ql][0] = in && x0 < L.width ? __ldg(src + x0) : 0.0f;
-                            v[ql][1] = in && x0 + 32 < L.width ? __ldg(src + x0 + 32) : 0.0f;
-                            v[ql][2] = in && lane < kBlock - 1 && x0 + 64 < L.width ? __ldg(src + x0 + 64) : 0.0f;
+                            // samples outside the frame (never part of a window's
+                            // patches) stay 0
+                            const float mu = q < planes_n ? plane_offset[q] : 0.0f;
+                            v[ql][0] = in && x0 < L.width ? __ldg(src + x0) - mu : 0.0f;
+                            v[ql][1] = in && x0 + 32 < L.width ? __ldg(src + x0 + 32) - mu : 0.0f;
+                            v[ql][2] = in && lane < kBlock - 1 && x0 + 64 < L.width ? __ldg(src + x0 + 64) - mu : 0.0f;
                         }
                     };
 #pragma unroll
@@ -442,8 +468,8 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                                 const float* src = anchor_frame +
                                                    (static_cast<size_t>(tt) * L.channels + c) * plane_values +
                                                    static_cast<size_t>(anc[half].y + py) * L.width + anc[half].x + px;
-                                r0 = __ldg(src);
-                                if (px + 1 < P) r1 = __ldg(src + 1);
+                                r0 = __ldg(src) - plane_offset[q];
+                                if (px + 1 < P) r1 = __ldg(src + 1) - plane_offset[q];
                             }
                             na[half] = fmaf(r0, r0, na[half]);
                             na[half] = fmaf(r1, r1, na[half]);
