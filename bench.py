@@ -1103,6 +1103,8 @@ def run_profile_case(args):
     width, height = WIDTH, HEIGHT
     if args.profile_size:
         width, height = (int(v) for v in args.profile_size.lower().split("x"))
+    if args.learned:
+        return run_learned_profile_case(width, height)
     _, noisy = synth.make_clip(width, height, 3, PLANES, SIGMA, seed=0)
     shape = np.empty((3, PLANES, height, width), np.float32)
     out = []
@@ -1124,6 +1126,31 @@ def run_profile_case(args):
         out.append(float(s.render_stack(1).sum()))
         s.close()
     print(json.dumps({"profile_case": "ok", "checksums": out}))
+    return 0
+
+
+def run_learned_profile_case(width, height):
+    """The learned form's small case for ncu (--learned --profile-case): the
+    contribution stack of anchor frame 2 of a 5-frame YUV444PS clip, Basic,
+    bm_range 16, radius 2, with an untrained network of the trained one's
+    shape and the learned rows always kept (threshold 0), then the same
+    anchor frame by the full search; the network's work does not depend on
+    its weights."""
+    import learned as LR
+    import vnlbgpu_lib as lib
+
+    kw = dict(CPU_DEFAULTS, bm_range=16, radius=2, variance_threshold=1.1)
+    _, noisy = synth.make_clip(width, height, 5, PLANES, SIGMA, seed=0)
+    inputs, outputs = LR.network_shape(lib.STAGE_BASIC, PLANES, kw, noisy, SIGMA)
+    net = lib.MLP(inputs, 128, 3, outputs, max_batch=4096, seed=3)
+    out = []
+    for form in ("learned", "plain"):
+        s = LR.session(lib.STAGE_BASIC, noisy, SIGMA, kw, form=form)
+        if form == "learned":
+            s.set_learned(net, 64, 0.0, 64)
+        out.append(float(s.render_stack(2).sum()))
+        s.close()
+    print(json.dumps({"profile_case": "ok", "form": "learned then plain", "checksums": out}))
     return 0
 
 

@@ -270,6 +270,34 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
+// The offset of each plane of each strip: the mean of the strip's first
+// anchor's reference patch, one warp per strip.  The distance kernel stages
+// candidates and references minus it (a distance does not change), so that
+// the BF16 roundings scale with the samples' spread around the local level
+// rather than with the level itself: at low noise the approximate distances
+// are small differences of large norms.
+template <int P>
+__global__ void __launch_bounds__(256) strip_offsets_kernel(MatchLaunch L) {
+    const int si = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (si >= L.strip_count) return;
+    const TcStrip st = L.tc_strips[si];
+    const int2 a = L.anchors[st.count[0] > 0 ? st.first[0] : st.first[1]];
+    const size_t plane_values = static_cast<size_t>(L.height) * L.width;
+    const float* frame = L.video + static_cast<size_t>(L.schedule[0] % L.ring) * L.channels * plane_values;
+    const int planes_n = L.search_channels * L.Pt;
+    for (int q = 0; q < planes_n; ++q) {
+        const int c = q / L.Pt, t = q % L.Pt;
+        const float* src = frame + (static_cast<size_t>(t) * L.channels + c) * plane_values +
+                           static_cast<size_t>(a.y) * L.width + a.x;
+        float sum = 0.0f;
+        for (int e = lane; e < P * P; e += 32) sum += __ldg(src + static_cast<size_t>(e / P) * L.width + e % P);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) L.strip_mu[static_cast<size_t>(si) * kChosenMaxPlanes + q] = sum / static_cast<float>(P * P);
+    }
+}
+
 // Persistent, warp-specialised distance kernel.  Each CTA walks the items
 // (strip, scheduled frame) of strips blockIdx.x, blockIdx.x + gridDim.x, ...;
 // item i takes tensor-memory half i % 2 and fills shared-memory stages with
@@ -314,7 +342,6 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
     // completion of every MMA this CTA issued, committed once before the
     // tensor memory is released
     __shared__ __align__(8) unsigned long long drain_bar;
-    __shared__ float plane_offset[kChosenMaxPlanes];  // the current strip's offset per plane (producers)
     const uint32_t drain = smem_addr(reinterpret_cast<unsigned char*>(&drain_bar));
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -364,28 +391,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                 has[half] = warp < strip.count[half];
                 anc[half] = has[half] ? L.anchors[strip.first[half] + warp] : make_int2(0, 0);
             }
-            // The strip's offset of each plane: the mean of its first
-            // anchor's reference patch.  Candidates and references are
-            // staged minus it (a distance does not change), so the BF16
-            // roundings scale with the samples' spread around the local level
-            // rather than with the level itself: at low noise the
-            // approximate distances are small differences of large norms.
-            producer_sync();  // the previous strip's groups are staged
-            if (warp == 0) {
-                const int first = strip.count[0] > 0 ? strip.first[0] : strip.first[1];
-                const int2 a0 = L.anchors[first];
-                for (int q = 0; q < planes_n; ++q) {
-                    const int c = q / L.Pt, tt = q % L.Pt;
-                    const float* src = anchor_frame + (static_cast<size_t>(tt) * L.channels + c) * plane_values +
-                                       static_cast<size_t>(a0.y) * L.width + a0.x;
-                    float sum = 0.0f;
-                    for (int e = lane; e < P * P; e += 32) sum += __ldg(src + static_cast<size_t>(e / P) * L.width + e % P);
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-                    if (lane == 0) plane_offset[q] = sum / static_cast<float>(P * P);
-                }
-            }
-            producer_sync();
+            // the strip's offset of each plane (strip_offsets_kernel):
+            // candidates and references are staged minus it
+            const float* mu = L.strip_mu + static_cast<size_t>(si) * kChosenMaxPlanes;
             for (int k = 0; k < T; ++k, ++i) {
                 const int h = i & 1;
                 const int frame = L.schedule[k];
@@ -436,10 +444,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                                 static_cast<size_t>(row_in ? gy : 0) * L.width;
                             // samples outside the frame (never part of a window's
                             // patches) stay 0
-                            const float mu = q < planes_n ? plane_offset[q] : 0.0f;
-                            v[ql][0] = in && x0 < L.width ? __ldg(src + x0) - mu : 0.0f;
-                            v[ql][1] = in && x0 + 32 < L.width ? __ldg(src + x0 + 32) - mu : 0.0f;
-                            v[ql][2] = in && lane < kBlock - 1 && x0 + 64 < L.width ? __ldg(src + x0 + 64) - mu : 0.0f;
+                            const float m = in ? __ldg(mu + q) : 0.0f;
+                            v[ql][0] = in && x0 < L.width ? __ldg(src + x0) - m : 0.0f;
+                            v[ql][1] = in && x0 + 32 < L.width ? __ldg(src + x0 + 32) - m : 0.0f;
+                            v[ql][2] = in && lane < kBlock - 1 && x0 + 64 < L.width ? __ldg(src + x0 + 64) - m : 0.0f;
                         }
                     };
 #pragma unroll
@@ -468,8 +476,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                                 const float* src = anchor_frame +
                                                    (static_cast<size_t>(tt) * L.channels + c) * plane_values +
                                                    static_cast<size_t>(anc[half].y + py) * L.width + anc[half].x + px;
-                                r0 = __ldg(src) - plane_offset[q];
-                                if (px + 1 < P) r1 = __ldg(src + 1) - plane_offset[q];
+                                const float m = __ldg(mu + q);
+                                r0 = __ldg(src) - m;
+                                if (px + 1 < P) r1 = __ldg(src + 1) - m;
                             }
                             na[half] = fmaf(r0, r0, na[half]);
                             na[half] = fmaf(r1, r1, na[half]);
@@ -962,7 +971,7 @@ cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t s
     const long long candidates = static_cast<long long>(L.window_cells) * L.schedule_len;
     const int cap = L.soft_cap < candidates ? L.soft_cap : static_cast<int>(candidates);
     if (!chosen_match_supported(L.P, planes_n, kChosenCols, L.window_rows) || !L.status || !L.approx_dist ||
-        !L.tc_strips ||
+        !L.tc_strips || !L.strip_mu ||
         L.approx_stride < L.schedule_len * L.window_cells || L.strip_count != strips || L.K > 32 ||
         static_cast<unsigned long long>(L.anchor_count) * static_cast<unsigned long long>(L.approx_stride) >
             0xffffffffull ||
@@ -984,6 +993,10 @@ cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t s
     const int select_blocks = (L.anchor_count + kChosenWarps - 1) / kChosenWarps;
     auto launch = [&](auto distance, auto select) {
         err = raise_smem_limit(reinterpret_cast<const void*>(distance), static_cast<int>(smem));
+        if (err != cudaSuccess) return;
+        if (L.P == 8) strip_offsets_kernel<8><<<(strips + 7) / 8, 256, 0, stream>>>(L);
+        else strip_offsets_kernel<7><<<(strips + 7) / 8, 256, 0, stream>>>(L);
+        err = cudaGetLastError();
         if (err != cudaSuccess) return;
         distance<<<grid, kPipeThreads, smem, stream>>>(L);
         err = cudaGetLastError();

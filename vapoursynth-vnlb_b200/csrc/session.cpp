@@ -381,6 +381,7 @@ struct Session {
         DeviceArray<FrameCounters> counters;
         DeviceArray<float> filtered, weights, gmeans, gram, eig, dual, logw;
         DeviceArray<float> approx;  // tensor-core form: approximate distances [G][approx_stride]
+        DeviceArray<float> tc_mu;   // tensor-core matcher: per-strip plane offsets [strips][kChosenMaxPlanes]
         // learned form
         DeviceArray<float> features, cells, mlp_acts, mlp_logits;
         DeviceArray<int> shortlist, check_counts, check_vcounts, check_victims, tile_fail;
@@ -761,7 +762,7 @@ struct Session {
         // bytes of one lane's buffers, as allocated below
         const size_t lane_bytes =
             G * max_rows * sizeof(MatchRow) + G * (6 * sizeof(int) + sizeof(int2) + victim_stride * sizeof(int)) +
-            (chosen ? G * static_cast<size_t>(approx_stride) * sizeof(float) : 0) +
+            (chosen ? G * (static_cast<size_t>(approx_stride) + kChosenMaxPlanes) * sizeof(float) : 0) +
             R * (static_cast<size_t>(row_dim) + 1 + (models > 1 ? models : 0)) * sizeof(float) +
             R * (sizeof(MatchRow) + sizeof(int)) +
             M * (2 * static_cast<size_t>(dim) + N * N + rank1 + rank1 * N) * sizeof(float) + M * sizeof(int);
@@ -780,7 +781,10 @@ struct Session {
             l.row_offset.allocate(G + 1, "cudaMalloc(row offsets)");
             l.active_prefix.allocate(G + 1, "cudaMalloc(active prefix)");
             l.counters.allocate(1, "cudaMalloc(counters)");
-            if (chosen) l.approx.allocate(G * approx_stride, "cudaMalloc(approximate distances)");
+            if (chosen) {
+                l.approx.allocate(G * approx_stride, "cudaMalloc(approximate distances)");
+                l.tc_mu.allocate(G * kChosenMaxPlanes, "cudaMalloc(strip offsets)");  // a strip has an anchor
+            }
             l.filtered.allocate(R * row_dim, "cudaMalloc(filtered rows)");
             l.gmeans.allocate(M * 2 * dim, "cudaMalloc(group means)");
             l.gram.allocate(M * N * N, "cudaMalloc(group Gram)");
@@ -1480,6 +1484,7 @@ struct Session {
             stats.kernel_launches += 6 + 2 * ((G + kLearnedChunk - 1) / kLearnedChunk) * (mlp_net.layers + 1);
         } else if (chosen) {
             m.tc_strips = grid.d_strips_chosen.ptr;
+            m.strip_mu = lane.tc_mu.ptr;
             m.tiles_x = chosen_tiles_x;
             m.approx_dist = lane.approx.ptr;
             m.approx_stride = approx_stride;

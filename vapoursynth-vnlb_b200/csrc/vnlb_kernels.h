@@ -60,6 +60,7 @@ struct MatchLaunch {
     const int2* anchors;  // grid anchors in raster order
     const Strip* strips;
     const TcStrip* tc_strips;  // tensor-core matcher strips
+    float* strip_mu;           // [strips][kChosenMaxPlanes] their per-plane offsets (tensor-core matcher)
     const int* anchor_map;  // [H][W] anchor index or -1
     int region_rows;      // shared rows per plane (incl. padding)
     int region_stride;    // shared row stride in floats
