@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                     // the first kPre loaded before the stage wait (their
                     // latency overlaps the stage's previous MMAs), each later
                     // one as soon as a register slot is free
-                    constexpr int kPre = G == 1 ? kRowsPerWarp : (G == 2 ? 4 : 3);
+                    constexpr int kPre = G == 1 ? kRowsPerWarp : 3;
                     float rowv[kPre][G][3];
                     auto load_row = [&](int r, float (&v)[G][3]) {
                         const int gy = yl + r;
@@ -442,17 +442,21 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                             const float* src =
                                 L.video + (static_cast<size_t>(frame % L.ring + tt) * L.channels + c) * plane_values +
                                 static_cast<size_t>(row_in ? gy : 0) * L.width;
-                            // samples outside the frame (never part of a window's
-                            // patches) stay 0
-                            const float m = in ? __ldg(mu + q) : 0.0f;
-                            v[ql][0] = in && x0 < L.width ? __ldg(src + x0) - m : 0.0f;
-                            v[ql][1] = in && x0 + 32 < L.width ? __ldg(src + x0 + 32) - m : 0.0f;
-                            v[ql][2] = in && lane < kBlock - 1 && x0 + 64 < L.width ? __ldg(src + x0 + 64) - m : 0.0f;
+                            // the loads only: their results are used (and the
+                            // offset taken off) when the row is staged
+                            v[ql][0] = in && x0 < L.width ? __ldg(src + x0) : 0.0f;
+                            v[ql][1] = in && x0 + 32 < L.width ? __ldg(src + x0 + 32) : 0.0f;
+                            v[ql][2] = in && lane < kBlock - 1 && x0 + 64 < L.width ? __ldg(src + x0 + 64) : 0.0f;
                         }
                     };
 #pragma unroll
                     for (int rr = 0; rr < kPre; ++rr)
                         if (warp + kProducerWarps * rr < Rs) load_row(warp + kProducerWarps * rr, rowv[rr]);
+                    // the group's plane offsets (samples outside the frame, never
+                    // part of a window's patches, become -offset: unused)
+                    float mq[G];
+#pragma unroll
+                    for (int ql = 0; ql < G; ++ql) mq[ql] = q0 + ql < planes_n ? __ldg(mu + q0 + ql) : 0.0f;
                     // the stage's MMAs of fill j - 2 have completed
                     wait(sfree_bar(bars, b), ((j >> 1) & 1) ^ 1);
                     unsigned char* st = smem + b * lay.stage_bytes;
@@ -495,6 +499,10 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                         const int r = warp + kProducerWarps * rr;
                         if (r >= Rs) break;
                         float (&cur)[G][3] = rowv[rr % kPre];
+#pragma unroll
+                        for (int ql = 0; ql < G; ++ql)
+#pragma unroll
+                            for (int e = 0; e < 3; ++e) cur[ql][e] -= mq[ql];
                         float sq0 = 0.0f, sq1 = 0.0f;
 #pragma unroll
                         for (int ql = 0; ql < G; ++ql) {
