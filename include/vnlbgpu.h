@@ -268,6 +268,20 @@ int vnlbgpu_shard_plan(int frames, int world, int rank, int basic_search_bwd, in
 
 int vnlbgpu_get_stats(vnlbgpu_session* session, vnlbgpu_stats* stats);
 
+/* Tile-shape autotuner (no reference counterpart).  On anchor frame `anchor`
+ * (its sources given), times the session's own kernels for each shape that
+ * fits and keeps the fastest for the session's later calls: the plain
+ * matcher's strip width (8, 4 or 2 anchors per CTA), the tensor-core
+ * matcher's planes per shared-memory stage (the chosen_tc form), and the
+ * warp-per-group against the row-tiled apply kernel where both fit.  The
+ * plain form's choices compute the same bits; the tensor-core plane grouping
+ * can move the approximate distances' last bits.  match_warps and
+ * apply_rows (either may be NULL) receive the plain matcher's and the
+ * apply's choices; log (log_size bytes, may be NULL) one "shape: ms" line per
+ * timing.  The learned form is not autotuned. */
+int vnlbgpu_autotune(vnlbgpu_session* session, int anchor, int* match_warps, int* apply_rows, char* log,
+                     size_t log_size);
+
 /* Learned block-match proposals (no reference counterpart): a multilayer
  * perceptron trained and run by this library's own CUDA kernels.
  *

@@ -964,10 +964,17 @@ bool chosen_match_supported(int P, int planes_n, int window_w, int window_h) {
            window_h <= kChosenMaxRows;
 }
 
+int chosen_max_plane_group(int planes_n, int window_rows) { return plane_group(planes_n, (window_rows + 1) / 2); }
+
+// planes per stage of a launch: the requested number when it fits, else the most that fit
+static int launch_plane_group(const MatchLaunch& L) {
+    const int most = chosen_max_plane_group(L.search_channels * L.Pt, L.window_rows);
+    return L.plane_group > 0 && L.plane_group < most ? L.plane_group : most;
+}
+
 size_t chosen_match_shared_bytes(const MatchLaunch& L) {
-    const int planes_n = L.search_channels * L.Pt;
     const int pairs = (L.window_rows + 1) / 2;
-    const PipeLayout lay = pipe_layout(plane_group(planes_n, pairs), pairs);
+    const PipeLayout lay = pipe_layout(launch_plane_group(L), pairs);
     return static_cast<size_t>(lay.bytes > kMinSharedBytes ? lay.bytes : kMinSharedBytes);
 }
 
@@ -990,8 +997,7 @@ cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t s
     if (err != cudaSuccess) return err;
     err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (err != cudaSuccess) return err;
-    const int pairs = (L.window_rows + 1) / 2;
-    const int group = plane_group(planes_n, pairs);
+    const int group = launch_plane_group(L);
     const size_t smem = chosen_match_shared_bytes(L);
     if (smem > static_cast<size_t>(kSharedLimit)) return cudaErrorInvalidValue;
     // a quarter of the SMs stays free for the other pipeline lane's kernels

@@ -137,6 +137,7 @@ struct Session {
     bool approx = false;
     bool chosen = false;
     int chosen_tiles_x = 0, chosen_wy = 0, approx_stride = 0;
+    int tc_group = 0;  // tensor-core matcher: planes per shared-memory stage (0: the most that fit; autotuned)
     bool coupled = true;
     int models = 1;   // filter models per group
     bool covariance_possible = false;  // some group takes the dim x dim covariance model
@@ -1485,6 +1486,7 @@ struct Session {
         } else if (chosen) {
             m.tc_strips = grid.d_strips_chosen.ptr;
             m.strip_mu = lane.tc_mu.ptr;
+            m.plane_group = tc_group;
             m.tiles_x = chosen_tiles_x;
             m.approx_dist = lane.approx.ptr;
             m.approx_stride = approx_stride;
@@ -1784,6 +1786,23 @@ struct Session {
             match_width_fits(warps);
             set_flow_region();
             grids.clear();
+        }
+        if (chosen && !flow_on()) {
+            // the tensor-core matcher's planes per shared-memory stage: fewer
+            // planes take more stages per frame but fewer registers per row
+            const int most = chosen_max_plane_group(search_channels * Pt, chosen_wy);
+            int best_g = most;
+            double best_t = 1e30;
+            for (int g = most; g >= 1 && most > 1; --g) {
+                tc_group = g;
+                const double t = time_class(anchor, kTimedMatch);
+                log.emplace_back("tensor-core planes per stage " + std::to_string(g), t);
+                if (t < best_t) {
+                    best_t = t;
+                    best_g = g;
+                }
+            }
+            tc_group = best_g;
         }
         FilterLaunch probe{};
         probe.dim = dim;

@@ -61,6 +61,7 @@ struct MatchLaunch {
     const Strip* strips;
     const TcStrip* tc_strips;  // tensor-core matcher strips
     float* strip_mu;           // [strips][kChosenMaxPlanes] their per-plane offsets (tensor-core matcher)
+    int plane_group;           // tensor-core matcher: planes per shared-memory stage (0: the most that fit)
     const int* anchor_map;  // [H][W] anchor index or -1
     int region_rows;      // shared rows per plane (incl. padding)
     int region_stride;    // shared row stride in floats
@@ -121,6 +122,8 @@ constexpr int kChosenMaxBuffer = 96;
 
 bool chosen_match_supported(int P, int planes_n, int window_w, int window_h);
 size_t chosen_match_shared_bytes(const MatchLaunch& L);
+// the most planes per shared-memory stage of the tensor-core matcher
+int chosen_max_plane_group(int planes_n, int window_rows);
 cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t stream);
 
 // One direction of MVTools motion vectors on the device (mvfw or mvbw).
