@@ -207,7 +207,7 @@ def run_reference(args):
             "config": workload_config("reference CPU core"),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    print(json.dumps(line, default=json_scalar), flush=True)
     return 0
 
 
@@ -364,7 +364,7 @@ def measure_form(form, args, ranks, stream, noisy, clean, d_noisy, local):
     # sequential one's within 1e-3 dB
     chained = d_final.cpu().numpy()
     chain_same = bool(np.array_equal(chained, final_out)) if form == "plain" else \
-        abs(synth.psnr(chained, clean) - synth.psnr(final_out, clean)) <= 1e-3
+        bool(abs(synth.psnr(chained, clean) - synth.psnr(final_out, clean)) <= 1e-3)
 
     # One more device-resident step with one pipeline lane per session: the
     # anchor frames' kernels then run one after another, so each launch's
@@ -615,6 +615,13 @@ def roofline_of(r, steps, which=None):
                 peak_source="nominal FP32 FMA rate x 2 (MEASURED_PEAKS.json has no FP32 figure)",
                 work="Gram B(B+1)D + basis 2rBD per active group, projection and reconstruction 5rD per "
                      "retained row, per call")
+
+
+def json_scalar(o):
+    """numpy scalars (a comparison's bool, a PSNR) in the JSON line as Python values."""
+    if isinstance(o, np.generic):
+        return o.item()
+    raise TypeError(f"{type(o).__name__} is not JSON serializable")
 
 
 def measured_peak(key: str, fallback: float) -> float:
@@ -1008,7 +1015,7 @@ def run_ours(args):
                 "data": "synthetic", "config": config, "roofline": roofline, "cpu_baseline": cpu_baseline,
                 "e2e": e2e,
                 "gpu_launches": head["stats"]["kernel_launches"], "clocks": clocks.summary()}
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, default=json_scalar), flush=True)
     ranks.close()
     return 0
 
@@ -1094,7 +1101,7 @@ def run_learned(args):
            "learned_threshold_0": render("learned", 0.0),
            "held_out_recall_at_64": {"basic": hold[lib.STAGE_BASIC], "final": hold[lib.STAGE_FINAL]},
            "training": {"basic": train_info[lib.STAGE_BASIC], "final": train_info[lib.STAGE_FINAL]}}
-    print(json.dumps(out), flush=True)
+    print(json.dumps(out, default=json_scalar), flush=True)
     return 0
 
 
