@@ -118,6 +118,26 @@ def test_learned_form_on_a_33x33x5_window():
         print(f"threshold {threshold}: tiles {st['learned_tiles']}, learned rows kept in {kept:.1%}; "
               f"PSNR {synth.psnr(out, clean):.4f} dB (plain {synth.psnr(plain, clean):.4f})")
         assert np.isfinite(out).all()
+    # a shortlisted candidate gets the full search's distance bits: the rows
+    # both matchers keep have equal distances
+    s = LR.session(lib.STAGE_BASIC, noisy, sigma, kw, form="learned")
+    s.set_learned(net, shortlist=64, recall_threshold=0.0, tile=64)
+    learned_rows = s.diag_anchor(2)
+    s.close()
+    s = LR.session(lib.STAGE_BASIC, noisy, sigma, kw)
+    plain_rows = s.diag_anchor(2)
+    s.close()
+    place = lambda r: (int(r["x"]), int(r["y"]), int(r["frame"]))
+    common = 0
+    for gi in range(len(plain_rows["counts"])):
+        a = plain_rows["grid_rows"][gi][: plain_rows["counts"][gi]]
+        b = learned_rows["grid_rows"][gi][: learned_rows["counts"][gi]]
+        ka = {place(x): np.float32(x["distance"]).view(np.uint32) for x in a}
+        kb = {place(x): np.float32(x["distance"]).view(np.uint32) for x in b}
+        for pos in set(ka) & set(kb):
+            assert ka[pos] == kb[pos], (gi, pos)
+            common += 1
+    assert common > len(plain_rows["counts"])  # more than the anchors themselves
     full, st = results[1.5]
     assert st["learned_fallback_tiles"] == st["learned_tiles"] > 0
     assert np.array_equal(full.view(np.uint32), plain.view(np.uint32))

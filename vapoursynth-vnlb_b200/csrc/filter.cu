@@ -1105,38 +1105,13 @@ __device__ __forceinline__ float octet_reduce(float v) {
 #define VNLB_APPLY_MIN_BLOCKS 4
 #endif
 
-// Vector reductions (sm_90+): each element is added atomically on its own.
-__device__ __forceinline__ void red_add_v4(float* p, float a, float b, float c, float d) {
-    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
-}
-__device__ __forceinline__ void red_add_v2(float* p, float a, float b) {
-    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
-}
-
-// Adds each lane's value at its pixel; with 8 x 8 patches the lanes of an
-// octet hold one patch row's 8 consecutive pixels (px = lane % 8), so when
-// the row starts on a 16-byte (8-byte) boundary every fourth (second) lane
-// adds its neighbours' values with it in one vector reduction: `mode` 4 or
-// 2; 1 adds one value per lane.  The warp is converged (the shuffles).
-__device__ __forceinline__ void add_pixels(float* dst, float v, int mode, int lane) {
-    const float v1 = __shfl_down_sync(0xffffffffu, v, 1);
-    const float v2 = __shfl_down_sync(0xffffffffu, v, 2);
-    const float v3 = __shfl_down_sync(0xffffffffu, v, 3);
-    if (mode == 4) {
-        if ((lane & 3) == 0) red_add_v4(dst, v, v1, v2, v3);
-    } else if (mode == 2) {
-        if ((lane & 1) == 0) red_add_v2(dst, v, v1);
-    } else {
-        atomicAdd(dst, v);
-    }
-}
-
 // Chosen forms: a lane's columns of one filtered row added into the anchor
 // frame's stack, weight cw times the window at each pixel; the weight plane
 // gets the same once per pixel (the columns of plane 0).  Slots outside the
 // window are dropped, as the stack tiles drop them.  The additions' order is
 // not fixed, so these forms are not bit-reproducible in the stacks' last
-// bits.
+// bits.  (Vector reductions of an octet's patch row, tried, were slower:
+// the shuffles that gather a row cost more than the reductions they save.)
 template <int kCols>
 __device__ __forceinline__ void scatter_row(const FilterLaunch& L, const MatchRow& m, const float (&o)[kCols],
                                             float cw, int lane) {
@@ -1145,14 +1120,9 @@ __device__ __forceinline__ void scatter_row(const FilterLaunch& L, const MatchRo
     const int P = L.P;
     const size_t base = static_cast<size_t>(m.y) * L.width + m.x;
     const int slot0 = m.frame + L.search_bwd - L.anchor_frame;
-    // vector reductions need 8 x 8 patches (an octet per patch row), rows and
-    // planes on the boundary (width a multiple of 4 or 2) and the row's start
-    const int mode = P != 8 ? 1 : ((L.width & 3) == 0 && (m.x & 3) == 0) ? 4
-                              : ((L.width & 1) == 0 && (m.x & 1) == 0) ? 2 : 1;
 #pragma unroll
     for (int jj = 0; jj < kCols; ++jj) {
-        // column (plane c, layer t, py, px); with 8 x 8 patches c and t are
-        // the same for the 32 lanes
+        // column (plane c, layer t, py, px)
         const int col = lane + 32 * jj;
         const int c = col / L.patch_dim;
         const int pos = col - c * L.patch_dim;
@@ -1160,18 +1130,11 @@ __device__ __forceinline__ void scatter_row(const FilterLaunch& L, const MatchRo
         const int rem = pos - t * P * P;
         const int py = rem / P;
         const int slot = slot0 + t;
-        const bool in = slot >= 0 && slot < L.slots;
-        if (mode > 1 ? !__any_sync(0xffffffffu, in) : !in) continue;
+        if (slot < 0 || slot >= L.slots) continue;
         const float w = L.windowed ? cw * __ldg(L.window + rem) : cw;
         const size_t at = base + static_cast<size_t>(py) * L.width + (rem - py * P);
-        float* stack = L.scatter + static_cast<size_t>(in ? slot : 0) * (C + 1) * plane;
-        if (mode > 1) {
-            add_pixels(stack + static_cast<size_t>(c) * plane + at, w * o[jj], mode, lane);
-            if (__any_sync(0xffffffffu, c == 0)) add_pixels(stack + static_cast<size_t>(C) * plane + at, w, mode, lane);
-        } else {
-            atomicAdd(stack + static_cast<size_t>(c) * plane + at, w * o[jj]);
-            if (c == 0) atomicAdd(stack + static_cast<size_t>(C) * plane + at, w);
-        }
+        atomicAdd(L.scatter + (static_cast<size_t>(slot) * (C + 1) + c) * plane + at, w * o[jj]);
+        if (c == 0) atomicAdd(L.scatter + (static_cast<size_t>(slot) * (C + 1) + C) * plane + at, w);
     }
 }
 

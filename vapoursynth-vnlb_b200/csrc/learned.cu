@@ -611,9 +611,10 @@ __global__ void features_kernel(LearnedLaunch L) {
     }
 }
 
-// One warp per anchor: the exact SSD (sub, mul, add per sample, the search
-// channels of the patch_time frames) of every shortlisted candidate and of
-// the anchor itself, then the plain matcher's selection on them: the K
+// One warp per anchor: the exact SSD (for 8 x 8 patches in the plain
+// matcher's arithmetic, so a shortlisted candidate gets the full search's
+// distance bits) of every shortlisted candidate and of the anchor itself,
+// then the plain matcher's selection on them: the K
 // nearest by (distance, candidate order), threshold max(tau, d_K), at most
 // soft_cap rows, nearest first; then the paste-mask victims.
 __global__ void learned_match_kernel(LearnedLaunch L) {
@@ -631,14 +632,19 @@ __global__ void learned_match_kernel(LearnedLaunch L) {
     const size_t hw = static_cast<size_t>(L.height) * L.width;
     const float* ref = L.video + static_cast<size_t>(L.anchor_frame % L.ring) * L.channels * hw +
                        static_cast<size_t>(a.y) * L.width + a.x;
+    __shared__ long long s_off[8][kShortlistMax + 1];  // candidate patch offsets in L.video (-1: none)
+    __shared__ float s_dist[8][kShortlistMax + 1];
+    const int wib = threadIdx.x >> 5;  // warp in block (blocks of 8 warps)
     float d[kPer];
     int id[kPer];
     const int n = L.shortlist_len + 1;
+    // each lane's candidates: offset and the full search's candidate order
     for (int j = 0; j < kPer; ++j) {
         const int q = lane + 32 * j;
         d[j] = kInf;
         id[j] = 0x7fffffff;
         if (q >= n) continue;
+        s_off[wib][q] = -1;
         int k, wx, wy;
         if (q == L.shortlist_len) {  // the anchor itself
             k = 0;
@@ -652,21 +658,68 @@ __global__ void learned_match_kernel(LearnedLaunch L) {
             wx = cls % W;
             if (k >= L.schedule_len || wx >= Wx || wy >= Wy) continue;
         }
-        const float* cand = L.video + static_cast<size_t>(L.schedule[k] % L.ring) * L.channels * hw +
-                            static_cast<size_t>(yl + wy) * L.width + xl + wx;
-        float s = 0.0f;
-        for (int c = 0; c < L.search_channels; ++c)
-            for (int t = 0; t < L.Pt; ++t) {
-                const size_t off = (static_cast<size_t>(t) * L.channels + c) * hw;
-                for (int py = 0; py < P; ++py)
-                    for (int px = 0; px < P; ++px) {
-                        const size_t o = off + static_cast<size_t>(py) * L.width + px;
-                        const float diff = __fsub_rn(__ldg(ref + o), __ldg(cand + o));
-                        s = __fadd_rn(s, __fmul_rn(diff, diff));
+        s_off[wib][q] = static_cast<long long>(static_cast<size_t>(L.schedule[k] % L.ring) * L.channels * hw +
+                                               static_cast<size_t>(yl + wy) * L.width + xl + wx);
+        id[j] = k * cells + wy * Wx + wx;
+    }
+    __syncwarp();
+    if (P == 8) {
+        // Exact SSD in the plain matcher's arithmetic (row_ssd8: each patch
+        // row's 8 squared differences folded ((0+4)+(2+6))+((1+5)+(3+7)),
+        // the rows added in order, planes (channel, t) in order): four
+        // candidates a pass, an octet of lanes per candidate, lane r of the
+        // octet folding patch row r, then the rows added in order.
+        const int oct = lane >> 3, r = lane & 7;
+        for (int base = 0; base < n; base += 4) {
+            const int q = base + oct;
+            const long long off = q < n ? s_off[wib][q] : -1;
+            float dsum = 0.0f;
+            for (int c = 0; c < L.search_channels; ++c)
+                for (int t = 0; t < L.Pt; ++t) {
+                    const size_t po = (static_cast<size_t>(t) * L.channels + c) * hw + static_cast<size_t>(r) * L.width;
+                    float part = 0.0f;
+                    if (off >= 0) {
+                        const float* rr = ref + po;
+                        const float* cr = L.video + static_cast<size_t>(off) + po;
+                        float sq[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const float df = __fsub_rn(__ldg(rr + i), __ldg(cr + i));
+                            sq[i] = __fmul_rn(df, df);
+                        }
+                        part = __fadd_rn(__fadd_rn(__fadd_rn(sq[0], sq[4]), __fadd_rn(sq[2], sq[6])),
+                                         __fadd_rn(__fadd_rn(sq[1], sq[5]), __fadd_rn(sq[3], sq[7])));
                     }
-            }
-        d[j] = isfinite(s) ? s : kInf;
-        id[j] = k * cells + wy * Wx + wx;  // the full search's candidate order
+#pragma unroll
+                    for (int row = 0; row < 8; ++row)
+                        dsum = __fadd_rn(dsum, __shfl_sync(0xffffffffu, part, (oct << 3) + row));
+                }
+            if (r == 0 && off >= 0) s_dist[wib][q] = isfinite(dsum) ? dsum : kInf;
+        }
+        __syncwarp();
+        for (int j = 0; j < kPer; ++j) {
+            const int q = lane + 32 * j;
+            if (q < n && id[j] != 0x7fffffff) d[j] = s_dist[wib][q];
+        }
+    } else {
+        // other patch sizes: one lane per candidate, the samples in order
+        for (int j = 0; j < kPer; ++j) {
+            const int q = lane + 32 * j;
+            if (q >= n || id[j] == 0x7fffffff) continue;
+            const float* cand = L.video + static_cast<size_t>(s_off[wib][q]);
+            float sum = 0.0f;
+            for (int c = 0; c < L.search_channels; ++c)
+                for (int t = 0; t < L.Pt; ++t) {
+                    const size_t off = (static_cast<size_t>(t) * L.channels + c) * hw;
+                    for (int py = 0; py < P; ++py)
+                        for (int px = 0; px < P; ++px) {
+                            const size_t o = off + static_cast<size_t>(py) * L.width + px;
+                            const float diff = __fsub_rn(__ldg(ref + o), __ldg(cand + o));
+                            sum = __fadd_rn(sum, __fmul_rn(diff, diff));
+                        }
+                }
+            d[j] = isfinite(sum) ? sum : kInf;
+        }
     }
     // duplicates (the anchor may also be shortlisted): keep the first copy
     for (int j = 0; j < kPer; ++j) {
