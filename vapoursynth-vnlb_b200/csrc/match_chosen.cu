@@ -799,13 +799,25 @@ __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
 
     for (int k = 0; k < L.schedule_len; ++k) {
         // the CPU's sequential selection over frame k (raster order) on the
-        // approximate distances: the K-smallest front and the capped buffer
+        // approximate distances: the K-smallest front and the capped buffer;
+        // kSelectBatch chunks of 32 candidates are loaded at once (the
+        // replay of a chunk is short next to a load's latency; fewer for the
+        // larger buffers, whose registers would spill)
+        constexpr int kSelectBatch = CW == 1 ? 8 : 4;
         const float* dk = approx + k * L.window_cells;
-        float next = lane < cells ? __ldg(dk + lane) : kInf;
-        for (int base = 0; base < cells; base += 32) {
+        for (int base0 = 0; base0 < cells; base0 += 32 * kSelectBatch) {
+          float vals[kSelectBatch];
+#pragma unroll
+          for (int b = 0; b < kSelectBatch; ++b) {
+              const int idx = base0 + 32 * b + lane;
+              vals[b] = idx < cells ? __ldg(dk + idx) : kInf;
+          }
+#pragma unroll
+          for (int b = 0; b < kSelectBatch; ++b) {
+            const int base = base0 + 32 * b;
+            if (base >= cells) break;  // uniform
             const int idx = base + lane;
-            const float mine = next;
-            next = idx + 32 < cells ? __ldg(dk + idx + 32) : kInf;  // the next chunk in flight
+            const float mine = vals[b];
             float limit = s.top_count >= K ? std_max(L.tau, s.top_front) : kInf;
             if (s.count >= s.cap) limit = std_min(limit, s.worst);
             unsigned pass = __ballot_sync(0xffffffffu, idx < cells && mine <= limit);
@@ -836,6 +848,7 @@ __global__ void __launch_bounds__(kTcThreads) tc_select_kernel(MatchLaunch L) {
                     s.top_front = __uint_as_float(__reduce_max_sync(0xffffffffu, reg_top));
                 }
             }
+          }
         }
     }
     // exact FP32 distance of every entry left in the buffer, in the plain
