@@ -191,3 +191,59 @@ def test_tensor_core_waits_run_out_and_report():
     s.close()
     fresh = vnlbcu.Basic(noisy, sigma=20.0, form="chosen_tc", **CPU_DEFAULTS, **BASIC)
     assert float(np.max(np.abs(again - fresh))) <= 1e-5
+
+
+def test_tensor_core_buffers_of_96():
+    """group_size 24 with cap factor 4: buffers of 96 entries, three slots per
+    lane in the selection replay (the mixed stream's sigma-5 setting); rank
+    24, patch_time 2 on a gray clip (two planes).  Rows agree with the plain
+    form's on most groups with its exact distance bits, and the output is
+    within 0.05 dB of the plain form's."""
+    clean, noisy = synth.make_clip(128, 96, 6, 1, 5.0, seed=88)
+    kw = dict(block_size=8, block_step=8, group_size=24, bm_range=9, radius=1, patch_time=2, rank=24,
+              cap_factor=4.0, tau=200.0)
+    frames, planes, h, w = noisy.shape
+    rows = {}
+    for form in ("plain", "chosen_tc"):
+        params = vnlbcu.parse_parameters(lib.STAGE_BASIC, noisy, 5.0, dict(kw, form=form))
+        s = lib.Session(params, w, h, frames, planes)
+        s.set_clip(lib.SOURCE_CLIP, noisy)
+        rows[form] = s.diag_anchor(2)
+        s.close()
+    assert rows["plain"]["max_rows"] == 96
+    place = lambda r: (int(r["x"]), int(r["y"]), int(r["frame"]))
+    same = 0
+    groups = len(rows["plain"]["counts"])
+    for gi in range(groups):
+        a = rows["plain"]["grid_rows"][gi][: rows["plain"]["counts"][gi]]
+        b = rows["chosen_tc"]["grid_rows"][gi][: rows["chosen_tc"]["counts"][gi]]
+        ka = {place(x): np.float32(x["distance"]).view(np.uint32) for x in a}
+        kb = {place(x): np.float32(x["distance"]).view(np.uint32) for x in b}
+        for pos in set(ka) & set(kb):
+            assert ka[pos] == kb[pos]
+        same += set(ka) == set(kb)
+    assert same / groups >= 0.8, (same, groups)
+    plain = vnlbcu.Basic(noisy, sigma=5.0, **kw)
+    tc = vnlbcu.Basic(noisy, sigma=5.0, form="chosen_tc", **kw)
+    assert synth.psnr(plain, clean) - synth.psnr(tc, clean) <= 0.05
+
+
+def test_autotuned_tensor_core_session():
+    """The autotuner times the tensor-core matcher's planes per shared-memory
+    stage (YUV444, 3 planes: 3, 2 and 1 per stage) and keeps the fastest; the
+    tuned session's output stays within 1e-3 dB of the untuned one's (the
+    grouping only moves the approximate distances' last bits)."""
+    clean, noisy = synth.make_clip(160, 128, 5, 3, 20.0, seed=89)
+    kw = dict(CPU_DEFAULTS, form="chosen_tc", **FINAL)
+    ref = vnlbcu.Basic(noisy, sigma=20.0, **CPU_DEFAULTS, **BASIC)
+    params = vnlbcu.parse_parameters(lib.STAGE_FINAL, noisy, 20.0, kw)
+    frames, planes, h, w = noisy.shape
+    s = lib.Session(params, w, h, frames, planes)
+    s.set_clip(lib.SOURCE_CLIP, noisy)
+    s.set_clip(lib.SOURCE_REF, ref)
+    untuned = s.render_clip()
+    tuning = s.autotune(1)
+    tuned = s.render_clip()
+    s.close()
+    assert any(t.startswith("tensor-core planes per stage") for t in tuning["timings"]), tuning
+    assert abs(synth.psnr(tuned, clean) - synth.psnr(untuned, clean)) <= 1e-3
