@@ -23,11 +23,19 @@
 // order its heap replay produces, which only changes the order in which
 // contributions are summed.
 //
-// Two kernels.  The distance kernel computes step 1 for every anchor and
-// candidate and writes the approximate distances to global memory
-// ([anchor][scheduled frame][window row][window column], 4 bytes each: the
-// 142 MB of a 1080p anchor frame cross HBM in tens of microseconds); the
-// selection kernel runs steps 2-4 with one warp per anchor at full occupancy.
+// Three kernels.  A small one computes each strip's plane offsets (below);
+// the distance kernel computes step 1 for every anchor and candidate and
+// writes the approximate distances to global memory ([anchor][scheduled
+// frame][window row][window column], 4 bytes each: the 82-87 MB of a 1080p
+// anchor frame cross HBM in tens of microseconds); the selection kernel runs
+// steps 2-4 with one warp per anchor at full occupancy.
+//
+// Samples are staged minus a per-strip, per-plane offset (the mean of the
+// strip's first anchor's reference patch).  A distance does not change, but
+// the BF16 roundings then scale with the samples' spread around the local
+// level rather than with the level: at low noise the approximate distance
+// is a small difference of large norms, and without the offset sigma-5
+// clips lost 0.05 dB against the plain form.
 //
 // Distance kernel.  One CTA takes a strip of up to 8 consecutive anchors of
 // each of one or two consecutive grid rows (anchor slots 0-7 and 8-15),
@@ -37,8 +45,10 @@
 // serves twice the anchors.  Per scheduled frame, and per group of up to
 // three planes of it:
 //
-//   a. The strip's search region is read from global memory once and written
-//      to shared memory as BF16 core matrices of the tcgen05 no-swizzle
+//   a. The strip's search region is read from global memory once (each
+//      producer warp loads its rows of the plane group ahead of the stage
+//      wait) and written to shared memory as BF16 core matrices of the
+//      tcgen05 no-swizzle
 //      K-major layout (8 rows of 16 bytes each): for region row r and column
 //      block b the 8x8 block H[i][j] = region[r][8b + i + j], so its row i is
 //      the 8-sample patch row of candidate column 8b + i.  Blocks are stored
