@@ -52,3 +52,37 @@ def test_vnlbcu_defaults_1080p_yuv_basic_and_final():
     finally:
         sb.close()
         sf.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.timeout(1500)
+def test_vnlbcu_defaults_full_width_band_bit_exact():
+    """vnlbcu's defaults on a full-width band (1920x136 YUV444PS, 4 frames:
+    three anchor frames with patch_time 2, 640 x 45 grid anchors each with
+    groups of up to 64 rows of dimension 294): Basic and Final of the plain
+    form equal the reference CPU core's (oracle/_ref, or the C restatement
+    when that build is absent) bit for bit, every frame."""
+    import os
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    import vnlbcu
+    import vnlbgpu_lib as lib
+
+    _, noisy = synth.make_clip(1920, 136, 4, 3, 20.0, seed=5)
+    basic = vnlbcu.Basic(noisy, sigma=20.0)
+    final = vnlbcu.Final(noisy, ref=basic, sigma=20.0)
+    pb = vnlbcu.parse_parameters(lib.STAGE_BASIC, noisy, 20.0, {})
+    pf = vnlbcu.parse_parameters(lib.STAGE_FINAL, noisy, 20.0, {})
+    to_stage = lambda p: O.StageParams(**{f: getattr(p, f) for f in O.StageParams.__dataclass_fields__})
+    kind = "ref" if O.REF_LIB.exists() else "port"
+    o = O.Oracle(kind)
+    threads = os.cpu_count()
+    ob = o.aggregate(o.stage_stacks(O.BASIC, to_stage(pb), noisy, threads=threads), noisy, pb.search_bwd,
+                     pb.search_fwd, pb.patch_time)
+    of = o.aggregate(o.stage_stacks(O.FINAL, to_stage(pf), noisy, ob, threads=threads), noisy, pf.search_bwd,
+                     pf.search_fwd, pf.patch_time)
+    bits = lambda a: np.ascontiguousarray(a, np.float32).view(np.uint32)
+    for name, g, r in (("basic", basic, ob), ("final", final, of)):
+        diff = np.flatnonzero(bits(g) != bits(r))
+        assert diff.size == 0, (name, kind, diff.size, float(np.max(np.abs(g - r))))
