@@ -93,6 +93,10 @@
 
 #include "vnlb_kernels.h"
 
+#ifndef VNLB_TC_SPARE_SMS
+#define VNLB_TC_SPARE_SMS 1
+#endif
+
 namespace vnlbgpu {
 namespace {
 
@@ -1023,9 +1027,10 @@ cudaError_t launch_match_chosen(const MatchLaunch& L, int strips, cudaStream_t s
     const int group = launch_plane_group(L);
     const size_t smem = chosen_match_shared_bytes(L);
     if (smem > static_cast<size_t>(kSharedLimit)) return cudaErrorInvalidValue;
-    // a quarter of the SMs stays free for the other pipeline lane's kernels
-    // (measured: +1.5% frames/s at 1080p over a grid of every SM)
-    const int persistent = sms - sms / 4;
+    // a quarter of the SMs stays free for the other pipeline lanes' kernels
+    // (measured: +1.5% frames/s at 1080p over a grid of every SM; the build
+    // parameter VNLB_TC_SPARE_SMS=0 takes every SM, for comparisons)
+    const int persistent = VNLB_TC_SPARE_SMS ? sms - sms / 4 : sms;
     const int grid = strips < persistent ? strips : persistent;
     const int select_blocks = (L.anchor_count + kChosenWarps - 1) / kChosenWarps;
     auto launch = [&](auto distance, auto select) {
