@@ -117,7 +117,6 @@ constexpr int kPipeThreads = 32 * (kMmaWarp + 1);
 constexpr int kStages = 2;  // shared-memory stages, and tensor-memory halves
 constexpr int kPipeTmemCols = kStages * kChosenTmemCols;
 constexpr int kMaxPlaneGroup = 3;
-constexpr int kVtStride = 33;  // a reader lane's 32 accumulators in shared memory, padded
 // region rows per producer warp and plane group (at most 2 * 16 + 7 rows)
 constexpr int kRowsPerWarp = (2 * kChosenMaxRows / 2 + kBlock - 1 + kProducerWarps - 1) / kProducerWarps;
 // shared memory of at least this size keeps a second distance CTA (and its
@@ -138,8 +137,6 @@ struct StageMeta {
     int win_wx[kTcN];  // 0: no anchor in the slot
     int gi[kTcN];      // anchor index
     float na[kTcN];    // reference norms
-    unsigned o0[kTcN]; // the distance of strip row 0, strip column 0 of the anchor's frame-k window, as an
-                       // offset into the distance buffer (mod 2^32): row cy, column x is at o0 + x + cy * wx
 };
 
 // The rows of a strip's windows: yl of the first grid row's anchors, and the
@@ -157,7 +154,7 @@ __device__ __forceinline__ void strip_rows(const MatchLaunch& L, const TcStrip& 
 // then per tensor-memory half the candidate norms and the metadata, the
 // producers' row sums, the mbarriers and the tensor-memory address.
 struct PipeLayout {
-    int hank, bop, stage_bytes, nb, meta, rowsq, vt, bars, tmem, bytes;
+    int hank, bop, stage_bytes, nb, meta, rowsq, bars, tmem, bytes;
 };
 
 __host__ __device__ inline int align128(int v) { return (v + 127) & ~127; }
@@ -175,7 +172,6 @@ __host__ __device__ inline PipeLayout pipe_layout(int group, int pairs) {
     l.nb = off;    off = align128(off + kStages * 2 * pairs * kChosenCols * 4);  // candidate norms per half
     l.meta = off;  off = align128(off + kStages * static_cast<int>(sizeof(StageMeta)));
     l.rowsq = off; off = align128(off + R * kChosenCols * 4);           // row sums of squares
-    l.vt = off;    off = align128(off + kConsumerWarps * 32 * kVtStride * 4);  // readers' accumulator rows
     l.bars = off;  off += 5 * kStages * 8;
     l.tmem = off;  off += 8;
     l.bytes = align128(off);
@@ -427,14 +423,9 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                         gi = strip.first[row] + idx;
                         spatial_range(L.anchors[gi].x, L.width, P, L.search_window, xl, xh);
                     }
-                    const int wx = xh - xl + 1;
                     meta->win_lo[m] = xl - rx0;
-                    meta->win_wx[m] = wx;
+                    meta->win_wx[m] = xh - xl + 1;
                     meta->gi[m] = gi;
-                    const int first_row = row == 0 ? 0 : yl1 - yl;  // the anchor's window row 0 in strip rows
-                    meta->o0[m] = static_cast<unsigned>(gi) * static_cast<unsigned>(L.approx_stride) +
-                                  static_cast<unsigned>(k) * static_cast<unsigned>(L.window_cells) -
-                                  static_cast<unsigned>(xl - rx0) - static_cast<unsigned>(first_row * wx);
                 }
                 if (threadIdx.x == 0) {
                     meta->k = k;
@@ -651,39 +642,44 @@ __global__ void __launch_bounds__(kPipeThreads, 1) tc_distance_kernel(MatchLaunc
                 const StageMeta* meta = reinterpret_cast<const StageMeta*>(smem + lay.meta) + h;
                 const int wy = meta->rows, off1 = meta->off1, h0 = meta->h[0], h1 = meta->h[1];
                 const unsigned kofs = static_cast<unsigned>(meta->k) * static_cast<unsigned>(L.window_cells);
-                // the anchor slots whose window columns hold this lane's
-                // column: the stores below visit only those
-                unsigned colmask = 0u;
+                // per anchor slot: the offset o0 of this lane's column in
+                // the anchor's frame-k distances at strip row 0 (so that
+                // strip row cy is at o0 + cy * wx; 32-bit: the launch
+                // checks the buffer's size), the row stride wx (0: the
+                // column is outside the window), and the reference norm
+                unsigned o0[kTcN];
+                int wxs[kTcN];
+                float na[kTcN];
 #pragma unroll
                 for (int n = 0; n < kTcN; ++n) {
                     const int r0 = x - meta->win_lo[n];
-                    if (r0 >= 0 && r0 < meta->win_wx[n]) colmask |= 1u << n;
+                    const int wxn = meta->win_wx[n];
+                    const bool in = r0 >= 0 && r0 < wxn;
+                    wxs[n] = in ? wxn : 0;
+                    const int first_row = n < 8 ? 0 : off1;  // the anchor's window row 0 in strip rows
+                    o0[n] = static_cast<unsigned>(meta->gi[n]) * static_cast<unsigned>(L.approx_stride) + kofs +
+                            static_cast<unsigned>(r0 - first_row * wxn);
+                    na[n] = meta->na[n];
                 }
-                float* vt = reinterpret_cast<float*>(smem + lay.vt) + (quarter * 32 + lane) * kVtStride;
                 const uint32_t ta = tmem + (static_cast<uint32_t>(32 * quarter) << 16) +
                                     static_cast<uint32_t>(h * kChosenTmemCols);
                 const int pairs_s = (wy + 1) >> 1;
                 for (int p0 = 0; p0 < pairs_s; p0 += 2) {
-                    // this lane's accumulators of two row pairs (16 anchor
-                    // slots each) to shared memory, to be read by slot
                     uint32_t v[32];
                     tmem_load32(ta + static_cast<uint32_t>(p0 * kTcN), v);
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) vt[j] = __uint_as_float(v[j]);
 #pragma unroll
                     for (int hh = 0; hh < 2; ++hh) {
                         const int cy = 2 * (p0 + hh) + dy;
                         if (cy >= wy) continue;
                         const float bn = nb[cy * kChosenCols + x];
-                        // slots whose window rows hold strip row cy
-                        unsigned m = colmask & ((cy < h0 ? 0x00FFu : 0u) |
-                                                (static_cast<unsigned>(cy - off1) < static_cast<unsigned>(h1) ? 0xFF00u
-                                                                                                            : 0u));
-                        while (m) {
-                            const int n = __ffs(m) - 1;
-                            m &= m - 1;
-                            L.approx_dist[meta->o0[n] + static_cast<unsigned>(x + cy * meta->win_wx[n])] =
-                                fmaxf(fmaf(-2.0f, vt[16 * hh + n], meta->na[n] + bn), 0.0f);
+                        // the strip rows of each grid row's windows
+                        const bool in0 = cy < h0;
+                        const bool in1 = static_cast<unsigned>(cy - off1) < static_cast<unsigned>(h1);
+#pragma unroll
+                        for (int n = 0; n < kTcN; ++n) {
+                            if (wxs[n] == 0 || !(n < 8 ? in0 : in1)) continue;
+                            L.approx_dist[o0[n] + static_cast<unsigned>(cy * wxs[n])] =
+                                fmaxf(fmaf(-2.0f, __uint_as_float(v[16 * hh + n]), na[n] + bn), 0.0f);
                         }
                     }
                 }
