@@ -637,10 +637,10 @@ def measured_peak(key: str, fallback: float) -> float:
 # headline (device-resident, Basic then Final, in each listed form): frames/s
 # with the same clock, PSNR against the clean clip.
 EXTRA_WORKLOADS = {
-    "configs0_gray_256x256x8_sigma10": dict(
+    "gray_256x256x8_sigma10_cpu_defaults": dict(
         forms=["plain"], width=256, height=256, frames=8, planes=1, sigma=10.0, steps=20, warmup=3,
         basic=dict(CPU_DEFAULTS), final=dict(CPU_DEFAULTS, tau=400.0, variance_threshold=1.7)),
-    "configs2_gray_1080p_32f_sigma25_tau400": dict(
+    "gray_1920x1080x32_sigma25_tau400_groups64": dict(
         forms=["plain", "chosen_tc"], width=1920, height=1080, frames=32, planes=1, sigma=25.0, steps=2, warmup=1,
         basic=dict(block_size=8, block_step=4, group_size=16, bm_range=9, radius=2, patch_time=2, rank=16,
                    cap_factor=4.0, tau=400.0),
@@ -947,7 +947,7 @@ def run_ours(args):
     if not args.no_workloads and PARAMS == "cpu":
         for name, spec in EXTRA_WORKLOADS.items():
             workloads[name] = workload_line(spec, args, ranks, stream, local)
-        workloads["configs4_mixed_stream"] = mixed_stream_line(args, ranks, local)
+        workloads["mixed_stream_7_clips_24f"] = mixed_stream_line(args, ranks, local)
     per_kernel = {}
     total_kernel_ms = sum(v[0] for v in head["kernels"].values())
     for k, v in head["kernels"].items():

@@ -46,7 +46,7 @@ def test_gradients_match_the_fp64_oracle():
 def test_tensor_core_output_layer_and_radix_shortlist():
     """The shortlist path (vnlbgpu_mlp_shortlist, as the learned form runs
     it): the output layer on the tensor cores (tcgen05, BF16 activations and
-    weights, FP32 accumulation) at the configs' shape (5445 offsets, hidden
+    weights, FP32 accumulation) at the 33 x 33 x 5 window's shape (5445 offsets, hidden
     128), a batch that is no multiple of the 128-row tile and outputs that
     are no multiple of the 256-column tile, then the top 64 by radix select.
     Against the FP64 oracle of the same arithmetic (activations rounded to
