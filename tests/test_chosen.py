@@ -247,3 +247,23 @@ def test_autotuned_tensor_core_session():
     s.close()
     assert any(t.startswith("tensor-core planes per stage") for t in tuning["timings"]), tuning
     assert abs(synth.psnr(tuned, clean) - synth.psnr(untuned, clean)) <= 1e-3
+
+
+@pytest.mark.parametrize("w,h,planes,kw", [
+    (97, 61, 1, dict(block_size=8, block_step=5, group_size=8, bm_range=9, radius=1, patch_time=1, rank=8)),
+    (70, 50, 3, dict(block_size=7, block_step=3, group_size=16, bm_range=6, radius=1, patch_time=2, rank=12)),
+    (130, 45, 1, dict(block_size=7, block_step=4, group_size=12, bm_range=13, radius=2, patch_time=2, rank=8)),
+], ids=["gray_odd_97x61", "yuv_p7_pt2_70x50", "gray_p7_radius2_130x45"])
+def test_tensor_core_odd_shapes(w, h, planes, kw):
+    """Frame sizes that are no multiple of 4, 8 or the strip width, windows
+    clipped by the frame edges, 7 x 7 and 8 x 8 patches, patch_time 1 and 2,
+    radius 1 and 2: the tensor-core form stays finite and within 0.05 dB of
+    the plain form, Basic and Final."""
+    clean, noisy = synth.make_clip(w, h, 6, planes, 20.0, seed=90)
+    pb = vnlbcu.Basic(noisy, sigma=20.0, **kw)
+    pf = vnlbcu.Final(noisy, ref=pb, sigma=20.0, **kw)
+    tb = vnlbcu.Basic(noisy, sigma=20.0, form="chosen_tc", **kw)
+    tf = vnlbcu.Final(noisy, ref=tb, sigma=20.0, form="chosen_tc", **kw)
+    for plain, tc in ((pb, tb), (pf, tf)):
+        assert np.isfinite(tc).all()
+        assert synth.psnr(plain, clean) - synth.psnr(tc, clean) <= 0.05
