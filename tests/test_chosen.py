@@ -267,3 +267,39 @@ def test_tensor_core_odd_shapes(w, h, planes, kw):
     for plain, tc in ((pb, tb), (pf, tf)):
         assert np.isfinite(tc).all()
         assert synth.psnr(plain, clean) - synth.psnr(tc, clean) <= 0.05
+
+
+@pytest.mark.parametrize("planes", [1, 3])
+def test_interleaved_stacks_read_back(planes):
+    """The chosen forms add filtered rows into pixel-interleaved stacks
+    (value planes and weight of a pixel side by side, one vector addition per
+    pixel) at 1 and 3 planes.  Both readers must agree on that layout: the
+    stacks read back in the vnlb.* frame layout, normalised here in anchor
+    order, give the device's output frame bit for bit, and their weights
+    cover the frame like the plain form's planar stacks do."""
+    w, h, f, n = 96, 80, 6, 2
+    clean, noisy = synth.make_clip(w, h, f, planes, 20.0, seed=93)
+    kw = dict(CPU_DEFAULTS, **BASIC)
+    out = {}
+    for form in ("plain", "chosen_tc"):
+        params = vnlbcu.parse_parameters(lib.STAGE_BASIC, noisy, 20.0, dict(kw, form=form))
+        s = lib.Session(params, w, h, f, planes)
+        s.set_clip(lib.SOURCE_CLIP, noisy)
+        bwd, fwd, pt = params.search_bwd, params.search_fwd, params.patch_time
+        anchors = [a for a in range(max(0, n - (fwd + pt - 1)), min(f - 1, n + bwd) + 1) if a <= f - pt]
+        stacks = {a: s.render_stack(a) for a in anchors}
+        frame = s.render_frame(n)
+        s.close()
+        num = np.zeros((planes, h, w), np.float32)
+        wsum = np.zeros((h, w), np.float32)
+        for a in anchors:
+            slot = n - a + bwd
+            num += stacks[a][:, 2 * slot * h:(2 * slot + 1) * h]
+            wsum += stacks[a][0, (2 * slot + 1) * h:(2 * slot + 2) * h]
+        safe = np.where(wsum > 0, wsum, np.float32(1))
+        host = np.where(wsum > 0, num / safe, noisy[n])
+        assert np.array_equal(host.view(np.uint32), frame.view(np.uint32)), form
+        out[form] = (wsum, frame)
+    (wp, fp), (wt, ft) = out["plain"], out["chosen_tc"]
+    assert abs(float(wt.sum()) / float(wp.sum()) - 1.0) < 0.02
+    assert synth.psnr(fp, clean[n]) - synth.psnr(ft, clean[n]) <= 0.05

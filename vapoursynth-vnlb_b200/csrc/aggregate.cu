@@ -317,15 +317,28 @@ __global__ void normalize_kernel(NormalizeLaunch L) {
         float w = 0.0f;
         for (int k = 0; k < L.count; ++k) {
             const float* s = L.stacks[k] + static_cast<size_t>(L.slots[k]) * (C + 1) * plane;
-            for (int c = 0; c < C; ++c) num[c] = __fadd_rn(num[c], s[c * plane + i]);
-            w = __fadd_rn(w, s[C * plane + i]);
+            if (L.packed[k] == 4) {  // [H][W][C+1] with C = 3: one 16-byte load
+                const float4 v = __ldg(reinterpret_cast<const float4*>(s) + i);
+                num[0] = __fadd_rn(num[0], v.x);
+                num[1] = __fadd_rn(num[1], v.y);
+                num[2] = __fadd_rn(num[2], v.z);
+                w = __fadd_rn(w, v.w);
+            } else if (L.packed[k] == 2) {  // C = 1
+                const float2 v = __ldg(reinterpret_cast<const float2*>(s) + i);
+                num[0] = __fadd_rn(num[0], v.x);
+                w = __fadd_rn(w, v.y);
+            } else {
+                for (int c = 0; c < C; ++c) num[c] = __fadd_rn(num[c], s[c * plane + i]);
+                w = __fadd_rn(w, s[C * plane + i]);
+            }
         }
         for (int c = 0; c < C; ++c)
             L.out[c * plane + i] = w > 0.0f ? __fdiv_rn(num[c], w) : L.source[c * plane + i];
     }
 }
 
-__global__ void pack_kernel(const float* stack, int width, int height, int channels, int slots, float* out) {
+__global__ void pack_kernel(const float* stack, int packed, int width, int height, int channels, int slots,
+                            float* out) {
     const size_t plane = static_cast<size_t>(width) * height;
     const size_t total = plane * channels * slots * 2;
     for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
@@ -336,7 +349,8 @@ __global__ void pack_kernel(const float* stack, int width, int height, int chann
         const int slot = static_cast<int>((rest / 2) % slots);
         const int c = static_cast<int>(rest / (2 * slots));
         const float* s = stack + static_cast<size_t>(slot) * (channels + 1) * plane;
-        out[i] = is_weight ? s[channels * plane + pix] : s[c * plane + pix];
+        const int e = is_weight ? channels : c;  // element of the pixel
+        out[i] = packed ? s[pix * packed + e] : s[e * plane + pix];
     }
 }
 
@@ -383,17 +397,25 @@ cudaError_t launch_tiles(const TileLaunch& L, cudaStream_t stream) {
 
 cudaError_t launch_normalize(const NormalizeLaunch& L, cudaStream_t stream) {
     if (L.channels > 4 || L.count > kMaxContributors) return cudaErrorInvalidValue;
+    for (int k = 0; k < L.count; ++k) {
+        // the vector layouts hold C = 3 (16-byte pixels) or C = 1 (8-byte pixels)
+        const int p = L.packed[k];
+        if (p != 0 && !(p == L.channels + 1 && (p == 2 || p == 4) &&
+                        reinterpret_cast<uintptr_t>(L.stacks[k]) % (p * sizeof(float)) == 0))
+            return cudaErrorInvalidValue;
+    }
     const size_t plane = static_cast<size_t>(L.width) * L.height;
     const int blocks = static_cast<int>(std::min<size_t>((plane + 255) / 256, 148 * 16));
     normalize_kernel<<<blocks, 256, 0, stream>>>(L);
     return cudaGetLastError();
 }
 
-cudaError_t launch_pack_stack(const float* stack, int width, int height, int channels, int slots, float* out,
-                              cudaStream_t stream) {
+cudaError_t launch_pack_stack(const float* stack, int packed, int width, int height, int channels, int slots,
+                              float* out, cudaStream_t stream) {
+    if (packed != 0 && !(packed == channels + 1 && (packed == 2 || packed == 4))) return cudaErrorInvalidValue;
     const size_t total = static_cast<size_t>(width) * height * channels * slots * 2;
     const int blocks = static_cast<int>(std::min<size_t>((total + 255) / 256, 148 * 16));
-    pack_kernel<<<blocks, 256, 0, stream>>>(stack, width, height, channels, slots, out);
+    pack_kernel<<<blocks, 256, 0, stream>>>(stack, packed, width, height, channels, slots, out);
     return cudaGetLastError();
 }
 

@@ -1110,8 +1110,15 @@ __device__ __forceinline__ float octet_reduce(float v) {
 // gets the same once per pixel (the columns of plane 0).  Slots outside the
 // window are dropped, as the stack tiles drop them.  The additions' order is
 // not fixed, so these forms are not bit-reproducible in the stacks' last
-// bits.  (Vector reductions of an octet's patch row, tried, were slower:
-// the shuffles that gather a row cost more than the reductions they save.)
+// bits.
+//
+// Pixel-interleaved stacks (L.scatter_pack = C+1): with C = 3 and 64
+// columns per plane, a lane's columns jj, jj + kCols/3 and jj + 2 kCols/3
+// are the same pixel of planes 0, 1 and 2, so the pixel's three values and
+// its weight go in one 16-byte vector addition (C = 1: value and weight in
+// one 8-byte one); a quarter (half) of the scalar atomics, and no shuffles.
+// (Vector reductions of an octet's patch row in the planar layout, tried,
+// were slower: the shuffles that gather a row cost more than they save.)
 template <int kCols>
 __device__ __forceinline__ void scatter_row(const FilterLaunch& L, const MatchRow& m, const float (&o)[kCols],
                                             float cw, int lane) {
@@ -1120,6 +1127,41 @@ __device__ __forceinline__ void scatter_row(const FilterLaunch& L, const MatchRo
     const int P = L.P;
     const size_t base = static_cast<size_t>(m.y) * L.width + m.x;
     const int slot0 = m.frame + L.search_bwd - L.anchor_frame;
+    if constexpr (kCols % 3 == 0) {
+        if (L.scatter_pack == 4) {
+            constexpr int kpp = kCols / 3;  // columns per plane and lane
+#pragma unroll
+            for (int jj = 0; jj < kpp; ++jj) {
+                const int pos = lane + 32 * jj;  // (layer t, py, px) within the plane's patch
+                const int t = pos / (P * P);
+                const int rem = pos - t * P * P;
+                const int py = rem / P;
+                const int slot = slot0 + t;
+                if (slot < 0 || slot >= L.slots) continue;
+                const float w = L.windowed ? cw * __ldg(L.window + rem) : cw;
+                const size_t at = base + static_cast<size_t>(py) * L.width + (rem - py * P);
+                atomicAdd(reinterpret_cast<float4*>(L.scatter) + static_cast<size_t>(slot) * plane + at,
+                          make_float4(w * o[jj], w * o[jj + kpp], w * o[jj + 2 * kpp], w));
+            }
+            return;
+        }
+    }
+    if (L.scatter_pack == 2) {
+#pragma unroll
+        for (int jj = 0; jj < kCols; ++jj) {
+            const int pos = lane + 32 * jj;
+            const int t = pos / (P * P);
+            const int rem = pos - t * P * P;
+            const int py = rem / P;
+            const int slot = slot0 + t;
+            if (slot < 0 || slot >= L.slots) continue;
+            const float w = L.windowed ? cw * __ldg(L.window + rem) : cw;
+            const size_t at = base + static_cast<size_t>(py) * L.width + (rem - py * P);
+            atomicAdd(reinterpret_cast<float2*>(L.scatter) + static_cast<size_t>(slot) * plane + at,
+                      make_float2(w * o[jj], w));
+        }
+        return;
+    }
 #pragma unroll
     for (int jj = 0; jj < kCols; ++jj) {
         // column (plane c, layer t, py, px)
@@ -1585,6 +1627,13 @@ bool filter_can_scatter(const FilterLaunch& L) {
            (D == 64 || D == 128 || D == 192 || D == 256);
 }
 
+int filter_scatter_pack(const FilterLaunch& L) {
+    if (!filter_can_scatter(L)) return 0;
+    if (L.channels == 1 && L.dim == L.patch_dim) return 2;
+    if (L.channels == 3 && L.dim == 192 && L.patch_dim == 64) return 4;
+    return 0;
+}
+
 cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t stream) {
     if (max_groups_in <= 0) return cudaSuccess;
     const int max_groups = max_groups_in * L.models;  // models to filter at most
@@ -1634,6 +1683,10 @@ cudaError_t launch_filter(const FilterLaunch& L, int max_groups_in, cudaStream_t
 #endif
     const bool warp_shape = R <= 8 && Bmax <= 8 && L.nmax == Bmax && (D == 64 || D == 128 || D == 192 || D == 256);
     if (L.scatter && !(warp_shape && L.models == 1)) return cudaErrorInvalidValue;  // see filter_can_scatter
+    if (L.scatter && L.scatter_pack != 0 &&
+        (L.scatter_pack != filter_scatter_pack(L) ||
+         reinterpret_cast<uintptr_t>(L.scatter) % (L.scatter_pack * sizeof(float)) != 0))
+        return cudaErrorInvalidValue;
     if ((VNLB_APPLY_WARP || L.scatter) && warp_shape && (!L.apply_general || L.scatter)) {
         cudaError_t err = D == 64    ? launch_apply_warp<64>(L, max_groups, stream)
                           : D == 128 ? launch_apply_warp<128>(L, max_groups, stream)

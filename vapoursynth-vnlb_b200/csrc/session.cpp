@@ -442,6 +442,7 @@ struct Session {
         int anchor = -1;
         long long last_use = 0;
         DeviceArray<float> data;
+        int packed = 0;  // layout of data: 0 planar, else pixel-interleaved (compute_anchor)
         cudaEvent_t ready = nullptr;
         std::vector<ReadEvent> reads;
     };
@@ -1326,8 +1327,10 @@ struct Session {
     }
 
     // One anchor frame on one lane: match -> paste mask -> filter -> stack
-    // tiles.  Everything is enqueued on the lane's stream.
-    void compute_anchor(int anchor, float* stack, Lane& lane) {
+    // tiles.  Everything is enqueued on the lane's stream.  Returns the
+    // stack's layout: 0 planar, else the floats of a pixel-interleaved one
+    // (FilterLaunch::scatter_pack).
+    int compute_anchor(int anchor, float* stack, Lane& lane) {
         Grid& grid = grid_for(anchor);
         const int G = static_cast<int>(grid.anchors.size());
         cudaStream_t ls = lane.stream;
@@ -1567,6 +1570,7 @@ struct Session {
         if (scatter) {
             check(cudaMemsetAsync(stack, 0, stack_values() * sizeof(float), ls), "cudaMemsetAsync(stack)");
             fl.scatter = stack;
+            fl.scatter_pack = filter_scatter_pack(fl);
             fl.window = d_window.ptr;
             fl.windowed = params.weight_gamma != 0.0f ? 1 : 0;
             fl.slots = slots;
@@ -1621,6 +1625,7 @@ struct Session {
         stats.anchor_frames += 1;
         stats.groups += G;
         stats.kernel_launches += (params.rank > 0 ? 6 : 5) - (scatter ? 1 : 0);
+        return scatter ? fl.scatter_pack : 0;
     }
 
     // The stack of `anchor`, computed on the next lane when not cached.  The
@@ -1641,7 +1646,7 @@ struct Session {
         // before anything read it (its reads then ordered nothing)
         check(cudaStreamWaitEvent(lane.stream, victim->ready, 0), "cudaStreamWaitEvent(stack written)");
         victim->anchor = -1;                     // until the work below is queued
-        compute_anchor(anchor, victim->data.ptr, lane);
+        victim->packed = compute_anchor(anchor, victim->data.ptr, lane);
         check(cudaEventRecord(victim->ready, lane.stream), "cudaEventRecord(stack ready)");
         victim->anchor = anchor;
         victim->last_use = ++use_clock;
@@ -1668,6 +1673,7 @@ struct Session {
             used[nl.count] = c;
             nl.stacks[nl.count] = c->data.ptr;
             nl.slots[nl.count] = n - a + params.search_bwd;
+            nl.packed[nl.count] = c->packed;
             ++nl.count;
         }
         for (int i = 0; i < nl.count; ++i)
@@ -2375,8 +2381,8 @@ int vnlbgpu_render_stack(vnlbgpu_session* session, int n, float* const* planes, 
             s.fork();
             Session::CachedStack* c = s.stack_for(n);
             vnlbgpu::check(cudaStreamWaitEvent(s.stream, c->ready, 0), "cudaStreamWaitEvent(stack ready)");
-            vnlbgpu::check(vnlbgpu::launch_pack_stack(c->data.ptr, s.width, s.height, s.channels, s.slots, s.d_pack.ptr,
-                                                      s.stream),
+            vnlbgpu::check(vnlbgpu::launch_pack_stack(c->data.ptr, c->packed, s.width, s.height, s.channels, s.slots,
+                                                      s.d_pack.ptr, s.stream),
                            "pack kernel launch");
             c->reads.push_back(s.record_read(s.stream));
             s.join();

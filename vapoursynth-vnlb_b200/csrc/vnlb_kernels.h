@@ -213,7 +213,9 @@ struct FilterLaunch {
     // row straight into the anchor frame's stack (atomics, any order) instead
     // of writing it out for the stack tiles; null = write the rows
     int apply_general;      // the row-tiled apply even where the warp-per-group one fits (autotuner)
-    float* scatter;         // [slots][C+1][H][W], cleared before the launch
+    float* scatter;         // the stack, cleared before the launch: [slots][C+1][H][W], or
+                            // [slots][H][W][C+1] where scatter_pack = C+1 (see filter_scatter_pack)
+    int scatter_pack;       // 0: planar stack; C+1: pixel-interleaved (one vector addition per pixel)
     const float* window;    // [P*P] aggregation window
     int windowed, slots, search_bwd, anchor_frame;
     StageConfig cfg;
@@ -253,6 +255,11 @@ size_t filter_shared_limit();
 // The shapes whose apply kernel can add rows straight into the stack
 // (FilterLaunch::scatter): warp-per-group, one model per group.
 bool filter_can_scatter(const FilterLaunch& L);
+// The stack layout such a launch adds into: C+1 when every pixel's C values
+// and weight can go in one 8- or 16-byte vector addition (C = 1, or C = 3
+// with 64 columns per plane, which puts a lane's columns of the three planes
+// on the same pixels), else 0 (planar).
+int filter_scatter_pack(const FilterLaunch& L);
 
 struct TileLaunch {
     int width, height, channels;
@@ -281,6 +288,7 @@ struct NormalizeLaunch {
     int width, height, channels;
     const float* stacks[kMaxContributors];  // contributing anchor stacks, in anchor order
     int slots[kMaxContributors];            // slot of the output frame in each stack
+    int packed[kMaxContributors];           // 0: planar stack; C+1: pixel-interleaved [slots][H][W][C+1]
     int count;
     const float* source;         // fallback plane set of the output frame [C][H][W]
     float* out;                  // [C][H][W]
@@ -302,7 +310,7 @@ struct AggregateLaunch {
 
 cudaError_t launch_aggregate_stacks(const AggregateLaunch& L, cudaStream_t stream);
 
-cudaError_t launch_pack_stack(const float* stack, int width, int height, int channels, int slots,
+cudaError_t launch_pack_stack(const float* stack, int packed, int width, int height, int channels, int slots,
                               float* out, cudaStream_t stream);
 
 // vnlb.Aggregate of output frame n through a fixed device scratch of
