@@ -544,8 +544,8 @@ TRAFFIC_PER_LAUNCH = {
     ("cpu", "match/plain"): 57.4e6,        # match_kernel<8,0,0>: Basic 31.8 MB, Final 83.0 MB
     ("cpu", "match/chosen_tc"): 342.7e6,   # strip offsets + tc_distance + tc_select: 286.9 / 398.5 MB
     ("cpu", "filter/plain"): 492.8e6,      # prepare + jacobi + apply: Basic 402.0 MB, Final 583.6 MB
-    ("cpu", "filter/chosen"): 514.0e6,     # the same, apply adding rows into the stacks: 423.0 / 604.9 MB
-    ("cpu", "filter/chosen_tc"): 514.0e6,
+    ("cpu", "filter/chosen"): 503.9e6,     # the same, apply adding rows into pixel-interleaved stacks:
+    ("cpu", "filter/chosen_tc"): 503.9e6,  # 415.3 / 592.5 MB
 }
 TRAFFIC_SOURCE = ("ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum "
                   "--clock-control none python bench.py --profile-case --form chosen_tc (and --form plain)")
