@@ -337,8 +337,7 @@ __global__ void normalize_kernel(NormalizeLaunch L) {
     }
 }
 
-__global__ void pack_kernel(const float* stack, int packed, int width, int height, int channels, int slots,
-                            float* out) {
+__global__ void pack_kernel(const float* stack, int width, int height, int channels, int slots, float* out) {
     const size_t plane = static_cast<size_t>(width) * height;
     const size_t total = plane * channels * slots * 2;
     for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
@@ -349,8 +348,41 @@ __global__ void pack_kernel(const float* stack, int packed, int width, int heigh
         const int slot = static_cast<int>((rest / 2) % slots);
         const int c = static_cast<int>(rest / (2 * slots));
         const float* s = stack + static_cast<size_t>(slot) * (channels + 1) * plane;
-        const int e = is_weight ? channels : c;  // element of the pixel
-        out[i] = packed ? s[pix * packed + e] : s[e * plane + pix];
+        out[i] = is_weight ? s[channels * plane + pix] : s[c * plane + pix];
+    }
+}
+
+// The same packing from a pixel-interleaved stack [slots][H][W][kPack]
+// (kPack = C+1 = 4 or 2): one thread per pixel and slot, one vector load,
+// 2C coalesced stores.
+template <int kPack>
+__global__ void pack_interleaved_kernel(const float* stack, int width, int height, int slots, float* out) {
+    constexpr int C = kPack - 1;
+    const size_t plane = static_cast<size_t>(width) * height;
+    const size_t total = plane * slots;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int slot = static_cast<int>(i / plane);
+        const size_t pix = i - static_cast<size_t>(slot) * plane;
+        const float* s = stack + (static_cast<size_t>(slot) * plane + pix) * kPack;
+        float v[kPack];
+        if constexpr (kPack == 4) {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(s));
+            v[0] = q.x;
+            v[1] = q.y;
+            v[2] = q.z;
+            v[3] = q.w;
+        } else {
+            const float2 q = __ldg(reinterpret_cast<const float2*>(s));
+            v[0] = q.x;
+            v[1] = q.y;
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            const size_t row = static_cast<size_t>(c * slots + slot) * 2;
+            out[row * plane + pix] = v[c];
+            out[(row + 1) * plane + pix] = v[C];
+        }
     }
 }
 
@@ -412,10 +444,19 @@ cudaError_t launch_normalize(const NormalizeLaunch& L, cudaStream_t stream) {
 
 cudaError_t launch_pack_stack(const float* stack, int packed, int width, int height, int channels, int slots,
                               float* out, cudaStream_t stream) {
-    if (packed != 0 && !(packed == channels + 1 && (packed == 2 || packed == 4))) return cudaErrorInvalidValue;
+    if (packed != 0 && !(packed == channels + 1 && (packed == 2 || packed == 4) &&
+                         reinterpret_cast<uintptr_t>(stack) % (packed * sizeof(float)) == 0))
+        return cudaErrorInvalidValue;
+    if (packed != 0) {
+        const size_t pixels = static_cast<size_t>(width) * height * slots;
+        const int blocks = static_cast<int>(std::min<size_t>((pixels + 255) / 256, 148 * 16));
+        if (packed == 4) pack_interleaved_kernel<4><<<blocks, 256, 0, stream>>>(stack, width, height, slots, out);
+        else pack_interleaved_kernel<2><<<blocks, 256, 0, stream>>>(stack, width, height, slots, out);
+        return cudaGetLastError();
+    }
     const size_t total = static_cast<size_t>(width) * height * channels * slots * 2;
     const int blocks = static_cast<int>(std::min<size_t>((total + 255) / 256, 148 * 16));
-    pack_kernel<<<blocks, 256, 0, stream>>>(stack, packed, width, height, channels, slots, out);
+    pack_kernel<<<blocks, 256, 0, stream>>>(stack, width, height, channels, slots, out);
     return cudaGetLastError();
 }
 
